@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""Design iterations per second of the SIMP compliance loop on one B200.
+
+Workload (one "step" = one design iteration): the 3-D cantilever at
+128x64x64 hexa8 voxels (524,288 elements, 1,622,400 free DOFs), E0 = 1,
+Emin = 1e-9, nu = 0.3, p = 3, uniform start 0.3, radius filter R = 2.5,
+MMA update with move 0.2 and the volume constraint of the sample drivers,
+FP64 K u inside 4-level geometric-multigrid PCG to relative residual 1e-8.
+A step is filter -> solve -> compliance/volume -> sensitivity -> filter^T ->
+MMA, exactly the loop body of the reference sample drivers.
+
+  value : device-resident loop (icarat_loop_step), CUDA events on the
+          library's stream, L2 flushed between steps (excluded from timing)
+  e2e   : the same step through the reference-facing host-pointer calls
+          (filter, set_design, solve, sensitivity, filter^T, MMASolver::Update)
+          with every host<->device copy inside the timed region
+  --impl reference : the CPU restatement of the reference path (oracle/,
+          Jacobi-PCG as the reference "Eigen_CG" solver) on all host cores
+
+Multi-GPU (torchrun): every rank optimises its own replica (independent
+designs, no data-path collective); value = all ranks' design iterations /
+max-over-ranks time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "design-iter/s"
+WORKLOAD = "SIMP cantilever 128x64x64 hexa8, MMA move 0.2, R=2.5, FP64 MG-PCG (4 levels) rtol 1e-8"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--grid", default="128x64x64")
+    p.add_argument("--radius", type=float, default=2.5)
+    p.add_argument("--levels", type=int, default=4)
+    p.add_argument("--smooth", type=int, default=2)
+    p.add_argument("--rtol", type=float, default=1e-8)
+    p.add_argument("--cpu-sample", action="store_true",
+                   help="internal: time one full CPU design iteration and print it")
+    p.add_argument("--cap", type=int, default=100,
+                   help="reference arm: PCG iterations run per timed step")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def grid_of(a):
+    nx, ny, nz = (int(v) for v in a.grid.split("x"))
+    return nx, ny, nz
+
+
+def config(a, extra=None):
+    nx, ny, nz = grid_of(a)
+    c = {"workload": WORKLOAD if a.grid == "128x64x64" else WORKLOAD.replace("128x64x64", a.grid),
+         "grid": [nx, ny, nz], "elements": nx * ny * nz,
+         "free_dofs": 3 * (nx + 1) * (ny + 1) * (nz + 1) - 3 * (ny + 1) * (nz + 1),
+         "update": "MMA", "move": 0.2, "filter_radius": a.radius, "volfrac": 0.3,
+         "solver": "MG-PCG" if a.impl == "ours" else "Jacobi-PCG (Eigen_CG semantics)",
+         "mg_levels": a.levels, "rtol": a.rtol}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# --------------------------------------------------------------------- CPU arm
+def cpu_design_iteration(a, cg_maxit, threads):
+    """One first-design iteration of the oracle; returns timings (s) and CG its."""
+    from oracle import oracle as O
+    O.lib.or_set_threads(threads)
+    nx, ny, nz = grid_of(a)
+    P = O.Problem(nx, ny, nz)
+    F = O.Filter(P, a.radius)
+    L = O.Loop(P, F, method="mma", x0=0.3, move=0.2, cg_tol=a.rtol, cg_maxit=cg_maxit)
+    t0 = time.perf_counter()
+    L.step()
+    t = time.perf_counter() - t0
+    s = L.scalars()
+    return t, s
+
+
+def reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    # warm-up: one uncapped design iteration measures the PCG iteration count
+    # N that rtol needs on this design and the per-iteration cost
+    t_full, s_full = cpu_design_iteration(a, 100000, threads)
+    n_full = s_full["cg_iters"]
+    times = []
+    for _ in range(a.steps):
+        t, s = cpu_design_iteration(a, a.cap, threads)
+        t_pcg = s["t_pcg"]
+        it = s["cg_iters"]
+        times.append(t - t_pcg + t_pcg * n_full / max(it, 1))
+    ms = 1000.0 * statistics.mean(times)
+    value = 1000.0 / ms
+    sample = ("first design iteration of the workload on the CPU restatement "
+              "(oracle/, OpenMP, %d threads): filter, CSR assembly, Jacobi-PCG "
+              "(reference Eigen_CG semantics), sensitivity, filter^T, MMA; each "
+              "timed step runs %d PCG iterations and scales the PCG time to the "
+              "%d iterations the uncapped warm-up solve needed for rtol %g "
+              "(uncapped warm-up step: %.2f s)" % (threads, a.cap + 1, n_full, a.rtol,
+                                                   t_full))
+    line = {"metric": METRIC, "value": value, "unit": "design-iter/s", "impl": "reference",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": 1, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": config(a),
+            "cpu_baseline": {"value": value, "unit": "design-iter/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "design-iter/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_sample(a):
+    threads = os.cpu_count() or 1
+    t, s = cpu_design_iteration(a, 100000, threads)
+    print(json.dumps({"t": t, "cg_iters": s["cg_iters"], "threads": threads}), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------- GPU arm
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id):
+        self.bus = (bus_id or "").lower()
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        mine = [r for r in rows if self.bus and r[0].lower().endswith(self.bus[-12:])]
+        rows = mine or rows
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """Measured FP64 dense peak (cuBLAS DGEMM 8192^3, best of 5)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def traffic_from_profiles(grid):
+    """dram bytes per launch of the stencil kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_cg_spmv_%s.txt" % grid)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def gpu_arm(a):
+    import torch
+    import torch.distributed as dist
+    import icarat2_b200 as G
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    cpu_line = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        # separate process: the oracle's OpenMP pool never shares this one
+        r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--cpu-sample",
+                            "--grid", a.grid, "--radius", str(a.radius), "--rtol",
+                            str(a.rtol)], capture_output=True, text=True)
+        if r.returncode == 0:
+            cpu_line = json.loads(r.stdout.strip().splitlines()[-1])
+
+    nx, ny, nz = grid_of(a)
+    opts = G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth)
+
+    def make_ctx():
+        return G.Context(nx, ny, nz, device=local)
+
+    # ---------------- value: device-resident loop
+    ctx = make_ctx()
+    ctx.loop_init(0.3, method="mma", filter_radius=a.radius, move=0.2, solve=opts)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB
+    for _ in range(a.warmup):
+        ctx.loop_step()
+    barrier()
+    torch.cuda.synchronize()
+    bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
+    clocks = ClockSampler(bus)
+    clocks.start()
+    l0 = G.kernel_launches()
+    evs, infos = [], []
+    for _ in range(a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        infos.append(ctx.loop_step())
+        e1.record(stream)
+        evs.append((e0, e1))
+        with torch.cuda.stream(stream):
+            flush.zero_()
+    torch.cuda.synchronize()
+    launches = G.kernel_launches() - l0
+    barrier()
+    clk = clocks.stop()
+    ms_steps = [e0.elapsed_time(e1) for e0, e1 in evs]
+    total_ms = sum(ms_steps)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * a.steps / (total_ms / 1000.0)
+
+    # ---------------- dominant kernel: FP64 stencil K u on the final design
+    ms_op = ctx.time_operator(30)
+    nelx, nd = nx * ny * nz, 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    flops = 1152.0 * nelx
+    bytes_alg = 16.0 * nd + 8.0 * nelx
+    peak64 = fp64_peak_tflops(torch, dev)
+    achieved = flops / (ms_op * 1e-3) / 1e12
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+
+    # ---------------- e2e: host-pointer reference-facing calls
+    e2e = None
+    if not a.no_e2e:
+        c2 = make_ctx()
+        c2.filter_setup(a.radius)
+        mma = G.MMASolver(nelx, 1, device=local)
+        mma.SetMoveLimit(0.2)
+        x = np.full(nelx, 0.3)
+        xmin, xmax = np.full(nelx, 1e-4), np.ones(nelx)
+        vol = c2.element_stiffness()[1]
+        s2 = torch.cuda.ExternalStream(c2.stream_ptr(), device=dev)
+        state = {"V0": None, "h2d": 0, "d2h": 0}
+
+        def host_step(k):
+            h2d = d2h = 0
+            xfil = c2.density_filter(x, False)
+            h2d += x.nbytes
+            d2h += xfil.nbytes
+            c2.set_design(xfil)
+            h2d += xfil.nbytes
+            val, info = c2.solve(opts)
+            d2h += val.nbytes
+            comp = c2.compliance()
+            d2h += 8
+            v = float((xfil * vol).sum())
+            if state["V0"] is None:
+                state["V0"] = v
+                g = 0.0
+            else:
+                g = v / state["V0"] - 1.0
+            dfds, dgds = c2.sensitivity(1.0 / state["V0"])
+            d2h += dfds.nbytes + dgds.nbytes
+            dfds = c2.density_filter(dfds, True)
+            dgds = c2.density_filter(dgds, True)
+            h2d += 2 * dfds.nbytes
+            d2h += 2 * dfds.nbytes
+            mma.Update(x, dfds, np.array([g]), dgds, xmin, xmax)
+            h2d += 5 * x.nbytes + 8
+            d2h += x.nbytes
+            state["h2d"], state["d2h"] = h2d, d2h
+            return comp
+
+        for k in range(a.warmup):
+            host_step(k)
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_ms = 0.0
+        for k in range(a.steps):
+            e0.record(s2)
+            host_step(a.warmup + k)
+            e1.record(s2)
+            e1.synchronize()
+            e_ms += e0.elapsed_time(e1)
+            with torch.cuda.stream(s2):
+                flush.zero_()
+            torch.cuda.synchronize()
+        te = torch.tensor([e_ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * a.steps / (float(te.item()) / 1000.0), "unit": "design-iter/s",
+               "h2d_bytes_per_step": state["h2d"], "d2h_bytes_per_step": state["d2h"]}
+        del mma
+        c2.close()
+
+    if rank == 0:
+        cg = [i.cg_iterations for i in infos]
+        line = {
+            "metric": METRIC, "value": value, "unit": "design-iter/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": config(a, {"l2": "256 MiB flush between steps, outside the per-step "
+                                       "CUDA events", "parallelism": "replicas" if world > 1
+                                 else "single GPU"}),
+            "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": {"bound": "fp64", "kernel": "FP64 K u stencil (k_apply_K_f64 / "
+                         "k_cg_spmv)", "achieved": achieved, "peak": peak64,
+                         "unit": "TFLOP/s", "frac": achieved / peak64,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                         "traffic": traffic_from_profiles(a.grid),
+                         "flops_per_launch": flops, "ms_per_launch": ms_op},
+            "roofline_hbm": {"achieved": bytes_alg / (ms_op * 1e-3) / 1e9, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": bytes_alg / (ms_op * 1e-3) / 1e9 / hbm_peak,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                             "bytes_per_launch": bytes_alg},
+            "ku_gdof_s": nd / (ms_op * 1e-3) / 1e9,
+            "cg_iterations_per_step": cg,
+            "compliance_last": infos[-1].compliance,
+            "clocks": clk,
+        }
+        if cpu_line:
+            line["cpu_baseline"] = {
+                "value": 1.0 / cpu_line["t"], "unit": "design-iter/s",
+                "cores": cpu_line["threads"], "kind": "port",
+                "sample": "first design iteration of the same workload on the CPU "
+                          "restatement (oracle/): filter, CSR assembly, Jacobi-PCG to rtol "
+                          "%g (%d iterations, reference Eigen_CG semantics), sensitivity, "
+                          "filter^T, MMA" % (a.rtol, cpu_line["cg_iters"])}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.cpu_sample:
+        return cpu_sample(a)
+    if a.impl == "reference":
+        return reference_arm(a)
+    return gpu_arm(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,512 @@
+"""icarat2_b200 -- B200 (sm_100a) implementation of ICARAT's linear-static
+SIMP topology-optimisation inner loop behind a C ABI (include/icarat_gpu.h).
+
+This module is the Python host side over that ABI.  Its classes mirror the
+reference call surface for the path:
+
+    Context            MeshIcarat + BCIcarat + device state
+    LinearAnalysis     src/analysis/linear.hpp:15-41   (solve)
+    Filter             src/optimization/filter.hpp:17-61
+    OC                 src/optimization/opt-solver/OCSolver.hpp:13-80
+    MMASolver          src/optimization/opt-solver/MMASolver.hpp:62-116
+
+Every call runs on the GPU through libicarat_gpu.so; there is no CPU path.
+Importing fails loudly when the library has not been built
+(``python -m icarat2_b200.build``).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libicarat_gpu.so")
+
+OK = 0
+WARN_MAXITER = 1
+ERR_ARG = -1
+ERR_CUDA = -2
+ERR_NAN = -4
+ERR_STATE = -5
+ERR_FILTER = -6
+ERR_UNSUPPORTED = -7
+ERR_NOMEM = -8
+
+JACOBI_PCG = 0
+MG_PCG = 1
+
+
+class IcaratError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (status %d)" % (msg, status))
+        self.status = status
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double)]
+
+
+class Material(C.Structure):
+    _fields_ = [("young_min", C.c_double), ("young_max", C.c_double),
+                ("poisson", C.c_double), ("penalty", C.c_double)]
+
+
+class Dirichlet(C.Structure):
+    _fields_ = [("flag", C.c_int * 3), ("val", C.c_double * 3),
+                ("box", (C.c_double * 2) * 3)]
+
+
+class Load(C.Structure):
+    _fields_ = [("val", C.c_double * 3), ("box", (C.c_double * 2) * 3)]
+
+
+class BC(C.Structure):
+    _fields_ = [("n_dirichlet", C.c_int), ("dirichlet", C.POINTER(Dirichlet)),
+                ("n_loads", C.c_int), ("loads", C.POINTER(Load))]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("method", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int),
+                ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("rel_residual", C.c_double),
+                ("status", C.c_int)]
+
+
+class OcOpts(C.Structure):
+    _fields_ = [("move", C.c_double), ("iota", C.c_double), ("lambda_min", C.c_double),
+                ("lambda_max", C.c_double), ("lambda_eps", C.c_double),
+                ("maxiter", C.c_int), ("use_threshold", C.c_int), ("beta", C.c_double),
+                ("T", C.c_double)]
+
+
+class LoopOpts(C.Structure):
+    _fields_ = [("method", C.c_int), ("use_threshold", C.c_int), ("T", C.c_double),
+                ("move", C.c_double), ("xmin", C.c_double), ("xmax", C.c_double),
+                ("filter_radius", C.c_double), ("solve", SolveOpts)]
+
+
+class StepInfo(C.Structure):
+    _fields_ = [("step", C.c_int), ("compliance", C.c_double),
+                ("constraint", C.c_double), ("cg_iterations", C.c_int),
+                ("cg_rel_residual", C.c_double), ("update_steps", C.c_int),
+                ("status", C.c_int)]
+
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+_P = C.POINTER
+
+# every symbol of include/icarat_gpu.h with its ctypes signature
+SIGNATURES = {
+    "icarat_version": (_i, []),
+    "icarat_status_string": (C.c_char_p, [_i]),
+    "icarat_last_error": (C.c_char_p, []),
+    "icarat_ctx_create": (_i, [_P(Grid), _P(Material), _P(BC), _i, _P(_vp)]),
+    "icarat_ctx_destroy": (_i, [_vp]),
+    "icarat_sizes": (_i, [_vp, _P(_i), _P(_i), _P(_i), _P(_i)]),
+    "icarat_stream": (_i, [_vp, _P(_vp)]),
+    "icarat_synchronize": (_i, [_vp]),
+    "icarat_dof_map": (_i, [_vp, _ip]),
+    "icarat_fext": (_i, [_vp, _dp]),
+    "icarat_element_stiffness": (_i, [_vp, _dp, _P(_d)]),
+    "icarat_set_design": (_i, [_vp, _dp]),
+    "icarat_set_design_dev": (_i, [_vp, _vp]),
+    "icarat_apply_K": (_i, [_vp, _dp, _dp]),
+    "icarat_apply_K_dev": (_i, [_vp, _vp, _vp]),
+    "icarat_solve": (_i, [_vp, _P(SolveOpts), _vp, _P(SolveInfo)]),
+    "icarat_solve_rhs": (_i, [_vp, _P(SolveOpts), _dp, _vp, _P(SolveInfo)]),
+    "icarat_node_values": (_i, [_vp, _dp]),
+    "icarat_compliance": (_i, [_vp, _P(_d)]),
+    "icarat_sensitivity": (_i, [_vp, _d, _vp, _vp]),
+    "icarat_sensitivity_dev": (_i, [_vp, _d, _vp, _vp]),
+    "icarat_filter_setup": (_i, [_vp, _d]),
+    "icarat_density_filter": (_i, [_vp, _dp, _dp, _i]),
+    "icarat_density_filter_dev": (_i, [_vp, _vp, _vp, _i]),
+    "icarat_sensitivity_filter": (_i, [_vp, _dp, _dp, _dp]),
+    "icarat_threshold": (_i, [_vp, _dp, _d, _d, _dp]),
+    "icarat_threshold_derivative": (_i, [_vp, _dp, _d, _d, _dp]),
+    "icarat_oc_update": (_i, [_vp, _dp, _dp, _d, _dp, _dp, _dp, _P(OcOpts), _P(_i)]),
+    "icarat_oc_update_dev": (_i, [_vp, _vp, _vp, _d, _vp, _vp, _vp, _P(OcOpts),
+                                  _P(_i)]),
+    "icarat_mma_create": (_i, [_i, _i, _i, _d, _d, _d, _P(_vp)]),
+    "icarat_mma_destroy": (_i, [_vp]),
+    "icarat_mma_set_move_limit": (_i, [_vp, _d]),
+    "icarat_mma_set_asymptotes": (_i, [_vp, _d, _d, _d]),
+    "icarat_mma_set_oscillation": (_i, [_vp, _d]),
+    "icarat_mma_update": (_i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "icarat_mma_update_dev": (_i, [_vp, _vp, _vp, _dp, _vp, _vp, _vp]),
+    "icarat_mma_last_loops": (_i, [_vp, _P(_i), _P(_i)]),
+    "icarat_kernel_launches": (_i, [_P(C.c_ulonglong)]),
+    "icarat_time_operator": (_i, [_vp, _i, _P(_d)]),
+    "icarat_loop_init": (_i, [_vp, _P(LoopOpts), _dp]),
+    "icarat_loop_step": (_i, [_vp, _P(StepInfo)]),
+    "icarat_loop_get": (_i, [_vp, _i, _dp]),
+}
+
+_lib = None
+
+
+def load_library(path=LIBPATH):
+    """Load libicarat_gpu.so (raises if it is missing: no fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError("libicarat_gpu.so not built; run python -m icarat2_b200.build")
+    L = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(status, what):
+    if status < 0:
+        msg = _lib.icarat_last_error().decode() or _lib.icarat_status_string(status).decode()
+        raise IcaratError(status, "%s: %s" % (what, msg))
+    return status
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _box(b):
+    arr = ((C.c_double * 2) * 3)()
+    for a in range(3):
+        arr[a][0], arr[a][1] = float(b[a][0]), float(b[a][1])
+    return arr
+
+
+def cantilever_bc(nx, ny, nz, lx=None, ly=None, lz=None, load_node=None, load=(0.0, 0.0, -1.0)):
+    """x = 0 face clamped; point load at node (nx, ny/2, 0) by default."""
+    lx = float(nx if lx is None else lx)
+    ly = float(ny if ly is None else ly)
+    lz = float(nz if lz is None else lz)
+    if load_node is None:
+        load_node = (nx, ny // 2, 0)
+    p = (load_node[0] * lx / nx, load_node[1] * ly / ny, load_node[2] * lz / nz)
+    dirichlet = [((1, 1, 1), (0.0, 0.0, 0.0), ((0.0, 0.0), (0.0, ly), (0.0, lz)))]
+    loads = [(tuple(load), ((p[0], p[0]), (p[1], p[1]), (p[2], p[2])))]
+    return dirichlet, loads
+
+
+def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
+               chunk=0):
+    return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk)
+
+
+class Context:
+    """A hexa8 voxel box with its boundary conditions, resident on one GPU."""
+
+    def __init__(self, nx, ny, nz, lx=None, ly=None, lz=None, young=(1e-9, 1.0),
+                 poisson=0.3, penalty=3.0, dirichlet=None, loads=None, device=0):
+        L = load_library()
+        lx = float(nx if lx is None else lx)
+        ly = float(ny if ly is None else ly)
+        lz = float(nz if lz is None else lz)
+        if dirichlet is None and loads is None:
+            dirichlet, loads = cantilever_bc(nx, ny, nz, lx, ly, lz)
+        dirichlet = list(dirichlet or [])
+        loads = list(loads or [])
+        self._dir = (Dirichlet * max(1, len(dirichlet)))()
+        for i, (fl, vl, bx) in enumerate(dirichlet):
+            self._dir[i].flag = (C.c_int * 3)(*fl)
+            self._dir[i].val = (C.c_double * 3)(*vl)
+            self._dir[i].box = _box(bx)
+        self._loads = (Load * max(1, len(loads)))()
+        for i, (vl, bx) in enumerate(loads):
+            self._loads[i].val = (C.c_double * 3)(*vl)
+            self._loads[i].box = _box(bx)
+        bc = BC(len(dirichlet), self._dir, len(loads), self._loads)
+        grid = Grid(nx, ny, nz, lx, ly, lz)
+        mat = Material(young[0], young[1], poisson, penalty)
+        h = C.c_void_p()
+        _check(L.icarat_ctx_create(C.byref(grid), C.byref(mat), C.byref(bc), device,
+                                   C.byref(h)), "icarat_ctx_create")
+        self.h = h
+        self.lib = L
+        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(L.icarat_sizes(h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)), "sizes")
+        self.numnp, self.nelx, self.neq, self.numeq = a.value, b.value, c.value, d.value
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.young, self.poisson, self.penalty = young, poisson, penalty
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.icarat_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- mesh / BC -----------------------------------------------------------
+    def stream_ptr(self):
+        s = C.c_void_p()
+        _check(self.lib.icarat_stream(self.h, C.byref(s)), "stream")
+        return s.value or 0
+
+    def synchronize(self):
+        _check(self.lib.icarat_synchronize(self.h), "synchronize")
+
+    def dof_map(self):
+        d = np.zeros(3 * self.numnp, np.int32)
+        _check(self.lib.icarat_dof_map(self.h, d), "dof_map")
+        return d.reshape(-1, 3)
+
+    def fext(self):
+        f = np.zeros(max(self.numeq, 1))
+        _check(self.lib.icarat_fext(self.h, f), "fext")
+        return f[:self.numeq]
+
+    def element_stiffness(self):
+        k = np.zeros(576)
+        v = C.c_double()
+        _check(self.lib.icarat_element_stiffness(self.h, k, C.byref(v)), "element_stiffness")
+        return k.reshape(24, 24), v.value
+
+    # --- analysis ------------------------------------------------------------
+    def set_design(self, design_s):
+        _check(self.lib.icarat_set_design(self.h, _f64(design_s)), "set_design")
+
+    def set_design_dev(self, ptr):
+        _check(self.lib.icarat_set_design_dev(self.h, C.c_void_p(ptr)), "set_design_dev")
+
+    def apply_K(self, u):
+        y = np.zeros(max(self.numeq, 1))
+        _check(self.lib.icarat_apply_K(self.h, _f64(u), y), "apply_K")
+        return y[:self.numeq]
+
+    def apply_K_dev(self, uptr, yptr):
+        _check(self.lib.icarat_apply_K_dev(self.h, C.c_void_p(uptr), C.c_void_p(yptr)),
+               "apply_K_dev")
+
+    def solve(self, opts=None, want_val=True):
+        """LinearAnalysis::solve: returns (value.val, SolveInfo)."""
+        info = SolveInfo()
+        val = np.zeros(max(self.numeq, 1)) if want_val else None
+        st = self.lib.icarat_solve(self.h, C.byref(opts) if opts is not None else None,
+                                   val.ctypes.data if want_val else None, C.byref(info))
+        _check(st, "solve")
+        return (val[:self.numeq] if want_val else None), info
+
+    def solve_rhs(self, f, opts=None):
+        info = SolveInfo()
+        u = np.zeros(max(self.numeq, 1))
+        st = self.lib.icarat_solve_rhs(self.h, C.byref(opts) if opts is not None else None,
+                                       _f64(f), u.ctypes.data, C.byref(info))
+        _check(st, "solve_rhs")
+        return u[:self.numeq], info
+
+    def node_values(self):
+        v = np.zeros(3 * self.numnp)
+        _check(self.lib.icarat_node_values(self.h, v), "node_values")
+        return v.reshape(-1, 3)
+
+    def compliance(self):
+        c = C.c_double()
+        _check(self.lib.icarat_compliance(self.h, C.byref(c)), "compliance")
+        return c.value
+
+    def sensitivity(self, dgds_scale=1.0):
+        dfds = np.zeros(self.nelx)
+        dgds = np.zeros(self.nelx)
+        _check(self.lib.icarat_sensitivity(self.h, dgds_scale, dfds.ctypes.data,
+                                           dgds.ctypes.data), "sensitivity")
+        return dfds, dgds
+
+    # --- filter ----------------------------------------------------------------
+    def filter_setup(self, radius):
+        _check(self.lib.icarat_filter_setup(self.h, radius), "filter_setup")
+
+    def density_filter(self, x, is_sens=False):
+        out = np.zeros(self.nelx)
+        _check(self.lib.icarat_density_filter(self.h, _f64(x), out, 1 if is_sens else 0),
+               "density_filter")
+        return out
+
+    def sensitivity_filter(self, design_s, dfds):
+        out = np.zeros(self.nelx)
+        _check(self.lib.icarat_sensitivity_filter(self.h, _f64(design_s), _f64(dfds), out),
+               "sensitivity_filter")
+        return out
+
+    def threshold(self, x, beta, T):
+        out = np.zeros(self.nelx)
+        _check(self.lib.icarat_threshold(self.h, _f64(x), beta, T, out), "threshold")
+        return out
+
+    def threshold_derivative(self, x, beta, T):
+        out = np.zeros(self.nelx)
+        _check(self.lib.icarat_threshold_derivative(self.h, _f64(x), beta, T, out),
+               "threshold_derivative")
+        return out
+
+    def oc_update(self, x, dfdx, g, dgdx, xmin, xmax, move=0.15, iota=0.5,
+                  lambda_min=0.0, lambda_max=1.0e4, lambda_eps=1.0e-5, maxiter=100,
+                  use_threshold=False, beta=1.0, T=0.5):
+        x = _f64(x).copy()
+        o = OcOpts(move, iota, lambda_min, lambda_max, lambda_eps, maxiter,
+                   1 if use_threshold else 0, beta, T)
+        steps = C.c_int()
+        _check(self.lib.icarat_oc_update(self.h, x, _f64(dfdx), g, _f64(dgdx), _f64(xmin),
+                                         _f64(xmax), C.byref(o), C.byref(steps)),
+               "oc_update")
+        return x, steps.value
+
+    # --- design loop -------------------------------------------------------------
+    def loop_init(self, x0, method="mma", filter_radius=1.5, move=None, xmin=1e-4,
+                  xmax=1.0, use_threshold=False, T=0.5, solve=None):
+        if move is None:
+            move = 0.2 if method == "mma" else 0.15
+        if np.isscalar(x0):
+            x0 = np.full(self.nelx, float(x0))
+        o = LoopOpts(1 if method == "mma" else 0, 1 if use_threshold else 0, T, move, xmin,
+                     xmax, filter_radius, solve if solve is not None else solve_opts())
+        _check(self.lib.icarat_loop_init(self.h, C.byref(o), _f64(x0)), "loop_init")
+
+    def time_operator(self, reps=20):
+        ms = C.c_double()
+        _check(self.lib.icarat_time_operator(self.h, reps, C.byref(ms)), "time_operator")
+        return ms.value
+
+    def loop_step(self):
+        info = StepInfo()
+        _check(self.lib.icarat_loop_step(self.h, C.byref(info)), "loop_step")
+        return info
+
+    def loop_get(self, which):
+        idx = {"x": 0, "xfil": 1, "xthr": 2, "dfds": 3, "dgds": 4}[which]
+        out = np.zeros(self.nelx)
+        _check(self.lib.icarat_loop_get(self.h, idx, out), "loop_get")
+        return out
+
+
+# ---- reference-named mirrors ------------------------------------------------------
+_SOLVER_NAMES = {"Eigen_CG": JACOBI_PCG, "Scaling_CG": JACOBI_PCG, "MG_CG": MG_PCG}
+
+
+class LinearAnalysis:
+    """LinearAnalysis<LinearElastic, Node> (src/analysis/linear.hpp:15-41)."""
+
+    def __init__(self, ctx, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2):
+        self.ctx = ctx
+        self.rtol, self.maxit = rtol, maxit
+        self.mg_levels, self.mg_smooth = mg_levels, mg_smooth
+        self.info = None
+        self.val = None
+
+    def solve(self, solvName="Eigen_CG", log=False):
+        if solvName not in _SOLVER_NAMES:
+            # Solvers::solve exits on an unknown name (solvers.cpp:56-60)
+            raise IcaratError(ERR_UNSUPPORTED, "Solver type name is wrong: %s" % solvName)
+        o = solve_opts(_SOLVER_NAMES[solvName], self.rtol, self.maxit, self.mg_levels,
+                       self.mg_smooth)
+        self.val, self.info = self.ctx.solve(o)
+        if log:
+            print("iteration: %d\nresidual: %g" % (self.info.iterations,
+                                                    self.info.rel_residual))
+        return self.val
+
+
+class Filter:
+    """Filter<E,N> (src/optimization/filter.hpp:17-61) on the voxel grid."""
+
+    def __init__(self, ctx, radius):
+        self.ctx = ctx
+        ctx.filter_setup(radius)
+
+    def densityFilter(self, design_s, isSens):
+        return self.ctx.density_filter(design_s, isSens)
+
+    def sensitivityFilter(self, design_s, dfds):
+        return self.ctx.sensitivity_filter(design_s, dfds)
+
+    def threshold(self, d, beta, T):
+        return self.ctx.threshold(d, beta, T)
+
+    def thresholdDerivative(self, d, beta, T):
+        return self.ctx.threshold_derivative(d, beta, T)
+
+
+class OC:
+    """OC (OCSolver.hpp:13-80); the volume functor is the drivers' filtered
+    volume, evaluated on the GPU with the context's filter."""
+
+    def __init__(self, ctx, use_threshold=False, beta=1.0, T=0.5):
+        self.ctx = ctx
+        self.movelimit = 0.15
+        self.use_threshold, self.beta, self.T = use_threshold, beta, T
+        self.steps = 0
+
+    def setMoveLimit(self, m):
+        self.movelimit = m
+
+    def UpdateVariables(self, xk, dfdx, g, dgdx, xmin, xmax):
+        x, self.steps = self.ctx.oc_update(xk, dfdx, g, dgdx, xmin, xmax,
+                                           move=self.movelimit,
+                                           use_threshold=self.use_threshold,
+                                           beta=self.beta, T=self.T)
+        xk[:] = x
+        return xk
+
+
+class MMASolver:
+    """MMASolver(n, m, a, c, d) (MMASolver.hpp:62-116) on the GPU."""
+
+    def __init__(self, n, m, a=0.0, c=100000.0, d=0.0, device=0):
+        L = load_library()
+        h = C.c_void_p()
+        _check(L.icarat_mma_create(device, n, m, a, c, d, C.byref(h)), "mma_create")
+        self.h, self.lib, self.n, self.m = h, L, n, m
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.icarat_mma_destroy(self.h)
+            self.h = None
+
+    def SetMoveLimit(self, m):
+        _check(self.lib.icarat_mma_set_move_limit(self.h, m), "SetMoveLimit")
+
+    def SetAsymptotes(self, init, decrease, increase):
+        _check(self.lib.icarat_mma_set_asymptotes(self.h, init, decrease, increase),
+               "SetAsymptotes")
+
+    def SetOscillation(self, a):
+        _check(self.lib.icarat_mma_set_oscillation(self.h, a), "SetOscillation")
+
+    def Update(self, xval, dfdx, gx, dgdx, xmin, xmax):
+        """In place on xval (a float64 numpy array), like the reference."""
+        assert xval.dtype == np.float64 and xval.flags.c_contiguous
+        _check(self.lib.icarat_mma_update(self.h, xval, _f64(dfdx),
+                                          _f64(np.atleast_1d(gx)), _f64(dgdx).ravel(),
+                                          _f64(xmin), _f64(xmax)), "Update")
+        return xval
+
+    def last_loops(self):
+        a, b = C.c_int(), C.c_int()
+        _check(self.lib.icarat_mma_last_loops(self.h, C.byref(a), C.byref(b)), "loops")
+        return a.value, b.value
+
+
+def kernel_launches():
+    """Kernels launched so far by libicarat_gpu.so in this process."""
+    L = load_library()
+    n = C.c_ulonglong()
+    _check(L.icarat_kernel_launches(C.byref(n)), "kernel_launches")
+    return n.value

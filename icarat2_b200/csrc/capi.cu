@@ -1,0 +1,476 @@
+// extern "C" entry points of include/icarat_gpu.h.  Each one converts C++
+// errors into a status code; host pointers are staged through device buffers
+// of the context.
+#include <atomic>
+#include <cstring>
+#include <string>
+
+#include "internal.cuh"
+
+int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
+                           const icarat_bc *bc, int device, icarat_ctx **out);
+int icarat_ctx_destroy_impl(icarat_ctx *c);
+
+namespace icarat_b200
+{
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+static std::atomic<unsigned long long> g_launches{0};
+static thread_local bool g_capturing = false;
+void note_launch(unsigned long long n)
+{
+  if(!g_capturing)
+    g_launches += n;
+}
+void set_capturing(bool on) { g_capturing = on; }
+
+void build_rhs(icarat_ctx *c);
+int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0);
+int loop_step(icarat_ctx *c, icarat_step_info *info);
+int loop_get(icarat_ctx *c, int which, double *out);
+void sensitivity_filter_dev(icarat_ctx *c, const double *s, const double *df,
+                            double *out);
+
+static double *stage(icarat_ctx *c, int k)
+{
+  if(!c->d_stage)
+    c->d_stage = dalloc(6 * (size_t)c->nelx);
+  return c->d_stage + (size_t)k * c->nelx;
+}
+
+static void h2d(icarat_ctx *c, double *dst, const double *src, size_t n)
+{
+  ICK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+}
+
+static void d2h(icarat_ctx *c, double *dst, const double *src, size_t n)
+{
+  ICK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
+}
+
+static void check_ctx(const icarat_ctx *c)
+{
+  IREQUIRE(c != nullptr, ICARAT_ERR_ARG, "null context");
+  ICK(cudaSetDevice(c->device));
+}
+
+static const icarat_solve_opts kDefaultSolve = {ICARAT_SOLVER_JACOBI_PCG, 1.0e-10,
+                                                10000, 4, 2, 0};
+
+} // namespace icarat_b200
+
+using namespace icarat_b200;
+
+extern "C" {
+
+int icarat_version(void) { return 10000; }
+
+int icarat_kernel_launches(unsigned long long *count)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(count, ICARAT_ERR_ARG, "null argument");
+  *count = g_launches.load();
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_time_operator(icarat_ctx *c, int reps, double *ms_per_launch)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(reps > 0 && ms_per_launch, ICARAT_ERR_ARG, "bad argument");
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+  cudaEvent_t a, b;
+  ICK(cudaEventCreate(&a));
+  ICK(cudaEventCreate(&b));
+  // warm-up launch, then reps launches of the FP64 stencil y = K u
+  launch_apply_K(c, g, c->d_E, c->d_fix, c->d_u, c->d_Ap, nullptr);
+  ICK(cudaEventRecord(a, c->stream));
+  for(int r = 0; r < reps; r++)
+    launch_apply_K(c, g, c->d_E, c->d_fix, c->d_u, c->d_Ap, nullptr);
+  ICK(cudaEventRecord(b, c->stream));
+  ICK(cudaEventSynchronize(b));
+  float ms = 0.f;
+  ICK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms_per_launch = (double)ms / reps;
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+const char *icarat_last_error(void) { return g_last_error.c_str(); }
+
+const char *icarat_status_string(int s)
+{
+  switch(s)
+  {
+  case ICARAT_OK: return "ok";
+  case ICARAT_WARN_MAXITER: return "iteration cap reached";
+  case ICARAT_ERR_ARG: return "bad argument";
+  case ICARAT_ERR_CUDA: return "CUDA error";
+  case ICARAT_ERR_NAN: return "non-finite value";
+  case ICARAT_ERR_STATE: return "call order violated";
+  case ICARAT_ERR_FILTER: return "filter weight sum too small";
+  case ICARAT_ERR_UNSUPPORTED: return "unsupported";
+  case ICARAT_ERR_NOMEM: return "out of memory";
+  default: return "unknown status";
+  }
+}
+
+int icarat_ctx_create(const icarat_grid *grid, const icarat_material *mat,
+                      const icarat_bc *bc, int device, icarat_ctx **out)
+{
+  ICARAT_API_BEGIN
+  return icarat_ctx_create_impl(grid, mat, bc, device, out);
+  ICARAT_API_END
+}
+
+int icarat_ctx_destroy(icarat_ctx *c)
+{
+  ICARAT_API_BEGIN
+  release_graphs(c);
+  return icarat_ctx_destroy_impl(c);
+  ICARAT_API_END
+}
+
+int icarat_sizes(const icarat_ctx *c, int *numnp, int *nelx, int *neq, int *numeq)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(c, ICARAT_ERR_ARG, "null context");
+  if(numnp)
+    *numnp = c->numnp;
+  if(nelx)
+    *nelx = c->nelx;
+  if(neq)
+    *neq = c->neq;
+  if(numeq)
+    *numeq = c->numeq;
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_stream(const icarat_ctx *c, void **stream)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(c && stream, ICARAT_ERR_ARG, "null argument");
+  *stream = (void *)c->stream;
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_synchronize(icarat_ctx *c)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  ICK(cudaStreamSynchronize(c->stream));
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_dof_map(const icarat_ctx *c, int *node_dof)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(c && node_dof, ICARAT_ERR_ARG, "null argument");
+  std::memcpy(node_dof, c->dof.data(), sizeof(int) * c->dof.size());
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_fext(const icarat_ctx *c, double *fext)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(c && fext, ICARAT_ERR_ARG, "null argument");
+  std::memcpy(fext, c->fext_h.data(), sizeof(double) * c->fext_h.size());
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_element_stiffness(const icarat_ctx *c, double *ke, double *volume)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(c, ICARAT_ERR_ARG, "null context");
+  if(ke)
+    std::memcpy(ke, c->ke0.k, sizeof(double) * 576);
+  if(volume)
+    *volume = c->vol0;
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_set_design(icarat_ctx *c, const double *design_s)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(design_s, ICARAT_ERR_ARG, "null argument");
+  h2d(c, c->d_rho, design_s, c->nelx);
+  set_design_device(c, c->d_rho);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_set_design_dev(icarat_ctx *c, const double *design_s)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(design_s, ICARAT_ERR_ARG, "null argument");
+  set_design_device(c, design_s);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+static int apply_K_impl(icarat_ctx *c, const double *u, double *y, bool host)
+{
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  IREQUIRE(u && y, ICARAT_ERR_ARG, "null argument");
+  GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+  to_full(c, u, c->d_v1, host);
+  launch_apply_K(c, g, c->d_E, c->d_fix, c->d_v1, c->d_Ap, nullptr);
+  from_full(c, c->d_Ap, y, host);
+  return ICARAT_OK;
+}
+
+int icarat_apply_K(icarat_ctx *c, const double *u, double *y)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  return apply_K_impl(c, u, y, true);
+  ICARAT_API_END
+}
+
+int icarat_apply_K_dev(icarat_ctx *c, const double *u, double *y)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  return apply_K_impl(c, u, y, false);
+  ICARAT_API_END
+}
+
+int icarat_solve(icarat_ctx *c, const icarat_solve_opts *opts, double *val,
+                 icarat_solve_info *info)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  const icarat_solve_opts &o = opts ? *opts : kDefaultSolve;
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  build_rhs(c);
+  icarat_solve_info si{};
+  int st = solve_full(c, &o, c->d_rhs, c->d_u, &si);
+  c->solved = true;
+  c->last_info = si;
+  if(info)
+    *info = si;
+  if(val)
+    from_full(c, c->d_u, val, true);
+  return st;
+  ICARAT_API_END
+}
+
+int icarat_solve_rhs(icarat_ctx *c, const icarat_solve_opts *opts, const double *f,
+                     double *u, icarat_solve_info *info)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(f, ICARAT_ERR_ARG, "null right-hand side");
+  const icarat_solve_opts &o = opts ? *opts : kDefaultSolve;
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  to_full(c, f, c->d_rhs, true);
+  icarat_solve_info si{};
+  int st = solve_full(c, &o, c->d_rhs, c->d_u, &si);
+  c->solved = true;
+  c->last_info = si;
+  if(info)
+    *info = si;
+  if(u)
+    from_full(c, c->d_u, u, true);
+  return st;
+  ICARAT_API_END
+}
+
+int icarat_node_values(icarat_ctx *c, double *node_val)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(node_val, ICARAT_ERR_ARG, "null argument");
+  IREQUIRE(c->solved, ICARAT_ERR_STATE, "solve first");
+  node_values_dev(c, c->d_v1);
+  d2h(c, node_val, c->d_v1, c->neq);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_compliance(icarat_ctx *c, double *compliance)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(compliance, ICARAT_ERR_ARG, "null argument");
+  IREQUIRE(c->solved, ICARAT_ERR_STATE, "solve first");
+  *compliance = compliance_dev(c);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_sensitivity(icarat_ctx *c, double scale, double *dfds, double *dgds)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  double *a = stage(c, 0), *b = stage(c, 1);
+  sensitivity_dev(c, scale, dfds ? a : nullptr, dgds ? b : nullptr);
+  if(dfds)
+    d2h(c, dfds, a, c->nelx);
+  if(dgds)
+    d2h(c, dgds, b, c->nelx);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_sensitivity_dev(icarat_ctx *c, double scale, double *dfds, double *dgds)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  sensitivity_dev(c, scale, dfds, dgds);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_filter_setup(icarat_ctx *c, double radius)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  filter_setup(c, radius);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_density_filter(icarat_ctx *c, const double *in, double *out, int is_sens)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(in && out, ICARAT_ERR_ARG, "null argument");
+  double *a = stage(c, 0), *b = stage(c, 1);
+  h2d(c, a, in, c->nelx);
+  filter_apply(c, a, b, is_sens != 0);
+  d2h(c, out, b, c->nelx);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_density_filter_dev(icarat_ctx *c, const double *in, double *out,
+                              int is_sens)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(in && out && in != out, ICARAT_ERR_ARG, "need distinct in/out");
+  filter_apply(c, in, out, is_sens != 0);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_sensitivity_filter(icarat_ctx *c, const double *design_s,
+                              const double *dfds, double *out)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(design_s && dfds && out, ICARAT_ERR_ARG, "null argument");
+  double *a = stage(c, 0), *b = stage(c, 1), *o = stage(c, 2);
+  h2d(c, a, design_s, c->nelx);
+  h2d(c, b, dfds, c->nelx);
+  sensitivity_filter_dev(c, a, b, o);
+  d2h(c, out, o, c->nelx);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+static int threshold_impl(icarat_ctx *c, const double *in, double beta, double T,
+                          double *out, bool der)
+{
+  check_ctx(c);
+  IREQUIRE(in && out, ICARAT_ERR_ARG, "null argument");
+  double *a = stage(c, 0), *b = stage(c, 1);
+  h2d(c, a, in, c->nelx);
+  threshold_dev(c, a, beta, T, b, der);
+  d2h(c, out, b, c->nelx);
+  return ICARAT_OK;
+}
+
+int icarat_threshold(icarat_ctx *c, const double *in, double beta, double T,
+                     double *out)
+{
+  ICARAT_API_BEGIN
+  return threshold_impl(c, in, beta, T, out, false);
+  ICARAT_API_END
+}
+
+int icarat_threshold_derivative(icarat_ctx *c, const double *in, double beta, double T,
+                                double *out)
+{
+  ICARAT_API_BEGIN
+  return threshold_impl(c, in, beta, T, out, true);
+  ICARAT_API_END
+}
+
+static const icarat_oc_opts kDefaultOc = {0.15, 0.5, 0.0, 1.0e4, 1.0e-5, 100, 0, 1.0, 0.5};
+
+int icarat_oc_update(icarat_ctx *c, double *x, const double *dfdx, double g,
+                     const double *dgdx, const double *xmin, const double *xmax,
+                     const icarat_oc_opts *opts, int *steps)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(x && dfdx && dgdx && xmin && xmax, ICARAT_ERR_ARG, "null argument");
+  double *dx = stage(c, 0), *ddf = stage(c, 1), *ddg = stage(c, 2),
+         *dmin = stage(c, 3), *dmax = stage(c, 4);
+  h2d(c, dx, x, c->nelx);
+  h2d(c, ddf, dfdx, c->nelx);
+  h2d(c, ddg, dgdx, c->nelx);
+  h2d(c, dmin, xmin, c->nelx);
+  h2d(c, dmax, xmax, c->nelx);
+  int st = oc_update_dev(c, dx, ddf, g, ddg, dmin, dmax, opts ? opts : &kDefaultOc,
+                         steps);
+  d2h(c, x, dx, c->nelx);
+  return st;
+  ICARAT_API_END
+}
+
+int icarat_oc_update_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
+                         const double *dgdx, const double *xmin, const double *xmax,
+                         const icarat_oc_opts *opts, int *steps)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(x && dfdx && dgdx && xmin && xmax, ICARAT_ERR_ARG, "null argument");
+  return oc_update_dev(c, x, dfdx, g, dgdx, xmin, xmax, opts ? opts : &kDefaultOc,
+                       steps);
+  ICARAT_API_END
+}
+
+int icarat_loop_init(icarat_ctx *c, const icarat_loop_opts *opts, const double *x0)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(opts && x0, ICARAT_ERR_ARG, "null argument");
+  return loop_init(c, opts, x0);
+  ICARAT_API_END
+}
+
+int icarat_loop_step(icarat_ctx *c, icarat_step_info *info)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  return loop_step(c, info);
+  ICARAT_API_END
+}
+
+int icarat_loop_get(icarat_ctx *c, int which, double *out)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(out, ICARAT_ERR_ARG, "null argument");
+  return loop_get(c, which, out);
+  ICARAT_API_END
+}
+
+} // extern "C"

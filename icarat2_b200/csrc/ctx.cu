@@ -1,0 +1,368 @@
+// Context setup: structured hexa8 box, Dirichlet boxes, DOF numbering, point
+// loads, device arrays, and the numeq <-> node-vector conversions.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "internal.cuh"
+
+namespace icarat_b200
+{
+
+double *dalloc(size_t n)
+{
+  void *p = nullptr;
+  if(n == 0)
+    n = 1;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(double));
+  if(e != cudaSuccess)
+    throw Error{ICARAT_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+  return static_cast<double *>(p);
+}
+
+void dfree(void *p)
+{
+  if(p)
+    cudaFree(p);
+}
+
+// numeq vector -> node vector (constrained components 0)
+__global__ void k_scatter_free(int numeq, const int *__restrict__ free_idx,
+                               const double *__restrict__ in,
+                               double *__restrict__ out)
+{
+  for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < numeq;
+      r += gridDim.x * blockDim.x)
+    out[free_idx[r]] = in[r];
+}
+
+__global__ void k_gather_free(int numeq, const int *__restrict__ free_idx,
+                              const double *__restrict__ in,
+                              double *__restrict__ out)
+{
+  for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < numeq;
+      r += gridDim.x * blockDim.x)
+    out[r] = in[free_idx[r]];
+}
+
+// SIMP (src/problem/elasticity.hpp:13-17)
+__global__ void k_simp(int n, const double *__restrict__ rho, double e1,
+                       double e2, double p, double *__restrict__ E)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+  {
+    double rp = pow(rho[i], p);
+    E[i] = (1.0 - rp) * e1 + rp * e2;
+  }
+}
+
+static int grid_for(int n, int threads = 256)
+{
+  int b = (n + threads - 1) / threads;
+  return b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b);
+}
+
+void to_full(icarat_ctx *c, const double *in, double *full_out, bool host_src)
+{
+  const double *src = in;
+  if(host_src)
+  {
+    ICK(cudaMemcpyAsync(c->d_v2, in, sizeof(double) * c->numeq,
+                        cudaMemcpyHostToDevice, c->stream));
+    src = c->d_v2;
+  }
+  ICK(cudaMemsetAsync(full_out, 0, sizeof(double) * c->neq, c->stream));
+  if(c->numeq > 0)
+  {
+    note_launch();
+    k_scatter_free<<<grid_for(c->numeq), 256, 0, c->stream>>>(c->numeq, c->d_free,
+                                                              src, full_out);
+  }
+  ICK(cudaGetLastError());
+}
+
+void from_full(icarat_ctx *c, const double *full_in, double *out, bool host_dst)
+{
+  double *dst = host_dst ? c->d_v2 : out;
+  if(c->numeq > 0)
+  {
+    note_launch();
+    k_gather_free<<<grid_for(c->numeq), 256, 0, c->stream>>>(c->numeq, c->d_free,
+                                                             full_in, dst);
+  }
+  ICK(cudaGetLastError());
+  if(host_dst)
+  {
+    ICK(cudaMemcpyAsync(out, c->d_v2, sizeof(double) * c->numeq,
+                        cudaMemcpyDeviceToHost, c->stream));
+    ICK(cudaStreamSynchronize(c->stream));
+  }
+}
+
+void set_design_device(icarat_ctx *c, const double *d_rho)
+{
+  if(d_rho != c->d_rho)
+    ICK(cudaMemcpyAsync(c->d_rho, d_rho, sizeof(double) * c->nelx,
+                        cudaMemcpyDeviceToDevice, c->stream));
+  note_launch();
+  k_simp<<<grid_for(c->nelx), 256, 0, c->stream>>>(
+      c->nelx, c->d_rho, c->mat.young_min, c->mat.young_max, c->mat.penalty,
+      c->d_E);
+  ICK(cudaGetLastError());
+  c->design_set = true;
+  c->solved = false;
+  c->design_version++;
+}
+
+// Mesh + BC on the host, mirroring MeshIcarat/BCIcarat:
+//  node coordinates x = (L / div) * index (mesh_icarat.hpp:468-476);
+//  Dirichlet boxes widened by 1e-7, flags kept once 1, values overwritten
+//  (boundary_condition_icarat.hpp:73-138, boundary_condition_base.hpp:19-33);
+//  countDOF numbering (boundary_condition_base.hpp:35-95);
+//  point loads on free components of nodes in the widened box
+//  (boundary_condition_icarat.hpp:213-264, 380-396).
+static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
+{
+  const double tol = 1.0e-7;
+  const long NX = c->NX, NY = c->NY;
+  auto coord = [&](long n, int d) -> double
+  {
+    long i = n % NX, j = (n / NX) % NY, k = n / (NX * NY);
+    if(d == 0)
+      return (c->lx / c->nx) * i;
+    if(d == 1)
+      return (c->ly / c->ny) * j;
+    return (c->lz / c->nz) * k;
+  };
+  std::vector<uint8_t> has(c->numnp, 0);
+  std::vector<int> flag(3 * (size_t)c->numnp, 0);
+  std::vector<double> val(3 * (size_t)c->numnp, 0.0);
+  for(int d = 0; d < (bc ? bc->n_dirichlet : 0); d++)
+  {
+    const icarat_dirichlet &D = bc->dirichlet[d];
+    for(int q = 0; q < 3; q++)
+      IREQUIRE(D.flag[q] == 0 || D.flag[q] == 1, ICARAT_ERR_ARG,
+               "dirichlet flags must be 0 or 1");
+    // index range of nodes inside the widened box along each axis
+    long lo[3], hi[3];
+    const int nn[3] = {c->NX, c->NY, c->NZ};
+    const double h[3] = {c->lx / c->nx, c->ly / c->ny, c->lz / c->nz};
+    for(int a = 0; a < 3; a++)
+    {
+      lo[a] = nn[a];
+      hi[a] = -1;
+      for(long i = 0; i < nn[a]; i++)
+      {
+        double x = h[a] * i;
+        if(x >= D.box[a][0] - tol && x <= D.box[a][1] + tol)
+        {
+          if(i < lo[a])
+            lo[a] = i;
+          hi[a] = i;
+        }
+      }
+    }
+    for(long k = lo[2]; k <= hi[2]; k++)
+      for(long j = lo[1]; j <= hi[1]; j++)
+        for(long i = lo[0]; i <= hi[0]; i++)
+        {
+          long n = i + j * NX + k * NX * NY;
+          has[n] = 1;
+          for(int q = 0; q < 3; q++)
+          {
+            if(flag[3 * n + q] != 1)
+              flag[3 * n + q] = D.flag[q];
+            val[3 * n + q] = D.val[q];
+          }
+        }
+  }
+  c->dof.assign(3 * (size_t)c->numnp, -1);
+  c->fix_h.assign(c->numnp, 0);
+  c->uD_h.assign(3 * (size_t)c->numnp, 0.0);
+  int counter = 0;
+  for(long n = 0; n < c->numnp; n++)
+    for(int q = 0; q < 3; q++)
+      if(!has[n] || flag[3 * n + q] == 0)
+        c->dof[3 * n + q] = counter++;
+  c->numeq = counter;
+  for(long n = 0; n < c->numnp; n++)
+    if(has[n])
+      for(int q = 0; q < 3; q++)
+        if(flag[3 * n + q] != 0)
+        {
+          c->dof[3 * n + q] = counter++;
+          c->fix_h[n] |= (uint8_t)(1u << q);
+          if(flag[3 * n + q] == 1)
+            c->uD_h[3 * n + q] = val[3 * n + q];
+          if(c->uD_h[3 * n + q] != 0.0)
+            c->has_uD = true;
+        }
+  // point loads
+  c->fext_h.assign(c->numeq, 0.0);
+  for(int l = 0; l < (bc ? bc->n_loads : 0); l++)
+  {
+    const icarat_load &L = bc->loads[l];
+    IREQUIRE(L.box[0][0] == L.box[0][1] && L.box[1][0] == L.box[1][1] &&
+                 L.box[2][0] == L.box[2][1],
+             ICARAT_ERR_UNSUPPORTED,
+             "only point loads (degenerate neumann boxes) are supported");
+    for(long n = 0; n < c->numnp; n++)
+    {
+      double x = coord(n, 0), y = coord(n, 1), z = coord(n, 2);
+      if(L.box[0][0] - tol <= x && x <= L.box[0][1] + tol &&
+         L.box[1][0] - tol <= y && y <= L.box[1][1] + tol &&
+         L.box[2][0] - tol <= z && z <= L.box[2][1] + tol)
+        for(int q = 0; q < 3; q++)
+        {
+          int d = c->dof[3 * n + q];
+          if(d < c->numeq)
+            c->fext_h[d] += L.val[q];
+        }
+    }
+  }
+}
+
+} // namespace icarat_b200
+
+using namespace icarat_b200;
+
+int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
+                           const icarat_bc *bc, int device, icarat_ctx **out)
+{
+  IREQUIRE(grid && mat && out, ICARAT_ERR_ARG, "null argument");
+  IREQUIRE(grid->nx >= 1 && grid->ny >= 1 && grid->nz >= 1, ICARAT_ERR_ARG,
+           "division must be >= 1");
+  IREQUIRE(grid->lx > 0 && grid->ly > 0 && grid->lz > 0, ICARAT_ERR_ARG,
+           "length must be > 0");
+  IREQUIRE(mat->young_max - mat->young_min >= 0.0, ICARAT_ERR_ARG,
+           "young = [E1, E2] needs E2 >= E1 (elasticity.hpp:15)");
+  IREQUIRE(mat->poisson > -1.0 && mat->poisson < 0.5, ICARAT_ERR_ARG,
+           "poisson out of range");
+  long long numnp = (long long)(grid->nx + 1) * (grid->ny + 1) * (grid->nz + 1);
+  IREQUIRE(3 * numnp < (1LL << 31) - 1, ICARAT_ERR_UNSUPPORTED,
+           "more than 2^31-1 DOFs");
+  icarat_ctx *c = new icarat_ctx();
+  try
+  {
+    c->device = device;
+    ICK(cudaSetDevice(device));
+    ICK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->nx = grid->nx;
+    c->ny = grid->ny;
+    c->nz = grid->nz;
+    c->lx = grid->lx;
+    c->ly = grid->ly;
+    c->lz = grid->lz;
+    c->hx = grid->lx / grid->nx;
+    c->hy = grid->ly / grid->ny;
+    c->hz = grid->lz / grid->nz;
+    c->NX = c->nx + 1;
+    c->NY = c->ny + 1;
+    c->NZ = c->nz + 1;
+    c->numnp = (int)numnp;
+    c->nelx = c->nx * c->ny * c->nz;
+    c->neq = 3 * c->numnp;
+    c->mat = *mat;
+    hexa8_stiffness(c->hx, c->hy, c->hz, mat->poisson, c->ke0.k, &c->vol0);
+    c->ke_diag_max = 0.0;
+    for(int a = 0; a < 24; a++)
+      c->ke_diag_max = std::fmax(c->ke_diag_max, c->ke0.k[25 * a]);
+    c->lam_max_dk = jacobi_bound(c->ke0.k);
+    build_mesh_bc(c, bc);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    c->red_blocks = sms * 4 > kMaxRedBlocks ? kMaxRedBlocks : sms * 4;
+
+    // free-DOF map: equation number -> 3 node + component
+    std::vector<int> freeidx(c->numeq > 0 ? c->numeq : 1);
+    for(long n = 0; n < c->numnp; n++)
+      for(int q = 0; q < 3; q++)
+        if(c->dof[3 * n + q] < c->numeq)
+          freeidx[c->dof[3 * n + q]] = (int)(3 * n + q);
+    ICK(cudaMalloc(&c->d_free, sizeof(int) * freeidx.size()));
+    ICK(cudaMemcpy(c->d_free, freeidx.data(), sizeof(int) * freeidx.size(),
+                   cudaMemcpyHostToDevice));
+    ICK(cudaMalloc(&c->d_fix, c->numnp));
+    ICK(cudaMemcpy(c->d_fix, c->fix_h.data(), c->numnp, cudaMemcpyHostToDevice));
+    const size_t nv = (size_t)c->neq;
+    c->d_fext = dalloc(nv);
+    c->d_rhs = dalloc(nv);
+    c->d_u = dalloc(nv);
+    c->d_invd = dalloc(nv);
+    c->d_r = dalloc(nv);
+    c->d_p = dalloc(nv);
+    c->d_z = dalloc(nv);
+    c->d_Ap = dalloc(nv);
+    c->d_v1 = dalloc(nv);
+    c->d_v2 = dalloc(nv);
+    c->d_rho = dalloc(c->nelx);
+    c->d_E = dalloc(c->nelx);
+    c->d_e1 = dalloc(c->nelx);
+    c->d_e2 = dalloc(c->nelx);
+    c->d_partials = dalloc((size_t)kMaxRedBlocks * 8);
+    c->d_scalar = dalloc(64);
+    ICK(cudaMalloc(&c->d_counter, sizeof(unsigned int) * 16));
+    ICK(cudaMemset(c->d_counter, 0, sizeof(unsigned int) * 16));
+    ICK(cudaMalloc(&c->d_cg, sizeof(CgScalars)));
+    ICK(cudaMemset(c->d_cg, 0, sizeof(CgScalars)));
+    ICK(cudaMallocHost(&c->h_cg, sizeof(CgScalars)));
+    ICK(cudaMallocHost(&c->h_scalar, sizeof(double) * 64));
+    if(c->has_uD)
+    {
+      c->d_uD = dalloc(nv);
+      ICK(cudaMemcpy(c->d_uD, c->uD_h.data(), sizeof(double) * nv,
+                     cudaMemcpyHostToDevice));
+    }
+    ICK(cudaMemset(c->d_u, 0, sizeof(double) * nv));
+    // fext in node layout
+    std::vector<double> ff(nv, 0.0);
+    for(long n = 0; n < c->numnp; n++)
+      for(int q = 0; q < 3; q++)
+        if(c->dof[3 * n + q] < c->numeq)
+          ff[3 * n + q] = c->fext_h[c->dof[3 * n + q]];
+    ICK(cudaMemcpy(c->d_fext, ff.data(), sizeof(double) * nv,
+                   cudaMemcpyHostToDevice));
+  }
+  catch(...)
+  {
+    icarat_ctx_destroy(c);
+    throw;
+  }
+  *out = c;
+  return ICARAT_OK;
+}
+
+int icarat_ctx_destroy_impl(icarat_ctx *c)
+{
+  if(!c)
+    return ICARAT_OK;
+  cudaSetDevice(c->device);
+  if(c->stream)
+    cudaStreamSynchronize(c->stream);
+  mg_free(c);
+  filter_free(c);
+  if(c->loop.mma)
+    icarat_mma_destroy(c->loop.mma);
+  for(double *p : {c->loop.x, c->loop.xfil, c->loop.xthr, c->loop.thrd,
+                   c->loop.dfds, c->loop.dgds, c->loop.tmp, c->loop.xmin,
+                   c->loop.xmax})
+    dfree(p);
+  dfree(c->d_free);
+  dfree(c->d_fix);
+  dfree(c->d_uD);
+  for(double *p : {c->d_fext, c->d_rhs, c->d_u, c->d_invd, c->d_r, c->d_p,
+                   c->d_z, c->d_Ap, c->d_v1, c->d_v2, c->d_rho, c->d_E,
+                   c->d_e1, c->d_e2, c->d_partials, c->d_scalar, c->d_stage})
+    dfree(p);
+  dfree(c->d_counter);
+  dfree(c->d_cg);
+  if(c->h_cg)
+    cudaFreeHost(c->h_cg);
+  if(c->h_scalar)
+    cudaFreeHost(c->h_scalar);
+  if(c->stream)
+    cudaStreamDestroy(c->stream);
+  delete c;
+  return ICARAT_OK;
+}

@@ -1,0 +1,330 @@
+// Internal declarations of the sm_100a implementation behind icarat_gpu.h.
+//
+// Layout in HBM (all contexts):
+//   node vectors  : double[3 * numnp], node-major, component fastest
+//                   (node id = i + j NX + k NX NY, NX = nx + 1), constrained
+//                   components always hold 0 (prescribed values live apart);
+//   element arrays: double[nelx], element id = i + j nx + k nx ny;
+//   "numeq" vectors of the C ABI are gathered / scattered through d_free
+//   (equation number -> 3 * node + component).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <exception>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/icarat_gpu.h"
+
+namespace icarat_b200
+{
+
+struct Error
+{
+  int status;
+  std::string msg;
+};
+
+void set_last_error(const std::string &msg);
+
+// Process-wide count of this library's kernel launches (graph replays count
+// their kernel nodes; launches recorded while capturing a graph do not count).
+void note_launch(unsigned long long n = 1);
+void set_capturing(bool on);
+
+#define ICK(call)                                                               \
+  do                                                                            \
+  {                                                                             \
+    cudaError_t e_ = (call);                                                    \
+    if(e_ != cudaSuccess)                                                       \
+      throw ::icarat_b200::Error{ICARAT_ERR_CUDA,                               \
+                                 std::string(#call) + ": " +                    \
+                                     cudaGetErrorString(e_)};                   \
+  } while(0)
+
+#define ICARAT_API_BEGIN                                                        \
+  try                                                                           \
+  {
+#define ICARAT_API_END                                                          \
+  }                                                                             \
+  catch(const ::icarat_b200::Error &e_)                                         \
+  {                                                                             \
+    ::icarat_b200::set_last_error(e_.msg);                                      \
+    return e_.status;                                                           \
+  }                                                                             \
+  catch(const std::exception &e_)                                               \
+  {                                                                             \
+    ::icarat_b200::set_last_error(e_.what());                                   \
+    return ICARAT_ERR_NOMEM;                                                    \
+  }                                                                             \
+  catch(...)                                                                    \
+  {                                                                             \
+    ::icarat_b200::set_last_error("unknown error");                             \
+    return ICARAT_ERR_CUDA;                                                     \
+  }
+
+#define IREQUIRE(cond, status, msg)                                             \
+  do                                                                            \
+  {                                                                             \
+    if(!(cond))                                                                 \
+      throw ::icarat_b200::Error{status, msg};                                  \
+  } while(0)
+
+// Element stiffness (E = 1), passed by value as a kernel parameter: every
+// coefficient index is a compile-time constant after unrolling, so the
+// 576 entries are read as uniform constant-bank operands.
+struct KeParam
+{
+  double k[576];
+};
+
+// Structured grid of one level.
+struct GridDev
+{
+  int nx, ny, nz; // elements
+  int NX, NY, NZ; // nodes
+  int numnp, nelx;
+};
+
+// Scalars of a device-resident Krylov loop.
+struct CgScalars
+{
+  double alpha, beta, zr, zr_new, pAp, rr, rnorm, bnorm, tol;
+  int iter, maxit, done, status;
+  unsigned int counter;
+  int pad;
+};
+
+// Reduction geometry: every grid-stride reduction kernel runs on
+// kRedBlocks blocks of kRedThreads threads so that partial sums are summed
+// in one fixed order (bit-reproducible on a given GPU).
+constexpr int kRedThreads = 256;
+constexpr int kMaxRedBlocks = 2048;
+
+struct MgLevel
+{
+  GridDev g;
+  double *E = nullptr;     // nelx, SIMP modulus x 2^level
+  uint8_t *fix = nullptr;  // numnp, bit c = component c constrained
+  double *invd = nullptr;  // 3 numnp, 1 / diag(K) (0 on constrained)
+  double *x = nullptr, *b = nullptr, *r = nullptr, *t = nullptr;
+};
+
+struct CoarseSolver
+{
+  int n = 0;              // free DOFs of the coarsest level
+  int *map = nullptr;     // n -> full index on the coarsest grid
+  double *A = nullptr;    // n x n dense, becomes A^-1
+  double *work = nullptr; // n x n
+  double *vin = nullptr, *vout = nullptr;
+};
+
+struct FilterState
+{
+  double radius = 0.0;
+  int nofs = 0;                 // stencil points
+  int rx = 0, ry = 0, rz = 0;   // index reach per axis
+  std::vector<int> ofs;         // 3 * nofs (di, dj, dk), ascending element id
+  std::vector<double> w;        // nofs weights R - d
+  int *d_ofs = nullptr;
+  double *d_w = nullptr;
+  double *d_aa = nullptr;       // nelx sums of weights (dfilters_ds)
+  bool have_forward = false;
+};
+
+struct MmaDev;
+
+struct LoopState
+{
+  bool init = false;
+  icarat_loop_opts opts;
+  int optstep = 0;
+  double V0 = 0.0;
+  double *x = nullptr, *xfil = nullptr, *xthr = nullptr, *thrd = nullptr,
+         *dfds = nullptr, *dgds = nullptr, *tmp = nullptr, *xmin = nullptr,
+         *xmax = nullptr;
+  icarat_mma *mma = nullptr;
+};
+
+} // namespace icarat_b200
+
+struct icarat_ctx
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nx, ny, nz;
+  double lx, ly, lz, hx, hy, hz;
+  int NX, NY, NZ, numnp, nelx, neq, numeq;
+  icarat_material mat;
+  icarat_b200::KeParam ke0;
+  double vol0;
+  double ke_diag_max; // max_a Ke0[a][a]
+  double lam_max_dk;  // bound on lambda_max(D^-1 K) from the element matrix
+  int red_blocks;     // reduction grid size
+  // host copies
+  std::vector<int> dof;        // 3 numnp
+  std::vector<double> fext_h;  // numeq
+  std::vector<uint8_t> fix_h;  // numnp
+  std::vector<double> uD_h;    // 3 numnp prescribed values (0 if free)
+  bool has_uD = false;
+  // device
+  int *d_free = nullptr;
+  uint8_t *d_fix = nullptr;
+  double *d_uD = nullptr;
+  double *d_fext = nullptr;
+  double *d_rho = nullptr, *d_E = nullptr;
+  double *d_rhs = nullptr, *d_u = nullptr, *d_invd = nullptr;
+  double *d_r = nullptr, *d_p = nullptr, *d_z = nullptr, *d_Ap = nullptr;
+  double *d_v1 = nullptr, *d_v2 = nullptr; // staging (3 numnp)
+  double *d_e1 = nullptr, *d_e2 = nullptr; // staging (nelx)
+  double *d_partials = nullptr;            // kMaxRedBlocks * 8
+  double *d_scalar = nullptr;              // small scalar results
+  double *d_stage = nullptr;               // host-API staging, 6 nelx
+  unsigned int *d_counter = nullptr;
+  icarat_b200::CgScalars *d_cg = nullptr;
+  icarat_b200::CgScalars *h_cg = nullptr; // pinned
+  double *h_scalar = nullptr;             // pinned
+  bool design_set = false, solved = false;
+  icarat_solve_info last_info{};
+  // multigrid
+  std::vector<icarat_b200::MgLevel> mg;
+  int mg_built_levels = 0;
+  icarat_b200::CoarseSolver coarse;
+  // filter
+  icarat_b200::FilterState filt;
+  // loop
+  icarat_b200::LoopState loop;
+  // instantiated solver graphs: (method, levels, smooth, chunk, x) -> exec
+  std::map<std::tuple<int, int, int, int, const void *>, cudaGraphExec_t> graphs;
+  std::map<std::tuple<int, int, int, int, const void *>, int> graph_kernels;
+  unsigned long design_version = 0;
+  unsigned long mg_version = ~0ul;
+};
+
+namespace icarat_b200
+{
+// ke0.cpp
+void hexa8_stiffness(double hx, double hy, double hz, double nu, double *ke,
+                     double *volume);
+double jacobi_bound(const double *ke);
+
+// ctx.cu
+void to_full(icarat_ctx *c, const double *numeq_in, double *full_out,
+             bool host_src);
+void from_full(icarat_ctx *c, const double *full_in, double *numeq_out,
+               bool host_dst);
+void set_design_device(icarat_ctx *c, const double *d_rho);
+double *dalloc(size_t n);
+void dfree(void *p);
+
+// stiffness.cu
+void launch_apply_K(icarat_ctx *c, const GridDev &g, const double *E,
+                    const uint8_t *fix, const double *u, double *y,
+                    double *dot_partials);
+void launch_diag(icarat_ctx *c, const GridDev &g, const double *E,
+                 const uint8_t *fix, double *invd);
+void launch_residual(icarat_ctx *c, const GridDev &g, const double *E,
+                     const uint8_t *fix, const double *b, const double *x,
+                     double *r);
+void launch_fint(icarat_ctx *c, double *d_out_full);
+
+// reduce helpers (stiffness.cu)
+double device_dot(icarat_ctx *c, const double *a, const double *b, int n);
+
+// pcg.cu
+void release_graphs(icarat_ctx *c);
+int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
+               double *d_x, icarat_solve_info *info);
+
+// multigrid.cu
+void mg_setup(icarat_ctx *c, int levels);
+void mg_vcycle(icarat_ctx *c, const double *r, double *z, int smooth);
+void mg_free(icarat_ctx *c);
+
+// filter.cu
+void filter_setup(icarat_ctx *c, double radius);
+void filter_apply(icarat_ctx *c, const double *d_in, double *d_out,
+                  bool is_sens);
+void filter_free(icarat_ctx *c);
+void threshold_dev(icarat_ctx *c, const double *d_in, double beta, double T,
+                   double *d_out, bool derivative);
+
+// sens.cu
+void node_values_dev(icarat_ctx *c, double *d_node_val);
+double compliance_dev(icarat_ctx *c);
+void sensitivity_dev(icarat_ctx *c, double dgds_scale, double *d_dfds,
+                     double *d_dgds);
+
+// oc.cu
+int oc_update_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
+                  const double *dgdx, const double *xmin, const double *xmax,
+                  const icarat_oc_opts *o, int *steps);
+
+// device reductions shared by several kernels
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *sh)
+{
+#pragma unroll
+  for(int q = 0; q < NV; q++)
+    for(int o = 16; o > 0; o >>= 1)
+      v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if(lane == 0)
+#pragma unroll
+    for(int q = 0; q < NV; q++)
+      sh[q * 32 + w] = v[q];
+  __syncthreads();
+  if(w == 0)
+  {
+#pragma unroll
+    for(int q = 0; q < NV; q++)
+    {
+      v[q] = lane < nw ? sh[q * 32 + lane] : 0.0;
+      for(int o = 16; o > 0; o >>= 1)
+        v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    }
+  }
+}
+
+// Called by all threads of every block after thread 0 wrote this block's
+// partials.  Returns true in exactly one block (the last to arrive), whose
+// threads may then read every block's partials.
+__device__ __forceinline__ bool last_block(unsigned int *counter)
+{
+  __shared__ bool am_last;
+  __threadfence();
+  __syncthreads();
+  if(threadIdx.x == 0)
+  {
+    unsigned int t = atomicAdd(counter, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if(am_last)
+    __threadfence();
+  return am_last;
+}
+
+// Sum NV partial arrays (layout [q][nparts]) in a fixed order; result in
+// thread 0 of the calling block.
+template <int NV>
+__device__ __forceinline__ void sum_partials(const double *partials, int nparts,
+                                             double (&v)[NV], double *sh)
+{
+#pragma unroll
+  for(int q = 0; q < NV; q++)
+  {
+    double s = 0.0;
+    for(int i = threadIdx.x; i < nparts; i += blockDim.x)
+      s += __ldcg(partials + q * nparts + i);
+    v[q] = s;
+  }
+  block_sum<NV>(v, sh);
+}
+
+} // namespace icarat_b200

@@ -1,0 +1,736 @@
+// Geometric multigrid preconditioner for the SIMP stiffness (no reference
+// counterpart: the reference solves with Jacobi-PCG or a direct solver).
+//
+// Level l + 1 halves every axis of level l.  Coarse operators are
+// rediscretised: a coarse element's modulus is the mean of its 8 children
+// times 2 (a hexa8 stiffness scales with its edge length), so every level
+// reuses the fine Ke0 and the matrix-free node stencil.  A coarse node is
+// constrained where its coincident fine node is.  Transfers are trilinear
+// prolongation P and restriction R = P^T.  Smoothing is a Chebyshev
+// polynomial in D^-1 K on [0.1 lmax, lmax], where lmax is the element bound
+// of the Jacobi-scaled Ke0 (a rigorous bound for every SIMP design), applied
+// identically before and after the coarse correction so that the V-cycle is
+// a symmetric positive definite preconditioner.  The coarsest level is solved
+// exactly with a dense inverse built on the GPU every time the design
+// changes: blocked Cholesky A = L L^T, W = L^-1, A^-1 = W^T W.
+#include <cmath>
+#include <cstring>
+
+#include "stencil.cuh"
+
+namespace icarat_b200
+{
+
+// ---------------------------------------------------------------- level data
+__global__ void k_coarsen_E(GridDev f, GridDev c, const double *__restrict__ Ef,
+                            double *__restrict__ Ec)
+{
+  for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < c.nelx;
+      e += gridDim.x * blockDim.x)
+  {
+    const int I = e % c.nx, J = (e / c.nx) % c.ny, K = e / (c.nx * c.ny);
+    double s = 0.0;
+#pragma unroll
+    for(int dz = 0; dz < 2; dz++)
+#pragma unroll
+      for(int dy = 0; dy < 2; dy++)
+#pragma unroll
+        for(int dx = 0; dx < 2; dx++)
+          s += Ef[(2 * I + dx) + (long)(2 * J + dy) * f.nx +
+                  (long)(2 * K + dz) * f.nx * f.ny];
+    Ec[e] = 0.25 * s; // mean of 8 children x 2
+  }
+}
+
+__global__ void k_coarsen_fix(GridDev f, GridDev c, const uint8_t *__restrict__ ff,
+                              uint8_t *__restrict__ fc)
+{
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    const int I = n % c.NX, J = (n / c.NX) % c.NY, K = n / (c.NX * c.NY);
+    fc[n] = ff[2 * I + (long)2 * J * f.NX + (long)2 * K * f.NX * f.NY];
+  }
+}
+
+// ---------------------------------------------------------------- transfers
+// coarse b = R r  (R = P^T, 27 fine nodes per coarse node, weights 1/2^d)
+__global__ void k_restrict(GridDev f, GridDev c, const double *__restrict__ rf,
+                           const uint8_t *__restrict__ fixc,
+                           double *__restrict__ bc)
+{
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    const int I = n % c.NX, J = (n / c.NX) % c.NY, K = n / (c.NX * c.NY);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for(int dz = -1; dz <= 1; dz++)
+#pragma unroll
+      for(int dy = -1; dy <= 1; dy++)
+#pragma unroll
+        for(int dx = -1; dx <= 1; dx++)
+        {
+          const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
+          if(i < 0 || i >= f.NX || j < 0 || j >= f.NY || k < 0 || k >= f.NZ)
+            continue;
+          const double w = (dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0);
+          const long m = i + (long)j * f.NX + (long)k * f.NX * f.NY;
+          s0 += w * rf[3 * m + 0];
+          s1 += w * rf[3 * m + 1];
+          s2 += w * rf[3 * m + 2];
+        }
+    const unsigned fx = fixc[n];
+    bc[3L * n + 0] = (fx & 1u) ? 0.0 : s0;
+    bc[3L * n + 1] = (fx & 2u) ? 0.0 : s1;
+    bc[3L * n + 2] = (fx & 4u) ? 0.0 : s2;
+  }
+}
+
+// fine x += P xc (masked)
+__global__ void k_prolong_add(GridDev f, GridDev c, const double *__restrict__ xc,
+                              const uint8_t *__restrict__ fixf,
+                              double *__restrict__ xf)
+{
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < f.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    const int i = n % f.NX, j = (n / f.NX) % f.NY, k = n / (f.NX * f.NY);
+    const int I0 = i >> 1, J0 = j >> 1, K0 = k >> 1;
+    const int I1 = I0 + (i & 1), J1 = J0 + (j & 1), K1 = K0 + (k & 1);
+    const double wx = (i & 1) ? 0.5 : 1.0, wy = (j & 1) ? 0.5 : 1.0,
+                 wz = (k & 1) ? 0.5 : 1.0;
+    double s[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for(int cz = 0; cz < 2; cz++)
+#pragma unroll
+      for(int cy = 0; cy < 2; cy++)
+#pragma unroll
+        for(int cx = 0; cx < 2; cx++)
+        {
+          // odd coordinates take both neighbours with 1/2, even ones the
+          // coincident coarse node once
+          if((cx && !(i & 1)) || (cy && !(j & 1)) || (cz && !(k & 1)))
+            continue;
+          const int I = cx ? I1 : I0, J = cy ? J1 : J0, K = cz ? K1 : K0;
+          const long m = I + (long)J * c.NX + (long)K * c.NX * c.NY;
+          const double w = wx * wy * wz;
+          s[0] += w * xc[3 * m + 0];
+          s[1] += w * xc[3 * m + 1];
+          s[2] += w * xc[3 * m + 2];
+        }
+    const unsigned fx = fixf[n];
+#pragma unroll
+    for(int q = 0; q < 3; q++)
+      if(!((fx >> q) & 1u))
+        xf[3L * n + q] += s[q];
+  }
+}
+
+// ---------------------------------------------------------------- smoother
+// First Chebyshev step from x = 0: d = invd b / theta, x = d.
+__global__ void k_cheb_first(int n, const double *__restrict__ b,
+                             const double *__restrict__ invd, double inv_theta,
+                             double *__restrict__ x, double *__restrict__ d)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+  {
+    const double di = inv_theta * invd[i] * b[i];
+    d[i] = di;
+    x[i] = di;
+  }
+}
+
+// One Chebyshev step: r = b - K x, d = c1 d + c2 invd r, xo = x + d.
+// x and xo are distinct buffers (neighbours of x are read by other threads).
+__global__ void __launch_bounds__(128)
+    k_cheb_step(GridDev g, KeParam ke, const double *__restrict__ E,
+                const uint8_t *__restrict__ fix, const double *__restrict__ invd,
+                const double *__restrict__ b, const double *__restrict__ x,
+                double *__restrict__ d, double *__restrict__ xo, double c1,
+                double c2)
+{
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    double acc[3], uc[3];
+    node_Ku(g, ke, E, x, n, acc, uc);
+    const unsigned f = fix[n];
+#pragma unroll
+    for(int q = 0; q < 3; q++)
+    {
+      const long id = 3L * n + q;
+      double dn = 0.0;
+      if(!((f >> q) & 1u))
+        dn = (c1 != 0.0 ? c1 * d[id] : 0.0) + c2 * invd[id] * (b[id] - acc[q]);
+      d[id] = dn;
+      xo[id] = uc[q] + dn;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- coarse
+// Dense coarse matrix, one thread per free row (fixed summation order).
+__global__ void k_coarse_assemble(GridDev g, KeParam ke, const double *__restrict__ E,
+                                  const int *__restrict__ rowmap,
+                                  const int *__restrict__ colmap, int nfree,
+                                  double *__restrict__ A)
+{
+  for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree;
+      r += gridDim.x * blockDim.x)
+  {
+    double *row = A + (long)r * nfree; // zeroed by the caller
+    const int full = rowmap[r];
+    const int n = full / 3, c = full % 3;
+    const int i = n % g.NX, j = (n / g.NX) % g.NY, k = n / (g.NX * g.NY);
+    for(int sz = 0; sz < 2; sz++)
+      for(int sy = 0; sy < 2; sy++)
+        for(int sx = 0; sx < 2; sx++)
+        {
+          const int ei = i - 1 + sx, ej = j - 1 + sy, ek = k - 1 + sz;
+          if(ei < 0 || ei >= g.nx || ej < 0 || ej >= g.ny || ek < 0 || ek >= g.nz)
+            continue;
+          const double e = E[ei + (long)ej * g.nx + (long)ek * g.nx * g.ny];
+          const int a = local_node(1 - sx, 1 - sy, 1 - sz);
+          for(int bz = 0; bz < 2; bz++)
+            for(int by = 0; by < 2; by++)
+              for(int bx = 0; bx < 2; bx++)
+              {
+                const int b = local_node(bx, by, bz);
+                const long m = (ei + bx) + (long)(ej + by) * g.NX +
+                               (long)(ek + bz) * g.NX * g.NY;
+                for(int d = 0; d < 3; d++)
+                {
+                  const int col = colmap[3 * m + d];
+                  if(col >= 0)
+                    row[col] += e * ke.k[(3 * a + c) * 24 + 3 * b + d];
+                }
+              }
+        }
+  }
+}
+
+constexpr int CB = 32; // Cholesky block
+
+// Cholesky of the diagonal block at kb (in place, lower); one CTA of CB x CB.
+__global__ void k_chol_diag(double *A, int n, int kb)
+{
+  __shared__ double L[CB][CB + 1];
+  const int tx = threadIdx.x, ty = threadIdx.y; // column, row
+  const int m = min(CB, n - kb);
+  L[ty][tx] = (ty < m && tx < m) ? A[(long)(kb + ty) * n + kb + tx]
+                                 : (ty == tx ? 1.0 : 0.0);
+  __syncthreads();
+  for(int j = 0; j < CB; j++)
+  {
+    if(ty == j && tx == j)
+      L[j][j] = sqrt(L[j][j]);
+    __syncthreads();
+    if(tx == j && ty > j)
+      L[ty][j] /= L[j][j];
+    __syncthreads();
+    if(ty > j && tx > j && tx <= ty)
+      L[ty][tx] -= L[ty][j] * L[tx][j];
+    __syncthreads();
+  }
+  if(ty < m && tx < m)
+    A[(long)(kb + ty) * n + kb + tx] = (tx <= ty) ? L[ty][tx] : 0.0;
+}
+
+// Panel: rows i >= kb + CB, A[i, kb:kb+CB] <- A[i, kb:kb+CB] L_kk^-T.
+__global__ void k_chol_panel(double *A, int n, int kb)
+{
+  __shared__ double L[CB][CB + 1];
+  const int m = min(CB, n - kb);
+  for(int t = threadIdx.x; t < CB * CB; t += blockDim.x)
+  {
+    const int r = t / CB, s = t % CB;
+    L[r][s] = (r < m && s < m) ? A[(long)(kb + r) * n + kb + s] : (r == s ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  const int i = kb + CB + blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n)
+    return;
+  double x[CB];
+  double *row = A + (long)i * n + kb;
+#pragma unroll
+  for(int t = 0; t < CB; t++)
+    x[t] = t < m ? row[t] : 0.0;
+#pragma unroll
+  for(int t = 0; t < CB; t++)
+  {
+    double v = x[t];
+#pragma unroll
+    for(int s = 0; s < t; s++)
+      v -= x[s] * L[t][s];
+    x[t] = v / L[t][t];
+  }
+#pragma unroll
+  for(int t = 0; t < CB; t++)
+    if(t < m)
+      row[t] = x[t];
+}
+
+// Trailing update of the lower triangle: A[i][j] -= sum_t P[i][t] P[j][t]
+// for i, j >= kb + CB, j <= i, tiles of 64 x 64 (16 outputs per thread).
+__global__ void __launch_bounds__(256) k_chol_update(double *A, int n, int kb)
+{
+  const int base = kb + CB;
+  const int tiles = (n - base + 63) / 64;
+  // blockIdx.x enumerates lower-triangle tiles (ti >= tj)
+  int t = blockIdx.x, ti = 0;
+  while(t >= ti + 1)
+  {
+    t -= ti + 1;
+    ti++;
+  }
+  const int tj = t;
+  if(ti >= tiles)
+    return;
+  __shared__ double Pi[64][CB + 1];
+  __shared__ double Pj[64][CB + 1];
+  const int i0 = base + ti * 64, j0 = base + tj * 64;
+  const int m = min(CB, n - kb);
+  for(int q = threadIdx.x; q < 64 * CB; q += blockDim.x)
+  {
+    const int r = q / CB, s = q % CB;
+    Pi[r][s] = (i0 + r < n && s < m) ? A[(long)(i0 + r) * n + kb + s] : 0.0;
+    Pj[r][s] = (j0 + r < n && s < m) ? A[(long)(j0 + r) * n + kb + s] : 0.0;
+  }
+  __syncthreads();
+  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+  double acc[4][4] = {};
+#pragma unroll 8
+  for(int s = 0; s < CB; s++)
+  {
+    double a[4], b[4];
+#pragma unroll
+    for(int u = 0; u < 4; u++)
+    {
+      a[u] = Pi[ty + 16 * u][s];
+      b[u] = Pj[tx + 16 * u][s];
+    }
+#pragma unroll
+    for(int u = 0; u < 4; u++)
+#pragma unroll
+      for(int v = 0; v < 4; v++)
+        acc[u][v] = fma(a[u], b[v], acc[u][v]);
+  }
+#pragma unroll
+  for(int u = 0; u < 4; u++)
+#pragma unroll
+    for(int v = 0; v < 4; v++)
+    {
+      const int i = i0 + ty + 16 * u, j = j0 + tx + 16 * v;
+      if(i < n && j < n && j <= i)
+        A[(long)i * n + j] -= acc[u][v];
+    }
+}
+
+// W = L^-1 for block row bi: diagonal block inverse then off-diagonal blocks
+// W_ij = -L_ii^-1 sum_{k=j}^{i-1} L_ik W_kj  (j < i), one CTA per j.
+__global__ void k_trinv_row(const double *L, double *W, int n, int bi)
+{
+  __shared__ double Lii[CB][CB + 1];
+  __shared__ double S[CB][CB + 1];
+  const int i0 = bi * CB;
+  const int mi = min(CB, n - i0);
+  const int bj = blockIdx.x; // 0..bi
+  const int j0 = bj * CB;
+  const int mj = min(CB, n - j0);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  Lii[ty][tx] = (ty < mi && tx < mi) ? L[(long)(i0 + ty) * n + i0 + tx]
+                                     : (ty == tx ? 1.0 : 0.0);
+  // S = (bj == bi) ? I : -sum_k L_ik W_kj
+  double s = 0.0;
+  if(bj == bi)
+    s = (ty == tx) ? 1.0 : 0.0;
+  else
+  {
+    for(int k0 = j0; k0 < i0; k0 += CB)
+    {
+      const int mk = min(CB, n - k0);
+      for(int t = 0; t < mk; t++)
+      {
+        const double l = (ty < mi) ? L[(long)(i0 + ty) * n + k0 + t] : 0.0;
+        const double w = (tx < mj) ? W[(long)(k0 + t) * n + j0 + tx] : 0.0;
+        s -= l * w;
+      }
+    }
+  }
+  S[ty][tx] = s;
+  __syncthreads();
+  // forward substitution Lii X = S, column tx by thread row 0..CB-1 in turn
+  for(int r = 0; r < CB; r++)
+  {
+    if(ty == r)
+    {
+      double v = S[r][tx];
+      for(int q = 0; q < r; q++)
+        v -= Lii[r][q] * S[q][tx];
+      S[r][tx] = v / Lii[r][r];
+    }
+    __syncthreads();
+  }
+  if(ty < mi && tx < mj)
+    W[(long)(i0 + ty) * n + j0 + tx] = S[ty][tx];
+}
+
+// Ainv = W^T W (lower triangle of tiles, mirrored): Ainv[i][j] =
+// sum_{k >= max(i,j)} W[k][i] W[k][j].
+__global__ void __launch_bounds__(256) k_wtw(const double *W, double *Ainv, int n)
+{
+  const int tiles = (n + 63) / 64;
+  int t = blockIdx.x, ti = 0;
+  while(t >= ti + 1)
+  {
+    t -= ti + 1;
+    ti++;
+  }
+  const int tj = t;
+  if(ti >= tiles)
+    return;
+  __shared__ double Wi[CB][64 + 1];
+  __shared__ double Wj[CB][64 + 1];
+  const int i0 = ti * 64, j0 = tj * 64;
+  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+  double acc[4][4] = {};
+  for(int k0 = i0; k0 < n; k0 += CB) // W lower: rows k >= i0 contribute
+  {
+    __syncthreads();
+    for(int q = threadIdx.x; q < CB * 64; q += blockDim.x)
+    {
+      const int r = q / 64, s = q % 64;
+      const int k = k0 + r;
+      Wi[r][s] = (k < n && i0 + s < n) ? W[(long)k * n + i0 + s] : 0.0;
+      Wj[r][s] = (k < n && j0 + s < n) ? W[(long)k * n + j0 + s] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for(int r = 0; r < CB; r++)
+    {
+      double a[4], b[4];
+#pragma unroll
+      for(int u = 0; u < 4; u++)
+      {
+        a[u] = Wi[r][ty + 16 * u];
+        b[u] = Wj[r][tx + 16 * u];
+      }
+#pragma unroll
+      for(int u = 0; u < 4; u++)
+#pragma unroll
+        for(int v = 0; v < 4; v++)
+          acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+  }
+#pragma unroll
+  for(int u = 0; u < 4; u++)
+#pragma unroll
+    for(int v = 0; v < 4; v++)
+    {
+      const int i = i0 + ty + 16 * u, j = j0 + tx + 16 * v;
+      if(i < n && j < n && j <= i)
+      {
+        Ainv[(long)i * n + j] = acc[u][v];
+        Ainv[(long)j * n + i] = acc[u][v];
+      }
+    }
+}
+
+// Coarse solve: x_full = scatter(Ainv gather(b_full)); one warp per row.
+__global__ void k_coarse_gather(int nfree, const int *__restrict__ rowmap,
+                                const double *__restrict__ b, double *__restrict__ v)
+{
+  for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree;
+      r += gridDim.x * blockDim.x)
+    v[r] = b[rowmap[r]];
+}
+
+__global__ void k_coarse_gemv(int nfree, const double *__restrict__ Ainv,
+                              const double *__restrict__ v,
+                              const int *__restrict__ rowmap, int nfull,
+                              double *__restrict__ x)
+{
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for(int r = warp; r < nfree; r += nw)
+  {
+    const double *row = Ainv + (long)r * nfree;
+    double s = 0.0;
+    for(int q = lane; q < nfree; q += 32)
+      s = fma(row[q], v[q], s);
+    for(int o = 16; o > 0; o >>= 1)
+      s += __shfl_down_sync(0xffffffffu, s, o);
+    if(lane == 0)
+      x[rowmap[r]] = s;
+  }
+  (void)nfull;
+}
+
+// ---------------------------------------------------------------- driver
+static GridDev make_grid(int nx, int ny, int nz)
+{
+  return GridDev{nx, ny, nz, nx + 1, ny + 1, nz + 1, (nx + 1) * (ny + 1) * (nz + 1),
+                 nx * ny * nz};
+}
+
+static int blocks_for(int n, int t)
+{
+  int b = (n + t - 1) / t;
+  return b < 1 ? 1 : b;
+}
+
+void mg_free(icarat_ctx *c)
+{
+  for(size_t l = 1; l < c->mg.size(); l++)
+  {
+    MgLevel &L = c->mg[l];
+    dfree(L.E);
+    dfree(L.fix);
+    dfree(L.invd);
+  }
+  for(size_t l = 0; l < c->mg.size(); l++)
+  {
+    MgLevel &L = c->mg[l];
+    dfree(L.x);
+    dfree(L.b);
+    dfree(L.r);
+    dfree(L.t);
+  }
+  c->mg.clear();
+  dfree(c->coarse.map);
+  dfree(c->coarse.A);
+  dfree(c->coarse.work);
+  dfree(c->coarse.vin);
+  dfree(c->coarse.vout);
+  c->coarse = CoarseSolver{};
+  c->mg_built_levels = 0;
+}
+
+static void allocate_levels(icarat_ctx *c, int levels)
+{
+  release_graphs(c); // captured solver graphs hold pointers to level arrays
+  mg_free(c);
+  int nx = c->nx, ny = c->ny, nz = c->nz;
+  for(int l = 0; l < levels; l++)
+  {
+    if(l > 0)
+    {
+      IREQUIRE(nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0, ICARAT_ERR_UNSUPPORTED,
+               "multigrid needs divisions divisible by 2^(levels-1)");
+      nx /= 2;
+      ny /= 2;
+      nz /= 2;
+    }
+    MgLevel L;
+    L.g = make_grid(nx, ny, nz);
+    const size_t nv = 3 * (size_t)L.g.numnp;
+    if(l == 0)
+    {
+      L.E = c->d_E;
+      L.fix = c->d_fix;
+      L.invd = c->d_invd;
+    }
+    else
+    {
+      L.E = dalloc(L.g.nelx);
+      ICK(cudaMalloc(&L.fix, L.g.numnp));
+      L.invd = dalloc(nv);
+    }
+    L.x = dalloc(nv);
+    L.b = dalloc(nv);
+    L.r = dalloc(nv);
+    L.t = dalloc(nv);
+    c->mg.push_back(L);
+  }
+  // coarse constraint pattern on the host (fixed for the context)
+  std::vector<uint8_t> fix = c->fix_h;
+  GridDev gf = c->mg[0].g;
+  for(int l = 1; l < levels; l++)
+  {
+    GridDev gc = c->mg[l].g;
+    std::vector<uint8_t> fc(gc.numnp);
+    for(int n = 0; n < gc.numnp; n++)
+    {
+      int I = n % gc.NX, J = (n / gc.NX) % gc.NY, K = n / (gc.NX * gc.NY);
+      fc[n] = fix[2 * I + (long)2 * J * gf.NX + (long)2 * K * gf.NX * gf.NY];
+    }
+    ICK(cudaMemcpy(c->mg[l].fix, fc.data(), gc.numnp, cudaMemcpyHostToDevice));
+    fix.swap(fc);
+    gf = gc;
+  }
+  // dense coarse system
+  GridDev gc = c->mg[levels - 1].g;
+  std::vector<int> rowmap, colmap(3 * (size_t)gc.numnp, -1);
+  for(int n = 0; n < gc.numnp; n++)
+    for(int q = 0; q < 3; q++)
+      if(!((fix[n] >> q) & 1u))
+      {
+        colmap[3 * (size_t)n + q] = (int)rowmap.size();
+        rowmap.push_back(3 * n + q);
+      }
+  const int nf = (int)rowmap.size();
+  IREQUIRE((double)nf * nf * 8.0 * 2 < 4.0e9, ICARAT_ERR_UNSUPPORTED,
+           "coarsest multigrid level too large for the dense solve; add levels");
+  c->coarse.n = nf;
+  ICK(cudaMalloc(&c->coarse.map, sizeof(int) * (rowmap.size() + colmap.size() + 1)));
+  if(nf > 0)
+    ICK(cudaMemcpy(c->coarse.map, rowmap.data(), sizeof(int) * nf,
+                   cudaMemcpyHostToDevice));
+  ICK(cudaMemcpy(c->coarse.map + nf, colmap.data(), sizeof(int) * colmap.size(),
+                 cudaMemcpyHostToDevice));
+  c->coarse.A = dalloc((size_t)nf * nf);
+  c->coarse.work = dalloc((size_t)nf * nf);
+  c->coarse.vin = dalloc(nf);
+  c->coarse.vout = dalloc(nf);
+  c->mg_built_levels = levels;
+}
+
+// Coarse operators and the dense inverse for the current design.
+void mg_setup(icarat_ctx *c, int levels)
+{
+  IREQUIRE(levels >= 2 && levels <= 12, ICARAT_ERR_ARG, "mg_levels must be in [2, 12]");
+  if((int)c->mg.size() != levels)
+    allocate_levels(c, levels);
+  else if(c->mg_version == c->design_version)
+    return; // operators of this design are built already
+  c->mg_version = c->design_version;
+  // moduli and Jacobi diagonals
+  for(int l = 0; l < levels; l++)
+  {
+    MgLevel &L = c->mg[l];
+    if(l > 0)
+    {
+      const MgLevel &F = c->mg[l - 1];
+      note_launch();
+      k_coarsen_E<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>(F.g, L.g, F.E, L.E);
+    }
+    launch_diag(c, L.g, L.E, L.fix, L.invd);
+  }
+  // dense coarsest system -> inverse
+  const MgLevel &C = c->mg[levels - 1];
+  const int n = c->coarse.n;
+  if(n > 0)
+  {
+    ICK(cudaMemsetAsync(c->coarse.A, 0, sizeof(double) * (size_t)n * n, c->stream));
+    note_launch();
+    k_coarse_assemble<<<blocks_for(n, 64), 64, 0, c->stream>>>(
+        C.g, c->ke0, C.E, c->coarse.map, c->coarse.map + n, n, c->coarse.A);
+    ICK(cudaGetLastError());
+    double *A = c->coarse.A, *W = c->coarse.work;
+    for(int kb = 0; kb < n; kb += CB)
+    {
+      note_launch();
+      k_chol_diag<<<1, dim3(CB, CB), 0, c->stream>>>(A, n, kb);
+      const int rows = n - kb - CB;
+      if(rows > 0)
+      {
+        note_launch();
+        k_chol_panel<<<blocks_for(rows, 128), 128, 0, c->stream>>>(A, n, kb);
+        const int tiles = (rows + 63) / 64;
+        note_launch();
+        k_chol_update<<<tiles * (tiles + 1) / 2, 256, 0, c->stream>>>(A, n, kb);
+      }
+    }
+    ICK(cudaMemsetAsync(W, 0, sizeof(double) * (size_t)n * n, c->stream));
+    const int nb = (n + CB - 1) / CB;
+    for(int bi = 0; bi < nb; bi++)
+    {
+      note_launch();
+      k_trinv_row<<<bi + 1, dim3(CB, CB), 0, c->stream>>>(A, W, n, bi);
+    }
+    const int tiles = (n + 63) / 64;
+    note_launch();
+    k_wtw<<<tiles * (tiles + 1) / 2, 256, 0, c->stream>>>(W, A, n);
+    ICK(cudaGetLastError());
+  }
+}
+
+// Chebyshev smoothing of K x = b on one level, deg steps.  from_zero: x = 0
+// on entry (the first step needs no product).
+static void smooth(icarat_ctx *c, MgLevel &L, const double *b, int deg,
+                   bool from_zero)
+{
+  const double lmax = c->lam_max_dk;
+  const double lmin = 0.1 * lmax;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  double rho_old = 1.0 / sigma;
+  const int nv = 3 * L.g.numnp;
+  const int nb = blocks_for(L.g.numnp, 128);
+  double *x = L.x, *xo = L.t, *d = L.r;
+  int k0 = 0;
+  if(from_zero)
+  {
+    note_launch();
+    k_cheb_first<<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, L.invd,
+                                                             1.0 / theta, x, d);
+    k0 = 1;
+  }
+  else
+  {
+    // first step from the current x: d = invd (b - K x) / theta
+    note_launch();
+    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, c->ke0, L.E, L.fix, L.invd, b, x,
+                                           d, xo, 0.0, 1.0 / theta);
+    std::swap(x, xo);
+    k0 = 1;
+  }
+  for(int k = k0; k < deg; k++)
+  {
+    const double rho = 1.0 / (2.0 * sigma - rho_old);
+    note_launch();
+    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, c->ke0, L.E, L.fix, L.invd, b, x,
+                                           d, xo, rho * rho_old, 2.0 * rho / delta);
+    std::swap(x, xo);
+    rho_old = rho;
+  }
+  if(x != L.x)
+    ICK(cudaMemcpyAsync(L.x, x, sizeof(double) * nv, cudaMemcpyDeviceToDevice,
+                        c->stream));
+}
+
+static void vcycle(icarat_ctx *c, int l, const double *b, int deg)
+{
+  MgLevel &L = c->mg[l];
+  const int levels = (int)c->mg.size();
+  if(l == levels - 1)
+  {
+    const int n = c->coarse.n;
+    ICK(cudaMemsetAsync(L.x, 0, sizeof(double) * 3 * L.g.numnp, c->stream));
+    if(n > 0)
+    {
+      note_launch();
+      k_coarse_gather<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, c->coarse.map, b,
+                                                                 c->coarse.vin);
+      note_launch();
+      k_coarse_gemv<<<blocks_for(n * 32, 256), 256, 0, c->stream>>>(
+          n, c->coarse.A, c->coarse.vin, c->coarse.map, 3 * L.g.numnp, L.x);
+    }
+    return;
+  }
+  MgLevel &C = c->mg[l + 1];
+  smooth(c, L, b, deg, true);
+  // residual into L.r (smooth() used L.r as scratch; done with it now)
+  launch_residual(c, L.g, L.E, L.fix, b, L.x, L.r);
+  note_launch();
+  k_restrict<<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, L.r, C.fix,
+                                                                C.b);
+  vcycle(c, l + 1, C.b, deg);
+  note_launch();
+  k_prolong_add<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, C.x,
+                                                                   L.fix, L.x);
+  smooth(c, L, b, deg, false);
+}
+
+void mg_vcycle(icarat_ctx *c, const double *r, double *z, int deg)
+{
+  vcycle(c, 0, r, deg);
+  ICK(cudaMemcpyAsync(z, c->mg[0].x, sizeof(double) * c->neq,
+                      cudaMemcpyDeviceToDevice, c->stream));
+  ICK(cudaGetLastError());
+}
+
+} // namespace icarat_b200

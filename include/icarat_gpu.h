@@ -1,0 +1,263 @@
+/*
+ * icarat_gpu.h -- C ABI of the B200 (sm_100a) implementation of ICARAT's
+ * linear-static SIMP topology-optimisation inner loop.
+ *
+ * Plain C: opaque handles, plain pointers and sizes.  Host pointers are owned
+ * by the caller and copied in/out; *_dev variants take device pointers on the
+ * context's device and copy nothing.  Every function returns an int status
+ * (ICARAT_OK = 0, a positive warning, or a negative error).  One context owns
+ * all of its device memory and one CUDA stream; a context is not thread-safe,
+ * separate contexts may be used from separate threads.
+ *
+ * Numbering follows the reference exactly:
+ *   node id    = i + j (nx+1) + k (nx+1)(ny+1)        (src/io/mesh_icarat.hpp:468)
+ *   element id = i + j nx + k nx ny                   (src/io/mesh_icarat.hpp:486)
+ *   equation numbers ("numeq" vectors) = free components, node-major, as
+ *   countDOF assigns them (src/io/boundary_condition_base.hpp:35-95).
+ */
+#ifndef ICARAT_GPU_H
+#define ICARAT_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICARAT_OK 0
+#define ICARAT_WARN_MAXITER 1    /* iterative loop stopped at its cap */
+#define ICARAT_ERR_ARG -1        /* bad argument / size */
+#define ICARAT_ERR_CUDA -2       /* CUDA runtime error */
+#define ICARAT_ERR_NAN -4        /* non-finite value met in a reduction */
+#define ICARAT_ERR_STATE -5      /* call order violated (e.g. transposed filter first) */
+#define ICARAT_ERR_FILTER -6     /* filter weight sum < 1e-10 (filter.hpp:130-134) */
+#define ICARAT_ERR_UNSUPPORTED -7
+#define ICARAT_ERR_NOMEM -8
+
+typedef struct icarat_ctx icarat_ctx;
+typedef struct icarat_mma icarat_mma;
+
+/* [mesh] division / length of a hexa8 box (MeshIcarat::setParameter,
+   src/io/mesh_icarat.hpp:72-140). */
+typedef struct
+{
+  int nx, ny, nz;
+  double lx, ly, lz;
+} icarat_grid;
+
+/* [material] young = [E1, E2], poisson, penalty (Elastic::setParameter,
+   src/problem/elasticity.cpp:19-33); E(rho) = SIMP (elasticity.hpp:13-17). */
+typedef struct
+{
+  double young_min, young_max;
+  double poisson;
+  double penalty;
+} icarat_material;
+
+/* one [boundary_condition] dirichlet entry: flags, values, [[x0,x1],[y0,y1],
+   [z0,z1]] (BCIcarat::input_dirich, boundary_condition_icarat.hpp:73-138) */
+typedef struct
+{
+  int flag[3];
+  double val[3];
+  double box[3][2];
+} icarat_dirichlet;
+
+/* one [boundary_condition] neumann entry; only degenerate (point) boxes are
+   supported (boundary_condition_icarat.hpp:231-239, 380-396) */
+typedef struct
+{
+  double val[3];
+  double box[3][2];
+} icarat_load;
+
+typedef struct
+{
+  int n_dirichlet;
+  const icarat_dirichlet *dirichlet;
+  int n_loads;
+  const icarat_load *loads;
+} icarat_bc;
+
+enum
+{
+  ICARAT_SOLVER_JACOBI_PCG = 0, /* "Eigen_CG" / "Scaling_CG" semantics */
+  ICARAT_SOLVER_MG_PCG = 1      /* geometric multigrid preconditioned CG */
+};
+
+typedef struct
+{
+  int method;    /* ICARAT_SOLVER_* */
+  double rtol;   /* stop when ||r|| < rtol ||b||  (solvers.hpp:89: 1e-10) */
+  int maxit;     /* iteration cap (solvers.hpp:90: 10000) */
+  int mg_levels; /* multigrid levels incl. the finest (MG_PCG) */
+  int mg_smooth; /* smoothing sweeps per level and direction (MG_PCG) */
+  int chunk;     /* iterations per host convergence check (0 = default) */
+} icarat_solve_opts;
+
+typedef struct
+{
+  int iterations;
+  double rel_residual;
+  int status;
+} icarat_solve_info;
+
+/* OC::UpdateVariables parameters (OCSolver.hpp:73-79) and the volume functor
+   of the sample drivers: g(x) = sum_i thr(filter(x))_i v_i
+   (opt_macro_oc.cpp:153-164), thr only when use_threshold != 0. */
+typedef struct
+{
+  double move, iota, lambda_min, lambda_max, lambda_eps;
+  int maxiter;
+  int use_threshold;
+  double beta, T;
+} icarat_oc_opts;
+
+/* ---- library ---------------------------------------------------------- */
+int icarat_version(void);
+const char *icarat_status_string(int status);
+/* message of the last failed call on this thread */
+const char *icarat_last_error(void);
+
+/* ---- context: mesh + BC + device state ----------------------------------
+ * Replaces MeshIcarat::setParameter/generate, BCIcarat::input_dirich,
+ * makeDOF and input_neumann (mesh_icarat.hpp:72-155,
+ * boundary_condition_icarat.hpp:73-148, 213-264) and the LinearAnalysis
+ * constructor (src/analysis/linear.hpp:43-52). */
+int icarat_ctx_create(const icarat_grid *grid, const icarat_material *mat,
+                      const icarat_bc *bc, int device, icarat_ctx **out);
+int icarat_ctx_destroy(icarat_ctx *ctx);
+/* numnp, nelx, neq (= 3 numnp), numeq */
+int icarat_sizes(const icarat_ctx *ctx, int *numnp, int *nelx, int *neq,
+                 int *numeq);
+/* the context's cudaStream_t, as void* */
+int icarat_stream(const icarat_ctx *ctx, void **stream);
+int icarat_synchronize(icarat_ctx *ctx);
+/* node.dof[0..2] for every node (countDOF, boundary_condition_base.hpp:35-95) */
+int icarat_dof_map(const icarat_ctx *ctx, int *node_dof);
+/* Force::fext_org (numeq) */
+int icarat_fext(const icarat_ctx *ctx, double *fext);
+/* E = 1 element stiffness (24x24, row-major, element DOF 3a + c) and volume
+   (LinearElastic::makeKeFint, src/problem/elasticity.cpp:211-255) */
+int icarat_element_stiffness(const icarat_ctx *ctx, double *ke, double *volume);
+
+/* ---- analysis ------------------------------------------------------------ */
+/* element[i].setDesignS(design_s[i]) for every element (nelx values) */
+int icarat_set_design(icarat_ctx *ctx, const double *design_s);
+int icarat_set_design_dev(icarat_ctx *ctx, const double *design_s);
+/* y = K_ff u on free DOFs (numeq vectors): the assembled globalK of
+   LinearAnalysis::assemblingK (src/analysis/linear.hpp:117-166) times u,
+   applied matrix-free. */
+int icarat_apply_K(icarat_ctx *ctx, const double *u, double *y);
+int icarat_apply_K_dev(icarat_ctx *ctx, const double *u, double *y);
+/* LinearAnalysis::solve (src/analysis/linear.hpp:55-104): rhs = fext - fint
+   (fint from prescribed values), solve K u = rhs.  val (numeq) may be NULL;
+   the solution stays resident for the calls below. */
+int icarat_solve(icarat_ctx *ctx, const icarat_solve_opts *opts, double *val,
+                 icarat_solve_info *info);
+/* solve K u = f for a given right-hand side (numeq) */
+int icarat_solve_rhs(icarat_ctx *ctx, const icarat_solve_opts *opts,
+                     const double *f, double *u, icarat_solve_info *info);
+/* node.val after divideValIntoNode (analysis_utility.hpp:9-31): numnp x 3,
+   prescribed values on constrained DOFs, |v| < 1e-15 -> 0 */
+int icarat_node_values(icarat_ctx *ctx, double *node_val);
+/* object_f = value.val . fext (opt_macro_oc.cpp:110) of the last solve */
+int icarat_compliance(icarat_ctx *ctx, double *compliance);
+/* driver sensitivity() (opt_macro_oc.cpp:182-212): dfds = -(dE/E) u_e^T Ke
+   u_e, dgds = volume * dgds_scale; either output may be NULL */
+int icarat_sensitivity(icarat_ctx *ctx, double dgds_scale, double *dfds,
+                       double *dgds);
+int icarat_sensitivity_dev(icarat_ctx *ctx, double dgds_scale, double *dfds,
+                           double *dgds);
+
+/* ---- density filter (Filter<E,N>, src/optimization/filter.hpp) ---------- */
+/* the constructor + preNeighbour (:63-70, :254-297) for radius R */
+int icarat_filter_setup(icarat_ctx *ctx, double radius);
+/* densityFilter (:107-155): forward, or transposed (is_sens != 0), which
+   needs an earlier forward call like the reference */
+int icarat_density_filter(icarat_ctx *ctx, const double *in, double *out,
+                          int is_sens);
+int icarat_density_filter_dev(icarat_ctx *ctx, const double *in, double *out,
+                              int is_sens);
+/* sensitivityFilter (:77-104) with element volumes of the mesh */
+int icarat_sensitivity_filter(icarat_ctx *ctx, const double *design_s,
+                              const double *dfds, double *out);
+/* threshold / thresholdDerivative (:217-249) */
+int icarat_threshold(icarat_ctx *ctx, const double *in, double beta, double T,
+                     double *out);
+int icarat_threshold_derivative(icarat_ctx *ctx, const double *in, double beta,
+                                double T, double *out);
+
+/* ---- OC (src/optimization/opt-solver/OCSolver.hpp:21-68) ----------------
+ * x is updated in place; g is the reference volume (the driver's V0); the
+ * volume functor runs on the GPU with the filter of icarat_filter_setup. */
+int icarat_oc_update(icarat_ctx *ctx, double *x, const double *dfdx, double g,
+                     const double *dgdx, const double *xmin,
+                     const double *xmax, const icarat_oc_opts *opts,
+                     int *steps);
+int icarat_oc_update_dev(icarat_ctx *ctx, double *x, const double *dfdx,
+                         double g, const double *dgdx, const double *xmin,
+                         const double *xmax, const icarat_oc_opts *opts,
+                         int *steps);
+
+/* ---- MMA (src/optimization/opt-solver/MMASolver.hpp:62-116) -------------
+ * MMASolver(n, m, a, c, d) on a device; m <= 8 constraints. */
+int icarat_mma_create(int device, int n, int m, double a, double c, double d,
+                      icarat_mma **out);
+int icarat_mma_destroy(icarat_mma *mma);
+int icarat_mma_set_move_limit(icarat_mma *mma, double move);
+int icarat_mma_set_asymptotes(icarat_mma *mma, double init, double decrease,
+                              double increase);
+int icarat_mma_set_oscillation(icarat_mma *mma, double albefa);
+/* MMASolver::Update (MMASolver.cpp:66-82); dgdx is n x m row-major */
+int icarat_mma_update(icarat_mma *mma, double *x, const double *dfdx,
+                      const double *gx, const double *dgdx,
+                      const double *xmin, const double *xmax);
+int icarat_mma_update_dev(icarat_mma *mma, double *x, const double *dfdx,
+                          const double *gx, const double *dgdx,
+                          const double *xmin, const double *xmax);
+/* outer interior-point loops of the last update ("MMA loop:", :151) */
+int icarat_mma_last_loops(const icarat_mma *mma, int *outer, int *newton);
+
+/* ---- one design iteration, device resident --------------------------------
+ * The loop body of the sample drivers (opt_macro_oc.cpp:83-172,
+ * opt_macro_mma_nondesign.cpp:90-178): filter -> (threshold) -> solve ->
+ * compliance/volume -> sensitivity -> filter^T -> OC or MMA update. */
+typedef struct
+{
+  int method;        /* 0 = OC, 1 = MMA */
+  int use_threshold; /* beta = min(2^(step/40), 16), T below */
+  double T;
+  double move;
+  double xmin, xmax;
+  double filter_radius;
+  icarat_solve_opts solve;
+} icarat_loop_opts;
+
+typedef struct
+{
+  int step;
+  double compliance;
+  double constraint;
+  int cg_iterations;
+  double cg_rel_residual;
+  int update_steps; /* OC bisection steps or MMA Newton steps */
+  int status;
+} icarat_step_info;
+
+/* ---- diagnostics (no reference counterpart) ------------------------------ */
+/* number of kernels this library has launched in this process */
+int icarat_kernel_launches(unsigned long long *count);
+/* average device time of the FP64 stiffness stencil y = K u on the current
+   design, over `reps` back-to-back launches timed with CUDA events on the
+   context's stream */
+int icarat_time_operator(icarat_ctx *ctx, int reps, double *ms_per_launch);
+
+int icarat_loop_init(icarat_ctx *ctx, const icarat_loop_opts *opts,
+                     const double *x0);
+int icarat_loop_step(icarat_ctx *ctx, icarat_step_info *info);
+/* which: 0 x, 1 filtered, 2 thresholded, 3 dfds, 4 dgds (nelx each) */
+int icarat_loop_get(icarat_ctx *ctx, int which, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ICARAT_GPU_H */

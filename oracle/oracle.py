@@ -1,0 +1,467 @@
+"""ctypes wrapper of the CPU restatement in icarat_oracle.c.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker.  The product (icarat2_b200) never
+imports this module.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_REFLIB = os.path.join(_HERE, "_ref", "libicarat_ref.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+VOLUME_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
+REF_VOLUME_FN = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_int, C.c_void_p)
+
+
+def build(ref=False):
+    """Compile liboracle.so (and, with ref=True, the reference MMA/OC)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+    if ref:
+        subprocess.check_call(["make", "-s", "-C", _HERE, "ref"])
+
+
+class _OCParams(C.Structure):
+    _fields_ = [("move", C.c_double), ("iota", C.c_double), ("lmin", C.c_double),
+                ("lmax", C.c_double), ("leps", C.c_double), ("maxiter", C.c_int)]
+
+
+def _load():
+    if not os.path.exists(_LIB):
+        build()
+    L = C.CDLL(_LIB)
+    sig = {
+        "or_num_threads": (C.c_int, []),
+        "or_set_threads": (None, [C.c_int]),
+        "or_mesh_box": (None, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                               C.c_double, _dp, _ip]),
+        "or_hexa8_ke": (None, [_dp, C.c_double, C.c_double, _dp, C.POINTER(C.c_double)]),
+        "or_elastic_D": (None, [C.c_double, C.c_double, _dp]),
+        "or_problem_create": (_vp, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_int, _ip, _dp, _dp, C.c_int, _dp,
+                                    _dp, C.POINTER(C.c_int)]),
+        "or_problem_destroy": (None, [_vp]),
+        "or_problem_sizes": (None, [_vp, _ip]),
+        "or_problem_nnz": (C.c_long, [_vp]),
+        "or_problem_dof": (None, [_vp, _ip]),
+        "or_problem_fext": (None, [_vp, _dp]),
+        "or_problem_ke0": (None, [_vp, _dp, C.POINTER(C.c_double)]),
+        "or_problem_xyz": (None, [_vp, _dp]),
+        "or_problem_conn": (None, [_vp, _ip]),
+        "or_problem_csr": (None, [_vp, _lp, _ip, _dp]),
+        "or_assemble": (None, [_vp, _dp]),
+        "or_apply_K": (None, [_vp, _dp, _dp]),
+        "or_pcg": (C.c_int, [_vp, _dp, _dp, C.c_double, C.c_int, C.POINTER(C.c_int),
+                             C.POINTER(C.c_double)]),
+        "or_linear_solve": (C.c_int, [_vp, _dp, C.c_double, C.c_int, _dp,
+                                      C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+        "or_node_values": (None, [_vp, _dp, _dp]),
+        "or_compliance": (C.c_double, [_vp, _dp]),
+        "or_sensitivity": (None, [_vp, _dp, _dp, C.c_double, _dp, _dp]),
+        "or_filter_create": (_vp, [_vp, C.c_double, C.c_int]),
+        "or_filter_create_centroids": (_vp, [C.c_int, _dp, C.c_double]),
+        "or_filter_destroy": (None, [_vp]),
+        "or_filter_nnz": (C.c_long, [_vp]),
+        "or_filter_lists": (None, [_vp, _lp, _ip, _dp]),
+        "or_filter_density": (C.c_int, [_vp, _dp, _dp, C.c_int]),
+        "or_filter_sensitivity": (None, [_vp, _dp, _dp, _dp, _dp]),
+        "or_threshold": (None, [C.c_int, _dp, C.c_double, C.c_double, _dp]),
+        "or_threshold_deriv": (None, [C.c_int, _dp, C.c_double, C.c_double, _dp]),
+        "or_oc_update": (C.c_int, [C.c_int, _dp, _dp, C.c_double, _dp, _dp, _dp,
+                                   C.POINTER(_OCParams), VOLUME_FN, C.c_void_p,
+                                   C.POINTER(C.c_int)]),
+        "or_mma_create": (_vp, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]),
+        "or_mma_destroy": (None, [_vp]),
+        "or_mma_set_move": (None, [_vp, C.c_double]),
+        "or_mma_set_asymptotes": (None, [_vp, C.c_double, C.c_double, C.c_double]),
+        "or_mma_set_oscillation": (None, [_vp, C.c_double]),
+        "or_mma_update": (None, [_vp, _dp, _dp, _dp, _dp, _dp, _dp]),
+        "or_mma_outloops": (C.c_int, [_vp]),
+        "or_mma_inner_total": (C.c_int, [_vp]),
+        "or_mma_state": (None, [_vp, _dp, _dp, _dp, _dp]),
+        "or_loop_create": (_vp, [_vp, _vp, C.c_int, C.c_int, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_int, _dp]),
+        "or_loop_destroy": (None, [_vp]),
+        "or_loop_step": (C.c_int, [_vp]),
+        "or_loop_get": (None, [_vp, C.c_int, _dp]),
+        "or_loop_scalars": (None, [_vp, _dp, _ip]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+lib = _load()
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def hexa8_ke(X, E=1.0, nu=0.3):
+    """24x24 element stiffness and volume of a hexa8 with nodes X (8x3)."""
+    ke = np.zeros(576)
+    vol = C.c_double()
+    lib.or_hexa8_ke(_f64(X).ravel(), E, nu, ke, C.byref(vol))
+    return ke.reshape(24, 24), vol.value
+
+
+def box_bc(dirichlet=(), loads=()):
+    """Pack Dirichlet boxes [(flag3, val3, box3x2)] and point loads [(val3, box3x2)]."""
+    nd = len(dirichlet)
+    df = np.zeros(max(nd, 1) * 3, np.int32)
+    dv = np.zeros(max(nd, 1) * 3)
+    db = np.zeros(max(nd, 1) * 6)
+    for i, (fl, vl, bx) in enumerate(dirichlet):
+        df[3 * i:3 * i + 3] = fl
+        dv[3 * i:3 * i + 3] = vl
+        db[6 * i:6 * i + 6] = np.asarray(bx, float).ravel()
+    nl = len(loads)
+    lv = np.zeros(max(nl, 1) * 3)
+    lb = np.zeros(max(nl, 1) * 6)
+    for i, (vl, bx) in enumerate(loads):
+        lv[3 * i:3 * i + 3] = vl
+        lb[6 * i:6 * i + 6] = np.asarray(bx, float).ravel()
+    return nd, df, dv, db, nl, lv, lb
+
+
+def cantilever_bc(nx, ny, nz, lx=None, ly=None, lz=None, load_node=None):
+    """x = 0 face clamped; unit load (0,0,-1) at node (nx, ny/2, 0) by default."""
+    lx = float(nx if lx is None else lx)
+    ly = float(ny if ly is None else ly)
+    lz = float(nz if lz is None else lz)
+    if load_node is None:
+        load_node = (nx, ny // 2, 0)
+    p = (load_node[0] * lx / nx, load_node[1] * ly / ny, load_node[2] * lz / nz)
+    dirichlet = [((1, 1, 1), (0.0, 0.0, 0.0), ((0.0, 0.0), (0.0, ly), (0.0, lz)))]
+    loads = [((0.0, 0.0, -1.0), ((p[0], p[0]), (p[1], p[1]), (p[2], p[2])))]
+    return dirichlet, loads
+
+
+class Problem:
+    """Mesh + boundary conditions + CSR K_ff of the CPU restatement."""
+
+    def __init__(self, nx, ny, nz, lx=None, ly=None, lz=None, E1=1e-9, E2=1.0,
+                 nu=0.3, penal=3.0, dirichlet=None, loads=None):
+        lx = float(nx if lx is None else lx)
+        ly = float(ny if ly is None else ly)
+        lz = float(nz if lz is None else lz)
+        if dirichlet is None and loads is None:
+            dirichlet, loads = cantilever_bc(nx, ny, nz, lx, ly, lz)
+        nd, df, dv, db, nl, lv, lb = box_bc(dirichlet or (), loads or ())
+        st = C.c_int()
+        self.h = lib.or_problem_create(nx, ny, nz, lx, ly, lz, E1, E2, nu, penal,
+                                       nd, df, dv, db, nl, lv, lb, C.byref(st))
+        if not self.h:
+            raise ValueError("or_problem_create failed: %d" % st.value)
+        s = np.zeros(4, np.int32)
+        lib.or_problem_sizes(self.h, s)
+        self.numnp, self.nelx, self.neq, self.numeq = (int(v) for v in s)
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.penal, self.E1, self.E2, self.nu = penal, E1, E2, nu
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_problem_destroy(self.h)
+            self.h = None
+
+    def dof(self):
+        d = np.zeros(3 * self.numnp, np.int32)
+        lib.or_problem_dof(self.h, d)
+        return d.reshape(-1, 3)
+
+    def fext(self):
+        f = np.zeros(max(self.numeq, 1))
+        lib.or_problem_fext(self.h, f)
+        return f[:self.numeq]
+
+    def ke0(self):
+        k = np.zeros(576)
+        v = C.c_double()
+        lib.or_problem_ke0(self.h, k, C.byref(v))
+        return k.reshape(24, 24), v.value
+
+    def xyz(self):
+        x = np.zeros(3 * self.numnp)
+        lib.or_problem_xyz(self.h, x)
+        return x.reshape(-1, 3)
+
+    def conn(self):
+        c = np.zeros(8 * self.nelx, np.int32)
+        lib.or_problem_conn(self.h, c)
+        return c.reshape(-1, 8)
+
+    def assemble(self, design_s):
+        lib.or_assemble(self.h, _f64(design_s))
+
+    def csr(self):
+        nnz = lib.or_problem_nnz(self.h)
+        rp = np.zeros(self.numeq + 1, np.int64)
+        col = np.zeros(max(nnz, 1), np.int32)
+        val = np.zeros(max(nnz, 1))
+        lib.or_problem_csr(self.h, rp, col, val)
+        return rp, col[:nnz], val[:nnz]
+
+    def apply_K(self, u):
+        y = np.zeros(self.numeq)
+        lib.or_apply_K(self.h, _f64(u), y)
+        return y
+
+    def pcg(self, rhs, tol=1e-10, maxit=10000):
+        sol = np.zeros(self.numeq)
+        it = C.c_int()
+        rr = C.c_double()
+        lib.or_pcg(self.h, _f64(rhs), sol, tol, maxit, C.byref(it), C.byref(rr))
+        return sol, it.value, rr.value
+
+    def solve(self, design_s, tol=1e-10, maxit=10000):
+        """LinearAnalysis::solve: returns (value.val, iterations, rel. residual)."""
+        val = np.zeros(max(self.numeq, 1))
+        it = C.c_int()
+        rr = C.c_double()
+        lib.or_linear_solve(self.h, _f64(design_s), tol, maxit, val, C.byref(it),
+                            C.byref(rr))
+        return val[:self.numeq], it.value, rr.value
+
+    def node_values(self, val):
+        nv = np.zeros(3 * self.numnp)
+        lib.or_node_values(self.h, _f64(val), nv)
+        return nv.reshape(-1, 3)
+
+    def compliance(self, val):
+        return lib.or_compliance(self.h, _f64(val))
+
+    def sensitivity(self, design_s, node_val, dgds_scale=1.0):
+        dfds = np.zeros(self.nelx)
+        dgds = np.zeros(self.nelx)
+        lib.or_sensitivity(self.h, _f64(design_s), _f64(node_val).ravel(), dgds_scale,
+                           dfds, dgds)
+        return dfds, dgds
+
+
+class Filter:
+    """Filter<E,N> restatement (radius density filter)."""
+
+    def __init__(self, problem=None, radius=1.5, faithful=False, centroids=None):
+        if centroids is not None:
+            cen = _f64(centroids).reshape(-1, 3)
+            self.n = cen.shape[0]
+            self.h = lib.or_filter_create_centroids(self.n, cen.ravel(), radius)
+        else:
+            self.n = problem.nelx
+            self.h = lib.or_filter_create(problem.h, radius, 1 if faithful else 0)
+        self.radius = radius
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_filter_destroy(self.h)
+            self.h = None
+
+    def lists(self):
+        nnz = lib.or_filter_nnz(self.h)
+        ptr = np.zeros(self.n + 1, np.int64)
+        ids = np.zeros(max(nnz, 1), np.int32)
+        dis = np.zeros(max(nnz, 1))
+        lib.or_filter_lists(self.h, ptr, ids, dis)
+        return ptr, ids[:nnz], dis[:nnz]
+
+    def density_filter(self, x, is_sens=False):
+        out = np.zeros(self.n)
+        st = lib.or_filter_density(self.h, _f64(x), out, 1 if is_sens else 0)
+        if st != 0:
+            raise RuntimeError("or_filter_density: status %d" % st)
+        return out
+
+    def sensitivity_filter(self, design_s, dfds, volume):
+        out = np.zeros(self.n)
+        lib.or_filter_sensitivity(self.h, _f64(design_s), _f64(dfds), _f64(volume), out)
+        return out
+
+
+def threshold(x, beta, T):
+    x = _f64(x)
+    out = np.zeros_like(x)
+    lib.or_threshold(x.size, x, beta, T, out)
+    return out
+
+
+def threshold_derivative(x, beta, T):
+    x = _f64(x)
+    out = np.zeros_like(x)
+    lib.or_threshold_deriv(x.size, x, beta, T, out)
+    return out
+
+
+def oc_update(x, dfdx, g, dgdx, xmin, xmax, volume_fn, move=0.15, iota=0.5,
+              lmin=0.0, lmax=1.0e4, leps=1.0e-5, maxiter=100):
+    """OC::UpdateVariables with a Python volume functor g(x)."""
+    x = _f64(x).copy()
+    n = x.size
+
+    def cb(ptr, user):
+        return float(volume_fn(np.ctypeslib.as_array(ptr, shape=(n,)).copy()))
+
+    fn = VOLUME_FN(cb)
+    prm = _OCParams(move, iota, lmin, lmax, leps, maxiter)
+    steps = C.c_int()
+    lib.or_oc_update(n, x, _f64(dfdx), g, _f64(dgdx), _f64(xmin), _f64(xmax),
+                     C.byref(prm), fn, None, C.byref(steps))
+    return x, steps.value
+
+
+class MMA:
+    """MMASolver restatement (Svanberg MMA, dual interior point)."""
+
+    def __init__(self, n, m, a=0.0, c=100000.0, d=0.0):
+        self.n, self.m = n, m
+        self.h = lib.or_mma_create(n, m, a, c, d)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_mma_destroy(self.h)
+            self.h = None
+
+    def set_move_limit(self, m):
+        lib.or_mma_set_move(self.h, m)
+
+    def set_asymptotes(self, init, dec, inc):
+        lib.or_mma_set_asymptotes(self.h, init, dec, inc)
+
+    def set_oscillation(self, a):
+        lib.or_mma_set_oscillation(self.h, a)
+
+    def update(self, x, dfdx, gx, dgdx, xmin, xmax):
+        x = _f64(x).copy()
+        lib.or_mma_update(self.h, x, _f64(dfdx), _f64(np.atleast_1d(gx)),
+                          _f64(dgdx).ravel(), _f64(xmin), _f64(xmax))
+        return x
+
+    def outloops(self):
+        return lib.or_mma_outloops(self.h)
+
+    def state(self):
+        a = [np.zeros(self.n) for _ in range(4)]
+        lib.or_mma_state(self.h, *a)
+        return dict(low=a[0], upp=a[1], xold1=a[2], xold2=a[3])
+
+
+class Loop:
+    """One design iteration per step() of the sample drivers (OC / MMA)."""
+
+    def __init__(self, problem, filt, method="mma", x0=0.3, move=None,
+                 use_threshold=False, xmin=1e-4, xmax=1.0, cg_tol=1e-10,
+                 cg_maxit=10000):
+        self.P, self.F = problem, filt
+        if move is None:
+            move = 0.15
+        x0 = np.full(problem.nelx, x0) if np.isscalar(x0) else _f64(x0)
+        self.h = lib.or_loop_create(problem.h, filt.h, 1 if method == "mma" else 0,
+                                    1 if use_threshold else 0, move, xmin, xmax,
+                                    cg_tol, cg_maxit, _f64(x0))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.or_loop_destroy(self.h)
+            self.h = None
+
+    def step(self):
+        st = lib.or_loop_step(self.h)
+        if st != 0:
+            raise RuntimeError("or_loop_step: status %d" % st)
+
+    def get(self, which):
+        idx = {"x": 0, "xfil": 1, "xthr": 2, "dfds": 3, "dgds": 4, "val": 5,
+               "node_val": 6}[which]
+        n = {5: self.P.numeq, 6: 3 * self.P.numnp}.get(idx, self.P.nelx)
+        out = np.zeros(max(n, 1))
+        lib.or_loop_get(self.h, idx, out)
+        return out[:n]
+
+    def scalars(self):
+        d = np.zeros(9)
+        iv = np.zeros(4, np.int32)
+        lib.or_loop_scalars(self.h, d, iv)
+        keys = ["compliance", "constraint", "V0", "cg_relres", "t_filter", "t_solve",
+                "t_sens", "t_update", "t_pcg"]
+        out = {k: float(v) for k, v in zip(keys, d)}
+        out.update(optstep=int(iv[0]), cg_iters=int(iv[1]), oc_steps=int(iv[2]),
+                   mma_outloops=int(iv[3]))
+        return out
+
+
+def ref_available():
+    return os.path.exists(_REFLIB)
+
+
+class RefMMA:
+    """The reference's own MMASolver (oracle/_ref, compiled from its sources)."""
+
+    _lib = None
+
+    @classmethod
+    def _get(cls):
+        if cls._lib is None:
+            L = C.CDLL(_REFLIB)
+            L.ref_mma_create.restype = _vp
+            L.ref_mma_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double,
+                                         C.c_double]
+            L.ref_mma_destroy.argtypes = [_vp]
+            L.ref_mma_set_move.argtypes = [_vp, C.c_double]
+            L.ref_mma_set_asymptotes.argtypes = [_vp, C.c_double, C.c_double, C.c_double]
+            L.ref_mma_set_oscillation.argtypes = [_vp, C.c_double]
+            L.ref_mma_update.argtypes = [_vp, _dp, _dp, _dp, _dp, _dp, _dp]
+            L.ref_oc_update.argtypes = [C.c_int, _dp, _dp, C.c_double, _dp, _dp, _dp,
+                                        C.c_double, REF_VOLUME_FN, C.c_void_p]
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, n, m, a=0.0, c=100000.0, d=0.0):
+        self.L = self._get()
+        self.h = self.L.ref_mma_create(n, m, a, c, d)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ref_mma_destroy(self.h)
+            self.h = None
+
+    def set_move_limit(self, m):
+        self.L.ref_mma_set_move(self.h, m)
+
+    def set_asymptotes(self, init, dec, inc):
+        self.L.ref_mma_set_asymptotes(self.h, init, dec, inc)
+
+    def set_oscillation(self, a):
+        self.L.ref_mma_set_oscillation(self.h, a)
+
+    def update(self, x, dfdx, gx, dgdx, xmin, xmax):
+        x = _f64(x).copy()
+        self.L.ref_mma_update(self.h, x, _f64(dfdx), _f64(np.atleast_1d(gx)),
+                              _f64(dgdx).ravel(), _f64(xmin), _f64(xmax))
+        return x
+
+
+def ref_oc_update(x, dfdx, g, dgdx, xmin, xmax, volume_fn, move=0.15):
+    """The reference's own OC::UpdateVariables (oracle/_ref)."""
+    L = RefMMA._get()
+    x = _f64(x).copy()
+    n = x.size
+
+    def cb(ptr, nn, user):
+        return float(volume_fn(np.ctypeslib.as_array(ptr, shape=(nn,)).copy()))
+
+    fn = REF_VOLUME_FN(cb)
+    L.ref_oc_update(n, x, _f64(dfdx).copy(), g, _f64(dgdx).copy(), _f64(xmin),
+                    _f64(xmax), move, fn, None)
+    return x
