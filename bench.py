@@ -67,7 +67,9 @@ def grid_of(a):
 
 def config(a, extra=None):
     nx, ny, nz = grid_of(a)
-    c = {"workload": WORKLOAD if a.grid == "128x64x64" else WORKLOAD.replace("128x64x64", a.grid),
+    c = {"workload": "SIMP cantilever %s hexa8, MMA move 0.2, R=%g, FP64, %s rtol %g" % (
+             a.grid, a.radius, "MG-PCG (%d levels)" % a.levels if a.impl == "ours"
+             else "Jacobi-PCG", a.rtol),
          "grid": [nx, ny, nz], "elements": nx * ny * nz,
          "free_dofs": 3 * (nx + 1) * (ny + 1) * (nz + 1) - 3 * (ny + 1) * (nz + 1),
          "update": "MMA", "move": 0.2, "filter_radius": a.radius, "volfrac": 0.3,
@@ -146,9 +148,16 @@ class ClockSampler:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, bus_id):
-        self.bus = (bus_id or "").lower()
+        self.bus = bus_id  # PCI bus number of this process's GPU (int) or None
         self.rows = []
         self.proc = None
+
+    def _mine(self, field):
+        # nvidia-smi pci.bus_id looks like 00000000:1B:00.0
+        try:
+            return self.bus is not None and int(field.split(":")[1], 16) == int(self.bus)
+        except (IndexError, ValueError):
+            return False
 
     def start(self):
         try:
@@ -175,7 +184,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         rows = [r for r in self.rows if len(r) >= 9]
-        mine = [r for r in rows if self.bus and r[0].lower().endswith(self.bus[-12:])]
+        mine = [r for r in rows if self._mine(r[0])]
         rows = mine or rows
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]

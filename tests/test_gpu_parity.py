@@ -144,8 +144,10 @@ def test_mg_pcg_matches_oracle(oracle, gpu, levels):
 
 
 def test_mg_pcg_high_contrast_large(gpu):
-    """128x64x64 SIMP design with 1e-9 void: MG-PCG reaches 1e-8 and the
-    true residual agrees."""
+    """128x64x64 random solid/void design (E contrast 5e8): MG-PCG reaches the
+    recursive rtol 1e-8 (the stop rule of CG.cpp:105-108), and the true
+    residual f - K u, evaluated in FP64 with displacements up to 1e6 times
+    the solid ones, is within the attainable accuracy (1e-6 relative)."""
     G = gpu.Context(128, 64, 64)
     rng = np.random.default_rng(9)
     rho = np.where(rng.uniform(size=G.nelx) < 0.4, 1.0, 1e-3)
@@ -154,7 +156,16 @@ def test_mg_pcg_high_contrast_large(gpu):
     assert info.status == gpu.OK and info.rel_residual < 1e-8
     f = G.fext()
     r = f - G.apply_K(val)
-    assert np.linalg.norm(r) <= 2e-8 * np.linalg.norm(f)
+    assert np.linalg.norm(r) <= 1e-6 * np.linalg.norm(f)
+
+
+def test_mg_pcg_true_residual_moderate_contrast(gpu):
+    G = gpu.Context(64, 32, 32)
+    rng = np.random.default_rng(10)
+    G.set_design(rng.uniform(0.2, 1.0, G.nelx))
+    val, info = G.solve(gpu.solve_opts(gpu.MG_PCG, rtol=1e-10, mg_levels=4))
+    f = G.fext()
+    assert np.linalg.norm(f - G.apply_K(val)) <= 2e-10 * np.linalg.norm(f)
 
 
 def test_solve_maxit_warning(gpu):
