@@ -66,7 +66,31 @@ def build(verbose=False, jobs=None):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    build_examples()
     return OUT
+
+
+EXAMPLES = os.path.join(HERE, "examples")
+
+
+def build_examples():
+    """C++ sample drivers written against include/icarat_b200.hpp."""
+    include = os.path.join(HERE, "..", "include")
+    for src in sorted(os.listdir(EXAMPLES)):
+        if not src.endswith(".cpp"):
+            continue
+        exe = os.path.join(EXAMPLES, src[:-4])
+        deps = [os.path.join(EXAMPLES, src), OUT, os.path.join(include, "icarat_b200.hpp"),
+                os.path.join(include, "icarat_gpu.h")]
+        if os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(d)
+                                       for d in deps):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", "-I", include, "-o", exe,
+               os.path.join(EXAMPLES, src), "-L", HERE, "-licarat_gpu",
+               "-Wl,-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("example build failed:\n%s\n%s" % (r.stdout, r.stderr))
 
 
 if __name__ == "__main__":

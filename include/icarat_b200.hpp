@@ -1,0 +1,244 @@
+// icarat_b200.hpp -- header-only C++ layer over icarat_gpu.h that keeps the
+// reference's class names, method names and argument meanings for the
+// linear-static SIMP path, so a sample-style main() switches by changing its
+// includes and constructor arguments:
+//
+//   reference (src/...)                          this header
+//   MeshIcarat + BCIcarat (io/*.hpp)        ->   icarat::b200::Model
+//   LinearAnalysis<E,N>::solve(name, log)   ->   icarat::b200::LinearAnalysis::solve
+//   Filter<E,N>::densityFilter(x, isSens)   ->   icarat::b200::Filter::densityFilter
+//   Filter::threshold / thresholdDerivative ->   same names
+//   OC::UpdateVariables(x, df, g, dg, ...)  ->   icarat::b200::OC::UpdateVariables
+//   MMASolver::Update(x, df, g, dg, ...)    ->   icarat::b200::MMASolver::Update
+//
+// Errors: the reference prints and calls exit(1) (solvers.cpp:59,
+// filter.hpp:130-134); here every failing call throws icarat::b200::Error with
+// the library status and message.
+#pragma once
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "icarat_gpu.h"
+
+namespace icarat
+{
+namespace b200
+{
+
+struct Error : std::runtime_error
+{
+  int status;
+  Error(int s, const std::string &what)
+      : std::runtime_error(what + ": " + icarat_last_error()), status(s)
+  {
+  }
+};
+
+inline int check(int status, const char *what)
+{
+  if(status < 0)
+    throw Error(status, what);
+  return status;
+}
+
+struct Box
+{
+  double lo[3], hi[3];
+};
+
+// [mesh] + [material] + [boundary_condition] of a voxel box
+class Model
+{
+public:
+  Model(int nx, int ny, int nz, double lx, double ly, double lz, double young_min,
+        double young_max, double poisson, double penalty,
+        const std::vector<icarat_dirichlet> &dirichlet,
+        const std::vector<icarat_load> &loads, int device = 0)
+  {
+    icarat_grid g{nx, ny, nz, lx, ly, lz};
+    icarat_material m{young_min, young_max, poisson, penalty};
+    icarat_bc bc{(int)dirichlet.size(), dirichlet.data(), (int)loads.size(),
+                 loads.data()};
+    check(icarat_ctx_create(&g, &m, &bc, device, &ctx_), "icarat_ctx_create");
+    check(icarat_sizes(ctx_, &numnp, &nelx, &neq, &numeq), "icarat_sizes");
+  }
+  ~Model() { icarat_ctx_destroy(ctx_); }
+  Model(const Model &) = delete;
+  Model &operator=(const Model &) = delete;
+
+  icarat_ctx *ctx() const { return ctx_; }
+  // element[i].setDesignS(design_s[i]) for all elements
+  void setDesignS(const std::vector<double> &design_s)
+  {
+    check(icarat_set_design(ctx_, design_s.data()), "setDesignS");
+  }
+  std::vector<double> fext() const
+  {
+    std::vector<double> f(numeq);
+    check(icarat_fext(ctx_, f.data()), "fext");
+    return f;
+  }
+
+  int numnp = 0, nelx = 0, neq = 0, numeq = 0;
+
+private:
+  icarat_ctx *ctx_ = nullptr;
+};
+
+// LinearAnalysis<LinearElastic, Node> (src/analysis/linear.hpp:15-41)
+class LinearAnalysis
+{
+public:
+  explicit LinearAnalysis(Model &m) : m_(m), val(m.numeq) {}
+  // solvName: "Eigen_CG" / "Scaling_CG" (Jacobi-PCG) or "MG_CG" (multigrid)
+  void solve(const std::string &solvName, bool log)
+  {
+    icarat_solve_opts o{ICARAT_SOLVER_JACOBI_PCG, tol, maxIter, mg_levels, mg_smooth, 0};
+    if(solvName == "MG_CG")
+      o.method = ICARAT_SOLVER_MG_PCG;
+    else if(solvName != "Eigen_CG" && solvName != "Scaling_CG")
+      throw Error(ICARAT_ERR_UNSUPPORTED, "Solver type name is wrong: " + solvName);
+    check(icarat_solve(m_.ctx(), &o, val.data(), &info), "LinearAnalysis::solve");
+    if(log)
+      printf("iteration: %d\nresidual: %g\n", info.iterations, info.rel_residual);
+  }
+  // object_f = value.val . fext
+  double compliance() const
+  {
+    double c = 0.0;
+    check(icarat_compliance(m_.ctx(), &c), "compliance");
+    return c;
+  }
+  // node.val of every node after divideValIntoNode (numnp x 3)
+  std::vector<double> nodeValues() const
+  {
+    std::vector<double> v(3 * (size_t)m_.numnp);
+    check(icarat_node_values(m_.ctx(), v.data()), "nodeValues");
+    return v;
+  }
+  // the sample drivers' sensitivity(): dfds, dgds (= volume * dgds_scale)
+  void sensitivity(std::vector<double> &dfds, std::vector<double> &dgds,
+                   double dgds_scale = 1.0) const
+  {
+    dfds.resize(m_.nelx);
+    dgds.resize(m_.nelx);
+    check(icarat_sensitivity(m_.ctx(), dgds_scale, dfds.data(), dgds.data()),
+          "sensitivity");
+  }
+
+  double tol = 1.0e-10; // solvers.hpp:89
+  int maxIter = 10000;  // solvers.hpp:90
+  int mg_levels = 4, mg_smooth = 2;
+  std::vector<double> val; // Value::val
+  icarat_solve_info info{};
+
+private:
+  Model &m_;
+};
+
+// Filter<E,N> (src/optimization/filter.hpp:17-61)
+class Filter
+{
+public:
+  Filter(Model &m, double radius) : m_(m)
+  {
+    check(icarat_filter_setup(m.ctx(), radius), "Filter");
+  }
+  std::vector<double> densityFilter(const std::vector<double> &design_s, bool isSens)
+  {
+    std::vector<double> out(m_.nelx);
+    check(icarat_density_filter(m_.ctx(), design_s.data(), out.data(), isSens ? 1 : 0),
+          "densityFilter");
+    return out;
+  }
+  std::vector<double> sensitivityFilter(const std::vector<double> &design_s,
+                                        const std::vector<double> &dfds)
+  {
+    std::vector<double> out(m_.nelx);
+    check(icarat_sensitivity_filter(m_.ctx(), design_s.data(), dfds.data(), out.data()),
+          "sensitivityFilter");
+    return out;
+  }
+  std::vector<double> threshold(const std::vector<double> &d, double beta, double T)
+  {
+    std::vector<double> out(m_.nelx);
+    check(icarat_threshold(m_.ctx(), d.data(), beta, T, out.data()), "threshold");
+    return out;
+  }
+  std::vector<double> thresholdDerivative(const std::vector<double> &d, double beta,
+                                          double T)
+  {
+    std::vector<double> out(m_.nelx);
+    check(icarat_threshold_derivative(m_.ctx(), d.data(), beta, T, out.data()),
+          "thresholdDerivative");
+    return out;
+  }
+
+private:
+  Model &m_;
+};
+
+// OC (src/optimization/opt-solver/OCSolver.hpp:13-80).  The reference takes
+// the volume functor as a lambda; here it is the sample drivers' functor,
+// g(x) = sum thr(filter(x)) v, evaluated on the GPU with the Model's Filter
+// (threshold on when useThreshold is set).
+class OC
+{
+public:
+  OC(Model &m, int n) : m_(m), n_(n) {}
+  void setMoveLimit(double mv) { movelimit = mv; }
+  void UpdateVariables(std::vector<double> &xk, std::vector<double> &dfdx, double g,
+                       std::vector<double> &dgdx, std::vector<double> &xmin,
+                       std::vector<double> &xmax, bool useThreshold = false,
+                       double beta = 1.0, double T = 0.5)
+  {
+    icarat_oc_opts o{movelimit, 0.5, 0.0, 1.0e4, 1.0e-5, 100, useThreshold ? 1 : 0,
+                     beta, T};
+    int steps = 0;
+    check(icarat_oc_update(m_.ctx(), xk.data(), dfdx.data(), g, dgdx.data(), xmin.data(),
+                           xmax.data(), &o, &steps),
+          "OC::UpdateVariables");
+    (void)n_;
+  }
+
+private:
+  Model &m_;
+  int n_;
+  double movelimit = 0.15;
+};
+
+// MMASolver (src/optimization/opt-solver/MMASolver.hpp:62-116)
+class MMASolver
+{
+public:
+  MMASolver(int n, int m, double a = 0.0, double c = 100000.0, double d = 0.0,
+            int device = 0)
+  {
+    check(icarat_mma_create(device, n, m, a, c, d, &h_), "MMASolver");
+  }
+  ~MMASolver() { icarat_mma_destroy(h_); }
+  MMASolver(const MMASolver &) = delete;
+  MMASolver &operator=(const MMASolver &) = delete;
+  void SetAsymptotes(double init, double decrease, double increase)
+  {
+    check(icarat_mma_set_asymptotes(h_, init, decrease, increase), "SetAsymptotes");
+  }
+  void SetMoveLimit(double m) { check(icarat_mma_set_move_limit(h_, m), "SetMoveLimit"); }
+  void SetOscillation(double a)
+  {
+    check(icarat_mma_set_oscillation(h_, a), "SetOscillation");
+  }
+  void Update(double *xval, const double *dfdx, const double *gx, const double *dgdx,
+              const double *xmin, const double *xmax)
+  {
+    check(icarat_mma_update(h_, xval, dfdx, gx, dgdx, xmin, xmax), "MMASolver::Update");
+  }
+
+private:
+  icarat_mma *h_ = nullptr;
+};
+
+} // namespace b200
+} // namespace icarat
