@@ -143,6 +143,7 @@ SIGNATURES = {
     "icarat_mma_update": (_i, [_vp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "icarat_mma_update_dev": (_i, [_vp, _vp, _vp, _dp, _vp, _vp, _vp]),
     "icarat_mma_last_loops": (_i, [_vp, _P(_i), _P(_i)]),
+    "icarat_solve_noalloc": (_i, [_vp, _P(SolveOpts), _vp, _vp, _P(SolveInfo)]),
     "icarat_kernel_launches": (_i, [_P(C.c_ulonglong)]),
     "icarat_time_operator": (_i, [_vp, _i, _P(_d)]),
     "icarat_loop_init": (_i, [_vp, _P(LoopOpts), _dp]),
@@ -312,6 +313,16 @@ class Context:
                                        _f64(f), u.ctypes.data, C.byref(info))
         _check(st, "solve_rhs")
         return u[:self.numeq], info
+
+    def solve_noalloc(self, f_ptr, u_ptr, opts=None):
+        """Jacobi-PCG solve on device pointers that allocates no device memory
+        (work vectors in the library's static buffer); returns SolveInfo."""
+        info = SolveInfo()
+        st = self.lib.icarat_solve_noalloc(self.h, C.byref(opts) if opts is not None else None,
+                                           C.c_void_p(f_ptr), C.c_void_p(u_ptr),
+                                           C.byref(info))
+        _check(st, "solve_noalloc")
+        return info
 
     def node_values(self):
         v = np.zeros(3 * self.numnp)

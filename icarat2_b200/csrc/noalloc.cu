@@ -1,0 +1,161 @@
+// icarat_solve_noalloc: the Jacobi-PCG solve of icarat_solve_rhs, for callers
+// that cannot allocate device memory when they call the solver -- for example
+// a host application that reserved the whole GPU for its own memory pool at
+// start-up, or a deployment that forbids device allocations after
+// initialisation.  Every work vector lives in one file-scope static device
+// array of fixed size, so the call performs no cudaMalloc / cudaFree and calls
+// no allocating library routine.
+//
+// The kernels are the ones of the ordinary solve (pcg.cu, stiffness.cu,
+// ctx.cu); only the work buffers differ.  Host code cannot use the array's
+// name as a device address, so the address is resolved once per device with
+// cudaGetSymbolAddress (on the first call on that device, with that device
+// current) and passed to the kernels.
+#include <mutex>
+
+#include "internal.cuh"
+
+namespace icarat_b200
+{
+// kernels defined in pcg.cu, stiffness.cu and ctx.cu
+__global__ void k_cg_init(int n, const double *__restrict__ b,
+                          const double *__restrict__ invd, double *__restrict__ x,
+                          double *__restrict__ r, double *__restrict__ z,
+                          double *__restrict__ p, double *__restrict__ partials,
+                          CgScalars *s, double tol, int maxit, int jacobi);
+__global__ void k_cg_spmv(GridDev g, KeParam ke, const double *__restrict__ E,
+                          const uint8_t *__restrict__ fix, const double *__restrict__ p,
+                          double *__restrict__ Ap, double *__restrict__ partials,
+                          CgScalars *s);
+__global__ void k_cg_update_jacobi(int n, const double *__restrict__ invd,
+                                   double *__restrict__ x, double *__restrict__ r,
+                                   double *__restrict__ z, const double *__restrict__ p,
+                                   const double *__restrict__ Ap,
+                                   double *__restrict__ partials, CgScalars *s);
+__global__ void k_cg_pupdate(int n, const double *__restrict__ z, double *__restrict__ p,
+                             const CgScalars *s);
+__global__ void k_inv_diag(GridDev g, KeParam ke, const double *__restrict__ E,
+                           const uint8_t *__restrict__ fix, double *__restrict__ invd);
+__global__ void k_scatter_free(int numeq, const int *__restrict__ free_idx,
+                               const double *__restrict__ in, double *__restrict__ out);
+__global__ void k_gather_free(int numeq, const int *__restrict__ free_idx,
+                              const double *__restrict__ in, double *__restrict__ out);
+
+// b, x, r, p, z, Ap, 1/diag (node vectors of up to the maximum DOF count),
+// reduction partials, and the CG scalars.
+constexpr size_t kNaVec = ICARAT_NOALLOC_MAX_DOFS;
+constexpr size_t kNaPartials = 2 * (size_t)kMaxRedBlocks;
+constexpr size_t kNaScalars = (sizeof(CgScalars) + sizeof(double) - 1) / sizeof(double);
+constexpr size_t kNaDoubles = 7 * kNaVec + kNaPartials + kNaScalars;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNaDoubles];
+
+static std::mutex g_noalloc_mutex;
+static double *g_noalloc_addr[128];
+
+// Device address of the static array on the current device (resolved once).
+static double *noalloc_scratch(int device)
+{
+  IREQUIRE(device >= 0 && device < 128, ICARAT_ERR_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if(!g_noalloc_addr[device])
+  {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    IREQUIRE(e == cudaSuccess && ptr != nullptr, ICARAT_ERR_CUDA,
+             std::string("cudaGetSymbolAddress of the solve buffer: ") +
+                 cudaGetErrorString(e));
+    g_noalloc_addr[device] = static_cast<double *>(ptr);
+  }
+  return g_noalloc_addr[device];
+}
+
+static int solve_noalloc(icarat_ctx *c, const icarat_solve_opts *opts, const double *f,
+                         double *u, icarat_solve_info *info)
+{
+  IREQUIRE(c && f && u, ICARAT_ERR_ARG, "null argument");
+  ICK(cudaSetDevice(c->device));
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  icarat_solve_opts o{ICARAT_SOLVER_JACOBI_PCG, 1.0e-10, 10000, 0, 0, 0};
+  if(opts)
+    o = *opts;
+  IREQUIRE(o.method == ICARAT_SOLVER_JACOBI_PCG, ICARAT_ERR_UNSUPPORTED,
+           "icarat_solve_noalloc runs Jacobi-PCG only");
+  IREQUIRE((size_t)c->neq <= kNaVec, ICARAT_ERR_ARG,
+           "grid too large for icarat_solve_noalloc: 3*(nx+1)*(ny+1)*(nz+1) = " +
+               std::to_string(c->neq) + " DOFs, limit ICARAT_NOALLOC_MAX_DOFS = " +
+               std::to_string(kNaVec));
+  double *S = noalloc_scratch(c->device);
+  double *b = S, *x = S + kNaVec, *r = S + 2 * kNaVec, *p = S + 3 * kNaVec,
+         *z = S + 4 * kNaVec, *Ap = S + 5 * kNaVec, *invd = S + 6 * kNaVec;
+  double *partials = S + 7 * kNaVec;
+  CgScalars *s = reinterpret_cast<CgScalars *>(partials + kNaPartials);
+  const GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+  const int n = c->neq;
+  const int nb_node = (c->numnp + 255) / 256;
+  int nb_spmv = (c->numnp + 127) / 128;
+  nb_spmv = nb_spmv > kMaxRedBlocks ? kMaxRedBlocks : nb_spmv;
+  // the buffer keeps the previous call's contents: clear the scalars (their
+  // reduction counter must start at 0) and the right-hand side (constrained
+  // components stay 0); every other vector is written before it is read
+  ICK(cudaMemsetAsync(s, 0, sizeof(CgScalars), c->stream));
+  ICK(cudaMemsetAsync(b, 0, sizeof(double) * n, c->stream));
+  if(c->numeq > 0)
+  {
+    note_launch(1);
+    k_scatter_free<<<(c->numeq + 255) / 256, 256, 0, c->stream>>>(c->numeq, c->d_free, f,
+                                                                   b);
+  }
+  note_launch(2);
+  k_inv_diag<<<nb_node, 256, 0, c->stream>>>(g, c->ke0, c->d_E, c->d_fix, invd);
+  k_cg_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, b, invd, x, r, z, p,
+                                                          partials, s, o.rtol, o.maxit, 1);
+  ICK(cudaGetLastError());
+  const int chunk = o.chunk > 0 ? o.chunk : 16;
+  CgScalars hs{};
+  const long max_chunks = (long)(o.maxit + 1 + chunk - 1) / chunk + 1;
+  for(long ch = 0; ch < max_chunks; ch++)
+  {
+    ICK(cudaMemcpyAsync(&hs, s, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->stream));
+    ICK(cudaStreamSynchronize(c->stream));
+    if(hs.done)
+      break;
+    for(int k = 0; k < chunk; k++)
+    {
+      note_launch(3);
+      k_cg_spmv<<<nb_spmv, 128, 0, c->stream>>>(g, c->ke0, c->d_E, c->d_fix, p, Ap,
+                                                 partials, s);
+      k_cg_update_jacobi<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
+          n, invd, x, r, z, p, Ap, partials, s);
+      k_cg_pupdate<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, z, p, s);
+    }
+    ICK(cudaGetLastError());
+  }
+  if(c->numeq > 0)
+  {
+    note_launch(1);
+    k_gather_free<<<(c->numeq + 255) / 256, 256, 0, c->stream>>>(c->numeq, c->d_free, x,
+                                                                  u);
+  }
+  ICK(cudaGetLastError());
+  ICK(cudaMemcpyAsync(&hs, s, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
+  const int status = hs.done ? hs.status : ICARAT_WARN_MAXITER;
+  if(info)
+  {
+    info->iterations = hs.iter;
+    info->rel_residual = hs.bnorm > 0 ? hs.rnorm / hs.bnorm : 0.0;
+    info->status = status;
+  }
+  return status;
+}
+
+} // namespace icarat_b200
+
+extern "C" int icarat_solve_noalloc(icarat_ctx *ctx, const icarat_solve_opts *opts,
+                                    const double *f, double *u, icarat_solve_info *info)
+{
+  ICARAT_API_BEGIN
+  return icarat_b200::solve_noalloc(ctx, opts, f, u, info);
+  ICARAT_API_END
+}

@@ -243,6 +243,27 @@ typedef struct
   int status;
 } icarat_step_info;
 
+/* ---- solve without device allocation --------------------------------------
+ * No counterpart in the reference.  The Jacobi-PCG solve of
+ * icarat_solve_rhs (same kernels, same results) for callers that cannot
+ * allocate device memory when they call the solver, e.g. a host application
+ * that reserved the whole GPU for its own memory pool at start-up, or a
+ * deployment that forbids device allocations after initialisation.  This call
+ * allocates nothing: its work vectors live in one static device buffer of
+ * the library (about 7.4 MB, held on every GPU that loads the library until
+ * the process exits).  f and u are device pointers to numeq vectors (the
+ * context's equation numbering); opts may be NULL (rtol 1e-10, maxit 10000)
+ * and must select ICARAT_SOLVER_JACOBI_PCG.
+ * Limit: 3 (nx+1)(ny+1)(nz+1) <= ICARAT_NOALLOC_MAX_DOFS, larger grids return
+ * ICARAT_ERR_ARG.  The first call on a device resolves the buffer's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the one buffer, which keeps the last call's
+ * contents (each call clears what must start at zero): calls that overlap on
+ * the GPU -- from two threads, or on two contexts of one device -- race. */
+#define ICARAT_NOALLOC_MAX_DOFS 131072
+int icarat_solve_noalloc(icarat_ctx *ctx, const icarat_solve_opts *opts,
+                         const double *f, double *u, icarat_solve_info *info);
+
 /* ---- diagnostics (no reference counterpart) ------------------------------ */
 /* number of kernels this library has launched in this process */
 int icarat_kernel_launches(unsigned long long *count);
