@@ -57,6 +57,8 @@ def parse():
                    help="reference arm: PCG iterations run per timed step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--alt-levels", type=int, default=5,
+                   help="also time the loop with this many multigrid levels (0: skip)")
     return p.parse_args()
 
 
@@ -293,6 +295,36 @@ def gpu_arm(a):
     total_ms = float(t.item())
     value = world * a.steps / (total_ms / 1000.0)
 
+    # ---------------- the same loop with one more multigrid level (coarsest
+    # level 8x4x4 instead of 16x8x8: a 600-DOF dense solve instead of 3,888)
+    alt = None
+    if a.alt_levels:
+        ca = make_ctx()
+        ca.loop_init(0.3, method="mma", filter_radius=a.radius, move=0.2,
+                     solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, a.alt_levels, a.smooth))
+        sa = torch.cuda.ExternalStream(ca.stream_ptr(), device=dev)
+        for _ in range(a.warmup):
+            ca.loop_step()
+        torch.cuda.synchronize()
+        alt_ms = 0.0
+        for _ in range(a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(sa)
+            ca.loop_step()
+            e1.record(sa)
+            e1.synchronize()
+            alt_ms += e0.elapsed_time(e1)
+            with torch.cuda.stream(sa):
+                flush.zero_()
+        torch.cuda.synchronize()
+        ta = torch.tensor([alt_ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(ta, op=dist.ReduceOp.MAX)
+        alt = {"mg_levels": a.alt_levels,
+               "value": world * a.steps / (float(ta.item()) / 1000.0),
+               "unit": "design-iter/s", "ms_per_step": float(ta.item()) / a.steps}
+        ca.close()
+
     # ---------------- dominant kernel: FP64 stencil K u on the final design
     ms_op = ctx.time_operator(30)
     nelx, nd = nx * ny * nz, 3 * (nx + 1) * (ny + 1) * (nz + 1)
@@ -395,6 +427,7 @@ def gpu_arm(a):
                              "bytes_per_launch": bytes_alg},
             "ku_gdof_s": nd / (ms_op * 1e-3) / 1e9,
             "cg_iterations_per_step": cg,
+            "alt_levels": alt,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }

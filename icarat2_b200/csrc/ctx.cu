@@ -279,7 +279,7 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     for(long n = 0; n < c->numnp; n++)
       for(int q = 0; q < 3; q++)
         if(c->dof[3 * n + q] < c->numeq)
-          freeidx[c->dof[3 * n + q]] = (int)(3 * n + q);
+          freeidx[c->dof[3 * n + q]] = (int)((long)q * c->numnp + n);
     ICK(cudaMalloc(&c->d_free, sizeof(int) * freeidx.size()));
     ICK(cudaMemcpy(c->d_free, freeidx.data(), sizeof(int) * freeidx.size(),
                    cudaMemcpyHostToDevice));
@@ -311,8 +311,11 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     if(c->has_uD)
     {
       c->d_uD = dalloc(nv);
-      ICK(cudaMemcpy(c->d_uD, c->uD_h.data(), sizeof(double) * nv,
-                     cudaMemcpyHostToDevice));
+      std::vector<double> uD(nv);
+      for(long n = 0; n < c->numnp; n++)
+        for(int q = 0; q < 3; q++)
+          uD[(long)q * c->numnp + n] = c->uD_h[3 * n + q];
+      ICK(cudaMemcpy(c->d_uD, uD.data(), sizeof(double) * nv, cudaMemcpyHostToDevice));
     }
     ICK(cudaMemset(c->d_u, 0, sizeof(double) * nv));
     // fext in node layout
@@ -320,7 +323,7 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     for(long n = 0; n < c->numnp; n++)
       for(int q = 0; q < 3; q++)
         if(c->dof[3 * n + q] < c->numeq)
-          ff[3 * n + q] = c->fext_h[c->dof[3 * n + q]];
+          ff[(long)q * c->numnp + n] = c->fext_h[c->dof[3 * n + q]];
     ICK(cudaMemcpy(c->d_fext, ff.data(), sizeof(double) * nv,
                    cudaMemcpyHostToDevice));
   }

@@ -1,12 +1,14 @@
 // Internal declarations of the sm_100a implementation behind icarat_gpu.h.
 //
 // Layout in HBM (all contexts):
-//   node vectors  : double[3 * numnp], node-major, component fastest
-//                   (node id = i + j NX + k NX NY, NX = nx + 1), constrained
-//                   components always hold 0 (prescribed values live apart);
+//   node vectors  : double[3 * numnp], component-major: (node n, component c)
+//                   at c * numnp + n (node id = i + j NX + k NX NY, NX =
+//                   nx + 1), so a warp's 32 consecutive nodes read 256
+//                   contiguous bytes per component; constrained components
+//                   always hold 0 (prescribed values live apart);
 //   element arrays: double[nelx], element id = i + j nx + k nx ny;
 //   "numeq" vectors of the C ABI are gathered / scattered through d_free
-//   (equation number -> 3 * node + component).
+//   (equation number -> c * numnp + node).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -117,9 +119,12 @@ struct CoarseSolver
 {
   int n = 0;              // free DOFs of the coarsest level
   int *map = nullptr;     // n -> full index on the coarsest grid
-  double *A = nullptr;    // n x n dense, becomes A^-1
-  double *work = nullptr; // n x n
+  double *A = nullptr;    // n x n dense SPD matrix, becomes its Cholesky factor L
+  double *W = nullptr;    // n x n, L^-1
+  double *work = nullptr; // n x n scratch of the triangular inversion
   double *vin = nullptr, *vout = nullptr;
+  cudaGraphExec_t setup = nullptr; // per-design setup of all levels
+  int setup_kernels = 0;
 };
 
 struct FilterState

@@ -76,14 +76,14 @@ __global__ void k_restrict(GridDev f, GridDev c, const double *__restrict__ rf,
             continue;
           const double w = (dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0);
           const long m = i + (long)j * f.NX + (long)k * f.NX * f.NY;
-          s0 += w * rf[3 * m + 0];
-          s1 += w * rf[3 * m + 1];
-          s2 += w * rf[3 * m + 2];
+          s0 += w * rf[m];
+          s1 += w * rf[(long)f.numnp + m];
+          s2 += w * rf[2L * f.numnp + m];
         }
     const unsigned fx = fixc[n];
-    bc[3L * n + 0] = (fx & 1u) ? 0.0 : s0;
-    bc[3L * n + 1] = (fx & 2u) ? 0.0 : s1;
-    bc[3L * n + 2] = (fx & 4u) ? 0.0 : s2;
+    bc[n] = (fx & 1u) ? 0.0 : s0;
+    bc[(long)c.numnp + n] = (fx & 2u) ? 0.0 : s1;
+    bc[2L * c.numnp + n] = (fx & 4u) ? 0.0 : s2;
   }
 }
 
@@ -115,15 +115,15 @@ __global__ void k_prolong_add(GridDev f, GridDev c, const double *__restrict__ x
           const int I = cx ? I1 : I0, J = cy ? J1 : J0, K = cz ? K1 : K0;
           const long m = I + (long)J * c.NX + (long)K * c.NX * c.NY;
           const double w = wx * wy * wz;
-          s[0] += w * xc[3 * m + 0];
-          s[1] += w * xc[3 * m + 1];
-          s[2] += w * xc[3 * m + 2];
+          s[0] += w * xc[m];
+          s[1] += w * xc[(long)c.numnp + m];
+          s[2] += w * xc[2L * c.numnp + m];
         }
     const unsigned fx = fixf[n];
 #pragma unroll
     for(int q = 0; q < 3; q++)
       if(!((fx >> q) & 1u))
-        xf[3L * n + q] += s[q];
+        xf[(long)q * f.numnp + n] += s[q];
   }
 }
 
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
     for(int q = 0; q < 3; q++)
     {
-      const long id = 3L * n + q;
+      const long id = (long)q * g.numnp + n;
       double dn = 0.0;
       if(!((f >> q) & 1u))
         dn = (c1 != 0.0 ? c1 * d[id] : 0.0) + c2 * invd[id] * (b[id] - acc[q]);
@@ -181,8 +181,8 @@ __global__ void k_coarse_assemble(GridDev g, KeParam ke, const double *__restric
       r += gridDim.x * blockDim.x)
   {
     double *row = A + (long)r * nfree; // zeroed by the caller
-    const int full = rowmap[r];
-    const int n = full / 3, c = full % 3;
+    const int full = rowmap[r]; // component-major index c * numnp + n
+    const int n = full % g.numnp, c = full / g.numnp;
     const int i = n % g.NX, j = (n / g.NX) % g.NY, k = n / (g.NX * g.NY);
     for(int sz = 0; sz < 2; sz++)
       for(int sy = 0; sy < 2; sy++)
@@ -211,232 +211,6 @@ __global__ void k_coarse_assemble(GridDev g, KeParam ke, const double *__restric
   }
 }
 
-constexpr int CB = 32; // Cholesky block
-
-// Cholesky of the diagonal block at kb (in place, lower); one CTA of CB x CB.
-__global__ void k_chol_diag(double *A, int n, int kb)
-{
-  __shared__ double L[CB][CB + 1];
-  const int tx = threadIdx.x, ty = threadIdx.y; // column, row
-  const int m = min(CB, n - kb);
-  L[ty][tx] = (ty < m && tx < m) ? A[(long)(kb + ty) * n + kb + tx]
-                                 : (ty == tx ? 1.0 : 0.0);
-  __syncthreads();
-  for(int j = 0; j < CB; j++)
-  {
-    if(ty == j && tx == j)
-      L[j][j] = sqrt(L[j][j]);
-    __syncthreads();
-    if(tx == j && ty > j)
-      L[ty][j] /= L[j][j];
-    __syncthreads();
-    if(ty > j && tx > j && tx <= ty)
-      L[ty][tx] -= L[ty][j] * L[tx][j];
-    __syncthreads();
-  }
-  if(ty < m && tx < m)
-    A[(long)(kb + ty) * n + kb + tx] = (tx <= ty) ? L[ty][tx] : 0.0;
-}
-
-// Panel: rows i >= kb + CB, A[i, kb:kb+CB] <- A[i, kb:kb+CB] L_kk^-T.
-__global__ void k_chol_panel(double *A, int n, int kb)
-{
-  __shared__ double L[CB][CB + 1];
-  const int m = min(CB, n - kb);
-  for(int t = threadIdx.x; t < CB * CB; t += blockDim.x)
-  {
-    const int r = t / CB, s = t % CB;
-    L[r][s] = (r < m && s < m) ? A[(long)(kb + r) * n + kb + s] : (r == s ? 1.0 : 0.0);
-  }
-  __syncthreads();
-  const int i = kb + CB + blockIdx.x * blockDim.x + threadIdx.x;
-  if(i >= n)
-    return;
-  double x[CB];
-  double *row = A + (long)i * n + kb;
-#pragma unroll
-  for(int t = 0; t < CB; t++)
-    x[t] = t < m ? row[t] : 0.0;
-#pragma unroll
-  for(int t = 0; t < CB; t++)
-  {
-    double v = x[t];
-#pragma unroll
-    for(int s = 0; s < t; s++)
-      v -= x[s] * L[t][s];
-    x[t] = v / L[t][t];
-  }
-#pragma unroll
-  for(int t = 0; t < CB; t++)
-    if(t < m)
-      row[t] = x[t];
-}
-
-// Trailing update of the lower triangle: A[i][j] -= sum_t P[i][t] P[j][t]
-// for i, j >= kb + CB, j <= i, tiles of 64 x 64 (16 outputs per thread).
-__global__ void __launch_bounds__(256) k_chol_update(double *A, int n, int kb)
-{
-  const int base = kb + CB;
-  const int tiles = (n - base + 63) / 64;
-  // blockIdx.x enumerates lower-triangle tiles (ti >= tj)
-  int t = blockIdx.x, ti = 0;
-  while(t >= ti + 1)
-  {
-    t -= ti + 1;
-    ti++;
-  }
-  const int tj = t;
-  if(ti >= tiles)
-    return;
-  __shared__ double Pi[64][CB + 1];
-  __shared__ double Pj[64][CB + 1];
-  const int i0 = base + ti * 64, j0 = base + tj * 64;
-  const int m = min(CB, n - kb);
-  for(int q = threadIdx.x; q < 64 * CB; q += blockDim.x)
-  {
-    const int r = q / CB, s = q % CB;
-    Pi[r][s] = (i0 + r < n && s < m) ? A[(long)(i0 + r) * n + kb + s] : 0.0;
-    Pj[r][s] = (j0 + r < n && s < m) ? A[(long)(j0 + r) * n + kb + s] : 0.0;
-  }
-  __syncthreads();
-  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-  double acc[4][4] = {};
-#pragma unroll 8
-  for(int s = 0; s < CB; s++)
-  {
-    double a[4], b[4];
-#pragma unroll
-    for(int u = 0; u < 4; u++)
-    {
-      a[u] = Pi[ty + 16 * u][s];
-      b[u] = Pj[tx + 16 * u][s];
-    }
-#pragma unroll
-    for(int u = 0; u < 4; u++)
-#pragma unroll
-      for(int v = 0; v < 4; v++)
-        acc[u][v] = fma(a[u], b[v], acc[u][v]);
-  }
-#pragma unroll
-  for(int u = 0; u < 4; u++)
-#pragma unroll
-    for(int v = 0; v < 4; v++)
-    {
-      const int i = i0 + ty + 16 * u, j = j0 + tx + 16 * v;
-      if(i < n && j < n && j <= i)
-        A[(long)i * n + j] -= acc[u][v];
-    }
-}
-
-// W = L^-1 for block row bi: diagonal block inverse then off-diagonal blocks
-// W_ij = -L_ii^-1 sum_{k=j}^{i-1} L_ik W_kj  (j < i), one CTA per j.
-__global__ void k_trinv_row(const double *L, double *W, int n, int bi)
-{
-  __shared__ double Lii[CB][CB + 1];
-  __shared__ double S[CB][CB + 1];
-  const int i0 = bi * CB;
-  const int mi = min(CB, n - i0);
-  const int bj = blockIdx.x; // 0..bi
-  const int j0 = bj * CB;
-  const int mj = min(CB, n - j0);
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  Lii[ty][tx] = (ty < mi && tx < mi) ? L[(long)(i0 + ty) * n + i0 + tx]
-                                     : (ty == tx ? 1.0 : 0.0);
-  // S = (bj == bi) ? I : -sum_k L_ik W_kj
-  double s = 0.0;
-  if(bj == bi)
-    s = (ty == tx) ? 1.0 : 0.0;
-  else
-  {
-    for(int k0 = j0; k0 < i0; k0 += CB)
-    {
-      const int mk = min(CB, n - k0);
-      for(int t = 0; t < mk; t++)
-      {
-        const double l = (ty < mi) ? L[(long)(i0 + ty) * n + k0 + t] : 0.0;
-        const double w = (tx < mj) ? W[(long)(k0 + t) * n + j0 + tx] : 0.0;
-        s -= l * w;
-      }
-    }
-  }
-  S[ty][tx] = s;
-  __syncthreads();
-  // forward substitution Lii X = S, column tx by thread row 0..CB-1 in turn
-  for(int r = 0; r < CB; r++)
-  {
-    if(ty == r)
-    {
-      double v = S[r][tx];
-      for(int q = 0; q < r; q++)
-        v -= Lii[r][q] * S[q][tx];
-      S[r][tx] = v / Lii[r][r];
-    }
-    __syncthreads();
-  }
-  if(ty < mi && tx < mj)
-    W[(long)(i0 + ty) * n + j0 + tx] = S[ty][tx];
-}
-
-// Ainv = W^T W (lower triangle of tiles, mirrored): Ainv[i][j] =
-// sum_{k >= max(i,j)} W[k][i] W[k][j].
-__global__ void __launch_bounds__(256) k_wtw(const double *W, double *Ainv, int n)
-{
-  const int tiles = (n + 63) / 64;
-  int t = blockIdx.x, ti = 0;
-  while(t >= ti + 1)
-  {
-    t -= ti + 1;
-    ti++;
-  }
-  const int tj = t;
-  if(ti >= tiles)
-    return;
-  __shared__ double Wi[CB][64 + 1];
-  __shared__ double Wj[CB][64 + 1];
-  const int i0 = ti * 64, j0 = tj * 64;
-  const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-  double acc[4][4] = {};
-  for(int k0 = i0; k0 < n; k0 += CB) // W lower: rows k >= i0 contribute
-  {
-    __syncthreads();
-    for(int q = threadIdx.x; q < CB * 64; q += blockDim.x)
-    {
-      const int r = q / 64, s = q % 64;
-      const int k = k0 + r;
-      Wi[r][s] = (k < n && i0 + s < n) ? W[(long)k * n + i0 + s] : 0.0;
-      Wj[r][s] = (k < n && j0 + s < n) ? W[(long)k * n + j0 + s] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll 8
-    for(int r = 0; r < CB; r++)
-    {
-      double a[4], b[4];
-#pragma unroll
-      for(int u = 0; u < 4; u++)
-      {
-        a[u] = Wi[r][ty + 16 * u];
-        b[u] = Wj[r][tx + 16 * u];
-      }
-#pragma unroll
-      for(int u = 0; u < 4; u++)
-#pragma unroll
-        for(int v = 0; v < 4; v++)
-          acc[u][v] = fma(a[u], b[v], acc[u][v]);
-    }
-  }
-#pragma unroll
-  for(int u = 0; u < 4; u++)
-#pragma unroll
-    for(int v = 0; v < 4; v++)
-    {
-      const int i = i0 + ty + 16 * u, j = j0 + tx + 16 * v;
-      if(i < n && j < n && j <= i)
-      {
-        Ainv[(long)i * n + j] = acc[u][v];
-        Ainv[(long)j * n + i] = acc[u][v];
-      }
-    }
-}
 
 // Coarse solve: x_full = scatter(Ainv gather(b_full)); one warp per row.
 __global__ void k_coarse_gather(int nfree, const int *__restrict__ rowmap,
@@ -447,27 +221,6 @@ __global__ void k_coarse_gather(int nfree, const int *__restrict__ rowmap,
     v[r] = b[rowmap[r]];
 }
 
-__global__ void k_coarse_gemv(int nfree, const double *__restrict__ Ainv,
-                              const double *__restrict__ v,
-                              const int *__restrict__ rowmap, int nfull,
-                              double *__restrict__ x)
-{
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for(int r = warp; r < nfree; r += nw)
-  {
-    const double *row = Ainv + (long)r * nfree;
-    double s = 0.0;
-    for(int q = lane; q < nfree; q += 32)
-      s = fma(row[q], v[q], s);
-    for(int o = 16; o > 0; o >>= 1)
-      s += __shfl_down_sync(0xffffffffu, s, o);
-    if(lane == 0)
-      x[rowmap[r]] = s;
-  }
-  (void)nfull;
-}
 
 // ---------------------------------------------------------------- driver
 static GridDev make_grid(int nx, int ny, int nz)
@@ -500,8 +253,11 @@ void mg_free(icarat_ctx *c)
     dfree(L.t);
   }
   c->mg.clear();
+  if(c->coarse.setup)
+    cudaGraphExecDestroy(c->coarse.setup);
   dfree(c->coarse.map);
   dfree(c->coarse.A);
+  dfree(c->coarse.W);
   dfree(c->coarse.work);
   dfree(c->coarse.vin);
   dfree(c->coarse.vout);
@@ -568,8 +324,8 @@ static void allocate_levels(icarat_ctx *c, int levels)
     for(int q = 0; q < 3; q++)
       if(!((fix[n] >> q) & 1u))
       {
-        colmap[3 * (size_t)n + q] = (int)rowmap.size();
-        rowmap.push_back(3 * n + q);
+        colmap[3 * (size_t)n + q] = (int)rowmap.size(); // node-major lookup table
+        rowmap.push_back(q * gc.numnp + n);               // component-major vector index
       }
   const int nf = (int)rowmap.size();
   IREQUIRE((double)nf * nf * 8.0 * 2 < 4.0e9, ICARAT_ERR_UNSUPPORTED,
@@ -582,22 +338,21 @@ static void allocate_levels(icarat_ctx *c, int levels)
   ICK(cudaMemcpy(c->coarse.map + nf, colmap.data(), sizeof(int) * colmap.size(),
                  cudaMemcpyHostToDevice));
   c->coarse.A = dalloc((size_t)nf * nf);
+  c->coarse.W = dalloc((size_t)nf * nf);
   c->coarse.work = dalloc((size_t)nf * nf);
   c->coarse.vin = dalloc(nf);
   c->coarse.vout = dalloc(nf);
   c->mg_built_levels = levels;
 }
 
-// Coarse operators and the dense inverse for the current design.
-void mg_setup(icarat_ctx *c, int levels)
+void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n);
+void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
+                     const double *v, double *t, const int *rowmap, double *x);
+
+// Everything that depends on the design: coarse moduli, Jacobi diagonals, the
+// dense coarsest matrix and W = L^-1 of its Cholesky factor.
+static void enqueue_mg_setup(icarat_ctx *c, int levels)
 {
-  IREQUIRE(levels >= 2 && levels <= 12, ICARAT_ERR_ARG, "mg_levels must be in [2, 12]");
-  if((int)c->mg.size() != levels)
-    allocate_levels(c, levels);
-  else if(c->mg_version == c->design_version)
-    return; // operators of this design are built already
-  c->mg_version = c->design_version;
-  // moduli and Jacobi diagonals
   for(int l = 0; l < levels; l++)
   {
     MgLevel &L = c->mg[l];
@@ -619,33 +374,54 @@ void mg_setup(icarat_ctx *c, int levels)
     k_coarse_assemble<<<blocks_for(n, 64), 64, 0, c->stream>>>(
         C.g, c->ke0, C.E, c->coarse.map, c->coarse.map + n, n, c->coarse.A);
     ICK(cudaGetLastError());
-    double *A = c->coarse.A, *W = c->coarse.work;
-    for(int kb = 0; kb < n; kb += CB)
-    {
-      note_launch();
-      k_chol_diag<<<1, dim3(CB, CB), 0, c->stream>>>(A, n, kb);
-      const int rows = n - kb - CB;
-      if(rows > 0)
-      {
-        note_launch();
-        k_chol_panel<<<blocks_for(rows, 128), 128, 0, c->stream>>>(A, n, kb);
-        const int tiles = (rows + 63) / 64;
-        note_launch();
-        k_chol_update<<<tiles * (tiles + 1) / 2, 256, 0, c->stream>>>(A, n, kb);
-      }
-    }
-    ICK(cudaMemsetAsync(W, 0, sizeof(double) * (size_t)n * n, c->stream));
-    const int nb = (n + CB - 1) / CB;
-    for(int bi = 0; bi < nb; bi++)
-    {
-      note_launch();
-      k_trinv_row<<<bi + 1, dim3(CB, CB), 0, c->stream>>>(A, W, n, bi);
-    }
-    const int tiles = (n + 63) / 64;
-    note_launch();
-    k_wtw<<<tiles * (tiles + 1) / 2, 256, 0, c->stream>>>(W, A, n);
-    ICK(cudaGetLastError());
+    dense_spd_inverse_factor(c->stream, c->coarse.A, c->coarse.W, c->coarse.work, n);
   }
+}
+
+// Coarse operators and the dense inverse for the current design.  The fixed
+// launch sequence is captured once per hierarchy into a CUDA graph and
+// replayed for every new design.
+void mg_setup(icarat_ctx *c, int levels)
+{
+  IREQUIRE(levels >= 2 && levels <= 12, ICARAT_ERR_ARG, "mg_levels must be in [2, 12]");
+  if((int)c->mg.size() != levels)
+    allocate_levels(c, levels);
+  else if(c->mg_version == c->design_version)
+    return; // operators of this design are built already
+  c->mg_version = c->design_version;
+  if(!c->coarse.setup)
+  {
+    cudaGraph_t graph;
+    ICK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    set_capturing(true);
+    try
+    {
+      enqueue_mg_setup(c, levels);
+    }
+    catch(...)
+    {
+      set_capturing(false);
+      cudaStreamEndCapture(c->stream, &graph);
+      throw;
+    }
+    set_capturing(false);
+    ICK(cudaStreamEndCapture(c->stream, &graph));
+    size_t nn = 0;
+    ICK(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    ICK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    c->coarse.setup_kernels = 0;
+    for(auto nd : nodes)
+    {
+      cudaGraphNodeType t;
+      ICK(cudaGraphNodeGetType(nd, &t));
+      c->coarse.setup_kernels += (t == cudaGraphNodeTypeKernel) ? 1 : 0;
+    }
+    ICK(cudaGraphInstantiate(&c->coarse.setup, graph, 0));
+    cudaGraphDestroy(graph);
+  }
+  ICK(cudaGraphLaunch(c->coarse.setup, c->stream));
+  note_launch(c->coarse.setup_kernels);
 }
 
 // Chebyshev smoothing of K x = b on one level, deg steps.  from_zero: x = 0
@@ -705,9 +481,8 @@ static void vcycle(icarat_ctx *c, int l, const double *b, int deg)
       note_launch();
       k_coarse_gather<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, c->coarse.map, b,
                                                                  c->coarse.vin);
-      note_launch();
-      k_coarse_gemv<<<blocks_for(n * 32, 256), 256, 0, c->stream>>>(
-          n, c->coarse.A, c->coarse.vin, c->coarse.map, 3 * L.g.numnp, L.x);
+      dense_spd_solve(c->stream, c->coarse.W, c->coarse.work, n, c->coarse.vin,
+                      c->coarse.vout, c->coarse.map, L.x);
     }
     return;
   }

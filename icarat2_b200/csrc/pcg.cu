@@ -96,9 +96,9 @@ __global__ void __launch_bounds__(128)
     const double y0 = (f & 1u) ? 0.0 : acc[0];
     const double y1 = (f & 2u) ? 0.0 : acc[1];
     const double y2 = (f & 4u) ? 0.0 : acc[2];
-    Ap[3L * n + 0] = y0;
-    Ap[3L * n + 1] = y1;
-    Ap[3L * n + 2] = y2;
+    Ap[n] = y0;
+    Ap[(long)g.numnp + n] = y1;
+    Ap[2L * g.numnp + n] = y2;
     dot += uc[0] * y0 + uc[1] * y1 + uc[2] * y2;
   }
   double v[1] = {dot};

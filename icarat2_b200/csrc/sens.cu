@@ -28,7 +28,7 @@ __global__ void k_node_values(int numnp, const double *__restrict__ u,
     const unsigned f = fix[n];
 #pragma unroll
     for(int q = 0; q < 3; q++)
-      out[3L * n + q] = node_value(u, uD, f, 3L * n + q, q);
+      out[3L * n + q] = node_value(u, uD, f, (long)q * numnp + n, q);
   }
 }
 
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(128)
           const unsigned f = fix[m];
 #pragma unroll
           for(int q = 0; q < 3; q++)
-            ue[3 * b + q] = node_value(u, uD, f, 3 * m + q, q);
+            ue[3 * b + q] = node_value(u, uD, f, (long)q * g.numnp + m, q);
         }
     const double dens = rho[e];
     const double young = (1.0 - pow(dens, p)) * e1 + pow(dens, p) * e2;

@@ -20,44 +20,69 @@ __host__ __device__ constexpr int local_node(int lx, int ly, int lz)
 }
 
 // One z-layer of 4 elements around node (i,j,k): SZ = 0 are the elements
-// below the node (element k index k-1), SZ = 1 the ones above.  ul[bz][s]
-// holds the displacements of node layer k - 1 + SZ + bz, s = (dy+1)*3+(dx+1).
+// below the node (element k index k-1), SZ = 1 the ones above.  ul[l][s]
+// holds the displacements of node layer k - 1 + SZ + l, s = (dy+1)*3+(dx+1).
+//
+// The box element is symmetric under reflection in its mid-planes, so its
+// 3x3 blocks satisfy Ke0[a][b] = S_a K^_beta S_a with beta = |b - a| (per
+// axis), K^_beta = Ke0[local node 0][local node beta] and S_a =
+// diag((-1)^a_x, (-1)^a_y, (-1)^a_z).  The loop therefore runs over the 8
+// canonical blocks: each block's 9 coefficients are read once and serve the 4
+// elements of the layer (the signs are free DFMA operand negations), and the
+// 12 partial sums t[element][row] are independent accumulation chains.
 template <int SZ>
 __device__ __forceinline__ void layer_contrib(const KeParam &ke,
                                               const double (&ul)[2][9][3],
                                               const double (&Ev)[4],
                                               double (&acc)[3])
 {
+  double t[4][3];
 #pragma unroll
-  for(int sy = 0; sy < 2; sy++)
+  for(int e = 0; e < 4; e++)
+    t[e][0] = t[e][1] = t[e][2] = 0.0;
 #pragma unroll
-    for(int sx = 0; sx < 2; sx++)
-    {
-      const int a = local_node(1 - sx, 1 - sy, 1 - SZ);
-      double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+  for(int bz = 0; bz < 2; bz++)
 #pragma unroll
-      for(int bz = 0; bz < 2; bz++)
+    for(int by = 0; by < 2; by++)
 #pragma unroll
-        for(int by = 0; by < 2; by++)
+      for(int bx = 0; bx < 2; bx++)
+      {
+        const int lb = local_node(bx, by, bz);
+        double kb[9];
 #pragma unroll
-          for(int bx = 0; bx < 2; bx++)
+        for(int c = 0; c < 3; c++)
+#pragma unroll
+          for(int d = 0; d < 3; d++)
+            kb[3 * c + d] = ke.k[c * 24 + 3 * lb + d];
+#pragma unroll
+        for(int sy = 0; sy < 2; sy++)
+#pragma unroll
+          for(int sx = 0; sx < 2; sx++)
           {
-            const int b = local_node(bx, by, bz);
-            const int s = (sy + by) * 3 + (sx + bx);
+            // element (sx, sy, SZ): the node's local corner a = 1 - s, the
+            // neighbour at canonical offset beta is n + beta * (2 s - 1)
+            const int ax = 1 - sx, ay = 1 - sy, az = 1 - SZ;
+            const int dx = bx * (2 * sx - 1), dy = by * (2 * sy - 1);
+            const int l = bz * (2 * SZ - 1) + 1 - SZ;
+            const int s = (dy + 1) * 3 + (dx + 1);
+            const int ac[3] = {ax, ay, az};
+            const int e = sy * 2 + sx;
 #pragma unroll
-            for(int d = 0; d < 3; d++)
-            {
-              const double u = ul[bz][s][d];
-              t0 = fma(ke.k[(3 * a + 0) * 24 + 3 * b + d], u, t0);
-              t1 = fma(ke.k[(3 * a + 1) * 24 + 3 * b + d], u, t1);
-              t2 = fma(ke.k[(3 * a + 2) * 24 + 3 * b + d], u, t2);
-            }
+            for(int c = 0; c < 3; c++)
+#pragma unroll
+              for(int d = 0; d < 3; d++)
+              {
+                const bool neg = (c != d) && ((ac[c] + ac[d]) & 1);
+                const double k = neg ? -kb[3 * c + d] : kb[3 * c + d];
+                t[e][c] = fma(k, ul[l][s][d], t[e][c]);
+              }
           }
-      const double e = Ev[sy * 2 + sx];
-      acc[0] = fma(e, t0, acc[0]);
-      acc[1] = fma(e, t1, acc[1]);
-      acc[2] = fma(e, t2, acc[2]);
-    }
+      }
+#pragma unroll
+  for(int e = 0; e < 4; e++)
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+      acc[c] = fma(Ev[e], t[e][c], acc[c]);
 }
 
 __device__ __forceinline__ void load_layer(const double *__restrict__ u,
@@ -76,7 +101,7 @@ __device__ __forceinline__ void load_layer(const double *__restrict__ u,
       const int s = (dy + 1) * 3 + (dx + 1);
 #pragma unroll
       for(int d = 0; d < 3; d++)
-        L[s][d] = in ? __ldg(u + 3 * m + d) : 0.0;
+        L[s][d] = in ? __ldg(u + (long)d * g.numnp + m) : 0.0;
     }
 }
 

@@ -26,9 +26,9 @@ __global__ void __launch_bounds__(128)
     const double y0 = (f & 1u) ? 0.0 : acc[0];
     const double y1 = (f & 2u) ? 0.0 : acc[1];
     const double y2 = (f & 4u) ? 0.0 : acc[2];
-    y[3L * n + 0] = y0;
-    y[3L * n + 1] = y1;
-    y[3L * n + 2] = y2;
+    y[n] = y0;
+    y[(long)g.numnp + n] = y1;
+    y[2L * g.numnp + n] = y2;
     dot += uc[0] * y0 + uc[1] * y1 + uc[2] * y2;
   }
   if(partials)
@@ -70,7 +70,7 @@ __global__ void k_inv_diag(GridDev g, KeParam ke, const double *__restrict__ E,
     for(int c = 0; c < 3; c++)
       // a zero diagonal is treated as 1, as Eigen's DiagonalPreconditioner
       // does for the "Eigen_CG" solver (solvers.cpp:63-91)
-      invd[3L * n + c] = ((f >> c) & 1u) ? 0.0 : (d[c] != 0.0 ? 1.0 / d[c] : 1.0);
+      invd[(long)c * g.numnp + n] = ((f >> c) & 1u) ? 0.0 : (d[c] != 0.0 ? 1.0 / d[c] : 1.0);
   }
 }
 
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(128)
     const unsigned f = fix[n];
 #pragma unroll
     for(int c = 0; c < 3; c++)
-      r[3L * n + c] = ((f >> c) & 1u) ? 0.0 : b[3L * n + c] - acc[c];
+      r[(long)c * g.numnp + n] = ((f >> c) & 1u) ? 0.0 : b[(long)c * g.numnp + n] - acc[c];
   }
 }
 
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(128)
     const unsigned f = fix[n];
 #pragma unroll
     for(int c = 0; c < 3; c++)
-      y[3L * n + c] = ((f >> c) & 1u) ? 0.0 : acc[c];
+      y[(long)c * g.numnp + n] = ((f >> c) & 1u) ? 0.0 : acc[c];
   }
 }
 
