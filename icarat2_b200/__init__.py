@@ -24,6 +24,7 @@ LIBPATH = os.path.join(_HERE, "libicarat_gpu.so")
 
 OK = 0
 WARN_MAXITER = 1
+WARN_STAGNATION = 2
 ERR_ARG = -1
 ERR_CUDA = -2
 ERR_NAN = -4
@@ -34,6 +35,7 @@ ERR_NOMEM = -8
 
 JACOBI_PCG = 0
 MG_PCG = 1
+MIXED_IR = 2
 
 
 class IcaratError(RuntimeError):
@@ -68,12 +70,13 @@ class BC(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int),
-                ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int)]
+                ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int),
+                ("refresh", C.c_double)]
 
 
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("rel_residual", C.c_double),
-                ("status", C.c_int)]
+                ("status", C.c_int), ("refreshes", C.c_int)]
 
 
 class OcOpts(C.Structure):
@@ -202,8 +205,8 @@ def cantilever_bc(nx, ny, nz, lx=None, ly=None, lz=None, load_node=None, load=(0
 
 
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
-               chunk=0):
-    return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk)
+               chunk=0, refresh=0.0):
+    return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh)
 
 
 class Context:
@@ -409,7 +412,8 @@ class Context:
 
 
 # ---- reference-named mirrors ------------------------------------------------------
-_SOLVER_NAMES = {"Eigen_CG": JACOBI_PCG, "Scaling_CG": JACOBI_PCG, "MG_CG": MG_PCG}
+_SOLVER_NAMES = {"Eigen_CG": JACOBI_PCG, "Scaling_CG": JACOBI_PCG, "MG_CG": MG_PCG,
+                 "Mixed_MG_CG": MIXED_IR}
 
 
 class LinearAnalysis:

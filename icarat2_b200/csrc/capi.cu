@@ -110,6 +110,7 @@ const char *icarat_status_string(int s)
   {
   case ICARAT_OK: return "ok";
   case ICARAT_WARN_MAXITER: return "iteration cap reached";
+  case ICARAT_WARN_STAGNATION: return "residual stagnated";
   case ICARAT_ERR_ARG: return "bad argument";
   case ICARAT_ERR_CUDA: return "CUDA error";
   case ICARAT_ERR_NAN: return "non-finite value";

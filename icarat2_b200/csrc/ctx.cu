@@ -265,6 +265,8 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     c->neq = 3 * c->numnp;
     c->mat = *mat;
     hexa8_stiffness(c->hx, c->hy, c->hz, mat->poisson, c->ke0.k, &c->vol0);
+    for(int q = 0; q < 576; q++)
+      c->ke0f.k[q] = (float)c->ke0.k[q];
     c->ke_diag_max = 0.0;
     for(int a = 0; a < 24; a++)
       c->ke_diag_max = std::fmax(c->ke_diag_max, c->ke0.k[25 * a]);
@@ -344,6 +346,7 @@ int icarat_ctx_destroy_impl(icarat_ctx *c)
   if(c->stream)
     cudaStreamSynchronize(c->stream);
   mg_free(c);
+  mixed_free(c);
   filter_free(c);
   if(c->loop.mma)
     icarat_mma_destroy(c->loop.mma);

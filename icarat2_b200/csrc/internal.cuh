@@ -82,6 +82,10 @@ struct KeParam
 {
   double k[576];
 };
+struct KeParamF
+{
+  float k[576];
+};
 
 // Structured grid of one level.
 struct GridDev
@@ -100,6 +104,18 @@ struct CgScalars
   int pad;
 };
 
+// Scalars of the mixed-precision loop (FP32 vectors, FP64 scalars).
+struct MxScalars
+{
+  double alpha, beta, zr, pAp, rr, rr_ref, rr_true, bb, tol2, delta2;
+  int iter, maxit, done, status;
+  int nstall;   // consecutive refreshes that cut the FP64 residual by < 10 %
+  int refresh;  // FP64 residual due after this iteration's update
+  int final_;   // iteration cap reached: last refresh, then stop
+  int nrefresh; // FP64 residuals evaluated
+  unsigned int counter;
+};
+
 // Reduction geometry: every grid-stride reduction kernel runs on
 // kRedBlocks blocks of kRedThreads threads so that partial sums are summed
 // in one fixed order (bit-reproducible on a given GPU).
@@ -113,6 +129,9 @@ struct MgLevel
   uint8_t *fix = nullptr;  // numnp, bit c = component c constrained
   double *invd = nullptr;  // 3 numnp, 1 / diag(K) (0 on constrained)
   double *x = nullptr, *b = nullptr, *r = nullptr, *t = nullptr;
+  // FP32 copies of E and invd and FP32 work vectors (mixed-precision solver)
+  float *E32 = nullptr, *invd32 = nullptr;
+  float *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *t32 = nullptr;
 };
 
 struct CoarseSolver
@@ -165,6 +184,7 @@ struct icarat_ctx
   int NX, NY, NZ, numnp, nelx, neq, numeq;
   icarat_material mat;
   icarat_b200::KeParam ke0;
+  icarat_b200::KeParamF ke0f; // ke0 rounded to FP32
   double vol0;
   double ke_diag_max; // max_a Ke0[a][a]
   double lam_max_dk;  // bound on lambda_max(D^-1 K) from the element matrix
@@ -192,6 +212,10 @@ struct icarat_ctx
   icarat_b200::CgScalars *d_cg = nullptr;
   icarat_b200::CgScalars *h_cg = nullptr; // pinned
   double *h_scalar = nullptr;             // pinned
+  // mixed-precision solver (allocated on first use): FP32 iterate x, residual
+  // r, preconditioned residual z, direction p and K p
+  float *f_x = nullptr, *f_r = nullptr, *f_z = nullptr, *f_p = nullptr, *f_Ap = nullptr;
+  icarat_b200::MxScalars *d_mx = nullptr, *h_mx = nullptr;
   bool design_set = false, solved = false;
   icarat_solve_info last_info{};
   // multigrid
@@ -205,6 +229,8 @@ struct icarat_ctx
   // instantiated solver graphs: (method, levels, smooth, chunk, x) -> exec
   std::map<std::tuple<int, int, int, int, const void *>, cudaGraphExec_t> graphs;
   std::map<std::tuple<int, int, int, int, const void *>, int> graph_kernels;
+  // right-hand side a graph reads (mixed solver graphs read b at each refresh)
+  std::map<std::tuple<int, int, int, int, const void *>, const void *> graph_b;
   unsigned long design_version = 0;
   unsigned long mg_version = ~0ul;
 };
@@ -244,9 +270,15 @@ void release_graphs(icarat_ctx *c);
 int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                double *d_x, icarat_solve_info *info);
 
+// mixed.cu
+int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
+                double *d_x, icarat_solve_info *info);
+void mixed_free(icarat_ctx *c);
+
 // multigrid.cu
 void mg_setup(icarat_ctx *c, int levels);
 void mg_vcycle(icarat_ctx *c, const double *r, double *z, int smooth);
+void mg_vcycle_f32(icarat_ctx *c, const float *r, float *z, int smooth);
 void mg_free(icarat_ctx *c);
 
 // filter.cu

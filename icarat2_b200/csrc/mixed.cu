@@ -1,0 +1,452 @@
+// Mixed-precision solve of K u = b (no reference counterpart; the reference
+// solves in FP64 only).
+//
+// The Krylov iteration runs on FP32 vectors: K p with the FP32 copy of Ke0 and
+// of the element moduli, and an FP32 multigrid V-cycle as the preconditioner.
+// Every dot product is accumulated in FP64 and every scalar is FP64.  The
+// solution is refined in FP64: the iteration accumulates a correction x32;
+// once the FP32 recurrence residual has fallen by the factor `refresh` below
+// the last FP64 residual (or below the stopping threshold, or at the
+// iteration cap) the correction is added to the FP64 solution x, x32 is
+// cleared and the residual is recomputed as r = b - K x with the FP64
+// operator.  Convergence is decided on that FP64 residual only:
+// ||b - K x|| < rtol ||b||; three refreshes in a row that cut it by less than
+// 10 % end the solve with ICARAT_WARN_STAGNATION (the residual is then at the
+// accuracy FP64 evaluation allows for the design).  The search direction
+// survives the refresh, so the refinement does not restart the Krylov space;
+// beta is the flexible
+// (Polak-Ribiere) form beta = -(z . K p) / (p . K p), which keeps
+// consecutive directions K-orthogonal under the inexact FP32 preconditioner
+// and across a refresh.
+//
+// Like the FP64 solvers, all scalars live in device memory and the host
+// replays a CUDA graph of `chunk` iterations, reading the stop flag once per
+// chunk.
+#include <cmath>
+
+#include "stencil.cuh"
+
+namespace icarat_b200
+{
+
+// x = 0, x32 = 0, r32 = b, ||b||.
+__global__ void k_mx_init(int n, const double *__restrict__ b, double *__restrict__ x,
+                          float *__restrict__ x32, float *__restrict__ r32,
+                          double *__restrict__ partials, MxScalars *s, double tol,
+                          double delta, int maxit)
+{
+  __shared__ double sh[32];
+  double bb = 0.0;
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  {
+    const double bi = b[i];
+    x[i] = 0.0;
+    x32[i] = 0.0f;
+    r32[i] = (float)bi;
+    bb += bi * bi;
+  }
+  double v[1] = {bb};
+  block_sum<1>(v, sh);
+  if(threadIdx.x == 0)
+    partials[blockIdx.x] = v[0];
+  if(last_block(&s->counter))
+  {
+    double t[1];
+    sum_partials<1>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      s->bb = t[0];
+      s->rr = s->rr_ref = s->rr_true = t[0];
+      s->tol2 = tol * tol * t[0];
+      s->delta2 = delta * delta;
+      s->maxit = maxit;
+      s->iter = 0;
+      s->refresh = 0;
+      s->final_ = 0;
+      s->nrefresh = 0;
+      s->nstall = 0;
+      s->status = ICARAT_OK;
+      s->done = (t[0] == 0.0) ? 1 : 0;
+      if(!(t[0] == t[0]))
+      {
+        s->done = 1;
+        s->status = ICARAT_ERR_NAN;
+      }
+      s->counter = 0;
+    }
+  }
+}
+
+// Ap = K32 p (constrained rows 0); alpha = zr / (p . Ap).
+__global__ void __launch_bounds__(128)
+    k_mx_spmv(GridDev g, KeParamF ke, const float *__restrict__ E,
+              const uint8_t *__restrict__ fix, const float *__restrict__ p,
+              float *__restrict__ Ap, double *__restrict__ partials, MxScalars *s)
+{
+  __shared__ double sh[32];
+  if(s->done)
+    return;
+  double dot = 0.0;
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    float acc[3], uc[3];
+    node_Ku(g, ke, E, p, n, acc, uc);
+    const unsigned f = fix[n];
+#pragma unroll
+    for(int q = 0; q < 3; q++)
+    {
+      const float y = ((f >> q) & 1u) ? 0.0f : acc[q];
+      Ap[(long)q * g.numnp + n] = y;
+      dot += (double)uc[q] * (double)y;
+    }
+  }
+  double v[1] = {dot};
+  block_sum<1>(v, sh);
+  if(threadIdx.x == 0)
+    partials[blockIdx.x] = v[0];
+  if(last_block(&s->counter))
+  {
+    double t[1];
+    sum_partials<1>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      s->pAp = t[0];
+      s->alpha = s->zr / t[0];
+      s->counter = 0;
+    }
+  }
+}
+
+// x32 += alpha p, r32 -= alpha Ap; decide whether an FP64 refresh is due.
+__global__ void k_mx_update(int n, float *__restrict__ x32, float *__restrict__ r32,
+                            const float *__restrict__ p, const float *__restrict__ Ap,
+                            double *__restrict__ partials, MxScalars *s)
+{
+  __shared__ double sh[32];
+  if(s->done)
+    return;
+  const float alpha = (float)s->alpha;
+  double rr = 0.0;
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  {
+    x32[i] = fmaf(alpha, p[i], x32[i]);
+    const float ri = fmaf(-alpha, Ap[i], r32[i]);
+    r32[i] = ri;
+    rr += (double)ri * (double)ri;
+  }
+  double v[1] = {rr};
+  block_sum<1>(v, sh);
+  if(threadIdx.x == 0)
+    partials[blockIdx.x] = v[0];
+  if(last_block(&s->counter))
+  {
+    double t[1];
+    sum_partials<1>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      const double r2 = t[0];
+      s->iter += 1;
+      s->rr = r2;
+      if(!(r2 == r2) || !(s->alpha == s->alpha))
+      {
+        s->done = 1;
+        s->status = ICARAT_ERR_NAN;
+      }
+      else
+      {
+        s->final_ = s->iter > s->maxit ? 1 : 0;
+        s->refresh = (r2 < s->delta2 * s->rr_ref || r2 < s->tol2 || s->final_) ? 1 : 0;
+      }
+      s->counter = 0;
+    }
+  }
+}
+
+// Refresh, part 1: x += x32, x32 = 0.
+__global__ void k_mx_flush(int n, double *__restrict__ x, float *__restrict__ x32,
+                           const MxScalars *s)
+{
+  if(s->done || !s->refresh)
+    return;
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  {
+    x[i] += (double)x32[i];
+    x32[i] = 0.0f;
+  }
+}
+
+// Refresh, part 2: r = b - K x in FP64, r32 = (float) r, stop test on ||r||.
+__global__ void __launch_bounds__(128)
+    k_mx_residual(GridDev g, KeParam ke, const double *__restrict__ E,
+                  const uint8_t *__restrict__ fix, const double *__restrict__ b,
+                  const double *__restrict__ x, float *__restrict__ r32,
+                  double *__restrict__ partials, MxScalars *s)
+{
+  __shared__ double sh[32];
+  if(s->done || !s->refresh)
+    return;
+  double rr = 0.0;
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    double acc[3], uc[3];
+    node_Ku(g, ke, E, x, n, acc, uc);
+    const unsigned f = fix[n];
+#pragma unroll
+    for(int q = 0; q < 3; q++)
+    {
+      const long id = (long)q * g.numnp + n;
+      const double r = ((f >> q) & 1u) ? 0.0 : b[id] - acc[q];
+      r32[id] = (float)r;
+      rr += r * r;
+    }
+  }
+  double v[1] = {rr};
+  block_sum<1>(v, sh);
+  if(threadIdx.x == 0)
+    partials[blockIdx.x] = v[0];
+  if(last_block(&s->counter))
+  {
+    double t[1];
+    sum_partials<1>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      const double r2 = t[0];
+      s->nstall = r2 > 0.81 * s->rr_true ? s->nstall + 1 : 0;
+      s->rr_true = s->rr_ref = s->rr = r2;
+      s->nrefresh += 1;
+      s->refresh = 0;
+      if(!(r2 == r2))
+      {
+        s->done = 1;
+        s->status = ICARAT_ERR_NAN;
+      }
+      else if(r2 < s->tol2)
+      {
+        s->done = 1;
+        s->status = ICARAT_OK;
+      }
+      else if(s->final_)
+      {
+        s->done = 1;
+        s->status = ICARAT_WARN_MAXITER;
+      }
+      else if(s->nstall >= 3)
+      {
+        // the FP64 residual is at the accuracy this operator and design allow
+        s->done = 1;
+        s->status = ICARAT_WARN_STAGNATION;
+      }
+      s->counter = 0;
+    }
+  }
+}
+
+// zr = z . r and beta = -(z . Ap) / pAp (first: beta = 0).
+__global__ void k_mx_zr(int n, const float *__restrict__ z, const float *__restrict__ r,
+                        const float *__restrict__ Ap, double *__restrict__ partials,
+                        MxScalars *s, int first)
+{
+  __shared__ double sh[64];
+  if(s->done)
+    return;
+  double zr = 0.0, zap = 0.0;
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+  {
+    const double zi = z[i];
+    zr += zi * (double)r[i];
+    if(!first)
+      zap += zi * (double)Ap[i];
+  }
+  double v[2] = {zr, zap};
+  block_sum<2>(v, sh);
+  if(threadIdx.x == 0)
+  {
+    partials[blockIdx.x] = v[0];
+    partials[gridDim.x + blockIdx.x] = v[1];
+  }
+  if(last_block(&s->counter))
+  {
+    double t[2];
+    sum_partials<2>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      s->zr = t[0];
+      s->beta = first ? 0.0 : -t[1] / s->pAp;
+      s->counter = 0;
+    }
+  }
+}
+
+// p = z + beta p (first: p = z)
+__global__ void k_mx_pupdate(int n, const float *__restrict__ z, float *__restrict__ p,
+                             const MxScalars *s, int first)
+{
+  if(s->done)
+    return;
+  const float beta = (float)s->beta;
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = first ? z[i] : fmaf(beta, p[i], z[i]);
+}
+
+static float *falloc(size_t n)
+{
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, (n ? n : 1) * sizeof(float));
+  if(e != cudaSuccess)
+    throw Error{ICARAT_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+  return static_cast<float *>(p);
+}
+
+static void mixed_alloc(icarat_ctx *c)
+{
+  if(c->f_x)
+    return;
+  const size_t nv = (size_t)c->neq;
+  c->f_x = falloc(nv);
+  c->f_r = falloc(nv);
+  c->f_z = falloc(nv);
+  c->f_p = falloc(nv);
+  c->f_Ap = falloc(nv);
+  ICK(cudaMalloc(&c->d_mx, sizeof(MxScalars)));
+  ICK(cudaMemset(c->d_mx, 0, sizeof(MxScalars)));
+  ICK(cudaMallocHost(&c->h_mx, sizeof(MxScalars)));
+}
+
+void mixed_free(icarat_ctx *c)
+{
+  for(void *p : {(void *)c->f_x, (void *)c->f_r, (void *)c->f_z, (void *)c->f_p,
+                 (void *)c->f_Ap, (void *)c->d_mx})
+    dfree(p);
+  if(c->h_mx)
+    cudaFreeHost(c->h_mx);
+  c->f_x = c->f_r = c->f_z = c->f_p = c->f_Ap = nullptr;
+  c->d_mx = c->h_mx = nullptr;
+}
+
+static int spmv_blocks(const icarat_ctx *c)
+{
+  int b = (c->numnp + 127) / 128;
+  return b > kMaxRedBlocks ? kMaxRedBlocks : (b < 1 ? 1 : b);
+}
+
+// z = M r32, zr, beta, p update
+static void enqueue_precondition(icarat_ctx *c, int smooth, int first)
+{
+  const int n = c->neq;
+  mg_vcycle_f32(c, c->f_r, c->f_z, smooth);
+  note_launch(2);
+  k_mx_zr<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_z, c->f_r, c->f_Ap,
+                                                        c->d_partials, c->d_mx, first);
+  k_mx_pupdate<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_z, c->f_p, c->d_mx,
+                                                             first);
+}
+
+static void enqueue_iteration(icarat_ctx *c, int smooth, const double *b, double *x)
+{
+  const MgLevel &L = c->mg[0];
+  const int n = c->neq;
+  note_launch(4);
+  k_mx_spmv<<<spmv_blocks(c), 128, 0, c->stream>>>(L.g, c->ke0f, L.E32, L.fix, c->f_p,
+                                                   c->f_Ap, c->d_partials, c->d_mx);
+  k_mx_update<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_x, c->f_r, c->f_p,
+                                                            c->f_Ap, c->d_partials,
+                                                            c->d_mx);
+  k_mx_flush<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, x, c->f_x, c->d_mx);
+  k_mx_residual<<<spmv_blocks(c), 128, 0, c->stream>>>(L.g, c->ke0, c->d_E, L.fix, b, x,
+                                                       c->f_r, c->d_partials, c->d_mx);
+  enqueue_precondition(c, smooth, 0);
+}
+
+int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
+                double *d_x, icarat_solve_info *info)
+{
+  IREQUIRE(o->rtol >= 0.0, ICARAT_ERR_ARG, "rtol must be non-negative");
+  IREQUIRE(o->refresh >= 0.0 && o->refresh < 1.0, ICARAT_ERR_ARG,
+           "refresh must be in [0, 1)");
+  const int levels = o->mg_levels > 0 ? o->mg_levels : 4;
+  const int smooth = o->mg_smooth > 0 ? o->mg_smooth : 2;
+  const double delta = o->refresh > 0.0 ? o->refresh : 1.0e-2;
+  const int chunk = o->chunk > 0 ? o->chunk : 4;
+  mg_setup(c, levels);
+  mixed_alloc(c);
+  const int n = c->neq;
+
+  note_launch();
+  k_mx_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
+      n, d_b, d_x, c->f_x, c->f_r, c->d_partials, c->d_mx, o->rtol, delta, o->maxit);
+  ICK(cudaGetLastError());
+  enqueue_precondition(c, smooth, 1);
+  ICK(cudaGetLastError());
+
+  const auto key = std::make_tuple((int)ICARAT_SOLVER_MIXED_IR, levels, smooth, chunk,
+                                   (const void *)d_x);
+  auto it = c->graphs.find(key);
+  cudaGraphExec_t exec = nullptr;
+  if(it == c->graphs.end() || c->graph_b.count(key) == 0 || c->graph_b[key] != d_b)
+  {
+    if(it != c->graphs.end())
+    {
+      cudaGraphExecDestroy(it->second);
+      c->graphs.erase(it);
+    }
+    cudaGraph_t graph;
+    ICK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    set_capturing(true);
+    try
+    {
+      for(int k = 0; k < chunk; k++)
+        enqueue_iteration(c, smooth, d_b, d_x);
+    }
+    catch(...)
+    {
+      set_capturing(false);
+      cudaStreamEndCapture(c->stream, &graph);
+      throw;
+    }
+    set_capturing(false);
+    ICK(cudaStreamEndCapture(c->stream, &graph));
+    size_t nn = 0;
+    ICK(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    ICK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    int kernels = 0;
+    for(auto nd : nodes)
+    {
+      cudaGraphNodeType t;
+      ICK(cudaGraphNodeGetType(nd, &t));
+      kernels += (t == cudaGraphNodeTypeKernel) ? 1 : 0;
+    }
+    ICK(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    c->graphs[key] = exec;
+    c->graph_kernels[key] = kernels;
+    c->graph_b[key] = d_b;
+  }
+  else
+    exec = it->second;
+  const int graph_kernels = c->graph_kernels[key];
+  const long max_chunks = (long)(o->maxit + 1 + chunk - 1) / chunk + 1;
+  for(long ch = 0; ch < max_chunks; ch++)
+  {
+    ICK(cudaMemcpyAsync(c->h_mx, c->d_mx, sizeof(MxScalars), cudaMemcpyDeviceToHost,
+                        c->stream));
+    ICK(cudaStreamSynchronize(c->stream));
+    if(c->h_mx->done)
+      break;
+    ICK(cudaGraphLaunch(exec, c->stream));
+    note_launch(graph_kernels);
+  }
+  ICK(cudaMemcpyAsync(c->h_mx, c->d_mx, sizeof(MxScalars), cudaMemcpyDeviceToHost,
+                      c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
+  const MxScalars &s = *c->h_mx;
+  info->iterations = s.iter;
+  info->rel_residual = s.bb > 0 ? std::sqrt(s.rr_true / s.bb) : 0.0;
+  info->status = s.done ? s.status : ICARAT_WARN_MAXITER;
+  info->refreshes = s.nrefresh;
+  return info->status;
+}
+
+} // namespace icarat_b200

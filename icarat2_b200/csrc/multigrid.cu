@@ -11,15 +11,24 @@
 // of the Jacobi-scaled Ke0 (a rigorous bound for every SIMP design), applied
 // identically before and after the coarse correction so that the V-cycle is
 // a symmetric positive definite preconditioner.  The coarsest level is solved
-// exactly with a dense inverse built on the GPU every time the design
-// changes: blocked Cholesky A = L L^T, W = L^-1, A^-1 = W^T W.
+// exactly: W = L^-1 of the Cholesky factor of its dense matrix is rebuilt on
+// the GPU for every design (dense.cu) and each V-cycle applies W^T W.
+//
+// The V-cycle exists in FP64 (preconditioner of the FP64 solver) and in FP32
+// (inner solver of the mixed-precision solver); the coarsest solve is FP64 in
+// both.
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "stencil.cuh"
 
 namespace icarat_b200
 {
+
+void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n);
+void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
+                     const double *v, double *t, const int *rowmap, double *x);
 
 // ---------------------------------------------------------------- level data
 __global__ void k_coarsen_E(GridDev f, GridDev c, const double *__restrict__ Ef,
@@ -42,28 +51,25 @@ __global__ void k_coarsen_E(GridDev f, GridDev c, const double *__restrict__ Ef,
   }
 }
 
-__global__ void k_coarsen_fix(GridDev f, GridDev c, const uint8_t *__restrict__ ff,
-                              uint8_t *__restrict__ fc)
+template <typename Tin, typename Tout>
+__global__ void k_cast(long n, const Tin *__restrict__ in, Tout *__restrict__ out)
 {
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.numnp;
-      n += gridDim.x * blockDim.x)
-  {
-    const int I = n % c.NX, J = (n / c.NX) % c.NY, K = n / (c.NX * c.NY);
-    fc[n] = ff[2 * I + (long)2 * J * f.NX + (long)2 * K * f.NX * f.NY];
-  }
+  for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+      i += (long)gridDim.x * blockDim.x)
+    out[i] = (Tout)in[i];
 }
 
 // ---------------------------------------------------------------- transfers
 // coarse b = R r  (R = P^T, 27 fine nodes per coarse node, weights 1/2^d)
-__global__ void k_restrict(GridDev f, GridDev c, const double *__restrict__ rf,
-                           const uint8_t *__restrict__ fixc,
-                           double *__restrict__ bc)
+template <typename T>
+__global__ void k_restrict(GridDev f, GridDev c, const T *__restrict__ rf,
+                           const uint8_t *__restrict__ fixc, T *__restrict__ bc)
 {
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.numnp;
       n += gridDim.x * blockDim.x)
   {
     const int I = n % c.NX, J = (n / c.NX) % c.NY, K = n / (c.NX * c.NY);
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    T s0 = 0, s1 = 0, s2 = 0;
 #pragma unroll
     for(int dz = -1; dz <= 1; dz++)
 #pragma unroll
@@ -74,23 +80,23 @@ __global__ void k_restrict(GridDev f, GridDev c, const double *__restrict__ rf,
           const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
           if(i < 0 || i >= f.NX || j < 0 || j >= f.NY || k < 0 || k >= f.NZ)
             continue;
-          const double w = (dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0);
+          const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
           const long m = i + (long)j * f.NX + (long)k * f.NX * f.NY;
           s0 += w * rf[m];
           s1 += w * rf[(long)f.numnp + m];
           s2 += w * rf[2L * f.numnp + m];
         }
     const unsigned fx = fixc[n];
-    bc[n] = (fx & 1u) ? 0.0 : s0;
-    bc[(long)c.numnp + n] = (fx & 2u) ? 0.0 : s1;
-    bc[2L * c.numnp + n] = (fx & 4u) ? 0.0 : s2;
+    bc[n] = (fx & 1u) ? T(0) : s0;
+    bc[(long)c.numnp + n] = (fx & 2u) ? T(0) : s1;
+    bc[2L * c.numnp + n] = (fx & 4u) ? T(0) : s2;
   }
 }
 
 // fine x += P xc (masked)
-__global__ void k_prolong_add(GridDev f, GridDev c, const double *__restrict__ xc,
-                              const uint8_t *__restrict__ fixf,
-                              double *__restrict__ xf)
+template <typename T>
+__global__ void k_prolong_add(GridDev f, GridDev c, const T *__restrict__ xc,
+                              const uint8_t *__restrict__ fixf, T *__restrict__ xf)
 {
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < f.numnp;
       n += gridDim.x * blockDim.x)
@@ -98,9 +104,9 @@ __global__ void k_prolong_add(GridDev f, GridDev c, const double *__restrict__ x
     const int i = n % f.NX, j = (n / f.NX) % f.NY, k = n / (f.NX * f.NY);
     const int I0 = i >> 1, J0 = j >> 1, K0 = k >> 1;
     const int I1 = I0 + (i & 1), J1 = J0 + (j & 1), K1 = K0 + (k & 1);
-    const double wx = (i & 1) ? 0.5 : 1.0, wy = (j & 1) ? 0.5 : 1.0,
-                 wz = (k & 1) ? 0.5 : 1.0;
-    double s[3] = {0.0, 0.0, 0.0};
+    const T wx = (i & 1) ? T(0.5) : T(1), wy = (j & 1) ? T(0.5) : T(1),
+            wz = (k & 1) ? T(0.5) : T(1);
+    T s[3] = {0, 0, 0};
 #pragma unroll
     for(int cz = 0; cz < 2; cz++)
 #pragma unroll
@@ -114,7 +120,7 @@ __global__ void k_prolong_add(GridDev f, GridDev c, const double *__restrict__ x
             continue;
           const int I = cx ? I1 : I0, J = cy ? J1 : J0, K = cz ? K1 : K0;
           const long m = I + (long)J * c.NX + (long)K * c.NX * c.NY;
-          const double w = wx * wy * wz;
+          const T w = wx * wy * wz;
           s[0] += w * xc[m];
           s[1] += w * xc[(long)c.numnp + m];
           s[2] += w * xc[2L * c.numnp + m];
@@ -129,14 +135,14 @@ __global__ void k_prolong_add(GridDev f, GridDev c, const double *__restrict__ x
 
 // ---------------------------------------------------------------- smoother
 // First Chebyshev step from x = 0: d = invd b / theta, x = d.
-__global__ void k_cheb_first(int n, const double *__restrict__ b,
-                             const double *__restrict__ invd, double inv_theta,
-                             double *__restrict__ x, double *__restrict__ d)
+template <typename T>
+__global__ void k_cheb_first(int n, const T *__restrict__ b, const T *__restrict__ invd,
+                             T inv_theta, T *__restrict__ x, T *__restrict__ d)
 {
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
       i += gridDim.x * blockDim.x)
   {
-    const double di = inv_theta * invd[i] * b[i];
+    const T di = inv_theta * invd[i] * b[i];
     d[i] = di;
     x[i] = di;
   }
@@ -144,29 +150,48 @@ __global__ void k_cheb_first(int n, const double *__restrict__ b,
 
 // One Chebyshev step: r = b - K x, d = c1 d + c2 invd r, xo = x + d.
 // x and xo are distinct buffers (neighbours of x are read by other threads).
+template <typename T, typename KP>
 __global__ void __launch_bounds__(128)
-    k_cheb_step(GridDev g, KeParam ke, const double *__restrict__ E,
-                const uint8_t *__restrict__ fix, const double *__restrict__ invd,
-                const double *__restrict__ b, const double *__restrict__ x,
-                double *__restrict__ d, double *__restrict__ xo, double c1,
-                double c2)
+    k_cheb_step(GridDev g, KP ke, const T *__restrict__ E, const uint8_t *__restrict__ fix,
+                const T *__restrict__ invd, const T *__restrict__ b,
+                const T *__restrict__ x, T *__restrict__ d, T *__restrict__ xo, T c1,
+                T c2)
 {
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
       n += gridDim.x * blockDim.x)
   {
-    double acc[3], uc[3];
+    T acc[3], uc[3];
     node_Ku(g, ke, E, x, n, acc, uc);
     const unsigned f = fix[n];
 #pragma unroll
     for(int q = 0; q < 3; q++)
     {
       const long id = (long)q * g.numnp + n;
-      double dn = 0.0;
+      T dn = 0;
       if(!((f >> q) & 1u))
-        dn = (c1 != 0.0 ? c1 * d[id] : 0.0) + c2 * invd[id] * (b[id] - acc[q]);
+        dn = (c1 != T(0) ? c1 * d[id] : T(0)) + c2 * invd[id] * (b[id] - acc[q]);
       d[id] = dn;
       xo[id] = uc[q] + dn;
     }
+  }
+}
+
+// r = b - K x (constrained rows 0)
+template <typename T, typename KP>
+__global__ void __launch_bounds__(128)
+    k_mg_residual(GridDev g, KP ke, const T *__restrict__ E,
+                  const uint8_t *__restrict__ fix, const T *__restrict__ b,
+                  const T *__restrict__ x, T *__restrict__ r)
+{
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    T acc[3], uc[3];
+    node_Ku(g, ke, E, x, n, acc, uc);
+    const unsigned f = fix[n];
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+      r[(long)c * g.numnp + n] = ((f >> c) & 1u) ? T(0) : b[(long)c * g.numnp + n] - acc[c];
   }
 }
 
@@ -181,7 +206,7 @@ __global__ void k_coarse_assemble(GridDev g, KeParam ke, const double *__restric
       r += gridDim.x * blockDim.x)
   {
     double *row = A + (long)r * nfree; // zeroed by the caller
-    const int full = rowmap[r]; // component-major index c * numnp + n
+    const int full = rowmap[r];        // component-major index c * numnp + n
     const int n = full % g.numnp, c = full / g.numnp;
     const int i = n % g.NX, j = (n / g.NX) % g.NY, k = n / (g.NX * g.NY);
     for(int sz = 0; sz < 2; sz++)
@@ -211,16 +236,15 @@ __global__ void k_coarse_assemble(GridDev g, KeParam ke, const double *__restric
   }
 }
 
-
-// Coarse solve: x_full = scatter(Ainv gather(b_full)); one warp per row.
+// free coarse components of b (any precision) into the dense solve's vector
+template <typename T>
 __global__ void k_coarse_gather(int nfree, const int *__restrict__ rowmap,
-                                const double *__restrict__ b, double *__restrict__ v)
+                                const T *__restrict__ b, double *__restrict__ v)
 {
   for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree;
       r += gridDim.x * blockDim.x)
-    v[r] = b[rowmap[r]];
+    v[r] = (double)b[rowmap[r]];
 }
-
 
 // ---------------------------------------------------------------- driver
 static GridDev make_grid(int nx, int ny, int nz)
@@ -229,28 +253,50 @@ static GridDev make_grid(int nx, int ny, int nz)
                  nx * ny * nz};
 }
 
-static int blocks_for(int n, int t)
+static int blocks_for(long n, int t)
 {
-  int b = (n + t - 1) / t;
-  return b < 1 ? 1 : b;
+  long b = (n + t - 1) / t;
+  return b < 1 ? 1 : (b > 65535L * 16 ? 65535 * 16 : (int)b);
 }
+
+// level buffers of one precision
+template <typename T> struct LevelBuf;
+template <> struct LevelBuf<double>
+{
+  static double *E(MgLevel &L) { return L.E; }
+  static double *invd(MgLevel &L) { return L.invd; }
+  static double *x(MgLevel &L) { return L.x; }
+  static double *b(MgLevel &L) { return L.b; }
+  static double *r(MgLevel &L) { return L.r; }
+  static double *t(MgLevel &L) { return L.t; }
+  static const KeParam &ke(icarat_ctx *c) { return c->ke0; }
+};
+template <> struct LevelBuf<float>
+{
+  static float *E(MgLevel &L) { return L.E32; }
+  static float *invd(MgLevel &L) { return L.invd32; }
+  static float *x(MgLevel &L) { return L.x32; }
+  static float *b(MgLevel &L) { return L.b32; }
+  static float *r(MgLevel &L) { return L.r32; }
+  static float *t(MgLevel &L) { return L.t32; }
+  static const KeParamF &ke(icarat_ctx *c) { return c->ke0f; }
+};
 
 void mg_free(icarat_ctx *c)
 {
-  for(size_t l = 1; l < c->mg.size(); l++)
-  {
-    MgLevel &L = c->mg[l];
-    dfree(L.E);
-    dfree(L.fix);
-    dfree(L.invd);
-  }
   for(size_t l = 0; l < c->mg.size(); l++)
   {
     MgLevel &L = c->mg[l];
-    dfree(L.x);
-    dfree(L.b);
-    dfree(L.r);
-    dfree(L.t);
+    if(l > 0)
+    {
+      dfree(L.E);
+      dfree(L.fix);
+      dfree(L.invd);
+    }
+    for(void *p : {(void *)L.x, (void *)L.b, (void *)L.r, (void *)L.t, (void *)L.E32,
+                   (void *)L.invd32, (void *)L.x32, (void *)L.b32, (void *)L.r32,
+                   (void *)L.t32})
+      dfree(p);
   }
   c->mg.clear();
   if(c->coarse.setup)
@@ -263,6 +309,15 @@ void mg_free(icarat_ctx *c)
   dfree(c->coarse.vout);
   c->coarse = CoarseSolver{};
   c->mg_built_levels = 0;
+}
+
+static float *falloc(size_t n)
+{
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, (n ? n : 1) * sizeof(float));
+  if(e != cudaSuccess)
+    throw Error{ICARAT_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+  return static_cast<float *>(p);
 }
 
 static void allocate_levels(icarat_ctx *c, int levels)
@@ -299,6 +354,12 @@ static void allocate_levels(icarat_ctx *c, int levels)
     L.b = dalloc(nv);
     L.r = dalloc(nv);
     L.t = dalloc(nv);
+    L.E32 = falloc(L.g.nelx);
+    L.invd32 = falloc(nv);
+    L.x32 = falloc(nv);
+    L.b32 = falloc(nv);
+    L.r32 = falloc(nv);
+    L.t32 = falloc(nv);
     c->mg.push_back(L);
   }
   // coarse constraint pattern on the host (fixed for the context)
@@ -325,10 +386,10 @@ static void allocate_levels(icarat_ctx *c, int levels)
       if(!((fix[n] >> q) & 1u))
       {
         colmap[3 * (size_t)n + q] = (int)rowmap.size(); // node-major lookup table
-        rowmap.push_back(q * gc.numnp + n);               // component-major vector index
+        rowmap.push_back(q * gc.numnp + n);             // component-major vector index
       }
   const int nf = (int)rowmap.size();
-  IREQUIRE((double)nf * nf * 8.0 * 2 < 4.0e9, ICARAT_ERR_UNSUPPORTED,
+  IREQUIRE((double)nf * nf * 8.0 * 3 < 6.0e9, ICARAT_ERR_UNSUPPORTED,
            "coarsest multigrid level too large for the dense solve; add levels");
   c->coarse.n = nf;
   ICK(cudaMalloc(&c->coarse.map, sizeof(int) * (rowmap.size() + colmap.size() + 1)));
@@ -345,12 +406,9 @@ static void allocate_levels(icarat_ctx *c, int levels)
   c->mg_built_levels = levels;
 }
 
-void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n);
-void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
-                     const double *v, double *t, const int *rowmap, double *x);
-
-// Everything that depends on the design: coarse moduli, Jacobi diagonals, the
-// dense coarsest matrix and W = L^-1 of its Cholesky factor.
+// Everything that depends on the design: coarse moduli, Jacobi diagonals (and
+// their FP32 copies), the dense coarsest matrix and W = L^-1 of its Cholesky
+// factor.
 static void enqueue_mg_setup(icarat_ctx *c, int levels)
 {
   for(int l = 0; l < levels; l++)
@@ -363,8 +421,11 @@ static void enqueue_mg_setup(icarat_ctx *c, int levels)
       k_coarsen_E<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>(F.g, L.g, F.E, L.E);
     }
     launch_diag(c, L.g, L.E, L.fix, L.invd);
+    note_launch(2);
+    k_cast<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>((long)L.g.nelx, L.E, L.E32);
+    k_cast<<<blocks_for(3L * L.g.numnp, 256), 256, 0, c->stream>>>(3L * L.g.numnp, L.invd,
+                                                                   L.invd32);
   }
-  // dense coarsest system -> inverse
   const MgLevel &C = c->mg[levels - 1];
   const int n = c->coarse.n;
   if(n > 0)
@@ -426,9 +487,10 @@ void mg_setup(icarat_ctx *c, int levels)
 
 // Chebyshev smoothing of K x = b on one level, deg steps.  from_zero: x = 0
 // on entry (the first step needs no product).
-static void smooth(icarat_ctx *c, MgLevel &L, const double *b, int deg,
-                   bool from_zero)
+template <typename T>
+static void smooth(icarat_ctx *c, MgLevel &L, const T *b, int deg, bool from_zero)
 {
+  using B = LevelBuf<T>;
   const double lmax = c->lam_max_dk;
   const double lmin = 0.1 * lmax;
   const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
@@ -436,21 +498,21 @@ static void smooth(icarat_ctx *c, MgLevel &L, const double *b, int deg,
   double rho_old = 1.0 / sigma;
   const int nv = 3 * L.g.numnp;
   const int nb = blocks_for(L.g.numnp, 128);
-  double *x = L.x, *xo = L.t, *d = L.r;
+  T *x = B::x(L), *xo = B::t(L), *d = B::r(L);
   int k0 = 0;
   if(from_zero)
   {
     note_launch();
-    k_cheb_first<<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, L.invd,
-                                                             1.0 / theta, x, d);
+    k_cheb_first<<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, B::invd(L),
+                                                             T(1.0 / theta), x, d);
     k0 = 1;
   }
   else
   {
     // first step from the current x: d = invd (b - K x) / theta
     note_launch();
-    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, c->ke0, L.E, L.fix, L.invd, b, x,
-                                           d, xo, 0.0, 1.0 / theta);
+    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, B::ke(c), B::E(L), L.fix, B::invd(L), b,
+                                           x, d, xo, T(0), T(1.0 / theta));
     std::swap(x, xo);
     k0 = 1;
   }
@@ -458,18 +520,19 @@ static void smooth(icarat_ctx *c, MgLevel &L, const double *b, int deg,
   {
     const double rho = 1.0 / (2.0 * sigma - rho_old);
     note_launch();
-    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, c->ke0, L.E, L.fix, L.invd, b, x,
-                                           d, xo, rho * rho_old, 2.0 * rho / delta);
+    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, B::ke(c), B::E(L), L.fix, B::invd(L), b,
+                                           x, d, xo, T(rho * rho_old),
+                                           T(2.0 * rho / delta));
     std::swap(x, xo);
     rho_old = rho;
   }
-  if(x != L.x)
-    ICK(cudaMemcpyAsync(L.x, x, sizeof(double) * nv, cudaMemcpyDeviceToDevice,
-                        c->stream));
+  if(x != B::x(L))
+    ICK(cudaMemcpyAsync(B::x(L), x, sizeof(T) * nv, cudaMemcpyDeviceToDevice, c->stream));
 }
 
-static void vcycle(icarat_ctx *c, int l, const double *b, int deg)
+template <typename T> static void vcycle(icarat_ctx *c, int l, const T *b, int deg)
 {
+  using B = LevelBuf<T>;
   MgLevel &L = c->mg[l];
   const int levels = (int)c->mg.size();
   if(l == levels - 1)
@@ -484,27 +547,43 @@ static void vcycle(icarat_ctx *c, int l, const double *b, int deg)
       dense_spd_solve(c->stream, c->coarse.W, c->coarse.work, n, c->coarse.vin,
                       c->coarse.vout, c->coarse.map, L.x);
     }
+    if(!std::is_same<T, double>::value)
+    {
+      note_launch();
+      k_cast<<<blocks_for(3L * L.g.numnp, 256), 256, 0, c->stream>>>(3L * L.g.numnp, L.x,
+                                                                     B::x(L));
+    }
     return;
   }
   MgLevel &C = c->mg[l + 1];
-  smooth(c, L, b, deg, true);
-  // residual into L.r (smooth() used L.r as scratch; done with it now)
-  launch_residual(c, L.g, L.E, L.fix, b, L.x, L.r);
+  smooth<T>(c, L, b, deg, true);
+  // residual into r (smooth() used r as scratch; done with it now)
   note_launch();
-  k_restrict<<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, L.r, C.fix,
-                                                                C.b);
-  vcycle(c, l + 1, C.b, deg);
+  k_mg_residual<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(
+      L.g, B::ke(c), B::E(L), L.fix, b, B::x(L), B::r(L));
   note_launch();
-  k_prolong_add<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, C.x,
-                                                                   L.fix, L.x);
-  smooth(c, L, b, deg, false);
+  k_restrict<<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, B::r(L), C.fix,
+                                                                B::b(C));
+  vcycle<T>(c, l + 1, B::b(C), deg);
+  note_launch();
+  k_prolong_add<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, B::x(C),
+                                                                   L.fix, B::x(L));
+  smooth<T>(c, L, b, deg, false);
 }
 
 void mg_vcycle(icarat_ctx *c, const double *r, double *z, int deg)
 {
-  vcycle(c, 0, r, deg);
-  ICK(cudaMemcpyAsync(z, c->mg[0].x, sizeof(double) * c->neq,
-                      cudaMemcpyDeviceToDevice, c->stream));
+  vcycle<double>(c, 0, r, deg);
+  ICK(cudaMemcpyAsync(z, c->mg[0].x, sizeof(double) * c->neq, cudaMemcpyDeviceToDevice,
+                      c->stream));
+  ICK(cudaGetLastError());
+}
+
+void mg_vcycle_f32(icarat_ctx *c, const float *r, float *z, int deg)
+{
+  vcycle<float>(c, 0, r, deg);
+  ICK(cudaMemcpyAsync(z, c->mg[0].x32, sizeof(float) * c->neq, cudaMemcpyDeviceToDevice,
+                      c->stream));
   ICK(cudaGetLastError());
 }
 

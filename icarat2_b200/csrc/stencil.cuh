@@ -1,16 +1,26 @@
-// Per-node FP64 stiffness stencil shared by the operator kernels.
+// Per-node stiffness stencil shared by the operator kernels (FP64 and FP32).
 //
 // (K u)_n = sum_{e containing n} E_e Ke0[rows of n in e] u_e, evaluated by
 // node ownership: the thread of node n gathers the 27 nodal displacements
 // around it and the moduli of its (up to) 8 elements, so no two threads
 // write the same output and no atomics or colouring are needed.  Ke0 is a
-// by-value kernel parameter; after full unrolling every coefficient is a
-// constant-bank operand of a DFMA (576 per node).
+// by-value kernel parameter (constant bank).
 #pragma once
 #include "internal.cuh"
 
 namespace icarat_b200
 {
+
+// element matrix of the value type T (the FP32 copy is rounded from FP64)
+template <typename T> struct KeOf;
+template <> struct KeOf<double>
+{
+  using type = KeParam;
+};
+template <> struct KeOf<float>
+{
+  using type = KeParamF;
+};
 
 // local node number of the corner (lx, ly, lz) of a hexa8
 // (mesh_icarat.hpp:489-509 order)
@@ -28,18 +38,16 @@ __host__ __device__ constexpr int local_node(int lx, int ly, int lz)
 // axis), K^_beta = Ke0[local node 0][local node beta] and S_a =
 // diag((-1)^a_x, (-1)^a_y, (-1)^a_z).  The loop therefore runs over the 8
 // canonical blocks: each block's 9 coefficients are read once and serve the 4
-// elements of the layer (the signs are free DFMA operand negations), and the
+// elements of the layer (the signs are free FMA operand negations), and the
 // 12 partial sums t[element][row] are independent accumulation chains.
-template <int SZ>
-__device__ __forceinline__ void layer_contrib(const KeParam &ke,
-                                              const double (&ul)[2][9][3],
-                                              const double (&Ev)[4],
-                                              double (&acc)[3])
+template <int SZ, typename T, typename KP>
+__device__ __forceinline__ void layer_contrib(const KP &ke, const T (&ul)[2][9][3],
+                                              const T (&Ev)[4], T (&acc)[3])
 {
-  double t[4][3];
+  T t[4][3];
 #pragma unroll
   for(int e = 0; e < 4; e++)
-    t[e][0] = t[e][1] = t[e][2] = 0.0;
+    t[e][0] = t[e][1] = t[e][2] = T(0);
 #pragma unroll
   for(int bz = 0; bz < 2; bz++)
 #pragma unroll
@@ -48,7 +56,7 @@ __device__ __forceinline__ void layer_contrib(const KeParam &ke,
       for(int bx = 0; bx < 2; bx++)
       {
         const int lb = local_node(bx, by, bz);
-        double kb[9];
+        T kb[9];
 #pragma unroll
         for(int c = 0; c < 3; c++)
 #pragma unroll
@@ -73,7 +81,7 @@ __device__ __forceinline__ void layer_contrib(const KeParam &ke,
               for(int d = 0; d < 3; d++)
               {
                 const bool neg = (c != d) && ((ac[c] + ac[d]) & 1);
-                const double k = neg ? -kb[3 * c + d] : kb[3 * c + d];
+                const T k = neg ? -kb[3 * c + d] : kb[3 * c + d];
                 t[e][c] = fma(k, ul[l][s][d], t[e][c]);
               }
           }
@@ -85,9 +93,9 @@ __device__ __forceinline__ void layer_contrib(const KeParam &ke,
       acc[c] = fma(Ev[e], t[e][c], acc[c]);
 }
 
-__device__ __forceinline__ void load_layer(const double *__restrict__ u,
-                                           const GridDev &g, int i, int j,
-                                           int kk, double (&L)[9][3])
+template <typename T>
+__device__ __forceinline__ void load_layer(const T *__restrict__ u, const GridDev &g,
+                                           int i, int j, int kk, T (&L)[9][3])
 {
   const bool kin = kk >= 0 && kk < g.NZ;
 #pragma unroll
@@ -101,31 +109,32 @@ __device__ __forceinline__ void load_layer(const double *__restrict__ u,
       const int s = (dy + 1) * 3 + (dx + 1);
 #pragma unroll
       for(int d = 0; d < 3; d++)
-        L[s][d] = in ? __ldg(u + (long)d * g.numnp + m) : 0.0;
+        L[s][d] = in ? __ldg(u + (long)d * g.numnp + m) : T(0);
     }
 }
 
-__device__ __forceinline__ double load_E(const double *__restrict__ E,
-                                         const GridDev &g, int ei, int ej,
-                                         int ek)
+template <typename T>
+__device__ __forceinline__ T load_E(const T *__restrict__ E, const GridDev &g, int ei,
+                                    int ej, int ek)
 {
   const bool in = ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny && ek >= 0 &&
                   ek < g.nz;
-  return in ? __ldg(E + ei + (long)ej * g.nx + (long)ek * g.nx * g.ny) : 0.0;
+  return in ? __ldg(E + ei + (long)ej * g.nx + (long)ek * g.nx * g.ny) : T(0);
 }
 
 // (K u) at node n (unmasked) and the node's own displacement uc.
-__device__ __forceinline__ void node_Ku(const GridDev &g, const KeParam &ke,
-                                        const double *__restrict__ E,
-                                        const double *__restrict__ u, int n,
-                                        double (&acc)[3], double (&uc)[3])
+template <typename T, typename KP>
+__device__ __forceinline__ void node_Ku(const GridDev &g, const KP &ke,
+                                        const T *__restrict__ E,
+                                        const T *__restrict__ u, int n, T (&acc)[3],
+                                        T (&uc)[3])
 {
   const int i = n % g.NX;
   const int j = (n / g.NX) % g.NY;
   const int k = n / (g.NX * g.NY);
-  acc[0] = acc[1] = acc[2] = 0.0;
-  double ul[2][9][3];
-  double Ev[4];
+  acc[0] = acc[1] = acc[2] = T(0);
+  T ul[2][9][3];
+  T Ev[4];
   // elements below the node: node layers k-1 (bz = 0) and k (bz = 1)
   load_layer(u, g, i, j, k - 1, ul[0]);
   load_layer(u, g, i, j, k, ul[1]);

@@ -92,12 +92,15 @@ class LinearAnalysis
 {
 public:
   explicit LinearAnalysis(Model &m) : m_(m), val(m.numeq) {}
-  // solvName: "Eigen_CG" / "Scaling_CG" (Jacobi-PCG) or "MG_CG" (multigrid)
+  // solvName: "Eigen_CG" / "Scaling_CG" (Jacobi-PCG), "MG_CG" (multigrid) or
+  // "Mixed_MG_CG" (FP32 multigrid-PCG refined by FP64 residuals)
   void solve(const std::string &solvName, bool log)
   {
-    icarat_solve_opts o{ICARAT_SOLVER_JACOBI_PCG, tol, maxIter, mg_levels, mg_smooth, 0};
+    icarat_solve_opts o{ICARAT_SOLVER_JACOBI_PCG, tol, maxIter, mg_levels, mg_smooth, 0, 0.0};
     if(solvName == "MG_CG")
       o.method = ICARAT_SOLVER_MG_PCG;
+    else if(solvName == "Mixed_MG_CG")
+      o.method = ICARAT_SOLVER_MIXED_IR;
     else if(solvName != "Eigen_CG" && solvName != "Scaling_CG")
       throw Error(ICARAT_ERR_UNSUPPORTED, "Solver type name is wrong: " + solvName);
     check(icarat_solve(m_.ctx(), &o, val.data(), &info), "LinearAnalysis::solve");

@@ -24,6 +24,7 @@ extern "C" {
 
 #define ICARAT_OK 0
 #define ICARAT_WARN_MAXITER 1    /* iterative loop stopped at its cap */
+#define ICARAT_WARN_STAGNATION 2 /* MIXED_IR: FP64 residual stopped falling */
 #define ICARAT_ERR_ARG -1        /* bad argument / size */
 #define ICARAT_ERR_CUDA -2       /* CUDA runtime error */
 #define ICARAT_ERR_NAN -4        /* non-finite value met in a reduction */
@@ -80,7 +81,9 @@ typedef struct
 enum
 {
   ICARAT_SOLVER_JACOBI_PCG = 0, /* "Eigen_CG" / "Scaling_CG" semantics */
-  ICARAT_SOLVER_MG_PCG = 1      /* geometric multigrid preconditioned CG */
+  ICARAT_SOLVER_MG_PCG = 1,     /* geometric multigrid preconditioned CG */
+  ICARAT_SOLVER_MIXED_IR = 2    /* FP32 multigrid-PCG iterations refined by FP64
+                                   residuals (no reference counterpart) */
 };
 
 typedef struct
@@ -88,16 +91,19 @@ typedef struct
   int method;    /* ICARAT_SOLVER_* */
   double rtol;   /* stop when ||r|| < rtol ||b||  (solvers.hpp:89: 1e-10) */
   int maxit;     /* iteration cap (solvers.hpp:90: 10000) */
-  int mg_levels; /* multigrid levels incl. the finest (MG_PCG) */
-  int mg_smooth; /* smoothing sweeps per level and direction (MG_PCG) */
+  int mg_levels; /* multigrid levels incl. the finest (MG_PCG, MIXED_IR) */
+  int mg_smooth; /* smoothing sweeps per level and direction (MG_PCG, MIXED_IR) */
   int chunk;     /* iterations per host convergence check (0 = default) */
+  double refresh; /* MIXED_IR: recompute the residual in FP64 once the FP32
+                     recurrence has fallen by this factor (0 = 1e-2) */
 } icarat_solve_opts;
 
 typedef struct
 {
   int iterations;
-  double rel_residual;
+  double rel_residual; /* MIXED_IR: of the last FP64 residual */
   int status;
+  int refreshes;       /* MIXED_IR: FP64 residual evaluations */
 } icarat_solve_info;
 
 /* OC::UpdateVariables parameters (OCSolver.hpp:73-79) and the volume functor
