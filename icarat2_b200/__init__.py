@@ -37,6 +37,11 @@ JACOBI_PCG = 0
 MG_PCG = 1
 MIXED_IR = 2
 
+OP_FP64 = 0
+OP_FP32 = 1
+OP_TC_BF16X3 = 2
+OP_TC_BF16 = 3
+
 
 class IcaratError(RuntimeError):
     def __init__(self, status, msg):
@@ -71,7 +76,7 @@ class BC(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int),
                 ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int),
-                ("refresh", C.c_double)]
+                ("refresh", C.c_double), ("fine_op", C.c_int), ("krylov_op", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -149,6 +154,8 @@ SIGNATURES = {
     "icarat_solve_noalloc": (_i, [_vp, _P(SolveOpts), _vp, _vp, _P(SolveInfo)]),
     "icarat_kernel_launches": (_i, [_P(C.c_ulonglong)]),
     "icarat_time_operator": (_i, [_vp, _i, _P(_d)]),
+    "icarat_apply_K_op": (_i, [_vp, _i, _dp, _dp]),
+    "icarat_time_operator_op": (_i, [_vp, _i, _i, _P(_d)]),
     "icarat_loop_init": (_i, [_vp, _P(LoopOpts), _dp]),
     "icarat_loop_step": (_i, [_vp, _P(StepInfo)]),
     "icarat_loop_get": (_i, [_vp, _i, _dp]),
@@ -205,8 +212,9 @@ def cantilever_bc(nx, ny, nz, lx=None, ly=None, lz=None, load_node=None, load=(0
 
 
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
-               chunk=0, refresh=0.0):
-    return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh)
+               chunk=0, refresh=0.0, fine_op=0, krylov_op=0):
+    return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,
+                     krylov_op)
 
 
 class Context:
@@ -394,10 +402,17 @@ class Context:
                      xmax, filter_radius, solve if solve is not None else solve_opts())
         _check(self.lib.icarat_loop_init(self.h, C.byref(o), _f64(x0)), "loop_init")
 
-    def time_operator(self, reps=20):
+    def time_operator(self, reps=20, op=OP_FP64):
         ms = C.c_double()
-        _check(self.lib.icarat_time_operator(self.h, reps, C.byref(ms)), "time_operator")
+        _check(self.lib.icarat_time_operator_op(self.h, op, reps, C.byref(ms)),
+               "time_operator")
         return ms.value
+
+    def apply_K_op(self, u, op):
+        """y = K u with operator `op` (OP_FP64, OP_FP32, OP_TC_BF16X3, OP_TC_BF16)."""
+        y = np.zeros(max(self.numeq, 1))
+        _check(self.lib.icarat_apply_K_op(self.h, op, _f64(u), y), "apply_K_op")
+        return y[:self.numeq]
 
     def loop_step(self):
         info = StepInfo()

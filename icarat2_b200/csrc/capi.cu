@@ -250,6 +250,69 @@ int icarat_apply_K_dev(icarat_ctx *c, const double *u, double *y)
   ICARAT_API_END
 }
 
+static void check_tc_err(icarat_ctx *c)
+{
+  int err = 0;
+  ICK(cudaMemcpy(&err, c->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if(err)
+  {
+    ICK(cudaMemset(c->d_tc_err, 0, sizeof(int)));
+    throw Error{ICARAT_ERR_CUDA, "tensor-core operator: a bounded wait expired"};
+  }
+}
+
+int icarat_apply_K_op(icarat_ctx *c, int op, const double *u, double *y)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(op >= ICARAT_OP_FP64 && op <= ICARAT_OP_TC_BF16, ICARAT_ERR_ARG,
+           "unknown operator");
+  if(op == ICARAT_OP_FP64)
+    return apply_K_impl(c, u, y, true);
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  IREQUIRE(u && y, ICARAT_ERR_ARG, "null argument");
+  mixed_alloc(c);
+  to_full(c, u, c->d_v1, true);
+  round_f32(c, c->neq, c->d_v1, c->f_p);
+  apply_K_lowp(c, op, c->f_p, c->f_Ap);
+  widen_f64(c, c->neq, c->f_Ap, c->d_Ap);
+  from_full(c, c->d_Ap, y, true);
+  check_tc_err(c);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_time_operator_op(icarat_ctx *c, int op, int reps, double *ms_per_launch)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(op >= ICARAT_OP_FP64 && op <= ICARAT_OP_TC_BF16, ICARAT_ERR_ARG,
+           "unknown operator");
+  if(op == ICARAT_OP_FP64)
+    return icarat_time_operator(c, reps, ms_per_launch);
+  IREQUIRE(reps > 0 && ms_per_launch, ICARAT_ERR_ARG, "bad argument");
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  mixed_alloc(c);
+  round_f32(c, c->neq, c->d_u, c->f_p);
+  cudaEvent_t a, b;
+  ICK(cudaEventCreate(&a));
+  ICK(cudaEventCreate(&b));
+  apply_K_lowp(c, op, c->f_p, c->f_Ap); // warm-up
+  ICK(cudaEventRecord(a, c->stream));
+  for(int r = 0; r < reps; r++)
+    apply_K_lowp(c, op, c->f_p, c->f_Ap);
+  ICK(cudaEventRecord(b, c->stream));
+  ICK(cudaEventSynchronize(b));
+  float ms = 0.f;
+  ICK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms_per_launch = (double)ms / reps;
+  check_tc_err(c);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
 int icarat_solve(icarat_ctx *c, const icarat_solve_opts *opts, double *val,
                  icarat_solve_info *info)
 {

@@ -46,14 +46,18 @@ __global__ void k_gather_free(int numeq, const int *__restrict__ free_idx,
 }
 
 // SIMP (src/problem/elasticity.hpp:13-17)
+// (E32: the same moduli rounded to FP32 for the reduced-precision operators)
 __global__ void k_simp(int n, const double *__restrict__ rho, double e1,
-                       double e2, double p, double *__restrict__ E)
+                       double e2, double p, double *__restrict__ E,
+                       float *__restrict__ E32)
 {
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
       i += gridDim.x * blockDim.x)
   {
     double rp = pow(rho[i], p);
-    E[i] = (1.0 - rp) * e1 + rp * e2;
+    const double e = (1.0 - rp) * e1 + rp * e2;
+    E[i] = e;
+    E32[i] = (float)e;
   }
 }
 
@@ -61,6 +65,23 @@ static int grid_for(int n, int threads = 256)
 {
   int b = (n + threads - 1) / threads;
   return b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b);
+}
+
+// FP32 -> BF16 bits, round to nearest even (finite inputs)
+static uint16_t bf16_round(float f)
+{
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+static float bf16_value(uint16_t h)
+{
+  const uint32_t u = (uint32_t)h << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
 }
 
 void to_full(icarat_ctx *c, const double *in, double *full_out, bool host_src)
@@ -108,7 +129,7 @@ void set_design_device(icarat_ctx *c, const double *d_rho)
   note_launch();
   k_simp<<<grid_for(c->nelx), 256, 0, c->stream>>>(
       c->nelx, c->d_rho, c->mat.young_min, c->mat.young_max, c->mat.penalty,
-      c->d_E);
+      c->d_E, c->d_E32);
   ICK(cudaGetLastError());
   c->design_set = true;
   c->solved = false;
@@ -274,6 +295,24 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     build_mesh_bc(c, bc);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    c->sm_count = sms;
+    {
+      // Ke0 = hi + lo in BF16 (round to nearest even), zero-padded to 32 x 32
+      std::vector<uint16_t> keb(2 * 32 * 32, 0);
+      for(int n = 0; n < 24; n++)
+        for(int k = 0; k < 24; k++)
+        {
+          const double v = c->ke0.k[n * 24 + k];
+          const uint16_t hi = bf16_round((float)v);
+          keb[n * 32 + k] = hi;
+          keb[1024 + n * 32 + k] = bf16_round((float)(v - (double)bf16_value(hi)));
+        }
+      ICK(cudaMalloc(&c->d_keb, sizeof(uint16_t) * keb.size()));
+      ICK(cudaMemcpy(c->d_keb, keb.data(), sizeof(uint16_t) * keb.size(),
+                     cudaMemcpyHostToDevice));
+      ICK(cudaMalloc(&c->d_tc_err, sizeof(int)));
+      ICK(cudaMemset(c->d_tc_err, 0, sizeof(int)));
+    }
     c->red_blocks = sms * 4 > kMaxRedBlocks ? kMaxRedBlocks : sms * 4;
 
     // free-DOF map: equation number -> 3 node + component
@@ -300,6 +339,7 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     c->d_v2 = dalloc(nv);
     c->d_rho = dalloc(c->nelx);
     c->d_E = dalloc(c->nelx);
+    ICK(cudaMalloc(&c->d_E32, sizeof(float) * (c->nelx > 0 ? c->nelx : 1)));
     c->d_e1 = dalloc(c->nelx);
     c->d_e2 = dalloc(c->nelx);
     c->d_partials = dalloc((size_t)kMaxRedBlocks * 8);
@@ -363,6 +403,9 @@ int icarat_ctx_destroy_impl(icarat_ctx *c)
     dfree(p);
   dfree(c->d_counter);
   dfree(c->d_cg);
+  dfree(c->d_keb);
+  dfree(c->d_E32);
+  dfree(c->d_tc_err);
   if(c->h_cg)
     cudaFreeHost(c->h_cg);
   if(c->h_scalar)

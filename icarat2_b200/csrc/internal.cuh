@@ -116,6 +116,32 @@ struct MxScalars
   unsigned int counter;
 };
 
+// Variants of the tensor-core element-by-element operator (tc_stencil.cu).
+enum TcOp
+{
+  TC_APPLY = 0, // y = K u (constrained rows 0)
+  TC_RESID = 1, // y = b - K u (constrained rows 0)
+  TC_CHEB = 2,  // d = c1 d + c2 invd (b - K u), y = u + d
+  TC_DOT = 3    // y = K u, s->pAp = u . y, s->alpha = s->zr / pAp
+};
+
+struct TcArgs
+{
+  GridDev g;
+  const float *E;
+  const uint8_t *fix;
+  const float *u;
+  float *y;
+  const uint16_t *keb = nullptr; // [hi, lo][32][32] BF16 bits, row n, column k
+  int tiles_x = 0, kc = 0;       // tiles along x; node layers per CTA
+  const float *b = nullptr, *invd = nullptr;
+  float *d = nullptr;
+  float c1 = 0.0f, c2 = 0.0f;
+  double *partials = nullptr;
+  MxScalars *s = nullptr;
+  int *err = nullptr;
+};
+
 // Reduction geometry: every grid-stride reduction kernel runs on
 // kRedBlocks blocks of kRedThreads threads so that partial sums are summed
 // in one fixed order (bit-reproducible on a given GPU).
@@ -201,6 +227,7 @@ struct icarat_ctx
   double *d_uD = nullptr;
   double *d_fext = nullptr;
   double *d_rho = nullptr, *d_E = nullptr;
+  float *d_E32 = nullptr; // the moduli rounded to FP32
   double *d_rhs = nullptr, *d_u = nullptr, *d_invd = nullptr;
   double *d_r = nullptr, *d_p = nullptr, *d_z = nullptr, *d_Ap = nullptr;
   double *d_v1 = nullptr, *d_v2 = nullptr; // staging (3 numnp)
@@ -216,6 +243,13 @@ struct icarat_ctx
   // r, preconditioned residual z, direction p and K p
   float *f_x = nullptr, *f_r = nullptr, *f_z = nullptr, *f_p = nullptr, *f_Ap = nullptr;
   icarat_b200::MxScalars *d_mx = nullptr, *h_mx = nullptr;
+  // tensor-core operator: Ke0 split into BF16 hi / lo ([2][32][32], padded)
+  // and the error flag of its bounded waits
+  uint16_t *d_keb = nullptr;
+  int *d_tc_err = nullptr;
+  int sm_count = 148;
+  // operator of the finest level of the FP32 V-cycle (ICARAT_OP_*)
+  int mx_fine_op = ICARAT_OP_FP32;
   bool design_set = false, solved = false;
   icarat_solve_info last_info{};
   // multigrid
@@ -255,6 +289,8 @@ void dfree(void *p);
 void launch_apply_K(icarat_ctx *c, const GridDev &g, const double *E,
                     const uint8_t *fix, const double *u, double *y,
                     double *dot_partials);
+void launch_apply_K_f32(icarat_ctx *c, const GridDev &g, const float *E,
+                        const uint8_t *fix, const float *u, float *y);
 void launch_diag(icarat_ctx *c, const GridDev &g, const double *E,
                  const uint8_t *fix, double *invd);
 void launch_residual(icarat_ctx *c, const GridDev &g, const double *E,
@@ -270,10 +306,19 @@ void release_graphs(icarat_ctx *c);
 int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                double *d_x, icarat_solve_info *info);
 
+// tc_stencil.cu
+void launch_ku_tc(icarat_ctx *c, int op, int terms, TcArgs a, cudaStream_t st);
+
 // mixed.cu
 int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                 double *d_x, icarat_solve_info *info);
+void mixed_alloc(icarat_ctx *c);
 void mixed_free(icarat_ctx *c);
+// y = K u on the fine grid with one of the reduced-precision operators
+// (ICARAT_OP_FP32 / ICARAT_OP_TC_BF16X3 / ICARAT_OP_TC_BF16), FP32 vectors
+void apply_K_lowp(icarat_ctx *c, int op, const float *u, float *y);
+void round_f32(icarat_ctx *c, long n, const double *in, float *out);
+void widen_f64(icarat_ctx *c, long n, const float *in, double *out);
 
 // multigrid.cu
 void mg_setup(icarat_ctx *c, int levels);

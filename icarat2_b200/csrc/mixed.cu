@@ -299,7 +299,7 @@ static float *falloc(size_t n)
   return static_cast<float *>(p);
 }
 
-static void mixed_alloc(icarat_ctx *c)
+void mixed_alloc(icarat_ctx *c)
 {
   if(c->f_x)
     return;
@@ -325,6 +325,61 @@ void mixed_free(icarat_ctx *c)
   c->d_mx = c->h_mx = nullptr;
 }
 
+__global__ void k_round_f32(long n, const double *__restrict__ in, float *__restrict__ out)
+{
+  for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+      i += (long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+__global__ void k_widen_f64(long n, const float *__restrict__ in, double *__restrict__ out)
+{
+  for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+      i += (long)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+void round_f32(icarat_ctx *c, long n, const double *in, float *out)
+{
+  note_launch();
+  k_round_f32<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, in, out);
+  ICK(cudaGetLastError());
+}
+
+void widen_f64(icarat_ctx *c, long n, const float *in, double *out)
+{
+  note_launch();
+  k_widen_f64<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, in, out);
+  ICK(cudaGetLastError());
+}
+
+void apply_K_lowp(icarat_ctx *c, int op, const float *u, float *y)
+{
+  const GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+  if(op == ICARAT_OP_FP32)
+  {
+    launch_apply_K_f32(c, g, c->d_E32, c->d_fix, u, y);
+    return;
+  }
+  IREQUIRE(op == ICARAT_OP_TC_BF16X3 || op == ICARAT_OP_TC_BF16, ICARAT_ERR_ARG,
+           "unknown operator");
+  TcArgs a;
+  a.g = g;
+  a.E = c->d_E32;
+  a.fix = c->d_fix;
+  a.u = u;
+  a.y = y;
+  launch_ku_tc(c, TC_APPLY, op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
+}
+
+// Operators of the FP32 iterations unless the options name others.  The
+// smoother tolerates the ~1e-5 relative error of the BF16 hi/lo tensor-core
+// product (the preconditioner is applied inexactly anyway; same iteration
+// counts as FP32); the Krylov product K p does not (an inexact K p costs
+// many more iterations), so it stays on the FP32 CUDA-core stencil.
+constexpr int kDefaultFineOp = ICARAT_OP_TC_BF16X3;
+constexpr int kDefaultKrylovOp = ICARAT_OP_FP32;
+
 static int spmv_blocks(const icarat_ctx *c)
 {
   int b = (c->numnp + 127) / 128;
@@ -343,13 +398,30 @@ static void enqueue_precondition(icarat_ctx *c, int smooth, int first)
                                                              first);
 }
 
-static void enqueue_iteration(icarat_ctx *c, int smooth, const double *b, double *x)
+static void enqueue_iteration(icarat_ctx *c, int smooth, int krylov_op, const double *b,
+                              double *x)
 {
   const MgLevel &L = c->mg[0];
   const int n = c->neq;
-  note_launch(4);
-  k_mx_spmv<<<spmv_blocks(c), 128, 0, c->stream>>>(L.g, c->ke0f, L.E32, L.fix, c->f_p,
-                                                   c->f_Ap, c->d_partials, c->d_mx);
+  if(krylov_op == ICARAT_OP_FP32)
+  {
+    note_launch();
+    k_mx_spmv<<<spmv_blocks(c), 128, 0, c->stream>>>(L.g, c->ke0f, L.E32, L.fix, c->f_p,
+                                                     c->f_Ap, c->d_partials, c->d_mx);
+  }
+  else
+  {
+    TcArgs a;
+    a.g = L.g;
+    a.E = L.E32;
+    a.fix = L.fix;
+    a.u = c->f_p;
+    a.y = c->f_Ap;
+    a.partials = c->d_partials;
+    a.s = c->d_mx;
+    launch_ku_tc(c, TC_DOT, krylov_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
+  }
+  note_launch(3);
   k_mx_update<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_x, c->f_r, c->f_p,
                                                             c->f_Ap, c->d_partials,
                                                             c->d_mx);
@@ -369,6 +441,12 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   const int smooth = o->mg_smooth > 0 ? o->mg_smooth : 2;
   const double delta = o->refresh > 0.0 ? o->refresh : 1.0e-2;
   const int chunk = o->chunk > 0 ? o->chunk : 4;
+  const int fine_op = o->fine_op > 0 ? o->fine_op : kDefaultFineOp;
+  const int krylov_op = o->krylov_op > 0 ? o->krylov_op : kDefaultKrylovOp;
+  for(int op : {fine_op, krylov_op})
+    IREQUIRE(op == ICARAT_OP_FP32 || op == ICARAT_OP_TC_BF16X3 || op == ICARAT_OP_TC_BF16,
+             ICARAT_ERR_ARG, "mixed solver operators must be FP32 or tensor-core");
+  c->mx_fine_op = fine_op;
   mg_setup(c, levels);
   mixed_alloc(c);
   const int n = c->neq;
@@ -380,8 +458,9 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   enqueue_precondition(c, smooth, 1);
   ICK(cudaGetLastError());
 
-  const auto key = std::make_tuple((int)ICARAT_SOLVER_MIXED_IR, levels, smooth, chunk,
-                                   (const void *)d_x);
+  // the operators are part of what a captured graph launches
+  const auto key = std::make_tuple((int)ICARAT_SOLVER_MIXED_IR + 16 * fine_op + 256 * krylov_op,
+                                   levels, smooth, chunk, (const void *)d_x);
   auto it = c->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
   if(it == c->graphs.end() || c->graph_b.count(key) == 0 || c->graph_b[key] != d_b)
@@ -397,7 +476,7 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
     try
     {
       for(int k = 0; k < chunk; k++)
-        enqueue_iteration(c, smooth, d_b, d_x);
+        enqueue_iteration(c, smooth, krylov_op, d_b, d_x);
     }
     catch(...)
     {

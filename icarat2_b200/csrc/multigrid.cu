@@ -292,10 +292,10 @@ void mg_free(icarat_ctx *c)
       dfree(L.E);
       dfree(L.fix);
       dfree(L.invd);
+      dfree(L.E32);
     }
-    for(void *p : {(void *)L.x, (void *)L.b, (void *)L.r, (void *)L.t, (void *)L.E32,
-                   (void *)L.invd32, (void *)L.x32, (void *)L.b32, (void *)L.r32,
-                   (void *)L.t32})
+    for(void *p : {(void *)L.x, (void *)L.b, (void *)L.r, (void *)L.t, (void *)L.invd32,
+                   (void *)L.x32, (void *)L.b32, (void *)L.r32, (void *)L.t32})
       dfree(p);
   }
   c->mg.clear();
@@ -341,12 +341,14 @@ static void allocate_levels(icarat_ctx *c, int levels)
     if(l == 0)
     {
       L.E = c->d_E;
+      L.E32 = c->d_E32;
       L.fix = c->d_fix;
       L.invd = c->d_invd;
     }
     else
     {
       L.E = dalloc(L.g.nelx);
+      L.E32 = falloc(L.g.nelx);
       ICK(cudaMalloc(&L.fix, L.g.numnp));
       L.invd = dalloc(nv);
     }
@@ -354,7 +356,6 @@ static void allocate_levels(icarat_ctx *c, int levels)
     L.b = dalloc(nv);
     L.r = dalloc(nv);
     L.t = dalloc(nv);
-    L.E32 = falloc(L.g.nelx);
     L.invd32 = falloc(nv);
     L.x32 = falloc(nv);
     L.b32 = falloc(nv);
@@ -421,8 +422,12 @@ static void enqueue_mg_setup(icarat_ctx *c, int levels)
       k_coarsen_E<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>(F.g, L.g, F.E, L.E);
     }
     launch_diag(c, L.g, L.E, L.fix, L.invd);
-    note_launch(2);
-    k_cast<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>((long)L.g.nelx, L.E, L.E32);
+    if(l > 0) // the finest FP32 moduli come with the design
+    {
+      note_launch();
+      k_cast<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>((long)L.g.nelx, L.E, L.E32);
+    }
+    note_launch();
     k_cast<<<blocks_for(3L * L.g.numnp, 256), 256, 0, c->stream>>>(3L * L.g.numnp, L.invd,
                                                                    L.invd32);
   }
@@ -485,10 +490,66 @@ void mg_setup(icarat_ctx *c, int levels)
   note_launch(c->coarse.setup_kernels);
 }
 
-// Chebyshev smoothing of K x = b on one level, deg steps.  from_zero: x = 0
+// the finest level of the FP32 V-cycle may run on the tensor-core operator
+template <typename T> static bool tc_level(icarat_ctx *c, int lvl)
+{
+  return std::is_same<T, float>::value && lvl == 0 &&
+         (c->mx_fine_op == ICARAT_OP_TC_BF16X3 || c->mx_fine_op == ICARAT_OP_TC_BF16);
+}
+
+// one Chebyshev step d = c1 d + c2 invd (b - K x), xo = x + d on level lvl
+template <typename T>
+static void cheb_step(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x, T *d, T *xo,
+                      double c1, double c2)
+{
+  using B = LevelBuf<T>;
+  if(tc_level<T>(c, lvl))
+  {
+    TcArgs a;
+    a.g = L.g;
+    a.E = reinterpret_cast<const float *>(B::E(L));
+    a.fix = L.fix;
+    a.u = reinterpret_cast<const float *>(x);
+    a.y = reinterpret_cast<float *>(xo);
+    a.b = reinterpret_cast<const float *>(b);
+    a.invd = reinterpret_cast<const float *>(B::invd(L));
+    a.d = reinterpret_cast<float *>(d);
+    a.c1 = (float)c1;
+    a.c2 = (float)c2;
+    launch_ku_tc(c, TC_CHEB, c->mx_fine_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
+    return;
+  }
+  note_launch();
+  k_cheb_step<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(
+      L.g, B::ke(c), B::E(L), L.fix, B::invd(L), b, x, d, xo, T(c1), T(c2));
+}
+
+// r = b - K x on level lvl
+template <typename T>
+static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x, T *r)
+{
+  using B = LevelBuf<T>;
+  if(tc_level<T>(c, lvl))
+  {
+    TcArgs a;
+    a.g = L.g;
+    a.E = reinterpret_cast<const float *>(B::E(L));
+    a.fix = L.fix;
+    a.u = reinterpret_cast<const float *>(x);
+    a.y = reinterpret_cast<float *>(r);
+    a.b = reinterpret_cast<const float *>(b);
+    launch_ku_tc(c, TC_RESID, c->mx_fine_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
+    return;
+  }
+  note_launch();
+  k_mg_residual<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, B::ke(c), B::E(L),
+                                                                  L.fix, b, x, r);
+}
+
+// Chebyshev smoothing of K x = b on level lvl, deg steps.  from_zero: x = 0
 // on entry (the first step needs no product).
 template <typename T>
-static void smooth(icarat_ctx *c, MgLevel &L, const T *b, int deg, bool from_zero)
+static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool from_zero)
 {
   using B = LevelBuf<T>;
   const double lmax = c->lam_max_dk;
@@ -497,7 +558,6 @@ static void smooth(icarat_ctx *c, MgLevel &L, const T *b, int deg, bool from_zer
   const double sigma = theta / delta;
   double rho_old = 1.0 / sigma;
   const int nv = 3 * L.g.numnp;
-  const int nb = blocks_for(L.g.numnp, 128);
   T *x = B::x(L), *xo = B::t(L), *d = B::r(L);
   int k0 = 0;
   if(from_zero)
@@ -510,19 +570,14 @@ static void smooth(icarat_ctx *c, MgLevel &L, const T *b, int deg, bool from_zer
   else
   {
     // first step from the current x: d = invd (b - K x) / theta
-    note_launch();
-    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, B::ke(c), B::E(L), L.fix, B::invd(L), b,
-                                           x, d, xo, T(0), T(1.0 / theta));
+    cheb_step<T>(c, L, lvl, b, x, d, xo, 0.0, 1.0 / theta);
     std::swap(x, xo);
     k0 = 1;
   }
   for(int k = k0; k < deg; k++)
   {
     const double rho = 1.0 / (2.0 * sigma - rho_old);
-    note_launch();
-    k_cheb_step<<<nb, 128, 0, c->stream>>>(L.g, B::ke(c), B::E(L), L.fix, B::invd(L), b,
-                                           x, d, xo, T(rho * rho_old),
-                                           T(2.0 * rho / delta));
+    cheb_step<T>(c, L, lvl, b, x, d, xo, rho * rho_old, 2.0 * rho / delta);
     std::swap(x, xo);
     rho_old = rho;
   }
@@ -556,11 +611,9 @@ template <typename T> static void vcycle(icarat_ctx *c, int l, const T *b, int d
     return;
   }
   MgLevel &C = c->mg[l + 1];
-  smooth<T>(c, L, b, deg, true);
+  smooth<T>(c, L, l, b, deg, true);
   // residual into r (smooth() used r as scratch; done with it now)
-  note_launch();
-  k_mg_residual<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(
-      L.g, B::ke(c), B::E(L), L.fix, b, B::x(L), B::r(L));
+  mg_residual<T>(c, L, l, b, B::x(L), B::r(L));
   note_launch();
   k_restrict<<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, B::r(L), C.fix,
                                                                 B::b(C));
@@ -568,7 +621,7 @@ template <typename T> static void vcycle(icarat_ctx *c, int l, const T *b, int d
   note_launch();
   k_prolong_add<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, B::x(C),
                                                                    L.fix, B::x(L));
-  smooth<T>(c, L, b, deg, false);
+  smooth<T>(c, L, l, b, deg, false);
 }
 
 void mg_vcycle(icarat_ctx *c, const double *r, double *z, int deg)

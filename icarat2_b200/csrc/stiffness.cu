@@ -156,6 +156,32 @@ void launch_apply_K(icarat_ctx *c, const GridDev &g, const double *E,
   ICK(cudaGetLastError());
 }
 
+// y = K u in FP32 (the FP32 copies of Ke0 and of the moduli)
+__global__ void __launch_bounds__(128)
+    k_apply_K_f32(GridDev g, KeParamF ke, const float *__restrict__ E,
+                  const uint8_t *__restrict__ fix, const float *__restrict__ u,
+                  float *__restrict__ y)
+{
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    float acc[3], uc[3];
+    node_Ku(g, ke, E, u, n, acc, uc);
+    const unsigned f = fix[n];
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+      y[(long)c * g.numnp + n] = ((f >> c) & 1u) ? 0.0f : acc[c];
+  }
+}
+
+void launch_apply_K_f32(icarat_ctx *c, const GridDev &g, const float *E,
+                        const uint8_t *fix, const float *u, float *y)
+{
+  note_launch();
+  k_apply_K_f32<<<node_blocks(g, 128), 128, 0, c->stream>>>(g, c->ke0f, E, fix, u, y);
+  ICK(cudaGetLastError());
+}
+
 void launch_diag(icarat_ctx *c, const GridDev &g, const double *E,
                  const uint8_t *fix, double *invd)
 {

@@ -96,6 +96,9 @@ typedef struct
   int chunk;     /* iterations per host convergence check (0 = default) */
   double refresh; /* MIXED_IR: recompute the residual in FP64 once the FP32
                      recurrence has fallen by this factor (0 = 1e-2) */
+  int fine_op;    /* MIXED_IR: ICARAT_OP_* of the finest-level smoothing and
+                     residual in the V-cycle (0 = default) */
+  int krylov_op;  /* MIXED_IR: ICARAT_OP_* of K p in the Krylov loop (0 = default) */
 } icarat_solve_opts;
 
 typedef struct
@@ -277,6 +280,21 @@ int icarat_kernel_launches(unsigned long long *count);
    design, over `reps` back-to-back launches timed with CUDA events on the
    context's stream */
 int icarat_time_operator(icarat_ctx *ctx, int reps, double *ms_per_launch);
+
+/* ---- stiffness operators by precision (no reference counterpart) -------- */
+enum
+{
+  ICARAT_OP_FP64 = 0,      /* FP64 node stencil on the CUDA cores */
+  ICARAT_OP_FP32 = 1,      /* FP32 node stencil on the CUDA cores */
+  ICARAT_OP_TC_BF16X3 = 2, /* element-by-element Ke0 U_e on the tensor cores:
+                              BF16 hi/lo split, 3 products, FP32 accumulation */
+  ICARAT_OP_TC_BF16 = 3    /* the same with the single product hi x hi */
+};
+/* y = K u (numeq host vectors) on the current design with operator `op`;
+   reduced-precision operators round u to FP32 first */
+int icarat_apply_K_op(icarat_ctx *ctx, int op, const double *u, double *y);
+/* icarat_time_operator for operator `op` (FP32 vectors for op > 0) */
+int icarat_time_operator_op(icarat_ctx *ctx, int op, int reps, double *ms_per_launch);
 
 int icarat_loop_init(icarat_ctx *ctx, const icarat_loop_opts *opts,
                      const double *x0);
