@@ -59,6 +59,10 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--alt-levels", type=int, default=5,
                    help="also time the loop with this many multigrid levels (0: skip)")
+    p.add_argument("--mixed-grid", default="256x128x128",
+                   help="grid of the mixed-precision section ('' skips it)")
+    p.add_argument("--mixed-levels", type=int, default=5)
+    p.add_argument("--mixed-steps", type=int, default=5)
     return p.parse_args()
 
 
@@ -225,6 +229,84 @@ def traffic_from_profiles(grid):
         if line.startswith("traffic_bytes_per_launch:"):
             return float(line.split(":")[1])
     return None
+
+
+def mixed_section(a, G, torch, dev, flush, world, dist):
+    """256x128x128 cantilever, densities U[0.1, 0.5] (seed 0), R = 3, MMA:
+    design iterations per second of the mixed-precision loop (FP32 multigrid
+    PCG with the tcgen05 BF16x3 smoother, FP64 residual refresh) against the
+    plain FP64 multigrid-PCG loop at the same residual, compliance and dc
+    error of one solve against an FP64 solve at rtol 1e-12, and K u GDOF/s
+    of every operator on the same design."""
+    nx, ny, nz = (int(v) for v in a.mixed_grid.split("x"))
+    nelx, nd = nx * ny * nz, 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    rho0 = np.random.default_rng(0).uniform(0.1, 0.5, nelx)
+    levels = a.mixed_levels
+    out = {"grid": [nx, ny, nz], "mg_levels": levels, "filter_radius": 3.0,
+           "update": "MMA move 0.2", "rho0": "U[0.1, 0.5] seed 0"}
+
+    def loop_rate(method, rtol):
+        c = G.Context(nx, ny, nz, device=dev.index)
+        c.loop_init(rho0, method="mma", filter_radius=3.0, move=0.2,
+                    solve=G.solve_opts(method, rtol, 10000, levels, a.smooth))
+        s = torch.cuda.ExternalStream(c.stream_ptr(), device=dev)
+        for _ in range(a.warmup):
+            c.loop_step()
+        torch.cuda.synchronize()
+        ms, its = 0.0, []
+        for _ in range(a.mixed_steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            its.append(c.loop_step().cg_iterations)
+            e1.record(s)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            with torch.cuda.stream(s):
+                flush.zero_()
+        torch.cuda.synchronize()
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        c.close()
+        return {"value": world * a.mixed_steps / (float(t.item()) / 1000.0),
+                "unit": "design-iter/s", "ms_per_step": float(t.item()) / a.mixed_steps,
+                "cg_iterations_per_step": its}
+
+    for rtol in (1e-6, 1e-8):
+        m = loop_rate(G.MIXED_IR, rtol)
+        p = loop_rate(G.MG_PCG, rtol)
+        out["rtol_%g" % rtol] = {"mixed": m, "fp64_mg_pcg": p,
+                                 "speedup_mixed_vs_fp64": m["value"] / p["value"]}
+    # accuracy of one solve on the first design against FP64 at rtol 1e-12
+    c = G.Context(nx, ny, nz, device=dev.index)
+    c.filter_setup(3.0)
+    c.set_design(c.density_filter(rho0, False))
+    c.solve(G.solve_opts(G.MG_PCG, 1e-12, 10000, levels, a.smooth), want_val=False)
+    c64 = c.compliance()
+    dc64, _ = c.sensitivity(1.0)
+    for rtol in (1e-6, 1e-8):
+        _, info = c.solve(G.solve_opts(G.MIXED_IR, rtol, 10000, levels, a.smooth),
+                          want_val=False)
+        dc, _ = c.sensitivity(1.0)
+        out["rtol_%g" % rtol]["compliance_rel_err"] = abs(c.compliance() - c64) / abs(c64)
+        out["rtol_%g" % rtol]["dc_max_rel_err"] = float(np.abs(dc - dc64).max() /
+                                                        np.abs(dc64).max())
+        out["rtol_%g" % rtol]["fp64_residual"] = info.rel_residual
+    # K u throughput of every operator on this design
+    ku = {}
+    for name, op in (("fp64", G.OP_FP64), ("fp32", G.OP_FP32),
+                     ("tc_bf16x3", G.OP_TC_BF16X3), ("tc_bf16", G.OP_TC_BF16)):
+        ms_op = c.time_operator(20, op)
+        ku[name] = {"ms": ms_op, "gdof_s": nd / (ms_op * 1e-3) / 1e9}
+    out["ku"] = ku
+    # the tensor-core kernel against HBM: algorithmic bytes of a K u with
+    # FP32 u, y and E
+    bytes32 = 8.0 * nd + 4.0 * nelx
+    ms_tc = ku["tc_bf16x3"]["ms"]
+    out["roofline_tc_bf16x3"] = {"bound": "hbm", "achieved": bytes32 / (ms_tc * 1e-3) / 1e9,
+                                 "unit": "GB/s", "bytes_per_launch": bytes32}
+    c.close()
+    return out
 
 
 def gpu_arm(a):
@@ -404,6 +486,10 @@ def gpu_arm(a):
         del mma
         c2.close()
 
+    mixed = None
+    if a.mixed_grid:
+        mixed = mixed_section(a, G, torch, dev, flush, world, dist)
+
     if rank == 0:
         cg = [i.cg_iterations for i in infos]
         line = {
@@ -428,6 +514,7 @@ def gpu_arm(a):
             "ku_gdof_s": nd / (ms_op * 1e-3) / 1e9,
             "cg_iterations_per_step": cg,
             "alt_levels": alt,
+            "mixed_256x128x128": mixed,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }
