@@ -97,6 +97,11 @@ class LoopOpts(C.Structure):
                 ("filter_radius", C.c_double), ("solve", SolveOpts)]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("maxit", C.c_int), ("refresh", C.c_double),
+                ("tile", C.c_int), ("blocks_per_sm", C.c_int)]
+
+
 class StepInfo(C.Structure):
     _fields_ = [("step", C.c_int), ("compliance", C.c_double),
                 ("constraint", C.c_double), ("cg_iterations", C.c_int),
@@ -155,6 +160,13 @@ SIGNATURES = {
     "icarat_kernel_launches": (_i, [_P(C.c_ulonglong)]),
     "icarat_time_operator": (_i, [_vp, _i, _P(_d)]),
     "icarat_apply_K_op": (_i, [_vp, _i, _dp, _dp]),
+    "icarat_batch_create": (_i, [_vp, _vp, _i, _P(Material), _i, _P(_vp)]),
+    "icarat_batch_destroy": (_i, [_vp]),
+    "icarat_batch_ctx": (_i, [_vp, _i, _P(_vp)]),
+    "icarat_batch_autotune": (_i, [_vp, _P(_i), _P(_i), _P(_d)]),
+    "icarat_batch_solve": (_i, [_vp, _P(BatchOpts), _vp]),
+    "icarat_batch_solution": (_i, [_vp, _i, _dp]),
+    "icarat_batch_loop_step": (_i, [_vp, _P(BatchOpts), _vp]),
     "icarat_time_operator_op": (_i, [_vp, _i, _i, _P(_d)]),
     "icarat_loop_init": (_i, [_vp, _P(LoopOpts), _dp]),
     "icarat_loop_step": (_i, [_vp, _P(StepInfo)]),
@@ -211,6 +223,21 @@ def cantilever_bc(nx, ny, nz, lx=None, ly=None, lz=None, load_node=None, load=(0
     return dirichlet, loads
 
 
+def _bc_struct(dirichlet, loads):
+    dirichlet = list(dirichlet or [])
+    loads = list(loads or [])
+    d = (Dirichlet * max(1, len(dirichlet)))()
+    for i, (fl, vl, bx) in enumerate(dirichlet):
+        d[i].flag = (C.c_int * 3)(*fl)
+        d[i].val = (C.c_double * 3)(*vl)
+        d[i].box = _box(bx)
+    lo = (Load * max(1, len(loads)))()
+    for i, (vl, bx) in enumerate(loads):
+        lo[i].val = (C.c_double * 3)(*vl)
+        lo[i].box = _box(bx)
+    return BC(len(dirichlet), d, len(loads), lo), d, lo
+
+
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
                chunk=0, refresh=0.0, fine_op=0, krylov_op=0):
     return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,
@@ -230,32 +257,35 @@ class Context:
             dirichlet, loads = cantilever_bc(nx, ny, nz, lx, ly, lz)
         dirichlet = list(dirichlet or [])
         loads = list(loads or [])
-        self._dir = (Dirichlet * max(1, len(dirichlet)))()
-        for i, (fl, vl, bx) in enumerate(dirichlet):
-            self._dir[i].flag = (C.c_int * 3)(*fl)
-            self._dir[i].val = (C.c_double * 3)(*vl)
-            self._dir[i].box = _box(bx)
-        self._loads = (Load * max(1, len(loads)))()
-        for i, (vl, bx) in enumerate(loads):
-            self._loads[i].val = (C.c_double * 3)(*vl)
-            self._loads[i].box = _box(bx)
-        bc = BC(len(dirichlet), self._dir, len(loads), self._loads)
+        bc, self._dir, self._loads = _bc_struct(dirichlet, loads)
         grid = Grid(nx, ny, nz, lx, ly, lz)
         mat = Material(young[0], young[1], poisson, penalty)
         h = C.c_void_p()
         _check(L.icarat_ctx_create(C.byref(grid), C.byref(mat), C.byref(bc), device,
                                    C.byref(h)), "icarat_ctx_create")
+        self._adopt(h, L, (nx, ny, nz), young, poisson, penalty, owned=True)
+
+    def _adopt(self, h, L, dims, young, poisson, penalty, owned):
         self.h = h
         self.lib = L
+        self._owned = owned
         a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         _check(L.icarat_sizes(h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)), "sizes")
         self.numnp, self.nelx, self.neq, self.numeq = a.value, b.value, c.value, d.value
-        self.nx, self.ny, self.nz = nx, ny, nz
+        self.nx, self.ny, self.nz = dims
         self.young, self.poisson, self.penalty = young, poisson, penalty
+
+    @classmethod
+    def _member(cls, h, L, dims, young, poisson, penalty):
+        """A context owned by a Batch (not destroyed by this object)."""
+        obj = cls.__new__(cls)
+        obj._adopt(h, L, dims, young, poisson, penalty, owned=False)
+        return obj
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.icarat_ctx_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.lib.icarat_ctx_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -540,3 +570,88 @@ def kernel_launches():
     n = C.c_ulonglong()
     _check(L.icarat_kernel_launches(C.byref(n)), "kernel_launches")
     return n.value
+
+
+class Batch:
+    """Many independent designs solved together (icarat_batch_*).
+
+    problems: list of (nx, ny, nz) or (nx, ny, nz, dirichlet, loads); unit
+    cubes (length = division) unless lengths are given as (nx, ny, nz, lx, ly,
+    lz, dirichlet, loads).  Every member is a Context (``batch[i]``) for the
+    per-design calls."""
+
+    def __init__(self, problems, young=(1e-9, 1.0), poisson=0.3, penalty=3.0, device=0):
+        L = load_library()
+        n = len(problems)
+        grids = (Grid * n)()
+        bcs = (BC * n)()
+        self._keep = []
+        dims = []
+        for i, pr in enumerate(problems):
+            pr = tuple(pr)
+            nx, ny, nz = pr[:3]
+            if len(pr) >= 8:
+                lx, ly, lz, dirichlet, loads = pr[3:8]
+            else:
+                lx, ly, lz = float(nx), float(ny), float(nz)
+                dirichlet, loads = pr[3:5] if len(pr) >= 5 else cantilever_bc(nx, ny, nz)
+            grids[i] = Grid(nx, ny, nz, lx, ly, lz)
+            bc, d, lo = _bc_struct(dirichlet, loads)
+            bcs[i] = bc
+            self._keep += [d, lo]
+            dims.append((nx, ny, nz))
+        mat = Material(young[0], young[1], poisson, penalty)
+        h = C.c_void_p()
+        _check(L.icarat_batch_create(C.cast(grids, C.c_void_p), C.cast(bcs, C.c_void_p), n,
+                                     C.byref(mat), device, C.byref(h)), "icarat_batch_create")
+        self.h, self.lib = h, L
+        self.ctx = []
+        for i in range(n):
+            c = C.c_void_p()
+            _check(L.icarat_batch_ctx(h, i, C.byref(c)), "icarat_batch_ctx")
+            self.ctx.append(Context._member(c, L, dims[i], young, poisson, penalty))
+
+    def __len__(self):
+        return len(self.ctx)
+
+    def __getitem__(self, i):
+        return self.ctx[i]
+
+    def close(self):
+        if getattr(self, "h", None):
+            for c in self.ctx:
+                c.h = None
+            self.lib.icarat_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    @staticmethod
+    def opts(rtol=1e-8, maxit=10000, refresh=0.0, tile=0, blocks_per_sm=0):
+        return BatchOpts(rtol, maxit, refresh, tile, blocks_per_sm)
+
+    def autotune(self):
+        t, b, ms = C.c_int(), C.c_int(), C.c_double()
+        _check(self.lib.icarat_batch_autotune(self.h, C.byref(t), C.byref(b), C.byref(ms)),
+               "icarat_batch_autotune")
+        return t.value, b.value, ms.value
+
+    def solve(self, opts=None):
+        infos = (SolveInfo * len(self.ctx))()
+        st = self.lib.icarat_batch_solve(self.h, C.byref(opts) if opts is not None else None,
+                                         C.cast(infos, C.c_void_p))
+        _check(st, "icarat_batch_solve")
+        return list(infos)
+
+    def solution(self, i):
+        u = np.zeros(max(self.ctx[i].numeq, 1))
+        _check(self.lib.icarat_batch_solution(self.h, i, u), "icarat_batch_solution")
+        return u[:self.ctx[i].numeq]
+
+    def loop_step(self, opts=None):
+        infos = (StepInfo * len(self.ctx))()
+        st = self.lib.icarat_batch_loop_step(self.h, C.byref(opts) if opts is not None
+                                             else None, C.cast(infos, C.c_void_p))
+        _check(st, "icarat_batch_loop_step")
+        return list(infos)

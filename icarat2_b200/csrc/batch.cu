@@ -1,0 +1,870 @@
+// Batched solve of many independent designs (no reference counterpart; the
+// reference solves one design at a time).
+//
+// Every design is a full icarat_ctx (mesh, boundary conditions, SIMP moduli,
+// FP64 right-hand side and solution live there).  The batch adds one
+// cooperative persistent kernel that iterates all designs together.  Work
+// is a queue of (design, node tile) items, designs back to back, and each
+// CTA takes a contiguous run of items, so designs of different sizes share
+// the grid in proportion to their node counts.  Per iteration (grid-wide
+// barriers between phases):
+//   P1  Ap = K p (FP32 node stencil), per-item partial p . Ap
+//   P2  alpha = z.r / p.Ap (design sums of the partials, fixed order);
+//       x32 += alpha p, r -= alpha Ap, z = D^-1 r; partials z.r, z.Ap, r.r
+//   P3  beta = -z.Ap / p.Ap (flexible); p = z + beta p; the design's first
+//       item decides an FP64 refresh (r.r fell by `refresh`, below the target,
+//       or the cap) and counts it
+//   R   (only when some design asked) x += x32, x32 = 0; r = b - K x in FP64;
+//       stop on the FP64 residual (OK / MAXITER / STAGNATION / NAN)
+// Vectors are FP32 except the FP64 solution and right-hand side; dot products
+// and scalars are FP64.  Designs that stop drop out of the queue; the launch
+// ends when none is left or after maxit + 2 iterations.
+//
+// Tuning: nodes per item and CTAs per SM are picked by timing the candidate
+// shapes on the batch itself (icarat_batch_autotune).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "stencil.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace icarat_b200
+{
+int loop_step(icarat_ctx *c, icarat_step_info *info);
+double loop_pre(icarat_ctx *c);
+int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
+              icarat_step_info *info);
+void build_rhs(icarat_ctx *c);
+
+struct BatchDesign
+{
+  GridDev g;
+  const float *E32;
+  const double *E64;
+  const uint8_t *fix;
+  const double *b;
+  double *x64;
+  long off;   // first entry of this design in the FP32 node buffers
+  int item0;  // first work item
+  int nitems; // work items
+};
+
+struct BScal
+{
+  double rz, bb, rr_ref, rr_true, tol2, delta2;
+  int iter, maxit, done, status, refresh, final_, nrefresh, nstall;
+};
+
+struct BatchArgs
+{
+  KeParam ke;
+  KeParamF kef;
+  const BatchDesign *des;
+  int ndes;
+  const int *item_design;
+  int nitems, tile;
+  float *x32, *r, *z, *p, *Ap, *invd;
+  double *part; // 4 per item
+  BScal *s;
+  int *ctl; // [0] designs still iterating, [1], [2] refresh requests by parity
+  int maxit;
+  double tol, delta;
+};
+
+constexpr int kBatchThreads = 128;
+
+// Sum of partial k over the items of design D, in item order; every thread
+// of the block gets the result.
+__device__ double design_sum(const BatchArgs &a, const BatchDesign &D, int k, double *sh,
+                             double *bc)
+{
+  double v = 0.0;
+  for(int i = threadIdx.x; i < D.nitems; i += blockDim.x)
+    v += __ldcg(a.part + 4L * (D.item0 + i) + k);
+  double arr[1] = {v};
+  block_sum<1>(arr, sh);
+  if(threadIdx.x == 0)
+    *bc = arr[0];
+  __syncthreads();
+  const double r = *bc;
+  __syncthreads();
+  return r;
+}
+
+// (K x)_n in FP64 element by element: few live registers, for the refresh
+// phase, which runs rarely and must not raise the register count of the
+// whole persistent kernel.  Coherent (L2) loads: x changes inside the launch.
+__device__ __forceinline__ void node_Ku_lean(const GridDev &g, const KeParam &ke,
+                                             const double *__restrict__ E,
+                                             const double *__restrict__ x, int n,
+                                             double (&acc)[3])
+{
+  const int i = n % g.NX, j = (n / g.NX) % g.NY, k = n / (g.NX * g.NY);
+  acc[0] = acc[1] = acc[2] = 0.0;
+#pragma unroll
+  for(int sz = 0; sz < 2; sz++)
+#pragma unroll
+    for(int sy = 0; sy < 2; sy++)
+#pragma unroll
+      for(int sx = 0; sx < 2; sx++)
+      {
+        const int ei = i - 1 + sx, ej = j - 1 + sy, ek = k - 1 + sz;
+        const double e = load_E(E, g, ei, ej, ek);
+        if(e == 0.0)
+          continue;
+        const int la = local_node(1 - sx, 1 - sy, 1 - sz);
+        double t[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for(int bz = 0; bz < 2; bz++)
+#pragma unroll
+          for(int by = 0; by < 2; by++)
+#pragma unroll
+            for(int bx = 0; bx < 2; bx++)
+            {
+              const int lb = local_node(bx, by, bz);
+              const long m = (long)(ei + bx) + (long)(ej + by) * g.NX +
+                             (long)(ek + bz) * g.NX * g.NY;
+#pragma unroll
+              for(int d = 0; d < 3; d++)
+              {
+                const double u = __ldcg(x + (long)d * g.numnp + m);
+#pragma unroll
+                for(int c = 0; c < 3; c++)
+                  t[c] = fma(ke.k[(3 * la + c) * 24 + 3 * lb + d], u, t[c]);
+              }
+            }
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+          acc[c] = fma(e, t[c], acc[c]);
+      }
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 3) k_batch_pcg(BatchArgs a)
+{
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sh[4 * 32];
+  __shared__ double bc[4];
+  const int ipb = (a.nitems + gridDim.x - 1) / gridDim.x;
+  const int it0 = min(blockIdx.x * ipb, a.nitems), it1 = min(it0 + ipb, a.nitems);
+  const int t = threadIdx.x;
+  if(blockIdx.x == 0 && t == 0)
+  {
+    a.ctl[0] = a.ndes; // nobody reads the control words before the first barrier
+    a.ctl[1] = a.ctl[2] = 0;
+  }
+
+  // ---- init: x = 0, x32 = 0, r = b, z = D^-1 r, p = z; partials b.b, z.r
+  for(int item = it0; item < it1; item++)
+  {
+    const int d = a.item_design[item];
+    const BatchDesign &D = a.des[d];
+    const int n0 = (item - D.item0) * a.tile;
+    double bb = 0.0, rz = 0.0;
+    for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+    {
+      const int i = n % D.g.NX, j = (n / D.g.NX) % D.g.NY, k = n / (D.g.NX * D.g.NY);
+      double dg[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for(int sz = 0; sz < 2; sz++)
+#pragma unroll
+        for(int sy = 0; sy < 2; sy++)
+#pragma unroll
+          for(int sx = 0; sx < 2; sx++)
+          {
+            const double e = load_E(D.E64, D.g, i - 1 + sx, j - 1 + sy, k - 1 + sz);
+            const int la = local_node(1 - sx, 1 - sy, 1 - sz);
+#pragma unroll
+            for(int c = 0; c < 3; c++)
+              dg[c] = fma(e, a.ke.k[(3 * la + c) * 25], dg[c]);
+          }
+      const unsigned f = D.fix[n];
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+      {
+        const long id = (long)c * D.g.numnp + n, o = D.off + id;
+        const double bi = D.b[id];
+        const float iv = ((f >> c) & 1u) ? 0.0f : (float)(dg[c] != 0.0 ? 1.0 / dg[c] : 1.0);
+        const float ri = (float)bi, zi = iv * ri;
+        D.x64[id] = 0.0;
+        a.x32[o] = 0.0f;
+        a.invd[o] = iv;
+        a.r[o] = ri;
+        a.z[o] = zi;
+        a.p[o] = zi;
+        bb += bi * bi;
+        rz += (double)zi * (double)ri;
+      }
+    }
+    double v[2] = {bb, rz};
+    block_sum<2>(v, sh);
+    if(t == 0)
+    {
+      a.part[4L * item + 0] = v[0];
+      a.part[4L * item + 1] = v[1];
+    }
+    __syncthreads();
+  }
+  grid.sync();
+  for(int item = it0; item < it1; item++)
+  {
+    const int d = a.item_design[item];
+    const BatchDesign &D = a.des[d];
+    if(item != D.item0)
+      continue;
+    const double bb = design_sum(a, D, 0, sh, bc);
+    const double rz = design_sum(a, D, 1, sh, bc);
+    if(t == 0)
+    {
+      BScal &S = a.s[d];
+      S.bb = bb;
+      S.rz = rz;
+      S.rr_ref = S.rr_true = bb;
+      S.tol2 = a.tol * a.tol * bb;
+      S.delta2 = a.delta * a.delta;
+      S.iter = 0;
+      S.maxit = a.maxit;
+      S.refresh = S.final_ = S.nrefresh = S.nstall = 0;
+      S.status = ICARAT_OK;
+      S.done = 0;
+      if(!(bb == bb))
+      {
+        S.done = 1;
+        S.status = ICARAT_ERR_NAN;
+      }
+      else if(bb == 0.0)
+        S.done = 1;
+      if(S.done)
+        atomicSub(&a.ctl[0], 1);
+    }
+  }
+  grid.sync();
+
+  for(int it = 0; it < a.maxit + 2; it++)
+  {
+    if(*(volatile int *)&a.ctl[0] <= 0)
+      break;
+    // ---- P1: Ap = K p, partial p . Ap
+    for(int item = it0; item < it1; item++)
+    {
+      const int d = a.item_design[item];
+      if(*(volatile int *)&a.s[d].done)
+        continue;
+      const BatchDesign &D = a.des[d];
+      const int n0 = (item - D.item0) * a.tile;
+      double pap = 0.0;
+      for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+      {
+        float acc[3], uc[3];
+        node_Ku<float, KeParamF, true>(D.g, a.kef, D.E32, a.p + D.off, n, acc, uc);
+        const unsigned f = D.fix[n];
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          const float y = ((f >> c) & 1u) ? 0.0f : acc[c];
+          a.Ap[D.off + (long)c * D.g.numnp + n] = y;
+          pap += (double)uc[c] * (double)y;
+        }
+      }
+      double v[1] = {pap};
+      block_sum<1>(v, sh);
+      if(t == 0)
+        a.part[4L * item] = v[0];
+      __syncthreads();
+    }
+    grid.sync();
+    // ---- P2: x32, r, z updates; partials z.r, z.Ap, r.r
+    {
+      int cached = -1;
+      double alpha = 0.0;
+      for(int item = it0; item < it1; item++)
+      {
+        const int d = a.item_design[item];
+        if(*(volatile int *)&a.s[d].done)
+          continue;
+        const BatchDesign &D = a.des[d];
+        if(d != cached)
+        {
+          const double pap = design_sum(a, D, 0, sh, bc);
+          alpha = a.s[d].rz / pap;
+          cached = d;
+        }
+        const float al = (float)alpha;
+        const int n0 = (item - D.item0) * a.tile;
+        const long nv = 3L * D.g.numnp;
+        double rz = 0.0, zap = 0.0, rr = 0.0;
+        for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+#pragma unroll
+          for(int c = 0; c < 3; c++)
+          {
+            const long o = D.off + (long)c * D.g.numnp + n;
+            const float pi = a.p[o], api = a.Ap[o];
+            a.x32[o] = fmaf(al, pi, a.x32[o]);
+            const float ri = fmaf(-al, api, a.r[o]);
+            const float zi = a.invd[o] * ri;
+            a.r[o] = ri;
+            a.z[o] = zi;
+            rz += (double)zi * (double)ri;
+            zap += (double)zi * (double)api;
+            rr += (double)ri * (double)ri;
+          }
+        (void)nv;
+        double v[3] = {rz, zap, rr};
+        block_sum<3>(v, sh);
+        if(t == 0)
+        {
+          a.part[4L * item + 1] = v[0];
+          a.part[4L * item + 2] = v[1];
+          a.part[4L * item + 3] = v[2];
+          if(item == D.item0)
+            a.s[d].iter += 1;
+        }
+        __syncthreads();
+      }
+    }
+    grid.sync();
+    // ---- P3: p = z + beta p; refresh decision
+    {
+      int cached = -1;
+      double beta = 0.0;
+      for(int item = it0; item < it1; item++)
+      {
+        const int d = a.item_design[item];
+        if(*(volatile int *)&a.s[d].done)
+          continue;
+        const BatchDesign &D = a.des[d];
+        if(d != cached)
+        {
+          const double pap = design_sum(a, D, 0, sh, bc);
+          const double zap = design_sum(a, D, 2, sh, bc);
+          beta = -zap / pap;
+          cached = d;
+          if(item == D.item0)
+          {
+            const double rz = design_sum(a, D, 1, sh, bc);
+            const double rr = design_sum(a, D, 3, sh, bc);
+            if(t == 0)
+            {
+              BScal &S = a.s[d];
+              S.rz = rz;
+              const bool nan = !(rr == rr) || !(beta == beta);
+              S.final_ = (nan || S.iter >= S.maxit) ? 1 : 0;
+              S.refresh = (S.final_ || rr < S.tol2 || rr < S.delta2 * S.rr_ref) ? 1 : 0;
+              if(S.refresh)
+                atomicAdd(&a.ctl[1 + (it & 1)], 1);
+            }
+          }
+        }
+        const float be = (float)beta;
+        const int n0 = (item - D.item0) * a.tile;
+        for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+#pragma unroll
+          for(int c = 0; c < 3; c++)
+          {
+            const long o = D.off + (long)c * D.g.numnp + n;
+            a.p[o] = fmaf(be, a.p[o], a.z[o]);
+          }
+      }
+      if(blockIdx.x == 0 && t == 0)
+        a.ctl[1 + ((it + 1) & 1)] = 0; // the counter of the next iteration
+    }
+    grid.sync();
+    if(*(volatile int *)&a.ctl[1 + (it & 1)] == 0)
+      continue;
+    // ---- R1: x += x32, x32 = 0 for the designs that refresh
+    for(int item = it0; item < it1; item++)
+    {
+      const int d = a.item_design[item];
+      const BScal &S = a.s[d];
+      if(*(volatile const int *)&S.done || !*(volatile const int *)&S.refresh)
+        continue;
+      const BatchDesign &D = a.des[d];
+      const int n0 = (item - D.item0) * a.tile;
+      for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          const long id = (long)c * D.g.numnp + n;
+          D.x64[id] += (double)a.x32[D.off + id];
+          a.x32[D.off + id] = 0.0f;
+        }
+    }
+    grid.sync();
+    // ---- R2: r = b - K x in FP64, z = D^-1 r; partials r.r, z.r
+    for(int item = it0; item < it1; item++)
+    {
+      const int d = a.item_design[item];
+      const BScal &S = a.s[d];
+      if(*(volatile const int *)&S.done || !*(volatile const int *)&S.refresh)
+        continue;
+      const BatchDesign &D = a.des[d];
+      const int n0 = (item - D.item0) * a.tile;
+      double rr = 0.0, rz = 0.0;
+      for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+      {
+        double acc[3];
+        node_Ku_lean(D.g, a.ke, D.E64, D.x64, n, acc);
+        const unsigned f = D.fix[n];
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          const long id = (long)c * D.g.numnp + n, o = D.off + id;
+          const double ri = ((f >> c) & 1u) ? 0.0 : D.b[id] - acc[c];
+          const float r32 = (float)ri, zi = a.invd[o] * r32;
+          a.r[o] = r32;
+          a.z[o] = zi;
+          rr += ri * ri;
+          rz += (double)zi * (double)r32;
+        }
+      }
+      double v[2] = {rr, rz};
+      block_sum<2>(v, sh);
+      if(t == 0)
+      {
+        a.part[4L * item + 0] = v[0];
+        a.part[4L * item + 1] = v[1];
+      }
+      __syncthreads();
+    }
+    grid.sync();
+    // ---- R3: stop test on the FP64 residual
+    for(int item = it0; item < it1; item++)
+    {
+      const int d = a.item_design[item];
+      const BatchDesign &D = a.des[d];
+      if(item != D.item0)
+        continue;
+      BScal &S = a.s[d];
+      if(*(volatile int *)&S.done || !*(volatile int *)&S.refresh)
+        continue;
+      const double rr = design_sum(a, D, 0, sh, bc);
+      const double rz = design_sum(a, D, 1, sh, bc);
+      if(t == 0)
+      {
+        S.nstall = rr > 0.81 * S.rr_true ? S.nstall + 1 : 0;
+        S.rr_true = S.rr_ref = rr;
+        S.rz = rz;
+        S.nrefresh += 1;
+        S.refresh = 0;
+        if(!(rr == rr))
+        {
+          S.done = 1;
+          S.status = ICARAT_ERR_NAN;
+        }
+        else if(rr < S.tol2)
+        {
+          S.done = 1;
+          S.status = ICARAT_OK;
+        }
+        else if(S.final_)
+        {
+          S.done = 1;
+          S.status = ICARAT_WARN_MAXITER;
+        }
+        else if(S.nstall >= 3)
+        {
+          S.done = 1;
+          S.status = ICARAT_WARN_STAGNATION;
+        }
+        if(S.done)
+          atomicSub(&a.ctl[0], 1);
+      }
+    }
+    grid.sync();
+  }
+}
+
+} // namespace icarat_b200
+
+using namespace icarat_b200;
+
+struct icarat_batch
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<icarat_ctx *> ctx;
+  KeParam ke;
+  KeParamF kef;
+  long total_nv = 0; // FP32 node-vector length of all designs
+  float *buf = nullptr; // x32, r, z, p, Ap, invd back to back
+  BatchDesign *d_des = nullptr;
+  int *d_item_design = nullptr;
+  double *d_part = nullptr;
+  BScal *d_s = nullptr, *h_s = nullptr;
+  int *d_ctl = nullptr;
+  int nitems = 0, items_tile = 0; // items built for this tile
+  int tile = 0, blocks_per_sm = 0; // tuned shape (0 = not tuned)
+  int occ = 0;                     // co-resident CTAs per SM
+  cudaGraphExec_t graph = nullptr;
+  std::tuple<int, int, double, int, double> graph_key{};
+  std::vector<cudaEvent_t> ev;
+  cudaEvent_t done_ev = nullptr;
+};
+
+int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
+                           const icarat_bc *bc, int device, icarat_ctx **out);
+
+static void batch_items(icarat_batch *B, int tile)
+{
+  if(B->items_tile == tile)
+    return;
+  ICK(cudaStreamSynchronize(B->stream)); // launches in flight read the old tables
+  std::vector<BatchDesign> des(B->ctx.size());
+  std::vector<int> item_design;
+  long off = 0;
+  for(size_t d = 0; d < B->ctx.size(); d++)
+  {
+    icarat_ctx *c = B->ctx[d];
+    BatchDesign &D = des[d];
+    D.g = GridDev{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+    D.E32 = c->d_E32;
+    D.E64 = c->d_E;
+    D.fix = c->d_fix;
+    D.b = c->d_rhs;
+    D.x64 = c->d_u;
+    D.off = off;
+    D.item0 = (int)item_design.size();
+    D.nitems = (c->numnp + tile - 1) / tile;
+    for(int i = 0; i < D.nitems; i++)
+      item_design.push_back((int)d);
+    off += 3L * c->numnp;
+  }
+  dfree(B->d_item_design);
+  dfree(B->d_part);
+  B->d_item_design = nullptr;
+  B->d_part = nullptr;
+  B->nitems = (int)item_design.size();
+  ICK(cudaMalloc(&B->d_item_design, sizeof(int) * item_design.size()));
+  ICK(cudaMemcpy(B->d_item_design, item_design.data(), sizeof(int) * item_design.size(),
+                 cudaMemcpyHostToDevice));
+  B->d_part = dalloc(4 * item_design.size());
+  ICK(cudaMemcpy(B->d_des, des.data(), sizeof(BatchDesign) * des.size(),
+                 cudaMemcpyHostToDevice));
+  B->items_tile = tile;
+  if(B->graph)
+  {
+    cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+  }
+}
+
+// Right-hand sides of every design, and the batch stream ordered after
+// everything already queued on the design streams.
+static void batch_prepare(icarat_batch *B, bool rhs)
+{
+  for(size_t d = 0; d < B->ctx.size(); d++)
+  {
+    icarat_ctx *c = B->ctx[d];
+    IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design of every batch member first");
+    if(rhs)
+      build_rhs(c);
+    ICK(cudaEventRecord(B->ev[d], c->stream));
+    ICK(cudaStreamWaitEvent(B->stream, B->ev[d], 0));
+  }
+}
+
+static void batch_launch(icarat_batch *B, int tile, int bpsm, double rtol, int maxit,
+                         double refresh)
+{
+  batch_items(B, tile);
+  BatchArgs a;
+  a.ke = B->ke;
+  a.kef = B->kef;
+  a.des = B->d_des;
+  a.ndes = (int)B->ctx.size();
+  a.item_design = B->d_item_design;
+  a.nitems = B->nitems;
+  a.tile = tile;
+  const long nv = B->total_nv;
+  a.x32 = B->buf;
+  a.r = B->buf + nv;
+  a.z = B->buf + 2 * nv;
+  a.p = B->buf + 3 * nv;
+  a.Ap = B->buf + 4 * nv;
+  a.invd = B->buf + 5 * nv;
+  a.part = B->d_part;
+  a.s = B->d_s;
+  a.ctl = B->d_ctl;
+  a.maxit = maxit;
+  a.tol = rtol;
+  a.delta = refresh;
+  const int sms = B->ctx[0]->sm_count;
+  const int blocks = sms * std::max(1, std::min(bpsm, B->occ));
+  void *args[] = {&a};
+  note_launch();
+  ICK(cudaLaunchCooperativeKernel((void *)k_batch_pcg, dim3(blocks), dim3(kBatchThreads), args,
+                                  0, B->stream));
+}
+
+// The solve as a CUDA graph (one graph per shape and options).
+static void batch_run(icarat_batch *B, int tile, int bpsm, double rtol, int maxit,
+                      double refresh)
+{
+  const auto key = std::make_tuple(tile, bpsm, rtol, maxit, refresh);
+  if(!B->graph || B->graph_key != key)
+  {
+    if(B->graph)
+    {
+      cudaGraphExecDestroy(B->graph);
+      B->graph = nullptr;
+    }
+    batch_items(B, tile);
+    cudaGraph_t g;
+    ICK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+    set_capturing(true);
+    try
+    {
+      batch_launch(B, tile, bpsm, rtol, maxit, refresh);
+    }
+    catch(...)
+    {
+      set_capturing(false);
+      cudaStreamEndCapture(B->stream, &g);
+      throw;
+    }
+    set_capturing(false);
+    ICK(cudaStreamEndCapture(B->stream, &g));
+    ICK(cudaGraphInstantiate(&B->graph, g, 0));
+    cudaGraphDestroy(g);
+    B->graph_key = key;
+  }
+  ICK(cudaGraphLaunch(B->graph, B->stream));
+  note_launch();
+}
+
+static int pick_tile(icarat_batch *B, const icarat_batch_opts *o)
+{
+  if(o && o->tile > 0)
+    return o->tile;
+  return B->tile > 0 ? B->tile : 256;
+}
+
+static int pick_bpsm(icarat_batch *B, const icarat_batch_opts *o)
+{
+  if(o && o->blocks_per_sm > 0)
+    return std::min(o->blocks_per_sm, B->occ);
+  return B->blocks_per_sm > 0 ? B->blocks_per_sm : B->occ;
+}
+
+static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
+                            icarat_solve_info *infos)
+{
+  const double rtol = o ? o->rtol : 1e-8;
+  const int maxit = o && o->maxit > 0 ? o->maxit : 10000;
+  const double refresh = o && o->refresh > 0.0 ? o->refresh : 1e-2;
+  IREQUIRE(rtol >= 0.0 && refresh < 1.0, ICARAT_ERR_ARG, "bad batch options");
+  const int tile = pick_tile(B, o), bpsm = pick_bpsm(B, o);
+  IREQUIRE(tile >= 32 && tile <= (1 << 16), ICARAT_ERR_ARG, "tile must be in [32, 65536]");
+  batch_run(B, tile, bpsm, rtol, maxit, refresh);
+  const size_t n = B->ctx.size();
+  ICK(cudaMemcpyAsync(B->h_s, B->d_s, sizeof(BScal) * n, cudaMemcpyDeviceToHost, B->stream));
+  ICK(cudaEventRecord(B->done_ev, B->stream));
+  ICK(cudaStreamSynchronize(B->stream));
+  int worst = ICARAT_OK;
+  for(size_t d = 0; d < n; d++)
+  {
+    icarat_ctx *c = B->ctx[d];
+    ICK(cudaStreamWaitEvent(c->stream, B->done_ev, 0));
+    const BScal &S = B->h_s[d];
+    icarat_solve_info si{};
+    si.iterations = S.iter;
+    si.rel_residual = S.bb > 0 ? std::sqrt(S.rr_true / S.bb) : 0.0;
+    si.status = S.done ? S.status : ICARAT_WARN_MAXITER;
+    si.refreshes = S.nrefresh;
+    c->solved = true;
+    c->last_info = si;
+    if(infos)
+      infos[d] = si;
+    if(si.status < 0)
+      worst = std::min(worst, si.status);
+    else if(worst >= 0 && si.status > worst)
+      worst = si.status;
+  }
+  return worst;
+}
+
+extern "C" {
+
+int icarat_batch_create(const icarat_grid *grids, const icarat_bc *bcs, int count,
+                        const icarat_material *mat, int device, icarat_batch **out)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(grids && mat && out && count >= 1, ICARAT_ERR_ARG, "bad argument");
+  *out = nullptr;
+  icarat_batch *B = new icarat_batch;
+  B->device = device;
+  try
+  {
+    ICK(cudaSetDevice(device));
+    ICK(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    const double h0[3] = {grids[0].lx / grids[0].nx, grids[0].ly / grids[0].ny,
+                          grids[0].lz / grids[0].nz};
+    for(int d = 0; d < count; d++)
+    {
+      const double h[3] = {grids[d].lx / grids[d].nx, grids[d].ly / grids[d].ny,
+                           grids[d].lz / grids[d].nz};
+      for(int q = 0; q < 3; q++)
+        IREQUIRE(std::fabs(h[q] - h0[q]) <= 1e-12 * h0[q], ICARAT_ERR_UNSUPPORTED,
+                 "batch members must share the element size");
+      icarat_ctx *c = nullptr;
+      const int st = icarat_ctx_create_impl(&grids[d], mat, bcs ? &bcs[d] : nullptr, device, &c);
+      IREQUIRE(st == ICARAT_OK, st, "batch member creation failed");
+      B->ctx.push_back(c);
+      B->total_nv += 3L * c->numnp;
+      cudaEvent_t e;
+      ICK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      B->ev.push_back(e);
+    }
+    ICK(cudaEventCreateWithFlags(&B->done_ev, cudaEventDisableTiming));
+    B->ke = B->ctx[0]->ke0;
+    B->kef = B->ctx[0]->ke0f;
+    ICK(cudaMalloc(&B->buf, sizeof(float) * 6 * B->total_nv));
+    ICK(cudaMalloc(&B->d_des, sizeof(BatchDesign) * count));
+    ICK(cudaMalloc(&B->d_s, sizeof(BScal) * count));
+    ICK(cudaMemset(B->d_s, 0, sizeof(BScal) * count));
+    ICK(cudaMallocHost(&B->h_s, sizeof(BScal) * count));
+    ICK(cudaMalloc(&B->d_ctl, sizeof(int) * 4));
+    ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->occ, k_batch_pcg, kBatchThreads, 0));
+    IREQUIRE(B->occ >= 1, ICARAT_ERR_CUDA, "batch kernel cannot be resident");
+  }
+  catch(...)
+  {
+    icarat_batch_destroy(B);
+    throw;
+  }
+  *out = B;
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_batch_destroy(icarat_batch *B)
+{
+  if(!B)
+    return ICARAT_OK;
+  cudaSetDevice(B->device);
+  if(B->stream)
+    cudaStreamSynchronize(B->stream);
+  if(B->graph)
+    cudaGraphExecDestroy(B->graph);
+  for(icarat_ctx *c : B->ctx)
+    icarat_ctx_destroy(c);
+  for(cudaEvent_t e : B->ev)
+    cudaEventDestroy(e);
+  if(B->done_ev)
+    cudaEventDestroy(B->done_ev);
+  for(void *p : {(void *)B->buf, (void *)B->d_des, (void *)B->d_item_design,
+                 (void *)B->d_part, (void *)B->d_s, (void *)B->d_ctl})
+    dfree(p);
+  if(B->h_s)
+    cudaFreeHost(B->h_s);
+  if(B->stream)
+    cudaStreamDestroy(B->stream);
+  delete B;
+  return ICARAT_OK;
+}
+
+int icarat_batch_ctx(icarat_batch *B, int i, icarat_ctx **ctx)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(B && ctx && i >= 0 && i < (int)B->ctx.size(), ICARAT_ERR_ARG, "bad argument");
+  *ctx = B->ctx[i];
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_batch_solve(icarat_batch *B, const icarat_batch_opts *opts,
+                       icarat_solve_info *infos)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(B, ICARAT_ERR_ARG, "null batch");
+  ICK(cudaSetDevice(B->device));
+  batch_prepare(B, true);
+  return batch_solve_impl(B, opts, infos);
+  ICARAT_API_END
+}
+
+int icarat_batch_solution(icarat_batch *B, int i, double *u)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(B && u && i >= 0 && i < (int)B->ctx.size(), ICARAT_ERR_ARG, "bad argument");
+  icarat_ctx *c = B->ctx[i];
+  IREQUIRE(c->solved, ICARAT_ERR_STATE, "solve the batch first");
+  from_full(c, c->d_u, u, true);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_batch_autotune(icarat_batch *B, int *tile, int *bpsm, double *ms_per_iteration)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(B, ICARAT_ERR_ARG, "null batch");
+  ICK(cudaSetDevice(B->device));
+  batch_prepare(B, true);
+  // every candidate runs the same fixed work: 10 iterations of every design
+  // (tolerance 0, cap 10) and the final FP64 refresh
+  const int tiles[] = {128, 256, 512, 1024};
+  double best = 1e30;
+  int bt = 256, bb = B->occ;
+  cudaEvent_t e0, e1;
+  ICK(cudaEventCreate(&e0));
+  ICK(cudaEventCreate(&e1));
+  for(int tl : tiles)
+    for(int bp = 1; bp <= B->occ; bp++)
+    {
+      batch_launch(B, tl, bp, 0.0, 10, 1e-2); // warm-up (and item tables)
+      ICK(cudaEventRecord(e0, B->stream));
+      batch_launch(B, tl, bp, 0.0, 10, 1e-2);
+      ICK(cudaEventRecord(e1, B->stream));
+      ICK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      ICK(cudaEventElapsedTime(&ms, e0, e1));
+      if(ms < best)
+      {
+        best = ms;
+        bt = tl;
+        bb = bp;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  B->tile = bt;
+  B->blocks_per_sm = bb;
+  if(tile)
+    *tile = bt;
+  if(bpsm)
+    *bpsm = bb;
+  if(ms_per_iteration)
+    *ms_per_iteration = best / 10.0;
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_batch_loop_step(icarat_batch *B, const icarat_batch_opts *opts,
+                           icarat_step_info *infos)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(B, ICARAT_ERR_ARG, "null batch");
+  ICK(cudaSetDevice(B->device));
+  const size_t n = B->ctx.size();
+  std::vector<double> beta(n);
+  for(size_t d = 0; d < n; d++)
+    beta[d] = loop_pre(B->ctx[d]); // filter, design, right-hand side
+  batch_prepare(B, false);
+  std::vector<icarat_solve_info> si(n);
+  batch_solve_impl(B, opts, si.data());
+  int worst = ICARAT_OK;
+  for(size_t d = 0; d < n; d++)
+  {
+    const int st = loop_post(B->ctx[d], si[d].status, si[d], beta[d], infos ? &infos[d] : nullptr);
+    if(st < 0)
+      worst = std::min(worst, st);
+    else if(worst >= 0 && st > worst)
+      worst = st;
+  }
+  return worst;
+  ICARAT_API_END
+}
+
+} // extern "C"

@@ -97,7 +97,9 @@ int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
   return ICARAT_OK;
 }
 
-int loop_step(icarat_ctx *c, icarat_step_info *info)
+// First part of a design iteration: filter -> threshold -> element design ->
+// right-hand side.  Returns the threshold sharpness beta of this step.
+double loop_pre(icarat_ctx *c)
 {
   LoopState &L = c->loop;
   IREQUIRE(L.init, ICARAT_ERR_STATE, "icarat_loop_init first");
@@ -121,10 +123,18 @@ int loop_step(icarat_ctx *c, icarat_step_info *info)
     k_fill<<<eb(n), 256, 0, c->stream>>>(n, 1.0, L.thrd);
   }
   set_design_device(c, L.xthr);
-  // linear analysis
   build_rhs(c);
-  icarat_solve_info si{};
-  int st = solve_full(c, &o.solve, c->d_rhs, c->d_u, &si);
+  return beta;
+}
+
+// Rest of a design iteration after the solve (status st, info si):
+// compliance, volume, sensitivities, transposed filter and the update.
+int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
+              icarat_step_info *info)
+{
+  LoopState &L = c->loop;
+  const int n = c->nelx;
+  const icarat_loop_opts &o = L.opts;
   c->solved = true;
   c->last_info = si;
   // objective and constraint
@@ -175,6 +185,14 @@ int loop_step(icarat_ctx *c, icarat_step_info *info)
     info->status = st != ICARAT_OK ? st : ust;
   }
   return st < 0 ? st : (ust < 0 ? ust : (st != ICARAT_OK ? st : ust));
+}
+
+int loop_step(icarat_ctx *c, icarat_step_info *info)
+{
+  const double beta = loop_pre(c);
+  icarat_solve_info si{};
+  const int st = solve_full(c, &c->loop.opts.solve, c->d_rhs, c->d_u, &si);
+  return loop_post(c, st, si, beta, info);
 }
 
 int loop_get(icarat_ctx *c, int which, double *out)

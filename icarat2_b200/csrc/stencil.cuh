@@ -93,7 +93,10 @@ __device__ __forceinline__ void layer_contrib(const KP &ke, const T (&ul)[2][9][
       acc[c] = fma(Ev[e], t[e][c], acc[c]);
 }
 
-template <typename T>
+// CG = true loads through L2 only (ld.global.cg): for vectors that the same
+// (persistent) kernel rewrites between grid-wide barriers, where the
+// read-only path could serve stale lines.
+template <typename T, bool CG = false>
 __device__ __forceinline__ void load_layer(const T *__restrict__ u, const GridDev &g,
                                            int i, int j, int kk, T (&L)[9][3])
 {
@@ -109,7 +112,8 @@ __device__ __forceinline__ void load_layer(const T *__restrict__ u, const GridDe
       const int s = (dy + 1) * 3 + (dx + 1);
 #pragma unroll
       for(int d = 0; d < 3; d++)
-        L[s][d] = in ? __ldg(u + (long)d * g.numnp + m) : T(0);
+        L[s][d] = in ? (CG ? __ldcg(u + (long)d * g.numnp + m) : __ldg(u + (long)d * g.numnp + m))
+                     : T(0);
     }
 }
 
@@ -123,7 +127,7 @@ __device__ __forceinline__ T load_E(const T *__restrict__ E, const GridDev &g, i
 }
 
 // (K u) at node n (unmasked) and the node's own displacement uc.
-template <typename T, typename KP>
+template <typename T, typename KP, bool CG = false>
 __device__ __forceinline__ void node_Ku(const GridDev &g, const KP &ke,
                                         const T *__restrict__ E,
                                         const T *__restrict__ u, int n, T (&acc)[3],
@@ -136,8 +140,8 @@ __device__ __forceinline__ void node_Ku(const GridDev &g, const KP &ke,
   T ul[2][9][3];
   T Ev[4];
   // elements below the node: node layers k-1 (bz = 0) and k (bz = 1)
-  load_layer(u, g, i, j, k - 1, ul[0]);
-  load_layer(u, g, i, j, k, ul[1]);
+  load_layer<T, CG>(u, g, i, j, k - 1, ul[0]);
+  load_layer<T, CG>(u, g, i, j, k, ul[1]);
 #pragma unroll
   for(int sy = 0; sy < 2; sy++)
 #pragma unroll
@@ -153,7 +157,7 @@ __device__ __forceinline__ void node_Ku(const GridDev &g, const KP &ke,
 #pragma unroll
     for(int d = 0; d < 3; d++)
       ul[0][s][d] = ul[1][s][d];
-  load_layer(u, g, i, j, k + 1, ul[1]);
+  load_layer<T, CG>(u, g, i, j, k + 1, ul[1]);
 #pragma unroll
   for(int sy = 0; sy < 2; sy++)
 #pragma unroll

@@ -281,6 +281,49 @@ int icarat_kernel_launches(unsigned long long *count);
    context's stream */
 int icarat_time_operator(icarat_ctx *ctx, int reps, double *ms_per_launch);
 
+/* ---- batched solver (no reference counterpart) ---------------------------
+   Many independent designs, of equal or different grid sizes, solved
+   together.  Every design is a full context (icarat_batch_ctx returns it for
+   the per-design calls: set_design, filter, sensitivity, loop_init, ...);
+   icarat_batch_solve runs the Krylov iterations of all designs in ONE
+   persistent cooperative launch over a work queue of (design, node tile)
+   items, replayed from a CUDA graph: FP32 vectors and K p, Jacobi
+   preconditioner, flexible beta, FP64 dot products and per-design FP64
+   residual refresh (as ICARAT_SOLVER_MIXED_IR), each design stopping on its
+   own FP64 residual.  All designs share the element size and the material. */
+typedef struct icarat_batch icarat_batch;
+
+typedef struct
+{
+  double rtol;       /* per design: ||f - K u|| < rtol ||f|| in FP64 */
+  int maxit;         /* iteration cap per design */
+  double refresh;    /* FP64 refresh once the FP32 residual fell by this factor
+                        (0 = 1e-2) */
+  int tile;          /* nodes per work item (0 = autotuned, else 256) */
+  int blocks_per_sm; /* persistent CTAs per SM (0 = autotuned, else the
+                        occupancy limit) */
+} icarat_batch_opts;
+
+int icarat_batch_create(const icarat_grid *grids, const icarat_bc *bcs, int count,
+                        const icarat_material *mat, int device, icarat_batch **out);
+int icarat_batch_destroy(icarat_batch *batch);
+/* the context of design i (owned by the batch) */
+int icarat_batch_ctx(icarat_batch *batch, int i, icarat_ctx **ctx);
+/* time the candidate (tile, CTAs per SM) shapes on the current designs and
+   keep the fastest for later solves; any output pointer may be NULL */
+int icarat_batch_autotune(icarat_batch *batch, int *tile, int *blocks_per_sm,
+                          double *ms_per_iteration);
+/* K u = f for every design (f from its boundary conditions, u kept in its
+   context as after icarat_solve); infos: count entries (may be NULL) */
+int icarat_batch_solve(icarat_batch *batch, const icarat_batch_opts *opts,
+                       icarat_solve_info *infos);
+/* u of design i after icarat_batch_solve (numeq of that design) */
+int icarat_batch_solution(icarat_batch *batch, int i, double *u);
+/* one design iteration of every design (icarat_loop_init on each context
+   first) with the batched solve in place of each loop's own solver */
+int icarat_batch_loop_step(icarat_batch *batch, const icarat_batch_opts *opts,
+                           icarat_step_info *infos);
+
 /* ---- stiffness operators by precision (no reference counterpart) -------- */
 enum
 {
