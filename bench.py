@@ -63,6 +63,9 @@ def parse():
                    help="grid of the mixed-precision section ('' skips it)")
     p.add_argument("--mixed-levels", type=int, default=5)
     p.add_argument("--mixed-steps", type=int, default=5)
+    p.add_argument("--batch-steps", type=int, default=3,
+                   help="design iterations of the 80-design batch section (0: skip)")
+    p.add_argument("--batch-rtol", type=float, default=1e-6)
     return p.parse_args()
 
 
@@ -309,6 +312,82 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
     return out
 
 
+def batch_problems(G, seed=1):
+    """64 cantilevers 64x32x32 and 16 of nx in {32, 48, 64, 80, 96} (2:1:1,
+    cycled); load node uniform over the right-face nodes, volume fraction
+    U[0.2, 0.5] (the uniform start density), filter radius U[1.5, 3.0]."""
+    rng = np.random.default_rng(seed)
+    sizes = [(64, 32, 32)] * 64 + [(n, n // 2, n // 2) for n in [32, 48, 64, 80, 96] * 4][:16]
+    out = []
+    for nx, ny, nz in sizes:
+        node = (nx, int(rng.integers(0, ny + 1)), int(rng.integers(0, nz + 1)))
+        out.append({"grid": (nx, ny, nz), "bc": G.cantilever_bc(nx, ny, nz, load_node=node),
+                    "volfrac": float(rng.uniform(0.2, 0.5)),
+                    "radius": float(rng.uniform(1.5, 3.0))})
+    return out
+
+
+def batch_section(a, G, torch, dev):
+    """Design iterations per second of the batch: one batched solve (one
+    persistent launch for all 80 designs, FP32 Jacobi-PCG with FP64 refresh,
+    autotuned shape) per step, against the same designs stepped one by one
+    with each context's own FP64 multigrid-PCG (4 levels, 600-DOF coarse
+    solve for 64x32x32) at the same rtol."""
+    probs = batch_problems(G)
+    B = G.Batch([p["grid"] + tuple(p["bc"]) for p in probs], device=dev.index)
+    rtol = a.batch_rtol
+    for i, p in enumerate(probs):
+        B[i].loop_init(p["volfrac"], method="mma", filter_radius=p["radius"], move=0.2,
+                       solve=G.solve_opts(G.MG_PCG, rtol, 10000, 4, a.smooth))
+    opts = B.opts(rtol=rtol)
+    B.loop_step(opts)  # first step: V0, graphs
+    tile, bpsm, ms_it = B.autotune()
+    for _ in range(max(1, a.warmup - 1)):
+        B.loop_step(opts)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    its = []
+    for _ in range(a.batch_steps):
+        infos = B.loop_step(opts)
+        its.append(int(np.mean([x.cg_iterations for x in infos])))
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    # solve-only: one batched solve on the current designs
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    sinfo = B.solve(opts)
+    torch.cuda.synchronize()
+    t_solve = time.perf_counter() - t1
+    # the same designs stepped one at a time with their own FP64 MG-PCG
+    for i in range(len(B)):
+        B[i].loop_step()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    for _ in range(a.batch_steps):
+        for i in range(len(B)):
+            B[i].loop_step()
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t2
+    n = len(B)
+    nodes = sum((p["grid"][0] + 1) * (p["grid"][1] + 1) * (p["grid"][2] + 1) for p in probs)
+    out = {"designs": n, "grids": "64 x 64x32x32 + 16 of 32..96 (2:1:1)", "rtol": rtol,
+           "update": "MMA move 0.2", "tuned_tile": tile, "tuned_ctas_per_sm": bpsm,
+           "tuned_ms_per_iteration": ms_it, "nodes": nodes,
+           "batched": {"value": n * a.batch_steps / t_batch, "unit": "design-iter/s",
+                       "mean_cg_iterations_per_step": its,
+                       "timing": "host wall clock around whole batch steps (synchronised)"},
+           "one_by_one_fp64_mg_pcg": {"value": n * a.batch_steps / t_seq,
+                                      "unit": "design-iter/s"},
+           "batched_solve_only_ms": 1000.0 * t_solve,
+           "batched_solve_max_iterations": max(x.iterations for x in sinfo),
+           "statuses": sorted({x.status for x in sinfo})}
+    out["speedup_batched_vs_one_by_one"] = out["batched"]["value"] / \
+        out["one_by_one_fp64_mg_pcg"]["value"]
+    B.close()
+    return out
+
+
 def gpu_arm(a):
     import torch
     import torch.distributed as dist
@@ -489,6 +568,9 @@ def gpu_arm(a):
     mixed = None
     if a.mixed_grid:
         mixed = mixed_section(a, G, torch, dev, flush, world, dist)
+    batched = None
+    if a.batch_steps > 0:
+        batched = batch_section(a, G, torch, dev)
 
     if rank == 0:
         cg = [i.cg_iterations for i in infos]
@@ -515,6 +597,7 @@ def gpu_arm(a):
             "cg_iterations_per_step": cg,
             "alt_levels": alt,
             "mixed_256x128x128": mixed,
+            "batched_80_designs": batched,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }
