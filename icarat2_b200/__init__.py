@@ -76,7 +76,8 @@ class BC(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int),
                 ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int),
-                ("refresh", C.c_double), ("fine_op", C.c_int), ("krylov_op", C.c_int)]
+                ("refresh", C.c_double), ("fine_op", C.c_int), ("krylov_op", C.c_int),
+                ("warm_start", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -239,9 +240,9 @@ def _bc_struct(dirichlet, loads):
 
 
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
-               chunk=0, refresh=0.0, fine_op=0, krylov_op=0):
+               chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0):
     return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,
-                     krylov_op)
+                     krylov_op, warm_start)
 
 
 class Context:

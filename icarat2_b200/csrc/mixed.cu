@@ -29,6 +29,69 @@
 namespace icarat_b200
 {
 
+// Warm start: x kept, x32 = 0, r32 = b - K x in FP64; ||b|| and ||r||.
+__global__ void __launch_bounds__(128)
+    k_mx_init_warm(GridDev g, KeParam ke, const double *__restrict__ E,
+                   const uint8_t *__restrict__ fix, const double *__restrict__ b,
+                   const double *__restrict__ x, float *__restrict__ x32,
+                   float *__restrict__ r32, double *__restrict__ partials, MxScalars *s,
+                   double tol, double delta, int maxit)
+{
+  __shared__ double sh[64];
+  double bb = 0.0, rr = 0.0;
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    double acc[3], uc[3];
+    node_Ku(g, ke, E, x, n, acc, uc);
+    const unsigned f = fix[n];
+#pragma unroll
+    for(int q = 0; q < 3; q++)
+    {
+      const long id = (long)q * g.numnp + n;
+      const double bi = b[id];
+      const double r = ((f >> q) & 1u) ? 0.0 : bi - acc[q];
+      x32[id] = 0.0f;
+      r32[id] = (float)r;
+      bb += bi * bi;
+      rr += r * r;
+    }
+  }
+  double v[2] = {bb, rr};
+  block_sum<2>(v, sh);
+  if(threadIdx.x == 0)
+  {
+    partials[blockIdx.x] = v[0];
+    partials[gridDim.x + blockIdx.x] = v[1];
+  }
+  if(last_block(&s->counter))
+  {
+    double t[2];
+    sum_partials<2>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      s->bb = t[0];
+      s->rr = s->rr_ref = s->rr_true = t[1];
+      s->tol2 = tol * tol * t[0];
+      s->delta2 = delta * delta;
+      s->maxit = maxit;
+      s->iter = 0;
+      s->refresh = 0;
+      s->final_ = 0;
+      s->nrefresh = 0;
+      s->nstall = 0;
+      s->status = ICARAT_OK;
+      s->done = (t[0] == 0.0 || t[1] < s->tol2) ? 1 : 0;
+      if(!(t[0] == t[0]) || !(t[1] == t[1]))
+      {
+        s->done = 1;
+        s->status = ICARAT_ERR_NAN;
+      }
+      s->counter = 0;
+    }
+  }
+}
+
 // x = 0, x32 = 0, r32 = b, ||b||.
 __global__ void k_mx_init(int n, const double *__restrict__ b, double *__restrict__ x,
                           float *__restrict__ x32, float *__restrict__ r32,
@@ -452,8 +515,16 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   const int n = c->neq;
 
   note_launch();
-  k_mx_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
-      n, d_b, d_x, c->f_x, c->f_r, c->d_partials, c->d_mx, o->rtol, delta, o->maxit);
+  if(o->warm_start)
+  {
+    const MgLevel &L0 = c->mg[0];
+    k_mx_init_warm<<<spmv_blocks(c), 128, 0, c->stream>>>(L0.g, c->ke0, c->d_E, L0.fix, d_b,
+                                                          d_x, c->f_x, c->f_r, c->d_partials,
+                                                          c->d_mx, o->rtol, delta, o->maxit);
+  }
+  else
+    k_mx_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
+        n, d_b, d_x, c->f_x, c->f_r, c->d_partials, c->d_mx, o->rtol, delta, o->maxit);
   ICK(cudaGetLastError());
   enqueue_precondition(c, smooth, 1);
   ICK(cudaGetLastError());

@@ -99,6 +99,8 @@ typedef struct
   int fine_op;    /* MIXED_IR: ICARAT_OP_* of the finest-level smoothing and
                      residual in the V-cycle (0 = default) */
   int krylov_op;  /* MIXED_IR: ICARAT_OP_* of K p in the Krylov loop (0 = default) */
+  int warm_start; /* MIXED_IR: start from the solution held by the context (the
+                     previous solve, e.g. of the previous design) instead of 0 */
 } icarat_solve_opts;
 
 typedef struct

@@ -127,3 +127,25 @@ def test_mixed_design_loop(oracle, gpu):
         assert abs(info.compliance - s["compliance"]) <= 1e-6 * s["compliance"]
         assert abs(info.constraint - s["constraint"]) <= 1e-6 * max(1.0, abs(s["constraint"]))
     assert rel(G.loop_get("x"), L.get("x")) <= 1e-6
+
+
+def test_mixed_warm_start(gpu):
+    """Starting from the previous solution: a solve of the same system ends at
+    once, and the next design of a loop needs fewer iterations than from 0."""
+    G = gpu.Context(32, 16, 16)
+    rng = np.random.default_rng(35)
+    rho = rng.uniform(0.1, 0.5, G.nelx)
+    G.set_design(rho)
+    u0, i0 = G.solve(mixed(gpu, 1e-8))
+    u1, i1 = G.solve(mixed(gpu, 1e-8, warm_start=1))
+    assert i1.status == gpu.OK and i1.iterations == 0 and rel(u1, u0) == 0.0
+    rho2 = np.clip(rho * (1.0 + 0.05 * rng.standard_normal(G.nelx)), 0.05, 1.0)
+    G.set_design(rho2)
+    ucold, icold = G.solve(mixed(gpu, 1e-8))
+    G.set_design(rho)
+    G.solve(mixed(gpu, 1e-8))
+    G.set_design(rho2)
+    uwarm, iwarm = G.solve(mixed(gpu, 1e-8, warm_start=1))
+    assert iwarm.status == gpu.OK and iwarm.rel_residual < 1e-8
+    assert iwarm.iterations < icold.iterations
+    assert rel(uwarm, ucold) <= 1e-6
