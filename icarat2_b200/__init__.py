@@ -36,6 +36,7 @@ ERR_NOMEM = -8
 JACOBI_PCG = 0
 MG_PCG = 1
 MIXED_IR = 2
+LEARNED_FPCG = 3
 
 OP_FP64 = 0
 OP_FP32 = 1
@@ -82,7 +83,8 @@ class SolveOpts(C.Structure):
 
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("rel_residual", C.c_double),
-                ("status", C.c_int), ("refreshes", C.c_int)]
+                ("status", C.c_int), ("refreshes", C.c_int),
+                ("learned_iterations", C.c_int)]
 
 
 class OcOpts(C.Structure):
@@ -161,6 +163,15 @@ SIGNATURES = {
     "icarat_kernel_launches": (_i, [_P(C.c_ulonglong)]),
     "icarat_time_operator": (_i, [_vp, _i, _P(_d)]),
     "icarat_apply_K_op": (_i, [_vp, _i, _dp, _dp]),
+    "icarat_net_create": (_i, [_i, C.c_ulonglong, _P(_vp)]),
+    "icarat_net_destroy": (_i, [_vp]),
+    "icarat_net_num_params": (_i, [_vp, _P(C.c_longlong)]),
+    "icarat_net_get_params": (_i, [_vp, _vp]),
+    "icarat_net_set_params": (_i, [_vp, _vp]),
+    "icarat_net_train_step": (_i, [_vp, _vp, _dp, _dp, _dp, _d, _P(_d)]),
+    "icarat_net_get_grads": (_i, [_vp, _vp]),
+    "icarat_net_infer": (_i, [_vp, _vp, _dp, _dp]),
+    "icarat_ctx_set_net": (_i, [_vp, _vp]),
     "icarat_batch_create": (_i, [_vp, _vp, _i, _P(Material), _i, _P(_vp)]),
     "icarat_batch_destroy": (_i, [_vp]),
     "icarat_batch_ctx": (_i, [_vp, _i, _P(_vp)]),
@@ -439,6 +450,12 @@ class Context:
                "time_operator")
         return ms.value
 
+    def set_net(self, net):
+        """attach a Net for the LEARNED_FPCG solver (None detaches)"""
+        _check(self.lib.icarat_ctx_set_net(self.h, net.h if net is not None else None),
+               "icarat_ctx_set_net")
+        self._net = net
+
     def apply_K_op(self, u, op):
         """y = K u with operator `op` (OP_FP64, OP_FP32, OP_TC_BF16X3, OP_TC_BF16)."""
         y = np.zeros(max(self.numeq, 1))
@@ -656,3 +673,52 @@ class Batch:
                                              else None, C.cast(infos, C.c_void_p))
         _check(st, "icarat_batch_loop_step")
         return list(infos)
+
+
+class Net:
+    """The learned preconditioner (icarat_net_*): a 4-level, 16-channel 3-D
+    U-net with BF16 weights and activations, trained by the library's own
+    kernels."""
+
+    def __init__(self, seed=0, device=0):
+        L = load_library()
+        h = C.c_void_p()
+        _check(L.icarat_net_create(device, seed, C.byref(h)), "icarat_net_create")
+        self.h, self.lib = h, L
+        n = C.c_longlong()
+        _check(L.icarat_net_num_params(h, C.byref(n)), "icarat_net_num_params")
+        self.n = n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.icarat_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def params(self):
+        w = np.zeros(self.n, dtype=np.float32)
+        _check(self.lib.icarat_net_get_params(self.h, w.ctypes.data), "get_params")
+        return w
+
+    def set_params(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        assert w.size == self.n
+        _check(self.lib.icarat_net_set_params(self.h, w.ctypes.data), "set_params")
+
+    def grads(self):
+        g = np.zeros(self.n, dtype=np.float32)
+        _check(self.lib.icarat_net_get_grads(self.h, g.ctypes.data), "get_grads")
+        return g
+
+    def train_step(self, ctx, rho, f, u, lr):
+        loss = C.c_double()
+        _check(self.lib.icarat_net_train_step(self.h, ctx.h, _f64(rho), _f64(f), _f64(u), lr,
+                                              C.byref(loss)), "train_step")
+        return loss.value
+
+    def infer(self, ctx, f):
+        u = np.zeros(max(ctx.numeq, 1))
+        _check(self.lib.icarat_net_infer(self.h, ctx.h, _f64(f), u), "infer")
+        return u[:ctx.numeq]

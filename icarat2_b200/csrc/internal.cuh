@@ -250,6 +250,8 @@ struct icarat_ctx
   int sm_count = 148;
   // operator of the finest level of the FP32 V-cycle (ICARAT_OP_*)
   int mx_fine_op = ICARAT_OP_FP32;
+  // learned preconditioner attached by icarat_ctx_set_net (not owned)
+  icarat_net *net = nullptr;
   bool design_set = false, solved = false;
   icarat_solve_info last_info{};
   // multigrid
@@ -305,6 +307,10 @@ double device_dot(icarat_ctx *c, const double *a, const double *b, int n);
 void release_graphs(icarat_ctx *c);
 int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                double *d_x, icarat_solve_info *info);
+
+// net.cu: z = s net(r / s) on ctx's grid and current design
+template <typename T>
+void net_apply(icarat_net *N, icarat_ctx *c, const T *r, double s, T *z);
 
 // tc_stencil.cu
 void launch_ku_tc(icarat_ctx *c, int op, int terms, TcArgs a, cudaStream_t st);

@@ -362,6 +362,12 @@ static float *falloc(size_t n)
   return static_cast<float *>(p);
 }
 
+__global__ void k_scale_f64(int n, double a, double *__restrict__ x)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = a == 0.0 ? 0.0 : a * x[i];
+}
+
 void mixed_alloc(icarat_ctx *c)
 {
   if(c->f_x)
@@ -450,6 +456,7 @@ static int spmv_blocks(const icarat_ctx *c)
 }
 
 // z = M r32, zr, beta, p update
+// z = M r (the FP32 V-cycle), z . r, beta and p = z + beta p
 static void enqueue_precondition(icarat_ctx *c, int smooth, int first)
 {
   const int n = c->neq;
@@ -461,8 +468,17 @@ static void enqueue_precondition(icarat_ctx *c, int smooth, int first)
                                                              first);
 }
 
+// K p, the updates of x32 and r, and the FP64 refresh when one is due
+static void enqueue_krylov_step(icarat_ctx *c, int krylov_op, const double *b, double *x);
+
 static void enqueue_iteration(icarat_ctx *c, int smooth, int krylov_op, const double *b,
                               double *x)
+{
+  enqueue_krylov_step(c, krylov_op, b, x);
+  enqueue_precondition(c, smooth, 0);
+}
+
+static void enqueue_krylov_step(icarat_ctx *c, int krylov_op, const double *b, double *x)
 {
   const MgLevel &L = c->mg[0];
   const int n = c->neq;
@@ -491,8 +507,17 @@ static void enqueue_iteration(icarat_ctx *c, int smooth, int krylov_op, const do
   k_mx_flush<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, x, c->f_x, c->d_mx);
   k_mx_residual<<<spmv_blocks(c), 128, 0, c->stream>>>(L.g, c->ke0, c->d_E, L.fix, b, x,
                                                        c->f_r, c->d_partials, c->d_mx);
-  enqueue_precondition(c, smooth, 0);
 }
+
+static const MxScalars &read_scalars(icarat_ctx *c)
+{
+  ICK(cudaMemcpyAsync(c->h_mx, c->d_mx, sizeof(MxScalars), cudaMemcpyDeviceToHost, c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
+  return *c->h_mx;
+}
+
+// iterations preconditioned by the net at most, before the multigrid takes over
+constexpr int kLearnedMaxIterations = 50;
 
 int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                 double *d_x, icarat_solve_info *info)
@@ -510,12 +535,32 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
     IREQUIRE(op == ICARAT_OP_FP32 || op == ICARAT_OP_TC_BF16X3 || op == ICARAT_OP_TC_BF16,
              ICARAT_ERR_ARG, "mixed solver operators must be FP32 or tensor-core");
   c->mx_fine_op = fine_op;
+  const bool learned = o->method == ICARAT_SOLVER_LEARNED_FPCG;
+  IREQUIRE(!learned || c->net, ICARAT_ERR_STATE,
+           "attach a net with icarat_ctx_set_net before the learned solver");
   mg_setup(c, levels);
   mixed_alloc(c);
   const int n = c->neq;
+  const double nfree = c->numeq > 0 ? (double)c->numeq : 1.0;
+  if(learned)
+  {
+    // initial guess x0 = alpha s net(b / s), s = ||b|| over the free DOFs;
+    // alpha = (x0 . b) / (x0 . K x0) (either sign) minimises the energy norm
+    // of the error along x0, so the guess is never worse than 0 in that norm
+    // (no finite alpha: start from 0)
+    const double bb = device_dot(c, d_b, d_b, n);
+    net_apply<double>(c->net, c, d_b, bb > 0.0 ? std::sqrt(bb) : 1.0, d_x);
+    const GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+    launch_apply_K(c, g, c->d_E, c->d_fix, d_x, c->d_Ap, nullptr);
+    const double xb = device_dot(c, d_x, d_b, n), xkx = device_dot(c, d_x, c->d_Ap, n);
+    double alpha = (xkx > 0.0 && std::isfinite(xkx) && std::isfinite(xb)) ? xb / xkx : 0.0;
+    alpha = std::isfinite(alpha) ? alpha : 0.0;
+    note_launch();
+    k_scale_f64<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, alpha, d_x);
+  }
 
   note_launch();
-  if(o->warm_start)
+  if(o->warm_start || learned)
   {
     const MgLevel &L0 = c->mg[0];
     k_mx_init_warm<<<spmv_blocks(c), 128, 0, c->stream>>>(L0.g, c->ke0, c->d_E, L0.fix, d_b,
@@ -526,7 +571,66 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
     k_mx_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
         n, d_b, d_x, c->f_x, c->f_r, c->d_partials, c->d_mx, o->rtol, delta, o->maxit);
   ICK(cudaGetLastError());
-  enqueue_precondition(c, smooth, 1);
+  int learned_its = 0;
+  if(learned)
+  {
+    // the net preconditions while every iteration at least halves the
+    // residual; the first iteration that does not is preconditioned by the
+    // V-cycle, and so is every later one
+    // z = net(r); usable only if z . r > 0 (checked before p is updated)
+    // (the net is trained up to sign: z = -net(r) when net(r) . r < 0)
+    auto net_precondition = [&](int first, double rr) -> bool
+    {
+      double s = rr > 0.0 ? std::sqrt(rr) : 1.0;
+      for(int pass = 0; pass < 2; pass++)
+      {
+        net_apply<float>(c->net, c, c->f_r, s, c->f_z);
+        note_launch();
+        k_mx_zr<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_z, c->f_r, c->f_Ap,
+                                                              c->d_partials, c->d_mx, first);
+        const MxScalars &sz = read_scalars(c);
+        if(!std::isfinite(sz.zr) || sz.zr == 0.0)
+          return false;
+        if(sz.zr > 0.0)
+          break;
+        s = -s;
+      }
+      if(!(c->h_mx->zr > 0.0))
+        return false;
+      note_launch();
+      k_mx_pupdate<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_z, c->f_p, c->d_mx,
+                                                                 first);
+      return true;
+    };
+    const MxScalars &s0 = read_scalars(c);
+    if(!s0.done)
+    {
+      double rr_prev = s0.rr_true;
+      if(!net_precondition(1, rr_prev))
+        enqueue_precondition(c, smooth, 1); // the net is unusable: multigrid only
+      else
+      {
+        learned_its = 1;
+        for(int k = 0; k < kLearnedMaxIterations; k++)
+        {
+          enqueue_krylov_step(c, krylov_op, d_b, d_x);
+          const MxScalars &sk = read_scalars(c);
+          if(sk.done)
+            break;
+          const double rr = sk.rr;
+          if(!(rr <= 0.25 * rr_prev) || !net_precondition(0, rr))
+          {
+            enqueue_precondition(c, smooth, 0); // fallback to the multigrid V-cycle
+            break;
+          }
+          learned_its++;
+          rr_prev = rr;
+        }
+      }
+    }
+  }
+  else
+    enqueue_precondition(c, smooth, 1);
   ICK(cudaGetLastError());
 
   // the operators are part of what a captured graph launches
@@ -596,6 +700,7 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   info->rel_residual = s.bb > 0 ? std::sqrt(s.rr_true / s.bb) : 0.0;
   info->status = s.done ? s.status : ICARAT_WARN_MAXITER;
   info->refreshes = s.nrefresh;
+  info->learned_iterations = learned_its;
   return info->status;
 }
 

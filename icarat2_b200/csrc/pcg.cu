@@ -318,7 +318,7 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                double *d_x, icarat_solve_info *info)
 {
   IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design before solving");
-  if(o->method == ICARAT_SOLVER_MIXED_IR)
+  if(o->method == ICARAT_SOLVER_MIXED_IR || o->method == ICARAT_SOLVER_LEARNED_FPCG)
     return mixed_solve(c, o, d_b, d_x, info);
   const int method = o->method;
   IREQUIRE(method == ICARAT_SOLVER_JACOBI_PCG || method == ICARAT_SOLVER_MG_PCG,
@@ -412,6 +412,7 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   info->rel_residual = s.bnorm > 0 ? s.rnorm / s.bnorm : 0.0;
   info->status = s.done ? s.status : ICARAT_WARN_MAXITER;
   info->refreshes = 0;
+  info->learned_iterations = 0;
   return info->status;
 }
 

@@ -82,8 +82,10 @@ enum
 {
   ICARAT_SOLVER_JACOBI_PCG = 0, /* "Eigen_CG" / "Scaling_CG" semantics */
   ICARAT_SOLVER_MG_PCG = 1,     /* geometric multigrid preconditioned CG */
-  ICARAT_SOLVER_MIXED_IR = 2    /* FP32 multigrid-PCG iterations refined by FP64
+  ICARAT_SOLVER_MIXED_IR = 2,   /* FP32 multigrid-PCG iterations refined by FP64
                                    residuals (no reference counterpart) */
+  ICARAT_SOLVER_LEARNED_FPCG = 3 /* MIXED_IR with the context's learned net as
+                                    initial guess and first preconditioner */
 };
 
 typedef struct
@@ -109,6 +111,8 @@ typedef struct
   double rel_residual; /* MIXED_IR: of the last FP64 residual */
   int status;
   int refreshes;       /* MIXED_IR: FP64 residual evaluations */
+  int learned_iterations; /* LEARNED_FPCG: iterations preconditioned by the net
+                             before the multigrid fallback */
 } icarat_solve_info;
 
 /* OC::UpdateVariables parameters (OCSolver.hpp:73-79) and the volume functor
@@ -325,6 +329,39 @@ int icarat_batch_solution(icarat_batch *batch, int i, double *u);
    first) with the batched solve in place of each loop's own solver */
 int icarat_batch_loop_step(icarat_batch *batch, const icarat_batch_opts *opts,
                            icarat_step_info *infos);
+
+/* ---- learned preconditioner (no reference counterpart) -------------------
+   A 3-D U-net (4 levels, 16 base channels, BF16 weights and activations,
+   FP32 sums) on the node grid: input the residual divided by its L2 norm and
+   the node density, output the direction of K^-1 r.  Trained on the GPU
+   by this library's own forward and backward kernels (Adam) on samples
+   (design rho, load f, solution u) that the plain solver produces.
+   ICARAT_SOLVER_LEARNED_FPCG uses the net attached to a context: the net's
+   prediction as the initial guess, the net as the preconditioner of a
+   flexible PCG while every iteration at least halves the residual, and the
+   FP32 multigrid V-cycle from the first iteration that does not (fallback),
+   all inside the mixed-precision solver (FP64 residual refresh). */
+typedef struct icarat_net icarat_net;
+int icarat_net_create(int device, unsigned long long seed, icarat_net **out);
+int icarat_net_destroy(icarat_net *net);
+int icarat_net_num_params(icarat_net *net, long long *n);
+/* FP32 master weights in layer order (W[cout][cin][k^3] then b[cout]) */
+int icarat_net_get_params(icarat_net *net, float *w);
+int icarat_net_set_params(icarat_net *net, const float *w); /* resets Adam */
+/* one step on a sample of ctx's grid (rho: nelx, f and u: numeq): forward,
+   loss = 1 - cos^2(net(f / s), u) over free DOFs (s = ||f||; the uses of the
+   net do not depend on its output's scale) + 0.01 (|net|^2 - 1)^2 (keeps that
+   scale near 1), backward, then Adam with learning
+   rate lr (lr = 0: gradients only); *loss is the loss before the update */
+int icarat_net_train_step(icarat_net *net, icarat_ctx *ctx, const double *rho,
+                          const double *f, const double *u, double lr, double *loss);
+/* gradients of the last training step, in the order of the parameters */
+int icarat_net_get_grads(icarat_net *net, float *g);
+/* s net(f / s) on ctx's current design (numeq in and out): a vector along
+   the net's estimate of K^-1 f (its scale is not fitted) */
+int icarat_net_infer(icarat_net *net, icarat_ctx *ctx, const double *f, double *u);
+/* the net used by ICARAT_SOLVER_LEARNED_FPCG on this context (NULL: none) */
+int icarat_ctx_set_net(icarat_ctx *ctx, icarat_net *net);
 
 /* ---- stiffness operators by precision (no reference counterpart) -------- */
 enum

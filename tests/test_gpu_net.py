@@ -1,0 +1,208 @@
+"""Learned preconditioner: the GPU network kernels against the CPU oracle
+(oracle/net_oracle.py), training on the GPU, and the learned flexible PCG
+with its multigrid fallback.
+
+Loss: 1 - cos^2 between the net's output and the solution (scale-free).
+Tolerances: loss within 1e-3 relative of the oracle's (both round weights and
+activations to BF16 at the same points; FP32 sums in different orders);
+gradients within 3e-2 relative (L2 per layer) -- a sum that lands next to a
+BF16 rounding boundary can round the other way and move a gradient by
+2^-8 relative.  Solutions of the learned solver: the FP64 residual target and
+<= 1e-6 relative to an FP64 solve.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), ".."))
+from oracle import net_oracle as NO  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300)
+
+
+def node_fields(G, vec):
+    """numeq vector -> node-major [NZ][NY][NX][3] values and free mask"""
+    dof = G.dof_map()
+    free = dof < G.numeq
+    out = np.zeros(dof.shape)
+    out[free] = vec[dof[free]]
+    shape = (G.nz + 1, G.ny + 1, G.nx + 1, 3)
+    return out.reshape(shape), free.reshape(shape)
+
+
+def oracle_sample(G, rho, f, u):
+    fn, free = node_fields(G, f)
+    xin, s = NO.inputs(G.nx, G.ny, G.nz, rho, fn, ~free)
+    un, _ = node_fields(G, u)
+    P = xin.shape[1:]
+    t = np.zeros((3,) + P, dtype=np.float32)
+    m = np.zeros((3,) + P, dtype=bool)
+    NZ, NY, NX = G.nz + 1, G.ny + 1, G.nx + 1
+    for c in range(3):
+        t[c, :NZ, :NY, :NX] = np.where(free[..., c], un[..., c] / s, 0.0)
+        m[c, :NZ, :NY, :NX] = free[..., c]
+    return xin, t, m
+
+
+def layer_slices():
+    out, o = [], 0
+    for ci, co, k in NO.LAYERS:
+        n = co * ci * k ** 3 + co
+        out.append(slice(o, o + n))
+        o += n
+    return out
+
+
+def test_gpu_gradients_match_oracle(gpu):
+    G = gpu.Context(12, 6, 6)  # 13 x 7 x 7 nodes, padded to 16 x 8 x 8
+    rng = np.random.default_rng(11)
+    rho = rng.uniform(0.2, 1.0, G.nelx)
+    f = rng.standard_normal(G.numeq)
+    u = rng.standard_normal(G.numeq)
+    net = gpu.Net(seed=3)
+    w = net.params()
+    assert w.size == NO.n_params()
+    # non-zero biases so that every bias gradient path is exercised
+    w[layer_slices()[0]][-16:] = 0.05
+    net.set_params(w)
+    loss = net.train_step(G, rho, f, u, 0.0)
+    g = net.grads()
+    assert np.array_equal(net.params(), w)  # lr = 0 leaves the weights alone
+    xin, t, m = oracle_sample(G, rho, f, u)
+    loss_ref, g_ref, _ = NO.loss_and_grads(w, xin, t, m, bf=True)
+    assert abs(loss - loss_ref) <= 1e-3 * loss_ref
+    for i, sl in enumerate(layer_slices()):
+        a, b = g[sl].astype(np.float64), g_ref[sl].astype(np.float64)
+        nb = np.linalg.norm(b)
+        if nb == 0.0:
+            assert np.linalg.norm(a) == 0.0
+            continue
+        assert np.linalg.norm(a - b) <= 3e-2 * nb, (i, np.linalg.norm(a - b) / nb)
+
+
+def test_gpu_inference_matches_oracle(gpu):
+    G = gpu.Context(12, 6, 6)
+    rng = np.random.default_rng(12)
+    rho = rng.uniform(0.2, 1.0, G.nelx)
+    G.set_design(rho)
+    f = rng.standard_normal(G.numeq)
+    net = gpu.Net(seed=4)
+    w = net.params()
+    y = net.infer(G, f)
+    xin, t, m = oracle_sample(G, rho, f, f)
+    out, _, _ = NO.forward(w, xin, bf=True)
+    fn, free = node_fields(G, f)
+    s = np.sqrt((f ** 2).sum())
+    # oracle output back to numeq order
+    dof = G.dof_map().reshape(G.nz + 1, G.ny + 1, G.nx + 1, 3)
+    ref = np.zeros(G.numeq)
+    NZ, NY, NX = G.nz + 1, G.ny + 1, G.nx + 1
+    for c in range(3):
+        sel = free[..., c]
+        ref[dof[..., c][sel]] = s * out[c, :NZ, :NY, :NX][sel]
+    assert rel(y, ref) <= 1e-2
+
+
+def smooth_field(rng, nx, ny, nz, passes=3):
+    """Gaussian-like smoothed noise (box passes), zero mean, unit deviation"""
+    a = rng.standard_normal((nz, ny, nx))
+    for _ in range(passes):
+        b = np.zeros_like(a)
+        for ax in range(3):
+            b += np.roll(a, 1, ax) + np.roll(a, -1, ax)
+        a = (a + b) / 7.0
+    return (a - a.mean()) / a.std()
+
+
+def family(gpu, nx, ny, nz, n, seed, base_seed=30):
+    """Designs of one family, as a design loop produces them: a smooth base
+    density in [0.15, 0.9] with 10 % smooth perturbations, and a unit load at
+    a random node of the right face; solutions by FP64 MG-PCG."""
+    base = np.clip(0.5 + 0.25 * smooth_field(np.random.default_rng(base_seed), nx, ny, nz),
+                   0.15, 0.9)
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        node = (nx, int(rng.integers(0, ny + 1)), int(rng.integers(0, nz + 1)))
+        d, lo = gpu.cantilever_bc(nx, ny, nz, load_node=node)
+        G = gpu.Context(nx, ny, nz, dirichlet=d, loads=lo)
+        rho = np.clip(base * (1.0 + 0.1 * smooth_field(rng, nx, ny, nz)), 0.1, 1.0).ravel()
+        G.set_design(rho)
+        u, _ = G.solve(gpu.solve_opts(gpu.MG_PCG, rtol=1e-10, mg_levels=3))
+        out.append((G, rho, G.fext(), u))
+    return out
+
+
+def energy_error(G, x, u):
+    e = u - x
+    return (e @ G.apply_K(e)) / (u @ G.apply_K(u))
+
+
+def scaled_guess_error(G, net, f, u):
+    """energy-norm error of the learned solver's initial guess (the net's
+    output scaled by the energy-optimal factor), relative to the zero guess"""
+    x0 = net.infer(G, f)
+    return energy_error(G, (x0 @ f) / (x0 @ G.apply_K(x0)) * x0, u)
+
+
+def test_training_lowers_loss_and_learned_solver_gains(gpu):
+    train = family(gpu, 16, 8, 8, 128, 21)
+    held = family(gpu, 16, 8, 8, 6, 22)
+    net = gpu.Net(seed=5)
+    first = [net.train_step(G, r, f, u, 0.0) for G, r, f, u in train]
+    for epoch in range(6):
+        for G, r, f, u in train:
+            net.train_step(G, r, f, u, 2e-3)
+    last = [net.train_step(G, r, f, u, 0.0) for G, r, f, u in train]
+    print("training loss: first %.3f last %.3f" % (np.mean(first), np.mean(last)))
+    assert np.mean(last) < 0.6 * np.mean(first)
+    untrained = gpu.Net(seed=5)
+    gains = []
+    for G, r, f, u in held:
+        e_tr = scaled_guess_error(G, net, f, u)
+        e_un = scaled_guess_error(G, untrained, f, u)
+        gains.append(e_un / max(e_tr, 1e-30))
+        G.set_net(net)
+        v, info = G.solve(gpu.solve_opts(gpu.LEARNED_FPCG, rtol=1e-8, mg_levels=3))
+        _, ref = G.solve(gpu.solve_opts(gpu.MIXED_IR, rtol=1e-8, mg_levels=3))
+        print("held-out: initial energy error trained %.3g untrained %.3g; iterations "
+              "learned %d (net-preconditioned %d), mixed %d" %
+              (e_tr, e_un, info.iterations, info.learned_iterations, ref.iterations))
+        # the learned flexible PCG reaches the target and matches FP64
+        assert info.status == gpu.OK and info.rel_residual < 1e-8
+        assert rel(v, u) <= 1e-6
+        assert info.iterations <= ref.iterations + 3
+    # measured: held-out initial energy error 0.83-0.93 of the zero guess's
+    # (the cos^2 fit in the Euclidean norm leaves high-frequency error that
+    # the energy norm weights heavily); the trained net must beat the
+    # untrained one on every held-out sample
+    print("median gain in initial energy error: %.2f" % np.median(gains))
+    assert min(gains) > 1.02
+
+
+def test_zero_net_falls_back_to_multigrid(gpu):
+    """A stalled net (all weights 0: output 0) is caught before it is used:
+    the solve runs on the multigrid V-cycle alone and still converges."""
+    G = gpu.Context(16, 8, 8)
+    G.set_design(np.random.default_rng(13).uniform(0.1, 0.9, G.nelx))
+    u64, _ = G.solve(gpu.solve_opts(gpu.MG_PCG, rtol=1e-12, mg_levels=3))
+    net = gpu.Net(seed=6)
+    net.set_params(np.zeros(net.n, dtype=np.float32))
+    G.set_net(net)
+    u, info = G.solve(gpu.solve_opts(gpu.LEARNED_FPCG, rtol=1e-9, mg_levels=3))
+    assert info.status == gpu.OK and info.learned_iterations == 0
+    assert rel(u, u64) <= 1e-6
+
+
+def test_learned_solver_needs_a_net(gpu):
+    G = gpu.Context(8, 4, 4)
+    G.set_design(np.full(G.nelx, 0.5))
+    with pytest.raises(gpu.IcaratError) as e:
+        G.solve(gpu.solve_opts(gpu.LEARNED_FPCG, rtol=1e-8, mg_levels=2))
+    assert e.value.status == gpu.ERR_STATE
