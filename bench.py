@@ -66,6 +66,11 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=3,
                    help="design iterations of the 80-design batch section (0: skip)")
     p.add_argument("--batch-rtol", type=float, default=1e-6)
+    p.add_argument("--learned-grid", default="96x48x48",
+                   help="grid of the learned-preconditioner section ('' skips it)")
+    p.add_argument("--learned-train", type=int, default=64,
+                   help="training samples generated by the plain solver")
+    p.add_argument("--learned-epochs", type=int, default=3)
     return p.parse_args()
 
 
@@ -391,6 +396,102 @@ def batch_section(a, G, torch, dev):
     return out
 
 
+def smooth_field(rng, nx, ny, nz, passes=3):
+    a = rng.standard_normal((nz, ny, nx))
+    for _ in range(passes):
+        b = np.zeros_like(a)
+        for ax in range(3):
+            b += np.roll(a, 1, ax) + np.roll(a, -1, ax)
+        a = (a + b) / 7.0
+    return (a - a.mean()) / a.std()
+
+
+def learned_samples(G, nx, ny, nz, n, seed, levels):
+    """Designs of one family (smooth base density in [0.15, 0.9], 10 %
+    smooth perturbations) with a unit load at a random right-face node;
+    solutions by the plain FP64 MG-PCG (rtol 1e-10)."""
+    base = np.clip(0.5 + 0.25 * smooth_field(np.random.default_rng(30), nx, ny, nz), 0.15, 0.9)
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        node = (nx, int(rng.integers(0, ny + 1)), int(rng.integers(0, nz + 1)))
+        d, lo = G.cantilever_bc(nx, ny, nz, load_node=node)
+        c = G.Context(nx, ny, nz, dirichlet=d, loads=lo)
+        rho = np.clip(base * (1.0 + 0.1 * smooth_field(rng, nx, ny, nz)), 0.1, 1.0).ravel()
+        c.set_design(rho)
+        u, _ = c.solve(G.solve_opts(G.MG_PCG, 1e-10, 10000, levels, 2))
+        out.append((c, rho, c.fext(), u))
+    return out
+
+
+def learned_section(a, G, torch):
+    """Learned flexible PCG against the mixed and the FP64 multigrid solvers
+    on held-out samples: iterations and wall time to rtol 1e-6 (one solve
+    each, synchronised host clock), after training the net on the GPU on a
+    bounded sample of the data set."""
+    nx, ny, nz = (int(v) for v in a.learned_grid.split("x"))
+    levels = 4
+    t0 = time.perf_counter()
+    train = learned_samples(G, nx, ny, nz, a.learned_train, 21, levels)
+    t_data = time.perf_counter() - t0
+    net = G.Net(seed=5)
+    losses = []
+    t1 = time.perf_counter()
+    for ep in range(a.learned_epochs):
+        losses.append(float(np.mean([net.train_step(c, r, f, u, 2e-3) for c, r, f, u in train])))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    steps = a.learned_epochs * len(train)
+    out = {"grid": [nx, ny, nz], "mg_levels": levels, "train_samples": len(train),
+           "epochs": a.learned_epochs, "data_generation_s": t_data, "train_s": t_train,
+           "train_ms_per_step": 1000.0 * t_train / max(steps, 1), "epoch_losses": losses,
+           "loss": "1 - cos^2 (scale-free) + 0.01 (|y|^2 - 1)^2", "held_out": []}
+    for c, r, f, u in learned_samples(G, nx, ny, nz, 3, 22, levels):
+        c.set_net(net)
+        row = {}
+        for name, meth in (("learned_fpcg", G.LEARNED_FPCG), ("mixed", G.MIXED_IR),
+                           ("fp64_mg_pcg", G.MG_PCG)):
+            c.solve(G.solve_opts(meth, 1e-6, 10000, levels, 2), want_val=False)  # warm-up
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            _, info = c.solve(G.solve_opts(meth, 1e-6, 10000, levels, 2), want_val=False)
+            torch.cuda.synchronize()
+            row[name] = {"iterations": info.iterations, "ms": 1000.0 * (time.perf_counter() - ts),
+                         "status": info.status}
+            if meth == G.LEARNED_FPCG:
+                row[name]["net_preconditioned_iterations"] = info.learned_iterations
+        out["held_out"].append(row)
+    # the same net at the mixed-precision grid: inference time and the solve
+    gx, gy, gz = (int(v) for v in a.mixed_grid.split("x")) if a.mixed_grid else (0, 0, 0)
+    if gx:
+        c = G.Context(gx, gy, gz)
+        rho = np.random.default_rng(0).uniform(0.1, 0.5, gx * gy * gz)
+        c.set_design(rho)
+        f = c.fext()
+        net.infer(c, f)
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
+        net.infer(c, f)
+        torch.cuda.synchronize()
+        big = {"grid": [gx, gy, gz], "net_inference_ms": 1000.0 * (time.perf_counter() - ts),
+               "note": "net trained at the smaller grid"}
+        c.set_net(net)
+        for name, meth in (("learned_fpcg", G.LEARNED_FPCG), ("mixed", G.MIXED_IR),
+                           ("fp64_mg_pcg", G.MG_PCG)):
+            c.solve(G.solve_opts(meth, 1e-6, 10000, a.mixed_levels, 2), want_val=False)
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            _, info = c.solve(G.solve_opts(meth, 1e-6, 10000, a.mixed_levels, 2),
+                              want_val=False)
+            torch.cuda.synchronize()
+            big[name] = {"iterations": info.iterations,
+                         "ms": 1000.0 * (time.perf_counter() - ts), "status": info.status}
+        out["at_mixed_grid"] = big
+        c.close()
+    net.close()
+    return out
+
+
 def gpu_arm(a):
     import torch
     import torch.distributed as dist
@@ -574,6 +675,9 @@ def gpu_arm(a):
     batched = None
     if a.batch_steps > 0:
         batched = batch_section(a, G, torch, dev)
+    learned = None
+    if a.learned_grid:
+        learned = learned_section(a, G, torch)
 
     if rank == 0:
         cg = [i.cg_iterations for i in infos]
@@ -601,6 +705,7 @@ def gpu_arm(a):
             "alt_levels": alt,
             "mixed_256x128x128": mixed,
             "batched_80_designs": batched,
+            "learned": learned,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }
