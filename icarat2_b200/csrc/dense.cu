@@ -12,6 +12,8 @@
 //   2. W by recursive triangular inversion: with L = [L11 0; L21 L22],
 //      W21 = -W22 (L21 W11), two GEMMs per split.
 // Matrices are row-major with leading dimension n.
+#include <type_traits>
+
 #include "internal.cuh"
 
 namespace icarat_b200
@@ -167,65 +169,172 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmArgs g)
       }
 }
 
-// Factor the 64 x 64 diagonal block at k0 in shared memory, write L_kk into A
-// (zeros above the diagonal) and W_kk = L_kk^-1 into W.  Rows / columns past
-// n are padded with the identity.
-constexpr int kPotrfSmem = 2 * 64 * 65 * sizeof(double);
+// Factor the 64 x 64 diagonal block at k0, write L_kk into A (zeros above the
+// diagonal) and W_kk = L_kk^-1 into W.  Rows / columns past n are padded with
+// the identity.
+//
+// The block lives in registers: thread (ty, tx) of a 16 x 16 grid holds rows
+// 4ty..4ty+3 and columns 4tx..4tx+3.  Elimination is right-looking in the
+// unscaled form a_rc -= a_rj a_cj / a_jj (the square roots and the column
+// scaling come after the loop): per column j the owners publish column j to
+// shared memory and one barrier later every thread updates its 16 entries.
+// The inverse is a forward substitution by rows in the same tiles (row k of
+// L^-1 and column k of L published per step).  The published vectors are
+// double-buffered, so each step needs a single barrier.
+constexpr int kPotrfSmem = (4 * 64 + 2 * 64) * sizeof(double);
+
+// 1 / x and 1 / sqrt(x) for x > 0 by Newton's method from an FP32 seed
+// (y <- y (2 - x y), and y <- y (3/2 - x y^2 / 2)): each step doubles the
+// correct digits, three steps reach double precision from the seed's ~2^-22.
+// Inline FMAs only: an out-of-line divide or square root inside the loops
+// below would save the register-resident block to the stack at every call.
+__device__ __forceinline__ double recip_newton(double x)
+{
+  double y = (double)__fdividef(1.0f, (float)x);
+#pragma unroll
+  for(int it = 0; it < 3; it++)
+    y = y * fma(-x, y, 2.0);
+  return y;
+}
+
+__device__ __forceinline__ double rsqrt_newton(double x)
+{
+  double y = (double)rsqrtf((float)x);
+#pragma unroll
+  for(int it = 0; it < 3; it++)
+    y = y * fma(-0.5 * x, y * y, 1.5);
+  return y;
+}
 
 __global__ void __launch_bounds__(256) k_potrf64(double *A, double *W, int n, int k0)
 {
   extern __shared__ double potrf_smem[];
-  double(*L)[65] = reinterpret_cast<double(*)[65]>(potrf_smem);
-  double(*Wi)[65] = reinterpret_cast<double(*)[65]>(potrf_smem + 64 * 65);
+  double(*vec)[64] = reinterpret_cast<double(*)[64]>(potrf_smem); // [4][64]
+  double *isq = potrf_smem + 4 * 64; // 1 / sqrt(pivot)
+  double *sq = isq + 64;              // sqrt(pivot)
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
   const int m = min(64, n - k0);
-  for(int t = threadIdx.x; t < 64 * 64; t += blockDim.x)
+  double a[4][4];
+#pragma unroll
+  for(int i = 0; i < 4; i++)
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+    {
+      const int r = 4 * ty + i, c = 4 * tx + q;
+      a[i][q] = (r < m && c < m) ? A[(long)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
+    }
+  // ---- elimination (by 4 columns, so that the published register column is
+  // a compile-time index)
+  auto elim = [&](auto qc, int j)
   {
-    const int r = t / 64, c = t % 64;
-    L[r][c] = (r < m && c < m) ? A[(long)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
+    constexpr int Q = decltype(qc)::value;
+    double *col = vec[j & 1];
+    if(tx == (j >> 2))
+#pragma unroll
+      for(int i = 0; i < 4; i++)
+        col[4 * ty + i] = a[i][Q];
+    __syncthreads();
+    const double inv = recip_newton(col[j]);
+    double fr[4], fc[4];
+#pragma unroll
+    for(int i = 0; i < 4; i++)
+    {
+      fr[i] = col[4 * ty + i];
+      fc[i] = col[4 * tx + i] * inv;
+    }
+#pragma unroll
+    for(int i = 0; i < 4; i++)
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+      {
+        const int r = 4 * ty + i, c = 4 * tx + q;
+        if(c > j && r >= c)
+          a[i][q] = fma(-fr[i], fc[q], a[i][q]);
+      }
+  };
+  for(int j = 0; j < 64; j += 4)
+  {
+    elim(std::integral_constant<int, 0>{}, j);
+    elim(std::integral_constant<int, 1>{}, j + 1);
+    elim(std::integral_constant<int, 2>{}, j + 2);
+    if(j + 3 < 63)
+      elim(std::integral_constant<int, 3>{}, j + 3);
   }
+  // ---- scaling: L_rc = a_rc / sqrt(a_cc), L_cc = sqrt(a_cc)
+  if(tx == ty)
+#pragma unroll
+    for(int i = 0; i < 4; i++)
+    {
+      const double y = rsqrt_newton(a[i][i]);
+      isq[4 * ty + i] = y;
+      sq[4 * ty + i] = a[i][i] * y;
+    }
   __syncthreads();
-  // right-looking: thread (column c, phase q) updates rows c + q, c + q + 4, ...
-  const int c = threadIdx.x & 63, q = threadIdx.x >> 6;
-  for(int j = 0; j < 64; j++)
-  {
-    if(threadIdx.x == 0)
-      L[j][j] = sqrt(L[j][j]);
-    __syncthreads();
-    if(threadIdx.x < 63 - j)
-      L[j + 1 + threadIdx.x][j] /= L[j][j];
-    __syncthreads();
-    if(c > j)
+#pragma unroll
+  for(int i = 0; i < 4; i++)
+#pragma unroll
+    for(int q = 0; q < 4; q++)
     {
-      const double lcj = L[c][j];
-      for(int r = c + q; r < 64; r += 4)
-        L[r][c] -= L[r][j] * lcj;
+      const int r = 4 * ty + i, c = 4 * tx + q;
+      a[i][q] = r > c ? a[i][q] * isq[c] : (r == c ? sq[c] : 0.0);
     }
+  // ---- inverse: w = I, then per row k: w_k /= L_kk (final), w_r -= L_rk w_k (r > k)
+  double w[4][4];
+#pragma unroll
+  for(int i = 0; i < 4; i++)
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+      w[i][q] = (4 * ty + i == 4 * tx + q) ? 1.0 : 0.0;
+  auto inv_step = [&](auto qc, int k)
+  {
+    constexpr int Q = decltype(qc)::value;
+    double *row = vec[2 + (k & 1)];
+    double *colL = vec[k & 1];
+    const double ilkk = isq[k]; // 1 / L_kk
+    if(ty == (k >> 2))
+#pragma unroll
+      for(int q = 0; q < 4; q++)
+      {
+        w[Q][q] *= ilkk;
+        row[4 * tx + q] = w[Q][q];
+      }
+    if(tx == (k >> 2))
+#pragma unroll
+      for(int i = 0; i < 4; i++)
+        colL[4 * ty + i] = a[i][Q];
     __syncthreads();
-  }
-  // column c of L^-1 by forward substitution (one thread per column)
-  if(threadIdx.x < 64)
-  {
-    const int c = threadIdx.x;
-    for(int r = 0; r < c; r++)
-      Wi[r][c] = 0.0;
-    for(int r = c; r < 64; r++)
+#pragma unroll
+    for(int i = 0; i < 4; i++)
     {
-      double s = (r == c) ? 1.0 : 0.0;
-      for(int k = c; k < r; k++)
-        s -= L[r][k] * Wi[k][c];
-      Wi[r][c] = s / L[r][r];
+      const int r = 4 * ty + i;
+      if(r > k)
+      {
+        const double l = colL[r];
+#pragma unroll
+        for(int q = 0; q < 4; q++)
+          w[i][q] = fma(-l, row[4 * tx + q], w[i][q]);
+      }
     }
-  }
-  __syncthreads();
-  for(int t = threadIdx.x; t < 64 * 64; t += blockDim.x)
+  };
+  for(int k = 0; k < 64; k += 4)
   {
-    const int r = t / 64, c = t % 64;
-    if(r < m && c < m)
-    {
-      A[(long)(k0 + r) * n + k0 + c] = (c <= r) ? L[r][c] : 0.0;
-      W[(long)(k0 + r) * n + k0 + c] = (c <= r) ? Wi[r][c] : 0.0;
-    }
+    inv_step(std::integral_constant<int, 0>{}, k);
+    inv_step(std::integral_constant<int, 1>{}, k + 1);
+    inv_step(std::integral_constant<int, 2>{}, k + 2);
+    inv_step(std::integral_constant<int, 3>{}, k + 3);
   }
+#pragma unroll
+  for(int i = 0; i < 4; i++)
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+    {
+      const int r = 4 * ty + i, c = 4 * tx + q;
+      if(r < m && c < m)
+      {
+        A[(long)(k0 + r) * n + k0 + c] = a[i][q];
+        W[(long)(k0 + r) * n + k0 + c] = (c <= r) ? w[i][q] : 0.0;
+      }
+    }
 }
 
 // t = W v (W lower triangular), one warp per row
