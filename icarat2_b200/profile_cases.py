@@ -1,0 +1,77 @@
+"""Profiling drivers: run exactly one piece of work between cudaProfilerStart
+and cudaProfilerStop, so that an external profiler started with
+`--profile-from-start off` (ncu) captures that piece and nothing of the
+set-up.
+
+    python -m icarat2_b200.profile_cases solve 128x64x64 mg 4 1e-8
+        one K u = f solve of the cantilever (densities U[0.1, 0.5], seed 0),
+        after a warm-up solve and a design change (so the per-design
+        multigrid set-up is inside the captured region);
+        methods: jacobi, mg, mixed
+    python -m icarat2_b200.profile_cases operator 256x128x128 2 3
+        `reps` launches of K u with operator 0 FP64, 1 FP32, 2 tensor cores
+        BF16x3, 3 tensor cores BF16 (after one warm-up launch)
+"""
+import ctypes as C
+import sys
+
+import numpy as np
+
+import icarat2_b200 as gpu
+
+
+def _profiler():
+    for name in ("libcudart.so.12", "libcudart.so"):
+        try:
+            return C.CDLL(name)
+        except OSError:
+            continue
+    raise OSError("libcudart not found")
+
+
+def _grid(s):
+    return tuple(int(v) for v in s.split("x"))
+
+
+def solve(grid, method, levels, rtol):
+    nx, ny, nz = _grid(grid)
+    G = gpu.Context(nx, ny, nz)
+    rho = np.random.default_rng(0).uniform(0.1, 0.5, G.nelx)
+    G.set_design(rho)
+    m = {"jacobi": gpu.JACOBI_PCG, "mg": gpu.MG_PCG, "mixed": gpu.MIXED_IR}[method]
+    o = gpu.solve_opts(m, rtol=float(rtol), mg_levels=int(levels))
+    G.solve(o, want_val=False)
+    G.set_design(rho * 1.01)
+    G.synchronize()
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    _, info = G.solve(o, want_val=False)
+    rt.cudaProfilerStop()
+    print("iterations %d rel_residual %.3g status %d" % (info.iterations, info.rel_residual,
+                                                         info.status))
+
+
+def operator(grid, op, reps):
+    nx, ny, nz = _grid(grid)
+    G = gpu.Context(nx, ny, nz)
+    G.set_design(np.random.default_rng(1).uniform(0.1, 0.5, G.nelx))
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    ms = G.time_operator(int(reps), int(op))
+    rt.cudaProfilerStop()
+    print("ms per launch %.4f" % ms)
+
+
+def main(argv):
+    if len(argv) >= 5 and argv[0] == "solve":
+        solve(*argv[1:5])
+    elif len(argv) >= 4 and argv[0] == "operator":
+        operator(*argv[1:4])
+    else:
+        sys.stderr.write(__doc__)
+        return 2
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))
