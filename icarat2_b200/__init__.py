@@ -102,7 +102,8 @@ class LoopOpts(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("maxit", C.c_int), ("refresh", C.c_double),
-                ("tile", C.c_int), ("blocks_per_sm", C.c_int)]
+                ("tile", C.c_int), ("blocks_per_sm", C.c_int), ("method", C.c_int),
+                ("mg_levels", C.c_int), ("chunk", C.c_int), ("warm_start", C.c_int)]
 
 
 class StepInfo(C.Structure):
@@ -646,8 +647,13 @@ class Batch:
         self.close()
 
     @staticmethod
-    def opts(rtol=1e-8, maxit=10000, refresh=0.0, tile=0, blocks_per_sm=0):
-        return BatchOpts(rtol, maxit, refresh, tile, blocks_per_sm)
+    def opts(rtol=1e-8, maxit=10000, refresh=0.0, tile=0, blocks_per_sm=0, method=0,
+             mg_levels=0, chunk=0, warm_start=False):
+        """method 0: one persistent Jacobi launch for all designs;
+        MIXED_IR: each design's own mixed-precision multigrid solve,
+        interleaved on the designs' streams."""
+        return BatchOpts(rtol, maxit, refresh, tile, blocks_per_sm, method, mg_levels, chunk,
+                         int(bool(warm_start)))
 
     def autotune(self):
         t, b, ms = C.c_int(), C.c_int(), C.c_double()

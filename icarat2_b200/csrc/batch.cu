@@ -648,6 +648,96 @@ static int pick_bpsm(icarat_batch *B, const icarat_batch_opts *o)
   return B->blocks_per_sm > 0 ? B->blocks_per_sm : B->occ;
 }
 
+// Largest level count <= want (at least 2) for which every division of the
+// design halves level-1 times.
+static int design_levels(const icarat_ctx *c, int want)
+{
+  int L = std::max(2, want);
+  while(L > 2)
+  {
+    const int m = 1 << (L - 1);
+    if(c->nx % m == 0 && c->ny % m == 0 && c->nz % m == 0)
+      break;
+    L--;
+  }
+  return L;
+}
+
+static void note_result(icarat_ctx *c, const icarat_solve_info &si, icarat_solve_info *out,
+                        int &worst)
+{
+  c->solved = true;
+  c->last_info = si;
+  if(out)
+    *out = si;
+  if(si.status < 0)
+    worst = std::min(worst, si.status);
+  else if(worst >= 0 && si.status > worst)
+    worst = si.status;
+}
+
+// Every design's own mixed-precision multigrid-PCG (the solver of
+// ICARAT_SOLVER_MIXED_IR with the FP32 operator on every level), the
+// designs interleaved: each round queues one graph replay of `chunk`
+// iterations on the stream of every design still running, then waits for
+// the designs one by one, so that while the host reads one design's stop
+// flag the others' replays run on the GPU.  The multigrid set-ups
+// (transfer of the moduli, coarse dense factor) are queued on the design
+// streams too and overlap in the same way.
+static int batch_solve_concurrent(icarat_batch *B, const icarat_batch_opts *o, double rtol,
+                                  int maxit, double refresh, icarat_solve_info *infos)
+{
+  const size_t n = B->ctx.size();
+  const int want = o->mg_levels > 0 ? o->mg_levels : 4;
+  IREQUIRE(want >= 2 && want <= 12, ICARAT_ERR_ARG, "mg_levels must be in [2, 12]");
+  IREQUIRE(o->chunk >= 0, ICARAT_ERR_ARG, "chunk must be non-negative");
+  std::vector<MixedRun> run(n);
+  for(size_t d = 0; d < n; d++)
+  {
+    icarat_ctx *c = B->ctx[d];
+    icarat_solve_opts so{};
+    so.method = ICARAT_SOLVER_MIXED_IR;
+    so.rtol = rtol;
+    so.maxit = maxit;
+    so.mg_levels = design_levels(c, want);
+    so.chunk = o->chunk;
+    so.refresh = refresh;
+    so.fine_op = ICARAT_OP_FP32;
+    so.krylov_op = ICARAT_OP_FP32;
+    so.warm_start = (o->warm_start && c->solved) ? 1 : 0;
+    mixed_begin(c, &so, c->d_rhs, c->d_u, run[d]);
+    ICK(cudaEventRecord(B->ev[d], c->stream));
+  }
+  std::vector<char> active(n, 1);
+  for(size_t live = n; live > 0;)
+  {
+    live = 0;
+    for(size_t d = 0; d < n; d++)
+    {
+      if(!active[d])
+        continue;
+      icarat_ctx *c = B->ctx[d];
+      ICK(cudaEventSynchronize(B->ev[d]));
+      if(!mixed_poll(c, run[d]))
+      {
+        active[d] = 0;
+        continue;
+      }
+      mixed_chunk(c, run[d]);
+      ICK(cudaEventRecord(B->ev[d], c->stream));
+      live++;
+    }
+  }
+  int worst = ICARAT_OK;
+  for(size_t d = 0; d < n; d++)
+  {
+    icarat_solve_info si{};
+    mixed_finish(B->ctx[d], run[d], &si);
+    note_result(B->ctx[d], si, infos ? &infos[d] : nullptr, worst);
+  }
+  return worst;
+}
+
 static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
                             icarat_solve_info *infos)
 {
@@ -655,6 +745,11 @@ static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
   const int maxit = o && o->maxit > 0 ? o->maxit : 10000;
   const double refresh = o && o->refresh > 0.0 ? o->refresh : 1e-2;
   IREQUIRE(rtol >= 0.0 && refresh < 1.0, ICARAT_ERR_ARG, "bad batch options");
+  const int method = o ? o->method : 0;
+  IREQUIRE(method == 0 || method == ICARAT_SOLVER_MIXED_IR, ICARAT_ERR_ARG,
+           "batch method must be 0 or ICARAT_SOLVER_MIXED_IR");
+  if(method == ICARAT_SOLVER_MIXED_IR)
+    return batch_solve_concurrent(B, o, rtol, maxit, refresh, infos);
   const int tile = pick_tile(B, o), bpsm = pick_bpsm(B, o);
   IREQUIRE(tile >= 32 && tile <= (1 << 16), ICARAT_ERR_ARG, "tile must be in [32, 65536]");
   batch_run(B, tile, bpsm, rtol, maxit, refresh);
@@ -673,14 +768,7 @@ static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
     si.rel_residual = S.bb > 0 ? std::sqrt(S.rr_true / S.bb) : 0.0;
     si.status = S.done ? S.status : ICARAT_WARN_MAXITER;
     si.refreshes = S.nrefresh;
-    c->solved = true;
-    c->last_info = si;
-    if(infos)
-      infos[d] = si;
-    if(si.status < 0)
-      worst = std::min(worst, si.status);
-    else if(worst >= 0 && si.status > worst)
-      worst = si.status;
+    note_result(c, si, infos ? &infos[d] : nullptr, worst);
   }
   return worst;
 }

@@ -316,6 +316,18 @@ void net_apply(icarat_net *N, icarat_ctx *c, const T *r, double s, T *z);
 void launch_ku_tc(icarat_ctx *c, int op, int terms, TcArgs a, cudaStream_t st);
 
 // mixed.cu
+struct MixedRun
+{
+  cudaGraphExec_t exec = nullptr; // chunk of iterations
+  int kernels = 0;                // kernel nodes per replay
+  long max_chunks = 0, chunks = 0;
+  int learned_its = 0;
+};
+void mixed_begin(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, double *d_x,
+                 MixedRun &run);
+bool mixed_poll(icarat_ctx *c, const MixedRun &run);
+void mixed_chunk(icarat_ctx *c, MixedRun &run);
+int mixed_finish(icarat_ctx *c, const MixedRun &run, icarat_solve_info *info);
 int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                 double *d_x, icarat_solve_info *info);
 void mixed_alloc(icarat_ctx *c);

@@ -519,8 +519,11 @@ static const MxScalars &read_scalars(icarat_ctx *c)
 // iterations preconditioned by the net at most, before the multigrid takes over
 constexpr int kLearnedMaxIterations = 50;
 
-int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
-                double *d_x, icarat_solve_info *info)
+// Everything before the chunk loop: set-up, initial guess and residual, the
+// first preconditioning (and the learned phase), and the captured iteration
+// graph.  Asynchronous on the context's stream except for the learned phase.
+void mixed_begin(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, double *d_x,
+                 MixedRun &run)
 {
   IREQUIRE(o->rtol >= 0.0, ICARAT_ERR_ARG, "rtol must be non-negative");
   IREQUIRE(o->refresh >= 0.0 && o->refresh < 1.0, ICARAT_ERR_ARG,
@@ -680,28 +683,57 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   }
   else
     exec = it->second;
-  const int graph_kernels = c->graph_kernels[key];
-  const long max_chunks = (long)(o->maxit + 1 + chunk - 1) / chunk + 1;
-  for(long ch = 0; ch < max_chunks; ch++)
-  {
-    ICK(cudaMemcpyAsync(c->h_mx, c->d_mx, sizeof(MxScalars), cudaMemcpyDeviceToHost,
-                        c->stream));
-    ICK(cudaStreamSynchronize(c->stream));
-    if(c->h_mx->done)
-      break;
-    ICK(cudaGraphLaunch(exec, c->stream));
-    note_launch(graph_kernels);
-  }
+  run.exec = exec;
+  run.kernels = c->graph_kernels[key];
+  run.max_chunks = (long)(o->maxit + 1 + chunk - 1) / chunk + 1;
+  run.chunks = 0;
+  run.learned_its = learned_its;
+  // the stop flag as it stands after the set-up (read by mixed_poll)
   ICK(cudaMemcpyAsync(c->h_mx, c->d_mx, sizeof(MxScalars), cudaMemcpyDeviceToHost,
                       c->stream));
-  ICK(cudaStreamSynchronize(c->stream));
+}
+
+// After the stream has passed the last copy of the scalars: true while the
+// solve needs another chunk.
+bool mixed_poll(icarat_ctx *c, const MixedRun &run)
+{
+  return !c->h_mx->done && run.chunks < run.max_chunks;
+}
+
+// One chunk of iterations (graph replay) and the copy of the scalars after it.
+void mixed_chunk(icarat_ctx *c, MixedRun &run)
+{
+  ICK(cudaGraphLaunch(run.exec, c->stream));
+  note_launch(run.kernels);
+  run.chunks++;
+  ICK(cudaMemcpyAsync(c->h_mx, c->d_mx, sizeof(MxScalars), cudaMemcpyDeviceToHost,
+                      c->stream));
+}
+
+int mixed_finish(icarat_ctx *c, const MixedRun &run, icarat_solve_info *info)
+{
   const MxScalars &s = *c->h_mx;
   info->iterations = s.iter;
   info->rel_residual = s.bb > 0 ? std::sqrt(s.rr_true / s.bb) : 0.0;
   info->status = s.done ? s.status : ICARAT_WARN_MAXITER;
   info->refreshes = s.nrefresh;
-  info->learned_iterations = learned_its;
+  info->learned_iterations = run.learned_its;
   return info->status;
+}
+
+int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
+                double *d_x, icarat_solve_info *info)
+{
+  MixedRun run;
+  mixed_begin(c, o, d_b, d_x, run);
+  for(;;)
+  {
+    ICK(cudaStreamSynchronize(c->stream));
+    if(!mixed_poll(c, run))
+      break;
+    mixed_chunk(c, run);
+  }
+  return mixed_finish(c, run, info);
 }
 
 } // namespace icarat_b200

@@ -308,6 +308,17 @@ typedef struct
   int tile;          /* nodes per work item (0 = autotuned, else 256) */
   int blocks_per_sm; /* persistent CTAs per SM (0 = autotuned, else the
                         occupancy limit) */
+  int method;        /* 0 = the persistent Jacobi launch above;
+                        ICARAT_SOLVER_MIXED_IR = every design's own
+                        mixed-precision multigrid-PCG (FP32 operator and
+                        V-cycle, FP64 refresh and stopping test), the designs
+                        interleaved on their own streams as CUDA-graph
+                        replays of `chunk` iterations */
+  int mg_levels;     /* MIXED_IR: levels (0 = 4); a design whose divisions
+                        do not halve that often gets fewer */
+  int chunk;         /* MIXED_IR: iterations per replay (0 = 4) */
+  int warm_start;    /* MIXED_IR: start from each design's last solution
+                        (designs not solved yet start from 0) */
 } icarat_batch_opts;
 
 int icarat_batch_create(const icarat_grid *grids, const icarat_bc *bcs, int count,

@@ -1,4 +1,5 @@
-"""Batched solver (one persistent launch over many designs of uneven size).
+"""Batched solver (one persistent launch over many designs of uneven size,
+or every design's own mixed-precision multigrid solve, interleaved).
 
 Every member is checked against the library's FP64 multigrid-PCG solve of the
 same design on its own context (rtol 1e-12): displacements <= 1e-6 relative
@@ -145,3 +146,97 @@ def test_batch_rejects_mixed_element_sizes(gpu):
     with pytest.raises(gpu.IcaratError) as e:
         gpu.Batch(prs)
     assert e.value.status == gpu.ERR_UNSUPPORTED
+
+
+# ---- interleaved per-design mixed-precision multigrid (method MIXED_IR) ----
+
+def test_batch_concurrent_mg_matches_individual_solves(gpu):
+    prs = problems(gpu, SIZES, 11)
+    B = gpu.Batch(prs)
+    rng = np.random.default_rng(12)
+    rhos = [rng.uniform(0.1, 0.9, B[i].nelx) for i in range(len(B))]
+    for i, r in enumerate(rhos):
+        B[i].set_design(r)
+    jac = B.solve(B.opts(rtol=1e-9))
+    infos = B.solve(B.opts(rtol=1e-9, method=gpu.MIXED_IR))
+    for i, pr in enumerate(prs):
+        assert infos[i].status == gpu.OK and infos[i].rel_residual < 1e-9
+        assert infos[i].refreshes >= 1
+        # multigrid needs far fewer iterations than the Jacobi launch
+        assert infos[i].iterations < jac[i].iterations
+        u = B.solution(i)
+        assert rel(u, reference(gpu, pr, rhos[i], 2)) <= 1e-6
+        f = B[i].fext()
+        assert np.linalg.norm(f - B[i].apply_K(u)) < 1.001e-9 * np.linalg.norm(f)
+
+
+def test_batch_concurrent_mg_levels_and_chunk(gpu):
+    # 32x16x16 takes 4 levels, 24x12x12 and 8x4x4 only 3
+    prs = problems(gpu, [(32, 16, 16), (24, 12, 12), (8, 4, 4)], 13)
+    B = gpu.Batch(prs)
+    rng = np.random.default_rng(14)
+    rhos = [rng.uniform(0.1, 0.9, B[i].nelx) for i in range(len(B))]
+    for i, r in enumerate(rhos):
+        B[i].set_design(r)
+    for chunk in (1, 3):
+        infos = B.solve(B.opts(rtol=1e-10, method=gpu.MIXED_IR, mg_levels=4, chunk=chunk))
+        for i, pr in enumerate(prs):
+            assert infos[i].status == gpu.OK
+            assert rel(B.solution(i), reference(gpu, pr, rhos[i], 2)) <= 1e-6
+
+
+def test_batch_concurrent_warm_start(gpu):
+    prs = problems(gpu, [(16, 8, 8), (32, 16, 16)], 15)
+    B = gpu.Batch(prs)
+    for i in range(len(B)):
+        B[i].set_design(np.full(B[i].nelx, 0.4))
+    o = B.opts(rtol=1e-9, method=gpu.MIXED_IR, warm_start=True)
+    cold = B.solve(o)  # nothing solved yet: starts from 0
+    warm = B.solve(o)  # same designs: starts at the solution
+    for c, w in zip(cold, warm):
+        assert c.status == gpu.OK and c.iterations > 0
+        assert w.status == gpu.OK and w.iterations == 0
+
+
+def test_batch_concurrent_iteration_cap_and_empty_load(gpu):
+    d = [((1, 1, 1), (0.0, 0.0, 0.0), ((0, 0), (0, 8), (0, 8)))]
+    prs = [(16, 8, 8, d, []), (16, 8, 8) + gpu.cantilever_bc(16, 8, 8)]
+    B = gpu.Batch(prs)
+    for i in range(2):
+        B[i].set_design(np.full(B[i].nelx, 0.5))
+    infos = B.solve(B.opts(rtol=1e-14, maxit=3, refresh=1e-6, method=gpu.MIXED_IR))
+    assert infos[0].status == gpu.OK and infos[0].iterations == 0
+    assert not B.solution(0).any()
+    # the mixed solver's cap: the iteration past maxit is the final refresh
+    assert infos[1].status == gpu.WARN_MAXITER and infos[1].iterations == 4
+
+
+def test_batch_concurrent_design_loop_tracks_individual_loops(gpu):
+    prs = problems(gpu, [(16, 8, 8), (24, 12, 12), (32, 16, 16)], 16)
+    B = gpu.Batch(prs)
+    solo = []
+    for i, (nx, ny, nz, d, lo) in enumerate(prs):
+        B[i].loop_init(0.3, method="mma", filter_radius=1.5, move=0.2)
+        G = gpu.Context(nx, ny, nz, dirichlet=d, loads=lo)
+        G.loop_init(0.3, method="mma", filter_radius=1.5, move=0.2,
+                    solve=gpu.solve_opts(gpu.MG_PCG, rtol=1e-12, mg_levels=2))
+        solo.append(G)
+    o = B.opts(rtol=1e-10, method=gpu.MIXED_IR, warm_start=True)
+    for _ in range(3):
+        infos = B.loop_step(o)
+        for i, G in enumerate(solo):
+            ref = G.loop_step()
+            assert infos[i].status == gpu.OK
+            assert abs(infos[i].compliance - ref.compliance) <= 1e-6 * ref.compliance
+    for i, G in enumerate(solo):
+        assert rel(B[i].loop_get("x"), G.loop_get("x")) <= 1e-6
+
+
+def test_batch_rejects_unknown_method(gpu):
+    B = gpu.Batch(problems(gpu, [(8, 4, 4)], 17))
+    B[0].set_design(np.full(B[0].nelx, 0.5))
+    for o in (B.opts(method=gpu.MG_PCG), B.opts(method=gpu.MIXED_IR, mg_levels=1),
+              B.opts(method=gpu.MIXED_IR, chunk=-1)):
+        with pytest.raises(gpu.IcaratError) as e:
+            B.solve(o)
+        assert e.value.status == gpu.ERR_ARG
