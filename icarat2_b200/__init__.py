@@ -42,6 +42,7 @@ OP_FP64 = 0
 OP_FP32 = 1
 OP_TC_BF16X3 = 2
 OP_TC_BF16 = 3
+OP_TC_FP64 = 4
 
 
 class IcaratError(RuntimeError):
@@ -78,7 +79,7 @@ class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int),
                 ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int),
                 ("refresh", C.c_double), ("fine_op", C.c_int), ("krylov_op", C.c_int),
-                ("warm_start", C.c_int)]
+                ("warm_start", C.c_int), ("fp64_tc", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -181,6 +182,7 @@ SIGNATURES = {
     "icarat_batch_solution": (_i, [_vp, _i, _dp]),
     "icarat_batch_loop_step": (_i, [_vp, _P(BatchOpts), _vp]),
     "icarat_time_operator_op": (_i, [_vp, _i, _i, _P(_d)]),
+    "icarat_mg_coarse_check": (_i, [_vp, _i, _P(_d), _P(_i)]),
     "icarat_loop_init": (_i, [_vp, _P(LoopOpts), _dp]),
     "icarat_loop_step": (_i, [_vp, _P(StepInfo)]),
     "icarat_loop_get": (_i, [_vp, _i, _dp]),
@@ -252,9 +254,11 @@ def _bc_struct(dirichlet, loads):
 
 
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
-               chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0):
+               chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0, fp64_tc=0):
+    """fp64_tc=1: FP64 products element by element on the FP64 tensor cores
+    instead of the node stencil (JACOBI_PCG, MG_PCG)."""
     return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,
-                     krylov_op, warm_start)
+                     krylov_op, warm_start, int(bool(fp64_tc)))
 
 
 class Context:
@@ -445,6 +449,14 @@ class Context:
                      xmax, filter_radius, solve if solve is not None else solve_opts())
         _check(self.lib.icarat_loop_init(self.h, C.byref(o), _f64(x0)), "loop_init")
 
+    def coarse_check(self, mg_levels=4):
+        """(||b - K_c x|| / ||b||, unknowns) of the multigrid's coarsest dense
+        solve on the current design."""
+        r, n = C.c_double(), C.c_int()
+        _check(self.lib.icarat_mg_coarse_check(self.h, mg_levels, C.byref(r), C.byref(n)),
+               "icarat_mg_coarse_check")
+        return r.value, n.value
+
     def time_operator(self, reps=20, op=OP_FP64):
         ms = C.c_double()
         _check(self.lib.icarat_time_operator_op(self.h, op, reps, C.byref(ms)),
@@ -458,7 +470,8 @@ class Context:
         self._net = net
 
     def apply_K_op(self, u, op):
-        """y = K u with operator `op` (OP_FP64, OP_FP32, OP_TC_BF16X3, OP_TC_BF16)."""
+        """y = K u with operator `op` (OP_FP64 node stencil, OP_FP32, OP_TC_BF16X3,
+        OP_TC_BF16, OP_TC_FP64)."""
         y = np.zeros(max(self.numeq, 1))
         _check(self.lib.icarat_apply_K_op(self.h, op, _f64(u), y), "apply_K_op")
         return y[:self.numeq]

@@ -76,6 +76,18 @@ int icarat_kernel_launches(unsigned long long *count)
   ICARAT_API_END
 }
 
+int icarat_mg_coarse_check(icarat_ctx *c, int mg_levels, double *rel_residual,
+                           int *n_coarse)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(rel_residual, ICARAT_ERR_ARG, "bad argument");
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  *rel_residual = mg_coarse_check(c, mg_levels, n_coarse);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
 int icarat_time_operator(icarat_ctx *c, int reps, double *ms_per_launch)
 {
   ICARAT_API_BEGIN
@@ -261,14 +273,44 @@ static void check_tc_err(icarat_ctx *c)
   }
 }
 
+} // extern "C"
+
+// Runs f with the context's FP64 products forced to the node stencil (tc = 0)
+// or to the FP64 tensor cores (tc = 1 where the grid is large enough, 2 on
+// every grid they fit).
+template <typename F> static int with_fp64_op(icarat_ctx *c, int tc, F f)
+{
+  const int saved = c->fp64_tc;
+  c->fp64_tc = tc;
+  try
+  {
+    const int st = f();
+    c->fp64_tc = saved;
+    return st;
+  }
+  catch(...)
+  {
+    c->fp64_tc = saved;
+    throw;
+  }
+}
+
+extern "C" {
+
 int icarat_apply_K_op(icarat_ctx *c, int op, const double *u, double *y)
 {
   ICARAT_API_BEGIN
   check_ctx(c);
-  IREQUIRE(op >= ICARAT_OP_FP64 && op <= ICARAT_OP_TC_BF16, ICARAT_ERR_ARG,
+  IREQUIRE(op >= ICARAT_OP_FP64 && op <= ICARAT_OP_TC_FP64, ICARAT_ERR_ARG,
            "unknown operator");
-  if(op == ICARAT_OP_FP64)
-    return apply_K_impl(c, u, y, true);
+  if(op == ICARAT_OP_FP64 || op == ICARAT_OP_TC_FP64)
+  {
+    GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+    IREQUIRE(op == ICARAT_OP_FP64 || dmma_fits(g), ICARAT_ERR_UNSUPPORTED,
+             "grid too large for the FP64 tensor-core operator");
+    return with_fp64_op(c, op == ICARAT_OP_TC_FP64 ? 2 : 0,
+                        [&] { return apply_K_impl(c, u, y, true); });
+  }
   IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
   IREQUIRE(u && y, ICARAT_ERR_ARG, "null argument");
   mixed_alloc(c);
@@ -286,10 +328,17 @@ int icarat_time_operator_op(icarat_ctx *c, int op, int reps, double *ms_per_laun
 {
   ICARAT_API_BEGIN
   check_ctx(c);
-  IREQUIRE(op >= ICARAT_OP_FP64 && op <= ICARAT_OP_TC_BF16, ICARAT_ERR_ARG,
+  IREQUIRE(op >= ICARAT_OP_FP64 && op <= ICARAT_OP_TC_FP64, ICARAT_ERR_ARG,
            "unknown operator");
-  if(op == ICARAT_OP_FP64)
-    return icarat_time_operator(c, reps, ms_per_launch);
+  if(op == ICARAT_OP_FP64 || op == ICARAT_OP_TC_FP64)
+  {
+    GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+    IREQUIRE(op == ICARAT_OP_FP64 || dmma_fits(g), ICARAT_ERR_UNSUPPORTED,
+             "grid too large for the FP64 tensor-core operator");
+    // the tensor-core operator on any grid size it fits (timing only)
+    return with_fp64_op(c, op == ICARAT_OP_TC_FP64 ? 2 : 0,
+                        [&] { return icarat_time_operator(c, reps, ms_per_launch); });
+  }
   IREQUIRE(reps > 0 && ms_per_launch, ICARAT_ERR_ARG, "bad argument");
   IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
   mixed_alloc(c);

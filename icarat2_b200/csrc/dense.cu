@@ -6,11 +6,14 @@
 // Cholesky factor A = L L^T, and every V-cycle solves A x = b as
 // x = W^T (W b) with two triangular matrix-vector products.
 //   1. right-looking blocked Cholesky, block 64: per block k the diagonal
-//      block is factored and inverted in shared memory (k_potrf64, which also
+//      block is factored and inverted in registers (k_potrf64, which also
 //      stores W_kk = L_kk^-1), the panel becomes L_ik = A_ik W_kk^T and the
-//      trailing matrix takes A -= L_ik L_jk^T (lower tiles), both as GEMMs;
-//   2. W by recursive triangular inversion: with L = [L11 0; L21 L22],
-//      W21 = -W22 (L21 W11), two GEMMs per split.
+//      trailing matrix takes A -= L_ik L_jk^T (lower tiles), both as GEMMs
+//      limited to the matrix's band (the caller orders the unknowns so that
+//      the band is narrow);
+//   2. W by triangular inversion in doubling steps: with L = [L11 0; L21 L22],
+//      W21 = -W22 (L21 W11), two batched GEMMs per block size over the band
+//      of L21.
 // Matrices are row-major with leading dimension n.
 #include <type_traits>
 
@@ -45,6 +48,11 @@ struct GemmArgs
   int lower;
   int a_lower; // op(A)(i,k) = 0 for k > i: K ends at the tile's last row
   int b_lower; // op(B)(k,j) = 0 for k < j: K starts at the tile's first column
+  // batch (grid z): product z uses A + z za, B + z zb, C + z zc; with
+  // rows0 > 0 it has at most rows0 - z rows_step rows (and, with k_clip, at
+  // most that many terms)
+  long za, zb, zc;
+  int rows0, rows_step, k_clip;
 };
 
 // Element t of a 64 x 16 A chunk / 16 x 64 B chunk, ordered so that the
@@ -82,6 +90,21 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmArgs g)
 {
   const int tm = blockIdx.y, tn = blockIdx.x;
   if(g.lower && tn > tm)
+    return;
+  if(blockIdx.z > 0)
+  {
+    g.A += blockIdx.z * g.za;
+    g.B += blockIdx.z * g.zb;
+    g.C += blockIdx.z * g.zc;
+  }
+  if(g.rows0 > 0)
+  {
+    const int rows = g.rows0 - (int)blockIdx.z * g.rows_step;
+    g.M = min(g.M, rows);
+    if(g.k_clip)
+      g.K = min(g.K, rows);
+  }
+  if(tm * 64 >= g.M)
     return;
   __shared__ double As[64][16 + 2];
   __shared__ double Bs[16][64 + 2];
@@ -174,25 +197,30 @@ __global__ void __launch_bounds__(128) k_gemm_f64(GemmArgs g)
 // the identity.
 //
 // The block lives in registers: thread (ty, tx) of a 16 x 16 grid holds rows
-// 4ty..4ty+3 and columns 4tx..4tx+3.  Elimination is right-looking in the
-// unscaled form a_rc -= a_rj a_cj / a_jj (the square roots and the column
-// scaling come after the loop): per column j the owners publish column j to
-// shared memory and one barrier later every thread updates its 16 entries.
-// The inverse is a forward substitution by rows in the same tiles (row k of
-// L^-1 and column k of L published per step).  The published vectors are
-// double-buffered, so each step needs a single barrier.
-constexpr int kPotrfSmem = (4 * 64 + 2 * 64) * sizeof(double);
+// 4ty..4ty+3 and columns 4tx..4tx+3 of the block (a) and of the inverse being
+// built (e).  Elimination is right-looking in the unscaled form: step j
+// subtracts m_rj = a_rj / a_jj times row j from every row r > j, both in a
+// (a_rc -= m_rj a_cj, lower part) and in e, which starts as the identity
+// (e_rc -= m_rj e_jc, c <= j), so that e ends as the inverse of the unit
+// lower factor; the square roots of the pivots scale both at the end
+// (L_rc = a_rc / sqrt(a_cc), W_rc = e_rc / sqrt(a_rr)).  Column j of a, row
+// j of e and 1 / a_jj are final after step j - 1: their owners publish them
+// to shared memory at the end of that step (the pivot's owner updates it
+// and starts its reciprocal before its other updates), double-buffered, so
+// each step needs a single barrier.
+constexpr int kPotrfSmem = (4 * 64 + 2 * 64 + 2) * sizeof(double);
 
 // 1 / x and 1 / sqrt(x) for x > 0 by Newton's method from an FP32 seed
 // (y <- y (2 - x y), and y <- y (3/2 - x y^2 / 2)): each step doubles the
-// correct digits, three steps reach double precision from the seed's ~2^-22.
-// Inline FMAs only: an out-of-line divide or square root inside the loops
-// below would save the register-resident block to the stack at every call.
+// correct digits, so two steps take the seed's ~2^-22 past double precision
+// (x must lie in the normal FP32 range).  Inline FMAs only: an out-of-line
+// divide or square root inside the loops below would save the
+// register-resident block to the stack at every call.
 __device__ __forceinline__ double recip_newton(double x)
 {
   double y = (double)__fdividef(1.0f, (float)x);
 #pragma unroll
-  for(int it = 0; it < 3; it++)
+  for(int it = 0; it < 2; it++)
     y = y * fma(-x, y, 2.0);
   return y;
 }
@@ -201,7 +229,7 @@ __device__ __forceinline__ double rsqrt_newton(double x)
 {
   double y = (double)rsqrtf((float)x);
 #pragma unroll
-  for(int it = 0; it < 3; it++)
+  for(int it = 0; it < 2; it++)
     y = y * fma(-0.5 * x, y * y, 1.5);
   return y;
 }
@@ -209,12 +237,14 @@ __device__ __forceinline__ double rsqrt_newton(double x)
 __global__ void __launch_bounds__(256) k_potrf64(double *A, double *W, int n, int k0)
 {
   extern __shared__ double potrf_smem[];
-  double(*vec)[64] = reinterpret_cast<double(*)[64]>(potrf_smem); // [4][64]
-  double *isq = potrf_smem + 4 * 64; // 1 / sqrt(pivot)
-  double *sq = isq + 64;              // sqrt(pivot)
+  double(*colbuf)[64] = reinterpret_cast<double(*)[64]>(potrf_smem); // [2][64] column j of a
+  double(*rowbuf)[64] = colbuf + 2;                                  // [2][64] row j of e
+  double *isq = potrf_smem + 4 * 64;                                  // 1 / sqrt(pivot)
+  double *sq = isq + 64;                                              // sqrt(pivot)
+  double *invbuf = sq + 64;                                           // [2] 1 / a_jj
   const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
   const int m = min(64, n - k0);
-  double a[4][4];
+  double a[4][4], e[4][4];
 #pragma unroll
   for(int i = 0; i < 4; i++)
 #pragma unroll
@@ -222,45 +252,75 @@ __global__ void __launch_bounds__(256) k_potrf64(double *A, double *W, int n, in
     {
       const int r = 4 * ty + i, c = 4 * tx + q;
       a[i][q] = (r < m && c < m) ? A[(long)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
+      e[i][q] = (r == c) ? 1.0 : 0.0;
     }
-  // ---- elimination (by 4 columns, so that the published register column is
-  // a compile-time index)
-  auto elim = [&](auto qc, int j)
-  {
-    constexpr int Q = decltype(qc)::value;
-    double *col = vec[j & 1];
-    if(tx == (j >> 2))
+  if(tx == 0)
 #pragma unroll
-      for(int i = 0; i < 4; i++)
-        col[4 * ty + i] = a[i][Q];
-    __syncthreads();
-    const double inv = recip_newton(col[j]);
-    double fr[4], fc[4];
+    for(int i = 0; i < 4; i++)
+      colbuf[0][4 * ty + i] = a[i][0];
+  if(ty == 0)
+#pragma unroll
+    for(int q = 0; q < 4; q++)
+      rowbuf[0][4 * tx + q] = e[0][q];
+  if(t == 0)
+    invbuf[0] = recip_newton(a[0][0]);
+  __syncthreads();
+  auto step = [&](auto qc, int j)
+  {
+    constexpr int Q = decltype(qc)::value; // j & 3
+    constexpr int Q1 = (Q + 1) & 3;        // (j + 1) & 3
+    const double *cj = colbuf[j & 1];
+    const double *ej = rowbuf[j & 1];
+    const double inv = invbuf[j & 1];
+    // multipliers zero outside the rows / columns that step j updates, so
+    // that every update below is unconditional: rows r > j of a (columns
+    // c > j; the entries above the diagonal follow the symmetric update and
+    // are never output) and of e (row j of e is zero past column j)
+    double fr[4], fc[4], er[4];
 #pragma unroll
     for(int i = 0; i < 4; i++)
     {
-      fr[i] = col[4 * ty + i];
-      fc[i] = col[4 * tx + i] * inv;
+      fr[i] = (4 * ty + i > j) ? cj[4 * ty + i] * inv : 0.0; // m_rj
+      fc[i] = (4 * tx + i > j) ? cj[4 * tx + i] : 0.0;       // a_cj
+      er[i] = ej[4 * tx + i];                                // e_jc
     }
+    const int j1 = j + 1;
+    // the next pivot's reciprocal, computed by every thread without a branch
+    // (only the pivot's owner publishes it) so that its latency hides behind
+    // the independent updates below
+    const bool pivot_owner = (tx == (j1 >> 2)) && (ty == (j1 >> 2)) && j1 < 64;
+    const double inv_next = recip_newton(fma(-fr[Q1], fc[Q1], a[Q1][Q1]));
 #pragma unroll
     for(int i = 0; i < 4; i++)
 #pragma unroll
       for(int q = 0; q < 4; q++)
       {
-        const int r = 4 * ty + i, c = 4 * tx + q;
-        if(c > j && r >= c)
-          a[i][q] = fma(-fr[i], fc[q], a[i][q]);
+        a[i][q] = fma(-fr[i], fc[q], a[i][q]);
+        e[i][q] = fma(-fr[i], er[q], e[i][q]);
       }
+    if(j1 < 64)
+    {
+      if(tx == (j1 >> 2))
+#pragma unroll
+        for(int i = 0; i < 4; i++)
+          colbuf[j1 & 1][4 * ty + i] = a[i][Q1];
+      if(ty == (j1 >> 2))
+#pragma unroll
+        for(int q = 0; q < 4; q++)
+          rowbuf[j1 & 1][4 * tx + q] = e[Q1][q];
+      if(pivot_owner)
+        invbuf[j1 & 1] = inv_next;
+    }
+    __syncthreads();
   };
   for(int j = 0; j < 64; j += 4)
   {
-    elim(std::integral_constant<int, 0>{}, j);
-    elim(std::integral_constant<int, 1>{}, j + 1);
-    elim(std::integral_constant<int, 2>{}, j + 2);
-    if(j + 3 < 63)
-      elim(std::integral_constant<int, 3>{}, j + 3);
+    step(std::integral_constant<int, 0>{}, j);
+    step(std::integral_constant<int, 1>{}, j + 1);
+    step(std::integral_constant<int, 2>{}, j + 2);
+    step(std::integral_constant<int, 3>{}, j + 3);
   }
-  // ---- scaling: L_rc = a_rc / sqrt(a_cc), L_cc = sqrt(a_cc)
+  // ---- scaling by the square roots of the pivots
   if(tx == ty)
 #pragma unroll
     for(int i = 0; i < 4; i++)
@@ -276,63 +336,10 @@ __global__ void __launch_bounds__(256) k_potrf64(double *A, double *W, int n, in
     for(int q = 0; q < 4; q++)
     {
       const int r = 4 * ty + i, c = 4 * tx + q;
-      a[i][q] = r > c ? a[i][q] * isq[c] : (r == c ? sq[c] : 0.0);
-    }
-  // ---- inverse: w = I, then per row k: w_k /= L_kk (final), w_r -= L_rk w_k (r > k)
-  double w[4][4];
-#pragma unroll
-  for(int i = 0; i < 4; i++)
-#pragma unroll
-    for(int q = 0; q < 4; q++)
-      w[i][q] = (4 * ty + i == 4 * tx + q) ? 1.0 : 0.0;
-  auto inv_step = [&](auto qc, int k)
-  {
-    constexpr int Q = decltype(qc)::value;
-    double *row = vec[2 + (k & 1)];
-    double *colL = vec[k & 1];
-    const double ilkk = isq[k]; // 1 / L_kk
-    if(ty == (k >> 2))
-#pragma unroll
-      for(int q = 0; q < 4; q++)
-      {
-        w[Q][q] *= ilkk;
-        row[4 * tx + q] = w[Q][q];
-      }
-    if(tx == (k >> 2))
-#pragma unroll
-      for(int i = 0; i < 4; i++)
-        colL[4 * ty + i] = a[i][Q];
-    __syncthreads();
-#pragma unroll
-    for(int i = 0; i < 4; i++)
-    {
-      const int r = 4 * ty + i;
-      if(r > k)
-      {
-        const double l = colL[r];
-#pragma unroll
-        for(int q = 0; q < 4; q++)
-          w[i][q] = fma(-l, row[4 * tx + q], w[i][q]);
-      }
-    }
-  };
-  for(int k = 0; k < 64; k += 4)
-  {
-    inv_step(std::integral_constant<int, 0>{}, k);
-    inv_step(std::integral_constant<int, 1>{}, k + 1);
-    inv_step(std::integral_constant<int, 2>{}, k + 2);
-    inv_step(std::integral_constant<int, 3>{}, k + 3);
-  }
-#pragma unroll
-  for(int i = 0; i < 4; i++)
-#pragma unroll
-    for(int q = 0; q < 4; q++)
-    {
-      const int r = 4 * ty + i, c = 4 * tx + q;
       if(r < m && c < m)
       {
-        A[(long)(k0 + r) * n + k0 + c] = a[i][q];
-        W[(long)(k0 + r) * n + k0 + c] = (c <= r) ? w[i][q] : 0.0;
+        A[(long)(k0 + r) * n + k0 + c] = r > c ? a[i][q] * isq[c] : (r == c ? sq[c] : 0.0);
+        W[(long)(k0 + r) * n + k0 + c] = (c <= r) ? e[i][q] * isq[r] : 0.0;
       }
     }
 }
@@ -408,58 +415,74 @@ static void gemm(cudaStream_t st, int M, int N, int K, double alpha, const doubl
   if(M <= 0 || N <= 0 || K <= 0)
     return;
   GemmArgs g{M,   N,  K,  alpha, beta, A,     lda,    ta,
-             B,   ldb, tb, C,    ldc,  lower, a_lower, b_lower};
+             B,   ldb, tb, C,    ldc,  lower, a_lower, b_lower, 0, 0, 0, 0, 0, 0};
   dim3 grid((N + 63) / 64, (M + 63) / 64);
   note_launch();
   k_gemm_f64<<<grid, 128, 0, st>>>(g);
 }
 
-// W rows/cols [off, off + nbk * 64) of L^-1, given the diagonal blocks W_kk.
-static void trinv_rec(cudaStream_t st, const double *L, double *W, double *T, int n,
-                      int off, int nbk)
+// W = L^-1 from the diagonal blocks W_kk by doubling: at block size s every
+// pair of neighbouring inverted blocks [o, o + s), [o + s, o + 2s) (o a
+// multiple of 2s; the second may be short or absent) becomes one, with
+// L = [L11 0; L21 L22], W21 = -W22 L21 W11.  All pairs of one size go in one
+// batched launch per product.  L has lower bandwidth bw, so L21 is zero
+// outside its top-right min(bw, s2) x min(bw, s) corner:
+//   T = L21[0:r, s-k:s] W11[s-k:s, :]   (r x s; the other rows are zero)
+//   W21 = -W22[:, 0:r] T                (columns past each row of the lower
+//                                        triangular W22 skipped)
+// T holds one r x s slab per pair.
+static void trinv_banded(cudaStream_t st, const double *L, double *W, double *T, int n,
+                         int bw)
 {
-  if(nbk <= 1)
-    return;
-  const int b1 = nbk / 2, b2 = nbk - b1;
-  const int s1 = b1 * 64;
-  const int s2 = std::min(b2 * 64, n - off - s1);
-  trinv_rec(st, L, W, T, n, off, b1);
-  trinv_rec(st, L, W, T, n, off + s1, b2);
-  // T = L21 W11  (s2 x s1), then W21 = -W22 T  (s2 x s1)
-  // (W11 and W22 are lower triangular: half of each product is skipped)
-  gemm(st, s2, s1, s1, 1.0, L + (long)(off + s1) * n + off, n, 0,
-       W + (long)off * n + off, n, 0, 0.0, T, s1, 0, 0, 1);
-  gemm(st, s2, s1, s2, -1.0, W + (long)(off + s1) * n + off + s1, n, 0, T, s1, 0, 0.0,
-       W + (long)(off + s1) * n + off, n, 0, 1, 0);
+  for(int s = 64; s < n; s *= 2)
+  {
+    const int pairs = (n - s + 2 * s - 1) / (2 * s); // pairs whose second block exists
+    const int k = std::min(bw, s);
+    const int r = std::min(bw, s);
+    const long step = 2L * s * n + 2L * s;           // from pair z to pair z + 1
+    const long tslab = (long)r * s;
+    note_launch(2);
+    // T_z = L21 W11 (rows clipped to the short second block of the last pair)
+    GemmArgs g1{r, s, k, 1.0, 0.0, L + (long)s * n + s - k, n, 0, W + (long)(s - k) * n, n, 0,
+                T, s, 0, 0, 0, step, step, tslab, n - s, 2 * s, 0};
+    k_gemm_f64<<<dim3((s + 63) / 64, (r + 63) / 64, pairs), 128, 0, st>>>(g1);
+    // W21_z = -W22 T_z (K clipped like the rows: W22 has s2 columns)
+    GemmArgs g2{s, s, r, -1.0, 0.0, W + (long)s * n + s, n, 0, T, s, 0, W + (long)s * n, n,
+                0, 1, 0, step, tslab, step, n - s, 2 * s, 1};
+    k_gemm_f64<<<dim3((s + 63) / 64, (s + 63) / 64, pairs), 128, 0, st>>>(g2);
+  }
 }
 
-// A (lower part) -> L in place; W <- L^-1 (upper part zero); T: n x n
-// scratch, which ends up holding W^T (upper part; rows contiguous for the
-// transposed product of every solve).
-void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n)
+// A (lower part, lower bandwidth bw) -> L in place; W <- L^-1 (upper part
+// zero); T: n x n scratch, which ends up holding W^T (upper part; rows
+// contiguous for the transposed product of every solve).  The Cholesky
+// factor keeps the band, so block column k updates only the bw rows below
+// its diagonal block; W = L^-1 is dense.
+void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n, int bw)
 {
   ICK(cudaFuncSetAttribute(k_potrf64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            kPotrfSmem));
   ICK(cudaMemsetAsync(W, 0, sizeof(double) * (size_t)n * n, st));
+  bw = std::max(1, std::min(bw, n));
   const int nb = (n + 63) / 64;
   for(int k = 0; k < nb; k++)
   {
     const int k0 = k * 64;
     note_launch();
     k_potrf64<<<1, 256, kPotrfSmem, st>>>(A, W, n, k0);
-    const int rest = n - k0 - 64;
+    const int rest = std::min(n - k0 - 64, bw);
     if(rest > 0)
     {
       double *panel = A + (long)(k0 + 64) * n + k0;
       // L_ik = A_ik W_kk^T (in place: each CTA reads its own rows first)
       gemm(st, rest, 64, 64, 1.0, panel, n, 0, W + (long)k0 * n + k0, n, 1, 0.0, panel, n,
            0);
-      // A22 -= L_i L_j^T on the lower tiles
+      // A22 -= L_i L_j^T on the lower tiles of the band
       gemm(st, rest, rest, 64, -1.0, panel, n, 0, panel, n, 1, 1.0,
            A + (long)(k0 + 64) * n + k0 + 64, n, 1);
     }
   }
-  trinv_rec(st, A, W, T, n, 0, nb);
+  trinv_banded(st, A, W, T, n, bw);
   note_launch();
   k_transpose_lower<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, st>>>(n, W, T);
   ICK(cudaGetLastError());

@@ -142,6 +142,24 @@ struct TcArgs
   int *err = nullptr;
 };
 
+// Arguments of the FP64 tensor-core element-by-element operator
+// (dmma_stencil.cu); the variants are those of TcOp, with CgScalars.
+struct DmArgs
+{
+  GridDev g;
+  KeParam ke;
+  const double *E;
+  const uint8_t *fix;
+  const double *u;
+  double *y;
+  const double *b = nullptr, *invd = nullptr;
+  double *d = nullptr;
+  double c1 = 0.0, c2 = 0.0;
+  double *partials = nullptr;
+  CgScalars *s = nullptr;
+  int tiles_x = 0, tiles = 0, kc = 0; // tiles along x, tiles, node layers per CTA
+};
+
 // Reduction geometry: every grid-stride reduction kernel runs on
 // kRedBlocks blocks of kRedThreads threads so that partial sums are summed
 // in one fixed order (bit-reproducible on a given GPU).
@@ -163,6 +181,7 @@ struct MgLevel
 struct CoarseSolver
 {
   int n = 0;              // free DOFs of the coarsest level
+  int bw = 0;             // lower bandwidth of the dense matrix in that order
   int *map = nullptr;     // n -> full index on the coarsest grid
   double *A = nullptr;    // n x n dense SPD matrix, becomes its Cholesky factor L
   double *W = nullptr;    // n x n, L^-1
@@ -250,6 +269,10 @@ struct icarat_ctx
   int sm_count = 148;
   // operator of the finest level of the FP32 V-cycle (ICARAT_OP_*)
   int mx_fine_op = ICARAT_OP_FP32;
+  // FP64 products on the FP64 tensor cores where the grid is large enough
+  // (0: the node stencil everywhere, the default; 2: the tensor cores on
+  // every grid they fit, for explicit operator requests)
+  int fp64_tc = 0;
   // learned preconditioner attached by icarat_ctx_set_net (not owned)
   icarat_net *net = nullptr;
   bool design_set = false, solved = false;
@@ -314,6 +337,12 @@ void net_apply(icarat_net *N, icarat_ctx *c, const T *r, double s, T *z);
 
 // tc_stencil.cu
 void launch_ku_tc(icarat_ctx *c, int op, int terms, TcArgs a, cudaStream_t st);
+int pick_layers(long tiles, int NZ, long slots, long max_ctas);
+// dmma_stencil.cu
+bool dmma_fits(const GridDev &g);
+void launch_ku_dmma(icarat_ctx *c, int op, DmArgs a, cudaStream_t st);
+// FP64 products of this grid by the FP64 tensor-core operator
+bool use_dmma(const icarat_ctx *c, const GridDev &g);
 
 // mixed.cu
 struct MixedRun
@@ -340,6 +369,7 @@ void widen_f64(icarat_ctx *c, long n, const float *in, double *out);
 
 // multigrid.cu
 void mg_setup(icarat_ctx *c, int levels);
+double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse);
 void mg_vcycle(icarat_ctx *c, const double *r, double *z, int smooth);
 void mg_vcycle_f32(icarat_ctx *c, const float *r, float *z, int smooth);
 void mg_free(icarat_ctx *c);

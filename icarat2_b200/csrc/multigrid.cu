@@ -12,21 +12,26 @@
 // identically before and after the coarse correction so that the V-cycle is
 // a symmetric positive definite preconditioner.  The coarsest level is solved
 // exactly: W = L^-1 of the Cholesky factor of its dense matrix is rebuilt on
-// the GPU for every design (dense.cu) and each V-cycle applies W^T W.
+// the GPU for every design (dense.cu) and each V-cycle applies W^T W.  The
+// dense unknowns are ordered by node planes across the longest axis, which
+// makes the matrix banded (about 3 plane sizes wide) and the factorization
+// work proportional to the band.
 //
 // The V-cycle exists in FP64 (preconditioner of the FP64 solver) and in FP32
 // (inner solver of the mixed-precision solver); the coarsest solve is FP64 in
 // both.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
+#include <vector>
 
 #include "stencil.cuh"
 
 namespace icarat_b200
 {
 
-void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n);
+void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n, int bw);
 void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
                      const double *v, double *t, const int *rowmap, double *x);
 
@@ -379,17 +384,51 @@ static void allocate_levels(icarat_ctx *c, int levels)
     fix.swap(fc);
     gf = gc;
   }
-  // dense coarse system
+  // dense coarse system: unknowns ordered by node planes across the longest
+  // axis (nodes within a plane, then the 3 components), so that the matrix
+  // is banded (a node couples to the planes either side only) with the
+  // narrowest band
   GridDev gc = c->mg[levels - 1].g;
   std::vector<int> rowmap, colmap(3 * (size_t)gc.numnp, -1);
-  for(int n = 0; n < gc.numnp; n++)
-    for(int q = 0; q < 3; q++)
-      if(!((fix[n] >> q) & 1u))
+  const int ext[3] = {gc.NX, gc.NY, gc.NZ};
+  int ax[3] = {0, 1, 2}; // slowest .. fastest
+  std::stable_sort(ax, ax + 3, [&](int p, int q) { return ext[p] > ext[q]; });
+  int id[3];
+  for(id[ax[0]] = 0; id[ax[0]] < ext[ax[0]]; id[ax[0]]++)
+    for(id[ax[1]] = 0; id[ax[1]] < ext[ax[1]]; id[ax[1]]++)
+      for(id[ax[2]] = 0; id[ax[2]] < ext[ax[2]]; id[ax[2]]++)
       {
-        colmap[3 * (size_t)n + q] = (int)rowmap.size(); // node-major lookup table
-        rowmap.push_back(q * gc.numnp + n);             // component-major vector index
+        const int n = id[0] + gc.NX * (id[1] + gc.NY * id[2]);
+        for(int q = 0; q < 3; q++)
+          if(!((fix[n] >> q) & 1u))
+          {
+            colmap[3 * (size_t)n + q] = (int)rowmap.size(); // node-major lookup table
+            rowmap.push_back(q * gc.numnp + n);             // component-major vector index
+          }
       }
   const int nf = (int)rowmap.size();
+  int bw = 0; // largest index distance of two coupled unknowns
+  for(int n = 0; n < gc.numnp; n++)
+  {
+    const int I = n % gc.NX, J = (n / gc.NX) % gc.NY, K = n / (gc.NX * gc.NY);
+    for(int dk = -1; dk <= 1; dk++)
+      for(int dj = -1; dj <= 1; dj++)
+        for(int di = -1; di <= 1; di++)
+        {
+          const int i2 = I + di, j2 = J + dj, k2 = K + dk;
+          if(i2 < 0 || j2 < 0 || k2 < 0 || i2 >= gc.NX || j2 >= gc.NY || k2 >= gc.NZ)
+            continue;
+          const int n2 = i2 + gc.NX * (j2 + gc.NY * k2);
+          for(int q = 0; q < 3; q++)
+            for(int q2 = 0; q2 < 3; q2++)
+            {
+              const int u = colmap[3 * (size_t)n + q], v = colmap[3 * (size_t)n2 + q2];
+              if(u >= 0 && v >= 0)
+                bw = std::max(bw, std::abs(u - v));
+            }
+        }
+  }
+  c->coarse.bw = bw;
   IREQUIRE((double)nf * nf * 8.0 * 3 < 6.0e9, ICARAT_ERR_UNSUPPORTED,
            "coarsest multigrid level too large for the dense solve; add levels");
   c->coarse.n = nf;
@@ -440,8 +479,45 @@ static void enqueue_mg_setup(icarat_ctx *c, int levels)
     k_coarse_assemble<<<blocks_for(n, 64), 64, 0, c->stream>>>(
         C.g, c->ke0, C.E, c->coarse.map, c->coarse.map + n, n, c->coarse.A);
     ICK(cudaGetLastError());
-    dense_spd_inverse_factor(c->stream, c->coarse.A, c->coarse.W, c->coarse.work, n);
+    dense_spd_inverse_factor(c->stream, c->coarse.A, c->coarse.W, c->coarse.work, n,
+                             c->coarse.bw);
   }
+}
+
+// ||b - K_c x|| / ||b|| of the coarsest dense solve for a fixed right-hand
+// side (a check of the factorization), K_c applied by the coarsest level's
+// stencil.
+double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
+{
+  mg_setup(c, levels);
+  const MgLevel &C = c->mg.back();
+  const int n = c->coarse.n;
+  if(n_coarse)
+    *n_coarse = n;
+  if(n == 0)
+    return 0.0;
+  const size_t nv = 3 * (size_t)C.g.numnp;
+  std::vector<int> rowmap(n);
+  std::vector<double> b(n), y(nv);
+  for(int i = 0; i < n; i++)
+    b[i] = 1.0 + (i % 7) / 7.0;
+  ICK(cudaStreamSynchronize(c->stream));
+  ICK(cudaMemcpy(rowmap.data(), c->coarse.map, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  ICK(cudaMemcpy(c->coarse.vin, b.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  ICK(cudaMemsetAsync(C.x, 0, sizeof(double) * nv, c->stream));
+  dense_spd_solve(c->stream, c->coarse.W, c->coarse.work, n, c->coarse.vin, c->coarse.vout,
+                  c->coarse.map, C.x);
+  launch_apply_K(c, C.g, C.E, C.fix, C.x, C.t, nullptr);
+  ICK(cudaMemcpyAsync(y.data(), C.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
+  double rr = 0.0, bb = 0.0;
+  for(int i = 0; i < n; i++)
+  {
+    const double r = b[i] - y[rowmap[i]];
+    rr += r * r;
+    bb += b[i] * b[i];
+  }
+  return std::sqrt(rr / bb);
 }
 
 // Coarse operators and the dense inverse for the current design.  The fixed
@@ -519,6 +595,23 @@ static void cheb_step(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x
     launch_ku_tc(c, TC_CHEB, c->mx_fine_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
     return;
   }
+  if constexpr(std::is_same<T, double>::value)
+    if(use_dmma(c, L.g))
+    {
+      DmArgs a;
+      a.g = L.g;
+      a.E = B::E(L);
+      a.fix = L.fix;
+      a.u = x;
+      a.y = xo;
+      a.b = b;
+      a.invd = B::invd(L);
+      a.d = d;
+      a.c1 = c1;
+      a.c2 = c2;
+      launch_ku_dmma(c, TC_CHEB, a, c->stream);
+      return;
+    }
   note_launch();
   k_cheb_step<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(
       L.g, B::ke(c), B::E(L), L.fix, B::invd(L), b, x, d, xo, T(c1), T(c2));
@@ -541,6 +634,19 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
     launch_ku_tc(c, TC_RESID, c->mx_fine_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
     return;
   }
+  if constexpr(std::is_same<T, double>::value)
+    if(use_dmma(c, L.g))
+    {
+      DmArgs a;
+      a.g = L.g;
+      a.E = B::E(L);
+      a.fix = L.fix;
+      a.u = x;
+      a.y = r;
+      a.b = b;
+      launch_ku_dmma(c, TC_RESID, a, c->stream);
+      return;
+    }
   note_launch();
   k_mg_residual<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, B::ke(c), B::E(L),
                                                                   L.fix, b, x, r);

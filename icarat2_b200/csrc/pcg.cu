@@ -282,10 +282,24 @@ static void enqueue_iteration(icarat_ctx *c, int method, int smooth,
   (void)b;
   const GridDev g = fine_grid(c);
   const int n = c->neq;
-  note_launch();
-  k_cg_spmv<<<spmv_blocks(c), 128, 0, c->stream>>>(g, c->ke0, c->d_E, c->d_fix,
-                                                   c->d_p, c->d_Ap,
-                                                   c->d_partials, c->d_cg);
+  if(use_dmma(c, g))
+  {
+    DmArgs a;
+    a.g = g;
+    a.E = c->d_E;
+    a.fix = c->d_fix;
+    a.u = c->d_p;
+    a.y = c->d_Ap;
+    a.partials = c->d_partials;
+    a.s = c->d_cg;
+    launch_ku_dmma(c, TC_DOT, a, c->stream);
+  }
+  else
+  {
+    note_launch();
+    k_cg_spmv<<<spmv_blocks(c), 128, 0, c->stream>>>(g, c->ke0, c->d_E, c->d_fix, c->d_p,
+                                                     c->d_Ap, c->d_partials, c->d_cg);
+  }
   if(method == ICARAT_SOLVER_JACOBI_PCG)
   {
     note_launch();
@@ -325,6 +339,7 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
            ICARAT_ERR_ARG, "unknown solver method");
   const GridDev g = fine_grid(c);
   const int n = c->neq;
+  c->fp64_tc = o->fp64_tc ? 1 : 0;
   int levels = 0, smooth = 0;
   if(method == ICARAT_SOLVER_MG_PCG)
   {
@@ -351,7 +366,8 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
     ICK(cudaMemcpyAsync(c->d_p, c->d_z, sizeof(double) * n,
                         cudaMemcpyDeviceToDevice, c->stream));
   }
-  const auto key = std::make_tuple(method, levels, smooth, chunk, (const void *)d_x);
+  const auto key =
+      std::make_tuple(method + 4096 * c->fp64_tc, levels, smooth, chunk, (const void *)d_x);
   auto it = c->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
   if(it == c->graphs.end())

@@ -143,10 +143,31 @@ static int node_blocks(const GridDev &g, int threads)
   return b < 1 ? 1 : b;
 }
 
+// Grids below this many nodes keep the node stencil: their element tiles
+// would leave most SMs idle.
+constexpr int kDmmaMinNodes = 1 << 15;
+
+bool use_dmma(const icarat_ctx *c, const GridDev &g)
+{
+  // fp64_tc == 2: on every grid that fits (explicit operator requests)
+  return c->fp64_tc && (g.numnp >= kDmmaMinNodes || c->fp64_tc == 2) && dmma_fits(g);
+}
+
 void launch_apply_K(icarat_ctx *c, const GridDev &g, const double *E,
                     const uint8_t *fix, const double *u, double *y,
                     double *dot_partials)
 {
+  if(!dot_partials && use_dmma(c, g))
+  {
+    DmArgs a;
+    a.g = g;
+    a.E = E;
+    a.fix = fix;
+    a.u = u;
+    a.y = y;
+    launch_ku_dmma(c, TC_APPLY, a, c->stream);
+    return;
+  }
   int blocks = node_blocks(g, 128);
   if(dot_partials && blocks > kMaxRedBlocks)
     blocks = kMaxRedBlocks;

@@ -540,7 +540,7 @@ template <int OP, int TERMS> static int tc_prepare()
 // Node layers per CTA: few enough that every SM slot gets work, many enough
 // that the one-layer z halo stays cheap; among those, the count whose last
 // wave is fullest.
-static int pick_layers(long tiles, int NZ, long slots, long max_ctas)
+int pick_layers(long tiles, int NZ, long slots, long max_ctas)
 {
   int best = NZ;
   double best_eff = -1.0;

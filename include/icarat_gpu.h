@@ -103,6 +103,11 @@ typedef struct
   int krylov_op;  /* MIXED_IR: ICARAT_OP_* of K p in the Krylov loop (0 = default) */
   int warm_start; /* MIXED_IR: start from the solution held by the context (the
                      previous solve, e.g. of the previous design) instead of 0 */
+  int fp64_tc;    /* JACOBI_PCG, MG_PCG: 1 = FP64 products K u element by
+                     element on the FP64 tensor cores (ICARAT_OP_TC_FP64) on
+                     every grid level large enough for it; 0 (default) = the
+                     node stencil on the CUDA cores.  Also the operator of
+                     later icarat_apply_K calls on the context. */
 } icarat_solve_opts;
 
 typedef struct
@@ -286,6 +291,13 @@ int icarat_kernel_launches(unsigned long long *count);
    design, over `reps` back-to-back launches timed with CUDA events on the
    context's stream */
 int icarat_time_operator(icarat_ctx *ctx, int reps, double *ms_per_launch);
+/* check of the multigrid's coarsest dense solve on the current design:
+   builds the hierarchy of `mg_levels` levels, solves K_c x = b for
+   b_i = 1 + (i mod 7) / 7 on the coarsest free unknowns through the dense
+   inverse factor and returns ||b - K_c x|| / ||b|| with K_c applied by the
+   coarsest level's stencil; *n_coarse (may be NULL): number of unknowns */
+int icarat_mg_coarse_check(icarat_ctx *ctx, int mg_levels, double *rel_residual,
+                           int *n_coarse);
 
 /* ---- batched solver (no reference counterpart) ---------------------------
    Many independent designs, of equal or different grid sizes, solved
@@ -381,12 +393,15 @@ enum
   ICARAT_OP_FP32 = 1,      /* FP32 node stencil on the CUDA cores */
   ICARAT_OP_TC_BF16X3 = 2, /* element-by-element Ke0 U_e on the tensor cores:
                               BF16 hi/lo split, 3 products, FP32 accumulation */
-  ICARAT_OP_TC_BF16 = 3    /* the same with the single product hi x hi */
+  ICARAT_OP_TC_BF16 = 3,   /* the same with the single product hi x hi */
+  ICARAT_OP_TC_FP64 = 4    /* element-by-element Ke0 U_e on the FP64 tensor cores
+                              (DMMA), FP64 throughout */
 };
-/* y = K u (numeq host vectors) on the current design with operator `op`;
+/* y = K u (numeq host vectors) on the current design with operator `op`
+   (ICARAT_OP_FP64: the node stencil, whatever the context's default);
    reduced-precision operators round u to FP32 first */
 int icarat_apply_K_op(icarat_ctx *ctx, int op, const double *u, double *y);
-/* icarat_time_operator for operator `op` (FP32 vectors for op > 0) */
+/* icarat_time_operator for operator `op` (FP32 vectors for ops 1-3) */
 int icarat_time_operator_op(icarat_ctx *ctx, int op, int reps, double *ms_per_launch);
 
 int icarat_loop_init(icarat_ctx *ctx, const icarat_loop_opts *opts,
