@@ -61,7 +61,7 @@ def parse():
                    help="also time the loop with this many multigrid levels (0: skip)")
     p.add_argument("--mixed-grid", default="256x128x128",
                    help="grid of the mixed-precision section ('' skips it)")
-    p.add_argument("--mixed-levels", type=int, default=5)
+    p.add_argument("--mixed-levels", type=int, default=6)
     p.add_argument("--mixed-steps", type=int, default=5)
     p.add_argument("--batch-steps", type=int, default=3,
                    help="design iterations of the 80-design batch section (0: skip)")
@@ -242,10 +242,11 @@ def traffic_from_profiles(grid):
 def mixed_section(a, G, torch, dev, flush, world, dist):
     """256x128x128 cantilever, densities U[0.1, 0.5] (seed 0), R = 3, MMA:
     design iterations per second of the mixed-precision loop (FP32 multigrid
-    PCG with the tcgen05 BF16x3 smoother, FP64 residual refresh) against the
-    plain FP64 multigrid-PCG loop at the same residual, compliance and dc
-    error of one solve against an FP64 solve at rtol 1e-12, and K u GDOF/s
-    of every operator on the same design."""
+    PCG with the tcgen05 BF16 smoother, FP64 residual refresh) against the
+    plain FP64 multigrid-PCG loop (FP64 tensor-core operator on the finest
+    level) at the same residual, compliance and dc error of one solve
+    against an FP64 solve at rtol 1e-12, and K u GDOF/s of every operator
+    on the same design."""
     nx, ny, nz = (int(v) for v in a.mixed_grid.split("x"))
     nelx, nd = nx * ny * nz, 3 * (nx + 1) * (ny + 1) * (nz + 1)
     rho0 = np.random.default_rng(0).uniform(0.1, 0.5, nelx)
@@ -305,7 +306,7 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
         out["rtol_%g" % rtol]["fp64_residual"] = info.rel_residual
     # K u throughput of every operator on this design
     ku = {}
-    for name, op in (("fp64", G.OP_FP64), ("fp32", G.OP_FP32),
+    for name, op in (("fp64", G.OP_FP64), ("tc_fp64", G.OP_TC_FP64), ("fp32", G.OP_FP32),
                      ("tc_bf16x3", G.OP_TC_BF16X3), ("tc_bf16", G.OP_TC_BF16)):
         ms_op = c.time_operator(20, op)
         ku[name] = {"ms": ms_op, "gdof_s": nd / (ms_op * 1e-3) / 1e9}
@@ -313,9 +314,15 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
     # the tensor-core kernel against HBM: algorithmic bytes of a K u with
     # FP32 u, y and E
     bytes32 = 8.0 * nd + 4.0 * nelx
-    ms_tc = ku["tc_bf16x3"]["ms"]
-    out["roofline_tc_bf16x3"] = {"bound": "hbm", "achieved": bytes32 / (ms_tc * 1e-3) / 1e9,
-                                 "unit": "GB/s", "bytes_per_launch": bytes32}
+    for name in ("tc_bf16x3", "tc_bf16"):
+        ms_tc = ku[name]["ms"]
+        out["roofline_" + name] = {"bound": "hbm", "achieved": bytes32 / (ms_tc * 1e-3) / 1e9,
+                                   "unit": "GB/s", "bytes_per_launch": bytes32}
+    # the FP64 tensor-core operator against the measured DGEMM rate
+    flops = 1152.0 * nelx
+    out["roofline_tc_fp64"] = {"bound": "fp64 tensor", "achieved":
+                               flops / (ku["tc_fp64"]["ms"] * 1e-3) / 1e12, "unit": "TFLOP/s",
+                               "flops_per_launch": flops}
     c.close()
     return out
 

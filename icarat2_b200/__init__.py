@@ -255,10 +255,11 @@ def _bc_struct(dirichlet, loads):
 
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
                chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0, fp64_tc=0):
-    """fp64_tc=1: FP64 products element by element on the FP64 tensor cores
-    instead of the node stencil (JACOBI_PCG, MG_PCG)."""
+    """fp64_tc (JACOBI_PCG, MG_PCG): FP64 products on the FP64 tensor cores
+    by grid size (0), on every level of 32k nodes and more (1), or the node
+    stencil only (-1)."""
     return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,
-                     krylov_op, warm_start, int(bool(fp64_tc)))
+                     krylov_op, warm_start, int(fp64_tc))
 
 
 class Context:

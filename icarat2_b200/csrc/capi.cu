@@ -275,9 +275,8 @@ static void check_tc_err(icarat_ctx *c)
 
 } // extern "C"
 
-// Runs f with the context's FP64 products forced to the node stencil (tc = 0)
-// or to the FP64 tensor cores (tc = 1 where the grid is large enough, 2 on
-// every grid they fit).
+// Runs f with the context's FP64 products forced to the node stencil
+// (tc = -1) or to the FP64 tensor cores on every grid they fit (tc = 2).
 template <typename F> static int with_fp64_op(icarat_ctx *c, int tc, F f)
 {
   const int saved = c->fp64_tc;
@@ -308,7 +307,7 @@ int icarat_apply_K_op(icarat_ctx *c, int op, const double *u, double *y)
     GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
     IREQUIRE(op == ICARAT_OP_FP64 || dmma_fits(g), ICARAT_ERR_UNSUPPORTED,
              "grid too large for the FP64 tensor-core operator");
-    return with_fp64_op(c, op == ICARAT_OP_TC_FP64 ? 2 : 0,
+    return with_fp64_op(c, op == ICARAT_OP_TC_FP64 ? 2 : -1,
                         [&] { return apply_K_impl(c, u, y, true); });
   }
   IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
@@ -336,7 +335,7 @@ int icarat_time_operator_op(icarat_ctx *c, int op, int reps, double *ms_per_laun
     IREQUIRE(op == ICARAT_OP_FP64 || dmma_fits(g), ICARAT_ERR_UNSUPPORTED,
              "grid too large for the FP64 tensor-core operator");
     // the tensor-core operator on any grid size it fits (timing only)
-    return with_fp64_op(c, op == ICARAT_OP_TC_FP64 ? 2 : 0,
+    return with_fp64_op(c, op == ICARAT_OP_TC_FP64 ? 2 : -1,
                         [&] { return icarat_time_operator(c, reps, ms_per_launch); });
   }
   IREQUIRE(reps > 0 && ms_per_launch, ICARAT_ERR_ARG, "bad argument");

@@ -31,6 +31,8 @@
 // memory (row-major by D row, 36 doubles per row: conflict-free fragment
 // writes and element-per-lane reads) to the element-per-lane order of the
 // node sums.
+#include <algorithm>
+
 #include "stencil.cuh"
 
 namespace icarat_b200
@@ -45,8 +47,8 @@ constexpr int kPitch = 36;                  // doubles per D row in shared memor
 
 struct Smem
 {
-  double D[kTY][24][kPitch];  // [warp][D row][element]
-  double xch[2][6][kTY][32];  // [stage][dz * 3 + c][warp][lane]
+  double D[2][kTY][24][kPitch]; // [stage][warp][D row][element]
+  double xch[2][6][kTY][32];    // [stage][dz * 3 + c][warp][lane]
   double red[32];
 };
 
@@ -58,8 +60,27 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b)
                : "d"(a), "d"(b));
 }
 
+// m16n8k8 (sm_90+): rows g and g + 8 of A / D are the two 8-element groups
+// of a pair, so with g = lane / 4, t = lane % 4 the fragments are those of
+// two m8n8k4 groups and two K chunks: a = {U0[k0], U1[k0], U0[k1], U1[k1]},
+// b = {K[k0], K[k1]}, d = {D0[0..1], D1[0..1]}
+__device__ __forceinline__ void dmma16(double (&d0)[2], double (&d1)[2], double a0, double a1,
+                                       double a2, double a3, double b0, double b1)
+{
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+               "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+d"(d0[0]), "+d"(d0[1]), "+d"(d1[0]), "+d"(d1[1])
+               : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
 } // namespace dm
 
+// Work: the (tile, node layer) pairs in tile-major order, split evenly over
+// the CTAs (one per SM); a CTA runs its range as one or two tile segments,
+// each with one element layer of z halo.  Per segment the element layers are
+// pipelined: the MMAs of layer e + 1 are issued before the node sums of
+// layer e, so the tensor pipe works while the sums run; D is
+// double-buffered in shared memory.
 template <int OP>
 __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
 {
@@ -71,19 +92,7 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
   const int t = threadIdx.x, w = t >> 5, l = t & 31;
   const int q = l & 3, r = l >> 2;
   const GridDev g = a.g;
-  const int tile = blockIdx.x % a.tiles, zc = blockIdx.x / a.tiles;
-  const int i0 = (tile % a.tiles_x) * kOX, j0 = (tile / a.tiles_x) * kOY;
-  const int kb = zc * a.kc;
-  const int ke = min(kb + a.kc, g.NZ);
   const int plane = g.NX * g.NY, eplane = g.nx * g.ny, numnp = g.numnp;
-  const int ej = j0 - 1 + w;
-  // the element of this lane in the node sums (x = lane, y = warp) and the
-  // node it owns
-  const int ei = i0 - 1 + l;
-  const bool e_ok = ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny;
-  const int e_off = ei + ej * g.nx;
-  const bool own = l >= 1 && w >= 1 && ei < g.NX && ej < g.NY;
-  const int own_off = ei + ej * g.NX;
 
   // Ke0^T fragments: kf[kc][nc] = Ke0[8 nc + r][4 kc + q]
   double kf[6][3];
@@ -93,185 +102,254 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
     for(int nc = 0; nc < 3; nc++)
       kf[kc][nc] = a.ke.k[(8 * nc + r) * 24 + 4 * kc + q];
 
-  // gather offsets: group gg, slot h = DOF 12 + 4 h + q (upper corner) and
-  // DOF 4 h + q (the same in-plane corner one layer down)
-  int goff[4][3];
-  bool gok[4][3];
-#pragma unroll
-  for(int h = 0; h < 3; h++)
-  {
-    const int d = 12 + 4 * h + q;
-    const int corner = d / 3 - 4, comp = d % 3;
-    const int ax = (corner == 1 || corner == 2) ? 1 : 0, ay = corner >= 2 ? 1 : 0;
-#pragma unroll
-    for(int gg = 0; gg < 4; gg++)
-    {
-      const int x = i0 - 1 + 8 * gg + r + ax, y = ej + ay;
-      gok[gg][h] = x >= 0 && x < g.NX && y >= 0 && y < g.NY;
-      goff[gg][h] = gok[gg][h] ? comp * numnp + x + y * g.NX : 0;
-    }
-  }
-  auto load_layer = [&](int k, double (&o)[4][3])
-  {
-    const bool kin = k >= 0 && k < g.NZ;
-    const int ko = kin ? k * plane : 0;
-#pragma unroll
-    for(int gg = 0; gg < 4; gg++)
-#pragma unroll
-      for(int h = 0; h < 3; h++)
-        o[gg][h] = (kin && gok[gg][h]) ? __ldg(a.u + goff[gg][h] + ko) : 0.0;
-  };
-  const double *Ebase = a.E + e_off;
-  auto load_E = [&](int e) -> double
-  { return (e_ok && e >= 0 && e < g.nz) ? __ldg(Ebase + e * eplane) : 0.0; };
-  // epilogue inputs of the own node, one node layer ahead
-  unsigned fpf = 0;
-  double upf[3] = {0.0, 0.0, 0.0}, bpf[3] = {0.0, 0.0, 0.0}, ipf[3] = {0.0, 0.0, 0.0},
-         dpf[3] = {0.0, 0.0, 0.0};
-  auto load_out_inputs = [&](int k)
-  {
-    if(!(own && k >= kb && k < ke))
-      return;
-    const int n = own_off + k * plane;
-    fpf = a.fix[n];
-#pragma unroll
-    for(int c = 0; c < 3; c++)
-    {
-      const int id = c * numnp + n;
-      if(OP == TC_DOT || OP == TC_CHEB)
-        upf[c] = __ldg(a.u + id);
-      if(OP == TC_RESID || OP == TC_CHEB)
-        bpf[c] = __ldg(a.b + id);
-      if(OP == TC_CHEB)
-      {
-        ipf[c] = __ldg(a.invd + id);
-        dpf[c] = a.c1 != 0.0 ? a.d[id] : 0.0;
-      }
-    }
-  };
-
-  const int e_first = kb - 1, e_last = ke - 1;
-  const int nlayers = e_last - e_first + 1;
-  double lo[4][3], up[4][3], pf[4][3];
-  load_layer(e_first, lo);
-  load_layer(e_first + 1, up);
-  load_layer(e_first + 2, pf);
-  double Ecur = load_E(e_first), Enext = load_E(e_first + 1);
-  load_out_inputs(kb);
-  double carry[3] = {0.0, 0.0, 0.0};
   double dot = 0.0;
-
-  // element layer e = e_first + it; P = it & 1 selects the exchange stage
-  auto step = [&](auto par, int it)
+  const long work = (long)a.tiles * g.NZ;
+  const long w_begin = work * blockIdx.x / gridDim.x;
+  const long w_end = work * (blockIdx.x + 1) / gridDim.x;
+  for(long wpos = w_begin; wpos < w_end;)
   {
-    constexpr int P = decltype(par)::value;
-    const int e = e_first + it;
-    // element products, group by group, into shared memory
+    const int tile = (int)(wpos / g.NZ);
+    const int kb = (int)(wpos % g.NZ);
+    const int ke = (int)min((long)g.NZ, kb + (w_end - wpos));
+    wpos += ke - kb;
+    const int i0 = (tile % a.tiles_x) * kOX, j0 = (tile / a.tiles_x) * kOY;
+    const int ej = j0 - 1 + w;
+    // the element of this lane in the node sums (x = lane, y = warp) and the
+    // node it owns
+    const int ei = i0 - 1 + l;
+    const bool e_ok = ei >= 0 && ei < g.nx && ej >= 0 && ej < g.ny;
+    const int e_off = ei + ej * g.nx;
+    const bool own = l >= 1 && w >= 1 && ei < g.NX && ej < g.NY;
+    const int own_off = ei + ej * g.NX;
+    // groups of 8 elements with at least one element inside the grid (warp
+    // uniform); the others skip their MMAs and contribute zeros
+    bool grp_ok[4];
 #pragma unroll
     for(int gg = 0; gg < 4; gg++)
     {
-      double acc[3][2];
-#pragma unroll
-      for(int nc = 0; nc < 3; nc++)
-        acc[nc][0] = acc[nc][1] = 0.0;
-#pragma unroll
-      for(int kc = 0; kc < 6; kc++)
-      {
-        const double av = kc < 3 ? lo[gg][kc] : up[gg][kc - 3];
-#pragma unroll
-        for(int nc = 0; nc < 3; nc++)
-          dmma(acc[nc], av, kf[kc][nc]);
-      }
-#pragma unroll
-      for(int nc = 0; nc < 3; nc++)
-#pragma unroll
-        for(int s = 0; s < 2; s++)
-          sm.D[w][8 * nc + 2 * q + s][8 * gg + r] = acc[nc][s];
+      const int x0 = i0 - 1 + 8 * gg;
+      grp_ok[gg] = ej >= 0 && ej < g.ny && x0 + 7 >= 0 && x0 < g.nx;
     }
-    // the next layer's gather: lower = this upper, upper = the prefetch
+
+    // gather offsets: group gg, slot h = DOF 12 + 4 h + q (upper corner) and
+    // DOF 4 h + q (the same in-plane corner one layer down)
+    int goff[4][3];
+    bool gok[4][3];
 #pragma unroll
-    for(int gg = 0; gg < 4; gg++)
-#pragma unroll
-      for(int h = 0; h < 3; h++)
-      {
-        lo[gg][h] = up[gg][h];
-        up[gg][h] = pf[gg][h];
-      }
-    if(it + 1 < nlayers)
-      load_layer(e + 3, pf);
-    const double Ee = Ecur;
-    Ecur = Enext;
-    Enext = load_E(e + 2);
-    __syncwarp();
-    double D[24];
-#pragma unroll
-    for(int rho = 0; rho < 24; rho++)
-      D[rho] = sm.D[w][rho][l];
-    // x pairs: node (ei, ej + dy, e + dz) <- element (ei, .) corner dx = 0 and
-    // element (ei - 1, .) corner dx = 1 (scaled by the sender's modulus)
-    double S[2][2][3];
-#pragma unroll
-    for(int dz = 0; dz < 2; dz++)
-#pragma unroll
-      for(int dy = 0; dy < 2; dy++)
-#pragma unroll
-        for(int c = 0; c < 3; c++)
-        {
-          const double nb =
-              __shfl_up_sync(0xffffffffu, Ee * D[3 * local_node(1, dy, dz) + c], 1);
-          S[dy][dz][c] = fma(Ee, D[3 * local_node(0, dy, dz) + c], nb);
-        }
-#pragma unroll
-    for(int dz = 0; dz < 2; dz++)
-#pragma unroll
-      for(int c = 0; c < 3; c++)
-        sm.xch[P][dz * 3 + c][w][l] = S[1][dz][c];
-    __syncthreads();
-    // y pairs: node (ei, ej) <- element rows ej (dy = 0) and ej - 1 (dy = 1)
-    double T[2][3];
-#pragma unroll
-    for(int dz = 0; dz < 2; dz++)
-#pragma unroll
-      for(int c = 0; c < 3; c++)
-        T[dz][c] = S[0][dz][c] + (w > 0 ? sm.xch[P][dz * 3 + c][w - 1][l] : 0.0);
-    if(e >= kb && own)
+    for(int h = 0; h < 3; h++)
     {
-      const int n = own_off + e * plane;
-      const unsigned f = fpf;
+      const int d = 12 + 4 * h + q;
+      const int corner = d / 3 - 4, comp = d % 3;
+      const int ax = (corner == 1 || corner == 2) ? 1 : 0, ay = corner >= 2 ? 1 : 0;
+#pragma unroll
+      for(int gg = 0; gg < 4; gg++)
+      {
+        const int x = i0 - 1 + 8 * gg + r + ax, y = ej + ay;
+        gok[gg][h] = x >= 0 && x < g.NX && y >= 0 && y < g.NY;
+        goff[gg][h] = gok[gg][h] ? comp * numnp + x + y * g.NX : 0;
+      }
+    }
+    auto load_layer = [&](int k, double (&o)[4][3])
+    {
+      const bool kin = k >= 0 && k < g.NZ;
+      const int ko = kin ? k * plane : 0;
+#pragma unroll
+      for(int gg = 0; gg < 4; gg++)
+#pragma unroll
+        for(int h = 0; h < 3; h++)
+          o[gg][h] = (kin && gok[gg][h]) ? __ldg(a.u + goff[gg][h] + ko) : 0.0;
+    };
+    const double *Ebase = a.E + e_off;
+    auto load_E = [&](int e) -> double
+    { return (e_ok && e >= 0 && e < g.nz) ? __ldg(Ebase + e * eplane) : 0.0; };
+    // epilogue inputs of the own node, one node layer ahead
+    unsigned fpf = 0;
+    double upf[3] = {0.0, 0.0, 0.0}, bpf[3] = {0.0, 0.0, 0.0}, ipf[3] = {0.0, 0.0, 0.0},
+           dpf[3] = {0.0, 0.0, 0.0};
+    auto load_out_inputs = [&](int k)
+    {
+      if(!(own && k >= kb && k < ke))
+        return;
+      const int n = own_off + k * plane;
+      fpf = a.fix[n];
 #pragma unroll
       for(int c = 0; c < 3; c++)
       {
         const int id = c * numnp + n;
-        const double ku = carry[c] + T[0][c];
-        const bool fixed = (f >> c) & 1u;
-        if(OP == TC_APPLY || OP == TC_DOT)
+        if(OP == TC_DOT || OP == TC_CHEB)
+          upf[c] = __ldg(a.u + id);
+        if(OP == TC_RESID || OP == TC_CHEB)
+          bpf[c] = __ldg(a.b + id);
+        if(OP == TC_CHEB)
         {
-          const double yv = fixed ? 0.0 : ku;
-          a.y[id] = yv;
-          if(OP == TC_DOT)
-            dot += upf[c] * yv;
-        }
-        else if(OP == TC_RESID)
-          a.y[id] = fixed ? 0.0 : bpf[c] - ku;
-        else
-        {
-          const double dn =
-              fixed ? 0.0 : (a.c1 != 0.0 ? a.c1 * dpf[c] : 0.0) + a.c2 * ipf[c] * (bpf[c] - ku);
-          a.d[id] = dn;
-          a.y[id] = upf[c] + dn;
+          ipf[c] = __ldg(a.invd + id);
+          dpf[c] = a.c1 != 0.0 ? a.d[id] : 0.0;
         }
       }
-    }
-    load_out_inputs(e + 1);
+    };
+
+    // element products of the layer whose lower / upper node values are in
+    // lo / up: issued into acc (the tensor pipe works on them meanwhile),
+    // stored to D[stage] later
+    // (interior tiles: all 4 groups in one branch-free sequence, so that the
+    // 12 accumulator chains interleave)
+    const bool all_ok = grp_ok[0] && grp_ok[1] && grp_ok[2] && grp_ok[3];
+    double acc[4][3][2];
+    auto mma_issue = [&](const double (&lo)[4][3], const double (&up)[4][3])
+    {
 #pragma unroll
-    for(int c = 0; c < 3; c++)
-      carry[c] = T[1][c];
-  };
-  for(int it = 0; it < nlayers; it += 2)
-  {
-    step(std::integral_constant<int, 0>{}, it);
-    if(it + 1 < nlayers)
-      step(std::integral_constant<int, 1>{}, it + 1);
+      for(int gg = 0; gg < 4; gg++)
+#pragma unroll
+        for(int nc = 0; nc < 3; nc++)
+          acc[gg][nc][0] = acc[gg][nc][1] = 0.0;
+      if(all_ok)
+      {
+        // group pairs (0, 1) and (2, 3) as M = 16, K chunk pairs as K = 8
+#pragma unroll
+        for(int k2 = 0; k2 < 3; k2++)
+#pragma unroll
+          for(int pr = 0; pr < 2; pr++)
+#pragma unroll
+            for(int nc = 0; nc < 3; nc++)
+            {
+              const int ka = 2 * k2, kb_ = 2 * k2 + 1, g0 = 2 * pr, g1 = 2 * pr + 1;
+              dmma16(acc[g0][nc], acc[g1][nc], ka < 3 ? lo[g0][ka] : up[g0][ka - 3],
+                     ka < 3 ? lo[g1][ka] : up[g1][ka - 3],
+                     kb_ < 3 ? lo[g0][kb_] : up[g0][kb_ - 3],
+                     kb_ < 3 ? lo[g1][kb_] : up[g1][kb_ - 3], kf[ka][nc], kf[kb_][nc]);
+            }
+      }
+      else
+      {
+#pragma unroll
+        for(int gg = 0; gg < 4; gg++)
+          if(grp_ok[gg])
+#pragma unroll
+            for(int kc = 0; kc < 6; kc++)
+#pragma unroll
+              for(int nc = 0; nc < 3; nc++)
+                dmma(acc[gg][nc], kc < 3 ? lo[gg][kc] : up[gg][kc - 3], kf[kc][nc]);
+      }
+    };
+    auto mma_store = [&](int st)
+    {
+#pragma unroll
+      for(int gg = 0; gg < 4; gg++)
+#pragma unroll
+        for(int nc = 0; nc < 3; nc++)
+#pragma unroll
+          for(int s_ = 0; s_ < 2; s_++)
+            sm.D[st][w][8 * nc + 2 * q + s_][8 * gg + r] = acc[gg][nc][s_];
+    };
+
+    const int e_first = kb - 1, e_last = ke - 1;
+    double lo[4][3], up[4][3];
+    load_layer(e_first, lo);
+    load_layer(e_first + 1, up);
+    mma_issue(lo, up);
+#pragma unroll
+    for(int gg = 0; gg < 4; gg++)
+#pragma unroll
+      for(int h = 0; h < 3; h++)
+        lo[gg][h] = up[gg][h];
+    load_layer(e_first + 2, up);
+    mma_store(0);
+    double Ecur = load_E(e_first), Enext = load_E(e_first + 1);
+    load_out_inputs(kb);
+    double carry[3] = {0.0, 0.0, 0.0};
+
+    // element layer e = e_first + it, stage P = it & 1
+    auto step = [&](auto par, int it)
+    {
+      constexpr int P = decltype(par)::value;
+      const int e = e_first + it;
+      const bool more = e < e_last;
+      if(more)
+      {
+        mma_issue(lo, up); // layer e + 1 (node layers e + 1, e + 2)
+#pragma unroll
+        for(int gg = 0; gg < 4; gg++)
+#pragma unroll
+          for(int h = 0; h < 3; h++)
+            lo[gg][h] = up[gg][h];
+        load_layer(e + 3, up);
+      }
+      const double Ee = Ecur;
+      Ecur = Enext;
+      Enext = load_E(e + 2);
+      __syncwarp();
+      // x pairs: node (ei, ej + dy, e + dz) <- element (ei, .) corner dx = 0
+      // and element (ei - 1, .) corner dx = 1 (scaled by the sender's modulus)
+      double S[2][2][3];
+#pragma unroll
+      for(int dz = 0; dz < 2; dz++)
+#pragma unroll
+        for(int dy = 0; dy < 2; dy++)
+#pragma unroll
+          for(int c = 0; c < 3; c++)
+          {
+            const double d1 = sm.D[P][w][3 * local_node(1, dy, dz) + c][l];
+            const double d0 = sm.D[P][w][3 * local_node(0, dy, dz) + c][l];
+            const double nb = __shfl_up_sync(0xffffffffu, Ee * d1, 1);
+            S[dy][dz][c] = fma(Ee, d0, nb);
+          }
+#pragma unroll
+      for(int dz = 0; dz < 2; dz++)
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+          sm.xch[P][dz * 3 + c][w][l] = S[1][dz][c];
+      __syncthreads();
+      // y pairs: node (ei, ej) <- element rows ej (dy = 0) and ej - 1 (dy = 1)
+      double T[2][3];
+#pragma unroll
+      for(int dz = 0; dz < 2; dz++)
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+          T[dz][c] = S[0][dz][c] + (w > 0 ? sm.xch[P][dz * 3 + c][w - 1][l] : 0.0);
+      if(e >= kb && own)
+      {
+        const int n = own_off + e * plane;
+        const unsigned f = fpf;
+#pragma unroll
+        for(int c = 0; c < 3; c++)
+        {
+          const int id = c * numnp + n;
+          const double ku = carry[c] + T[0][c];
+          const bool fixed = (f >> c) & 1u;
+          if(OP == TC_APPLY || OP == TC_DOT)
+          {
+            const double yv = fixed ? 0.0 : ku;
+            a.y[id] = yv;
+            if(OP == TC_DOT)
+              dot += upf[c] * yv;
+          }
+          else if(OP == TC_RESID)
+            a.y[id] = fixed ? 0.0 : bpf[c] - ku;
+          else
+          {
+            const double dn = fixed ? 0.0
+                                    : (a.c1 != 0.0 ? a.c1 * dpf[c] : 0.0) +
+                                          a.c2 * ipf[c] * (bpf[c] - ku);
+            a.d[id] = dn;
+            a.y[id] = upf[c] + dn;
+          }
+        }
+      }
+      load_out_inputs(e + 1);
+#pragma unroll
+      for(int c = 0; c < 3; c++)
+        carry[c] = T[1][c];
+      if(more)
+        mma_store(P ^ 1);
+    };
+    const int nlayers = e_last - e_first + 1;
+    for(int it = 0; it < nlayers; it += 2)
+    {
+      step(std::integral_constant<int, 0>{}, it);
+      if(it + 1 < nlayers)
+        step(std::integral_constant<int, 1>{}, it + 1);
+    }
+    __syncthreads(); // the next segment reuses the stages
   }
 
   if(OP == TC_DOT)
@@ -323,13 +401,14 @@ void launch_ku_dmma(icarat_ctx *c, int op, DmArgs a, cudaStream_t st)
   a.ke = c->ke0;
   a.tiles_x = (g.NX + dm::kOX - 1) / dm::kOX;
   a.tiles = a.tiles_x * ((g.NY + dm::kOY - 1) / dm::kOY);
+  // one CTA per SM slot, at least 8 node layers of work each
+  const long work = (long)a.tiles * g.NZ;
 #define ICARAT_DM_CASE(O)                                                         \
   if(op == O)                                                                     \
   {                                                                               \
     const int occ = dm_prepare<O>();                                              \
-    a.kc = pick_layers(a.tiles, g.NZ, (long)c->sm_count * occ,                    \
-                       O == TC_DOT ? (long)kMaxRedBlocks : (1L << 30));           \
-    const long grid = (long)a.tiles * ((g.NZ + a.kc - 1) / a.kc);                 \
+    long grid = std::min((long)c->sm_count * occ, std::max(1L, work / 8));        \
+    grid = std::min(grid, (long)kMaxRedBlocks);                                   \
     note_launch();                                                                \
     k_ku_dmma<O><<<(unsigned)grid, dm::kThreads, sizeof(dm::Smem), st>>>(a);      \
     ICK(cudaGetLastError());                                                      \

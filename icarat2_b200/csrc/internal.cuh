@@ -269,9 +269,10 @@ struct icarat_ctx
   int sm_count = 148;
   // operator of the finest level of the FP32 V-cycle (ICARAT_OP_*)
   int mx_fine_op = ICARAT_OP_FP32;
-  // FP64 products on the FP64 tensor cores where the grid is large enough
-  // (0: the node stencil everywhere, the default; 2: the tensor cores on
-  // every grid they fit, for explicit operator requests)
+  // FP64 products K u: 0 = by grid size (the FP64 tensor cores on grids of
+  // 2M nodes and more, the node stencil below: the measured crossover),
+  // 1 = the tensor cores on every grid of 32k nodes and more, 2 = on every
+  // grid they fit (explicit operator requests), -1 = the node stencil only
   int fp64_tc = 0;
   // learned preconditioner attached by icarat_ctx_set_net (not owned)
   icarat_net *net = nullptr;

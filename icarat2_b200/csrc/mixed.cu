@@ -442,11 +442,12 @@ void apply_K_lowp(icarat_ctx *c, int op, const float *u, float *y)
 }
 
 // Operators of the FP32 iterations unless the options name others.  The
-// smoother tolerates the ~1e-5 relative error of the BF16 hi/lo tensor-core
-// product (the preconditioner is applied inexactly anyway; same iteration
-// counts as FP32); the Krylov product K p does not (an inexact K p costs
-// many more iterations), so it stays on the FP32 CUDA-core stencil.
-constexpr int kDefaultFineOp = ICARAT_OP_TC_BF16X3;
+// smoother tolerates even the ~1e-3 relative error of the single-product
+// BF16 tensor-core operator (the preconditioner is applied inexactly anyway:
+// 15 iterations to 1e-6 at 256 x 128 x 128 with BF16, BF16 hi/lo and FP32
+// alike, BF16 the fastest); the Krylov product K p does not (an inexact K p
+// costs many more iterations), so it stays on the FP32 CUDA-core stencil.
+constexpr int kDefaultFineOp = ICARAT_OP_TC_BF16;
 constexpr int kDefaultKrylovOp = ICARAT_OP_FP32;
 
 static int spmv_blocks(const icarat_ctx *c)

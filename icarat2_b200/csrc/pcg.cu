@@ -339,7 +339,8 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
            ICARAT_ERR_ARG, "unknown solver method");
   const GridDev g = fine_grid(c);
   const int n = c->neq;
-  c->fp64_tc = o->fp64_tc ? 1 : 0;
+  IREQUIRE(o->fp64_tc >= -1 && o->fp64_tc <= 1, ICARAT_ERR_ARG, "fp64_tc must be -1, 0 or 1");
+  c->fp64_tc = o->fp64_tc;
   int levels = 0, smooth = 0;
   if(method == ICARAT_SOLVER_MG_PCG)
   {
@@ -367,7 +368,7 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                         cudaMemcpyDeviceToDevice, c->stream));
   }
   const auto key =
-      std::make_tuple(method + 4096 * c->fp64_tc, levels, smooth, chunk, (const void *)d_x);
+      std::make_tuple(method + 4096 * (c->fp64_tc + 1), levels, smooth, chunk, (const void *)d_x);
   auto it = c->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
   if(it == c->graphs.end())

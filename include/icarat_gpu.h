@@ -103,11 +103,13 @@ typedef struct
   int krylov_op;  /* MIXED_IR: ICARAT_OP_* of K p in the Krylov loop (0 = default) */
   int warm_start; /* MIXED_IR: start from the solution held by the context (the
                      previous solve, e.g. of the previous design) instead of 0 */
-  int fp64_tc;    /* JACOBI_PCG, MG_PCG: 1 = FP64 products K u element by
-                     element on the FP64 tensor cores (ICARAT_OP_TC_FP64) on
-                     every grid level large enough for it; 0 (default) = the
-                     node stencil on the CUDA cores.  Also the operator of
-                     later icarat_apply_K calls on the context. */
+  int fp64_tc;    /* JACOBI_PCG, MG_PCG: FP64 products K u element by element
+                     on the FP64 tensor cores (ICARAT_OP_TC_FP64) or by the
+                     node stencil on the CUDA cores: 0 (default) = by grid
+                     size (tensor cores on levels of 2M nodes and more),
+                     1 = tensor cores on every level of 32k nodes and more,
+                     -1 = node stencil only.  Also the operator of later
+                     icarat_apply_K calls on the context. */
 } icarat_solve_opts;
 
 typedef struct

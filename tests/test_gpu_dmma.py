@@ -52,13 +52,21 @@ def test_solvers_on_tc_fp64_match_node_stencil(gpu, method):
     m = gpu.MG_PCG if method == "mg" else gpu.JACOBI_PCG
     rtol = 1e-9 if method == "mg" else 1e-6
     u_tc, i_tc = G.solve(gpu.solve_opts(m, rtol=rtol, mg_levels=4, fp64_tc=1))
-    u_nd, i_nd = G.solve(gpu.solve_opts(m, rtol=rtol, mg_levels=4))
+    u_nd, i_nd = G.solve(gpu.solve_opts(m, rtol=rtol, mg_levels=4, fp64_tc=-1))
     assert i_tc.status == gpu.OK and i_nd.status == gpu.OK
     assert abs(i_tc.iterations - i_nd.iterations) <= 2
     assert rel_inf(u_tc, u_nd) <= 100 * rtol
     f = G.fext()
     r = f - G.apply_K_op(u_tc, gpu.OP_FP64)
     assert np.linalg.norm(r) <= 1.001 * rtol * np.linalg.norm(f)
+
+
+def test_fp64_tc_option_range(gpu):
+    G = gpu.Context(8, 4, 4)
+    G.set_design(np.full(G.nelx, 0.5))
+    with pytest.raises(gpu.IcaratError) as e:
+        G.solve(gpu.solve_opts(gpu.MG_PCG, mg_levels=2, fp64_tc=2))
+    assert e.value.status == gpu.ERR_ARG
 
 
 def test_tc_fp64_timing(gpu):
