@@ -47,8 +47,9 @@ constexpr int kPitch = 36;                  // doubles per D row in shared memor
 
 struct Smem
 {
-  double D[2][kTY][24][kPitch]; // [stage][warp][D row][element]
-  double xch[2][6][kTY][32];    // [stage][dz * 3 + c][warp][lane]
+  double D[kTY][24][kPitch];  // [warp][D row][element]
+  double xch[2][6][kTY][32];  // [stage][dz * 3 + c][warp][lane]
+  double kf[6][3][32];        // Ke0^T fragments [K chunk][N chunk][lane]
   double red[32];
 };
 
@@ -76,13 +77,12 @@ __device__ __forceinline__ void dmma16(double (&d0)[2], double (&d1)[2], double 
 } // namespace dm
 
 // Work: the (tile, node layer) pairs in tile-major order, split evenly over
-// the CTAs (one per SM); a CTA runs its range as one or two tile segments,
-// each with one element layer of z halo.  Per segment the element layers are
-// pipelined: the MMAs of layer e + 1 are issued before the node sums of
-// layer e, so the tensor pipe works while the sums run; D is
-// double-buffered in shared memory.
+// the CTAs (two per SM); a CTA runs its range as one or two tile segments,
+// each with one element layer of z halo.  The Ke0^T fragments live in shared
+// memory so that a thread fits in 128 registers: two CTAs per SM, whose
+// layers drift apart, keep the tensor pipe busy while the other one sums.
 template <int OP>
-__global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
+__global__ void __launch_bounds__(dm::kThreads, 2) k_ku_dmma(DmArgs a)
 {
   using namespace dm;
   extern __shared__ __align__(16) uint8_t dm_smem_raw[];
@@ -94,13 +94,13 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
   const GridDev g = a.g;
   const int plane = g.NX * g.NY, eplane = g.nx * g.ny, numnp = g.numnp;
 
-  // Ke0^T fragments: kf[kc][nc] = Ke0[8 nc + r][4 kc + q]
-  double kf[6][3];
-#pragma unroll
-  for(int kc = 0; kc < 6; kc++)
-#pragma unroll
-    for(int nc = 0; nc < 3; nc++)
-      kf[kc][nc] = a.ke.k[(8 * nc + r) * 24 + 4 * kc + q];
+  // Ke0^T fragments: kf[kc][nc][lane] = Ke0[8 nc + r][4 kc + q]
+  for(int i = t; i < 6 * 3 * 32; i += kThreads)
+  {
+    const int kc = i / 96, nc = (i / 32) % 3, ln = i % 32;
+    sm.kf[kc][nc][ln] = a.ke.k[(8 * nc + (ln >> 2)) * 24 + 4 * kc + (ln & 3)];
+  }
+  __syncthreads();
 
   double dot = 0.0;
   const long work = (long)a.tiles * g.NZ;
@@ -131,23 +131,22 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
       grp_ok[gg] = ej >= 0 && ej < g.ny && x0 + 7 >= 0 && x0 < g.nx;
     }
 
-    // gather offsets: group gg, slot h = DOF 12 + 4 h + q (upper corner) and
-    // DOF 4 h + q (the same in-plane corner one layer down)
-    int goff[4][3];
-    bool gok[4][3];
+    // gather of slot h = DOF 12 + 4 h + q (upper corner) and DOF 4 h + q (the
+    // same in-plane corner one layer down) of group gg: node x = gx0[h] + 8 gg
+    // on node row gy[h]; offsets are rebuilt per load to save registers
+    int gx0[3], gbase[3];
+    unsigned gymask = 0; // bit h: node row inside the grid
 #pragma unroll
     for(int h = 0; h < 3; h++)
     {
       const int d = 12 + 4 * h + q;
       const int corner = d / 3 - 4, comp = d % 3;
       const int ax = (corner == 1 || corner == 2) ? 1 : 0, ay = corner >= 2 ? 1 : 0;
-#pragma unroll
-      for(int gg = 0; gg < 4; gg++)
-      {
-        const int x = i0 - 1 + 8 * gg + r + ax, y = ej + ay;
-        gok[gg][h] = x >= 0 && x < g.NX && y >= 0 && y < g.NY;
-        goff[gg][h] = gok[gg][h] ? comp * numnp + x + y * g.NX : 0;
-      }
+      gx0[h] = i0 - 1 + r + ax;
+      const int y = ej + ay;
+      if(y >= 0 && y < g.NY)
+        gymask |= 1u << h;
+      gbase[h] = comp * numnp + y * g.NX;
     }
     auto load_layer = [&](int k, double (&o)[4][3])
     {
@@ -157,7 +156,11 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
       for(int gg = 0; gg < 4; gg++)
 #pragma unroll
         for(int h = 0; h < 3; h++)
-          o[gg][h] = (kin && gok[gg][h]) ? __ldg(a.u + goff[gg][h] + ko) : 0.0;
+        {
+          const int x = gx0[h] + 8 * gg;
+          const bool ok = kin && ((gymask >> h) & 1u) && x >= 0 && x < g.NX;
+          o[gg][h] = ok ? __ldg(a.u + (gbase[h] + x + ko)) : 0.0;
+        }
     };
     const double *Ebase = a.E + e_off;
     auto load_E = [&](int e) -> double
@@ -191,69 +194,63 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
     // element products of the layer whose lower / upper node values are in
     // lo / up: issued into acc (the tensor pipe works on them meanwhile),
     // stored to D[stage] later
-    // (interior tiles: all 4 groups in one branch-free sequence, so that the
-    // 12 accumulator chains interleave)
-    const bool all_ok = grp_ok[0] && grp_ok[1] && grp_ok[2] && grp_ok[3];
-    double acc[4][3][2];
-    auto mma_issue = [&](const double (&lo)[4][3], const double (&up)[4][3])
+    // element products of the layer whose lower / upper node values are in
+    // lo / up, one pair of groups (M = 16 for m16n8k8, K chunk pairs as
+    // K = 8) at a time, straight into D; groups outside the grid (warp
+    // uniform) skip their MMAs and store zeros
+    auto mma_layer = [&](const double (&lo)[4][3], const double (&up)[4][3])
     {
 #pragma unroll
-      for(int gg = 0; gg < 4; gg++)
-#pragma unroll
-        for(int nc = 0; nc < 3; nc++)
-          acc[gg][nc][0] = acc[gg][nc][1] = 0.0;
-      if(all_ok)
+      for(int pr = 0; pr < 2; pr++)
       {
-        // group pairs (0, 1) and (2, 3) as M = 16, K chunk pairs as K = 8
+        const int g0 = 2 * pr, g1 = 2 * pr + 1;
+        double acc[2][3][2];
 #pragma unroll
-        for(int k2 = 0; k2 < 3; k2++)
+        for(int m = 0; m < 2; m++)
 #pragma unroll
-          for(int pr = 0; pr < 2; pr++)
+          for(int nc = 0; nc < 3; nc++)
+            acc[m][nc][0] = acc[m][nc][1] = 0.0;
+        if(grp_ok[g0] && grp_ok[g1])
+        {
+#pragma unroll
+          for(int k2 = 0; k2 < 3; k2++)
 #pragma unroll
             for(int nc = 0; nc < 3; nc++)
             {
-              const int ka = 2 * k2, kb_ = 2 * k2 + 1, g0 = 2 * pr, g1 = 2 * pr + 1;
-              dmma16(acc[g0][nc], acc[g1][nc], ka < 3 ? lo[g0][ka] : up[g0][ka - 3],
+              const int ka = 2 * k2, kb_ = 2 * k2 + 1;
+              dmma16(acc[0][nc], acc[1][nc], ka < 3 ? lo[g0][ka] : up[g0][ka - 3],
                      ka < 3 ? lo[g1][ka] : up[g1][ka - 3],
                      kb_ < 3 ? lo[g0][kb_] : up[g0][kb_ - 3],
-                     kb_ < 3 ? lo[g1][kb_] : up[g1][kb_ - 3], kf[ka][nc], kf[kb_][nc]);
+                     kb_ < 3 ? lo[g1][kb_] : up[g1][kb_ - 3], sm.kf[ka][nc][l],
+                     sm.kf[kb_][nc][l]);
             }
+        }
+        else
+        {
+#pragma unroll
+          for(int m = 0; m < 2; m++)
+            if(grp_ok[g0 + m])
+#pragma unroll
+              for(int kc = 0; kc < 6; kc++)
+#pragma unroll
+                for(int nc = 0; nc < 3; nc++)
+                  dmma(acc[m][nc], kc < 3 ? lo[g0 + m][kc] : up[g0 + m][kc - 3],
+                       sm.kf[kc][nc][l]);
+        }
+#pragma unroll
+        for(int m = 0; m < 2; m++)
+#pragma unroll
+          for(int nc = 0; nc < 3; nc++)
+#pragma unroll
+            for(int s_ = 0; s_ < 2; s_++)
+              sm.D[w][8 * nc + 2 * q + s_][8 * (g0 + m) + r] = acc[m][nc][s_];
       }
-      else
-      {
-#pragma unroll
-        for(int gg = 0; gg < 4; gg++)
-          if(grp_ok[gg])
-#pragma unroll
-            for(int kc = 0; kc < 6; kc++)
-#pragma unroll
-              for(int nc = 0; nc < 3; nc++)
-                dmma(acc[gg][nc], kc < 3 ? lo[gg][kc] : up[gg][kc - 3], kf[kc][nc]);
-      }
-    };
-    auto mma_store = [&](int st)
-    {
-#pragma unroll
-      for(int gg = 0; gg < 4; gg++)
-#pragma unroll
-        for(int nc = 0; nc < 3; nc++)
-#pragma unroll
-          for(int s_ = 0; s_ < 2; s_++)
-            sm.D[st][w][8 * nc + 2 * q + s_][8 * gg + r] = acc[gg][nc][s_];
     };
 
     const int e_first = kb - 1, e_last = ke - 1;
     double lo[4][3], up[4][3];
     load_layer(e_first, lo);
     load_layer(e_first + 1, up);
-    mma_issue(lo, up);
-#pragma unroll
-    for(int gg = 0; gg < 4; gg++)
-#pragma unroll
-      for(int h = 0; h < 3; h++)
-        lo[gg][h] = up[gg][h];
-    load_layer(e_first + 2, up);
-    mma_store(0);
     double Ecur = load_E(e_first), Enext = load_E(e_first + 1);
     load_out_inputs(kb);
     double carry[3] = {0.0, 0.0, 0.0};
@@ -263,17 +260,14 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
     {
       constexpr int P = decltype(par)::value;
       const int e = e_first + it;
-      const bool more = e < e_last;
-      if(more)
-      {
-        mma_issue(lo, up); // layer e + 1 (node layers e + 1, e + 2)
+      mma_layer(lo, up); // node layers e, e + 1
 #pragma unroll
-        for(int gg = 0; gg < 4; gg++)
+      for(int gg = 0; gg < 4; gg++)
 #pragma unroll
-          for(int h = 0; h < 3; h++)
-            lo[gg][h] = up[gg][h];
-        load_layer(e + 3, up);
-      }
+        for(int h = 0; h < 3; h++)
+          lo[gg][h] = up[gg][h];
+      if(e < e_last)
+        load_layer(e + 2, up);
       const double Ee = Ecur;
       Ecur = Enext;
       Enext = load_E(e + 2);
@@ -288,8 +282,8 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
 #pragma unroll
           for(int c = 0; c < 3; c++)
           {
-            const double d1 = sm.D[P][w][3 * local_node(1, dy, dz) + c][l];
-            const double d0 = sm.D[P][w][3 * local_node(0, dy, dz) + c][l];
+            const double d1 = sm.D[w][3 * local_node(1, dy, dz) + c][l];
+            const double d0 = sm.D[w][3 * local_node(0, dy, dz) + c][l];
             const double nb = __shfl_up_sync(0xffffffffu, Ee * d1, 1);
             S[dy][dz][c] = fma(Ee, d0, nb);
           }
@@ -339,8 +333,6 @@ __global__ void __launch_bounds__(dm::kThreads, 1) k_ku_dmma(DmArgs a)
 #pragma unroll
       for(int c = 0; c < 3; c++)
         carry[c] = T[1][c];
-      if(more)
-        mma_store(P ^ 1);
     };
     const int nlayers = e_last - e_first + 1;
     for(int it = 0; it < nlayers; it += 2)

@@ -145,8 +145,8 @@ static int node_blocks(const GridDev &g, int threads)
 
 // Below kDmmaMinNodes the element tiles would leave most SMs idle; below
 // kDmmaAutoNodes the node stencil is the faster of the two on a B200
-// (measured: 60 us against 68 us at 129 x 65 x 65 nodes, 494 us against
-// 390 us at 257 x 129 x 129).
+// (measured: 60 us against 62 us at 129 x 65 x 65 nodes, 494 us against
+// 331 us at 257 x 129 x 129).
 constexpr int kDmmaMinNodes = 1 << 15;
 constexpr int kDmmaAutoNodes = 1 << 21;
 
