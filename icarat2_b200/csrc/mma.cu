@@ -155,7 +155,8 @@ __device__ __forceinline__ void mma_x(const MmaArgs &A, int i, const double *lam
     ql += A.qij[(long)i * M + j] * lam[j];
   }
   const double lo = A.low[i], up = A.upp[i];
-  xp = (sqrt(pl) * lo + sqrt(ql) * up) / (sqrt(pl) + sqrt(ql));
+  const double sp = sqrt(pl), sq = sqrt(ql);
+  xp = (sp * lo + sq * up) / (sp + sq);
   x = xp;
   if(x < A.alpha[i])
     x = A.alpha[i];
@@ -220,7 +221,11 @@ __device__ void mma_pass(const MmaArgs &A, MmaShared<M> &sm, cg::grid_group &gri
     double x, xp, pl, ql;
     mma_x<M>(A, i, lam, x, xp, pl, ql);
     const double ux = A.upp[i] - x, xl = x - A.low[i];
-    double df2 = -1.0 / (2.0 * pl / pow(ux, 3.0) + 2.0 * ql / pow(xl, 3.0));
+    // one reciprocal per distance, then products (the reference divides by
+    // pow(., 3) and by each power separately; the values agree to rounding)
+    const double rux = 1.0 / ux, rxl = 1.0 / xl;
+    const double rux2 = rux * rux, rxl2 = rxl * rxl;
+    double df2 = -1.0 / (2.0 * pl * (rux2 * rux) + 2.0 * ql * (rxl2 * rxl));
     if(xp < A.alpha[i])
       df2 = 0.0;
     if(xp > A.beta[i])
@@ -230,8 +235,8 @@ __device__ void mma_pass(const MmaArgs &A, MmaShared<M> &sm, cg::grid_group &gri
     for(int j = 0; j < M; j++)
     {
       const double p = A.pij[(long)i * M + j], q = A.qij[(long)i * M + j];
-      acc[j] += p / ux + q / xl;
-      PQ[j] = p / (ux * ux) - q / (xl * xl);
+      acc[j] += p * rux + q * rxl;
+      PQ[j] = p * rux2 - q * rxl2;
     }
 #pragma unroll
     for(int j = 0; j < M; j++)

@@ -10,7 +10,12 @@ set-up.
         methods: jacobi, mg, mixed
     python -m icarat2_b200.profile_cases operator 256x128x128 2 3
         `reps` launches of K u with operator 0 FP64, 1 FP32, 2 tensor cores
-        BF16x3, 3 tensor cores BF16 (after one warm-up launch)
+        BF16x3, 3 tensor cores BF16, 4 FP64 tensor cores (after one warm-up
+        launch)
+    python -m icarat2_b200.profile_cases loop 256x128x128 mixed 6 1e-6 3
+        one design iteration of the MMA loop (densities U[0.1, 0.5], seed 0,
+        filter radius 3, move 0.2) after `warm` warm-up iterations; methods
+        mg, mixed (warm-started), jacobi
 """
 import ctypes as C
 import sys
@@ -62,9 +67,31 @@ def operator(grid, op, reps):
     print("ms per launch %.4f" % ms)
 
 
+def loop(grid, method, levels, rtol, warm):
+    nx, ny, nz = _grid(grid)
+    G = gpu.Context(nx, ny, nz)
+    rho = np.random.default_rng(0).uniform(0.1, 0.5, G.nelx)
+    m = {"jacobi": gpu.JACOBI_PCG, "mg": gpu.MG_PCG, "mixed": gpu.MIXED_IR}[method]
+    o = gpu.solve_opts(m, rtol=float(rtol), mg_levels=int(levels),
+                       warm_start=1 if method == "mixed" else 0)
+    G.loop_init(rho, method="mma", filter_radius=3.0, move=0.2, solve=o)
+    for _ in range(int(warm)):
+        G.loop_step()
+    G.synchronize()
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    info = G.loop_step()
+    G.synchronize()
+    rt.cudaProfilerStop()
+    print("cg iterations %d compliance %.6g status %d" % (info.cg_iterations, info.compliance,
+                                                         info.status))
+
+
 def main(argv):
     if len(argv) >= 5 and argv[0] == "solve":
         solve(*argv[1:5])
+    elif len(argv) >= 6 and argv[0] == "loop":
+        loop(*argv[1:6])
     elif len(argv) >= 4 and argv[0] == "operator":
         operator(*argv[1:4])
     else:
