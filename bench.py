@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--grid", default="128x64x64")
     p.add_argument("--radius", type=float, default=2.5)
     p.add_argument("--levels", type=int, default=4)
+    p.add_argument("--coarse-lag", type=int, default=1,
+                   help="1: reuse the previous design's coarsest factor while this "
+                        "design's is computed on a second stream")
     p.add_argument("--smooth", type=int, default=2)
     p.add_argument("--rtol", type=float, default=1e-8)
     p.add_argument("--cpu-sample", action="store_true",
@@ -89,6 +92,9 @@ def config(a, extra=None):
          "update": "MMA", "move": 0.2, "filter_radius": a.radius, "volfrac": 0.3,
          "solver": "MG-PCG" if a.impl == "ours" else "Jacobi-PCG (Eigen_CG semantics)",
          "mg_levels": a.levels, "rtol": a.rtol}
+    if a.impl == "ours":
+        c["coarse_factor"] = ("previous design's, this design's computed on a second stream "
+                              "during the solve" if a.coarse_lag else "this design's")
     if extra:
         c.update(extra)
     return c
@@ -556,7 +562,7 @@ def gpu_arm(a):
             cpu_line = json.loads(r.stdout.strip().splitlines()[-1])
 
     nx, ny, nz = grid_of(a)
-    opts = G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth)
+    opts = G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth, coarse_lag=a.coarse_lag)
 
     def make_ctx():
         return G.Context(nx, ny, nz, device=local)
@@ -595,22 +601,20 @@ def gpu_arm(a):
     total_ms = float(t.item())
     value = world * a.steps / (total_ms / 1000.0)
 
-    # ---------------- the same loop with one more multigrid level (coarsest
-    # level 8x4x4 instead of 16x8x8: a 600-DOF dense solve instead of 3,888)
-    alt = None
-    if a.alt_levels:
+    def alt_loop(levels, lag):
         ca = make_ctx()
         ca.loop_init(0.3, method="mma", filter_radius=a.radius, move=0.2,
-                     solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, a.alt_levels, a.smooth))
+                     solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, levels, a.smooth,
+                                        coarse_lag=lag))
         sa = torch.cuda.ExternalStream(ca.stream_ptr(), device=dev)
         for _ in range(a.warmup):
             ca.loop_step()
         torch.cuda.synchronize()
-        alt_ms = 0.0
+        alt_ms, its = 0.0, []
         for _ in range(a.steps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(sa)
-            ca.loop_step()
+            its.append(ca.loop_step().cg_iterations)
             e1.record(sa)
             e1.synchronize()
             alt_ms += e0.elapsed_time(e1)
@@ -620,10 +624,17 @@ def gpu_arm(a):
         ta = torch.tensor([alt_ms], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(ta, op=dist.ReduceOp.MAX)
-        alt = {"mg_levels": a.alt_levels,
-               "value": world * a.steps / (float(ta.item()) / 1000.0),
-               "unit": "design-iter/s", "ms_per_step": float(ta.item()) / a.steps}
         ca.close()
+        return {"mg_levels": levels, "coarse_lag": lag,
+                "value": world * a.steps / (float(ta.item()) / 1000.0),
+                "unit": "design-iter/s", "ms_per_step": float(ta.item()) / a.steps,
+                "cg_iterations_per_step": its}
+
+    # ---------------- the same loop with the coarsest factor of each design
+    # computed before its solve, and with one more multigrid level (coarsest
+    # level 8x4x4 instead of 16x8x8: a 600-DOF dense solve instead of 3,888)
+    other_coarse = alt_loop(a.levels, 1 - a.coarse_lag) if a.alt_levels else None
+    alt = alt_loop(a.alt_levels, a.coarse_lag) if a.alt_levels else None
 
     # ---------------- dominant kernel: FP64 stencil K u on the final design
     ms_op = ctx.time_operator(30)
@@ -738,6 +749,7 @@ def gpu_arm(a):
             "ku_gdof_s": nd / (ms_op * 1e-3) / 1e9,
             "cg_iterations_per_step": cg,
             "alt_levels": alt,
+            "alt_coarse_lag": other_coarse,
             "mixed_256x128x128": mixed,
             "batched_80_designs": batched,
             "learned": learned,

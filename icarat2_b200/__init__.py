@@ -79,7 +79,7 @@ class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int),
                 ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int),
                 ("refresh", C.c_double), ("fine_op", C.c_int), ("krylov_op", C.c_int),
-                ("warm_start", C.c_int), ("fp64_tc", C.c_int)]
+                ("warm_start", C.c_int), ("fp64_tc", C.c_int), ("coarse_lag", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -254,12 +254,15 @@ def _bc_struct(dirichlet, loads):
 
 
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
-               chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0, fp64_tc=0):
+               chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0, fp64_tc=0,
+               coarse_lag=0):
     """fp64_tc (JACOBI_PCG, MG_PCG): FP64 products on the FP64 tensor cores
     by grid size (0), on every level of 32k nodes and more (1), or the node
-    stencil only (-1)."""
+    stencil only (-1).  coarse_lag (MG_PCG, MIXED_IR): keep the previous
+    design's coarsest factor while this design's is computed on a second
+    stream."""
     return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,
-                     krylov_op, warm_start, int(fp64_tc))
+                     krylov_op, warm_start, int(fp64_tc), int(bool(coarse_lag)))
 
 
 class Context:

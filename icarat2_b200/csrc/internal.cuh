@@ -183,12 +183,22 @@ struct CoarseSolver
   int n = 0;              // free DOFs of the coarsest level
   int bw = 0;             // lower bandwidth of the dense matrix in that order
   int *map = nullptr;     // n -> full index on the coarsest grid
-  double *A = nullptr;    // n x n dense SPD matrix, becomes its Cholesky factor L
-  double *W = nullptr;    // n x n, L^-1
-  double *work = nullptr; // n x n scratch of the triangular inversion
+  // two factor buffers (the second only once a lagged set-up needs it):
+  double *A[2] = {nullptr, nullptr};    // n x n dense SPD matrix -> its Cholesky factor L
+  double *W[2] = {nullptr, nullptr};    // n x n, L^-1
+  double *work[2] = {nullptr, nullptr}; // n x n scratch of the inversion, then W^T
   double *vin = nullptr, *vout = nullptr;
-  cudaGraphExec_t setup = nullptr; // per-design setup of all levels
-  int setup_kernels = 0;
+  int cur = 0;        // buffer the V-cycle reads
+  int pending = -1;   // buffer being factored on the side stream (-1: none)
+  bool have = false;  // buffer cur holds the factor of some design
+  // per-design set-up graphs: all levels with the factor into buffer b
+  // (synchronous), the levels alone, and the factor alone into buffer b
+  cudaGraphExec_t setup[2] = {nullptr, nullptr};
+  cudaGraphExec_t levels = nullptr;
+  cudaGraphExec_t factor[2] = {nullptr, nullptr};
+  int setup_kernels = 0, levels_kernels = 0, factor_kernels = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_levels = nullptr, ev_factor[2] = {nullptr, nullptr};
 };
 
 struct FilterState
@@ -318,7 +328,7 @@ void launch_apply_K(icarat_ctx *c, const GridDev &g, const double *E,
 void launch_apply_K_f32(icarat_ctx *c, const GridDev &g, const float *E,
                         const uint8_t *fix, const float *u, float *y);
 void launch_diag(icarat_ctx *c, const GridDev &g, const double *E,
-                 const uint8_t *fix, double *invd);
+                 const uint8_t *fix, double *invd, cudaStream_t st = nullptr);
 void launch_residual(icarat_ctx *c, const GridDev &g, const double *E,
                      const uint8_t *fix, const double *b, const double *x,
                      double *r);
@@ -369,7 +379,13 @@ void round_f32(icarat_ctx *c, long n, const double *in, float *out);
 void widen_f64(icarat_ctx *c, long n, const float *in, double *out);
 
 // multigrid.cu
-void mg_setup(icarat_ctx *c, int levels);
+// lag: the V-cycle keeps the coarsest factor of the previous design while
+// this design's factor is computed on a side stream (first call after a
+// hierarchy change: synchronous)
+void mg_setup(icarat_ctx *c, int levels, bool lag = false);
+// the context's stream waits for a lagged factorization in flight (so that a
+// solve's work, side stream included, ends with the solve)
+void mg_join(icarat_ctx *c);
 double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse);
 void mg_vcycle(icarat_ctx *c, const double *r, double *z, int smooth);
 void mg_vcycle_f32(icarat_ctx *c, const float *r, float *z, int smooth);

@@ -542,7 +542,7 @@ void mixed_begin(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, d
   const bool learned = o->method == ICARAT_SOLVER_LEARNED_FPCG;
   IREQUIRE(!learned || c->net, ICARAT_ERR_STATE,
            "attach a net with icarat_ctx_set_net before the learned solver");
-  mg_setup(c, levels);
+  mg_setup(c, levels, o->coarse_lag != 0);
   mixed_alloc(c);
   const int n = c->neq;
   const double nfree = c->numeq > 0 ? (double)c->numeq : 1.0;
@@ -639,7 +639,8 @@ void mixed_begin(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, d
 
   // the operators are part of what a captured graph launches
   const auto key = std::make_tuple((int)ICARAT_SOLVER_MIXED_IR + 16 * fine_op + 256 * krylov_op,
-                                   levels, smooth, chunk, (const void *)d_x);
+                                   levels + 32 * c->coarse.cur, smooth, chunk,
+                                   (const void *)d_x);
   auto it = c->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
   if(it == c->graphs.end() || c->graph_b.count(key) == 0 || c->graph_b[key] != d_b)
@@ -734,6 +735,8 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
       break;
     mixed_chunk(c, run);
   }
+  mg_join(c);
+  ICK(cudaStreamSynchronize(c->stream));
   return mixed_finish(c, run, info);
 }
 

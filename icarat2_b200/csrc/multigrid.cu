@@ -304,14 +304,30 @@ void mg_free(icarat_ctx *c)
       dfree(p);
   }
   c->mg.clear();
-  if(c->coarse.setup)
-    cudaGraphExecDestroy(c->coarse.setup);
-  dfree(c->coarse.map);
-  dfree(c->coarse.A);
-  dfree(c->coarse.W);
-  dfree(c->coarse.work);
-  dfree(c->coarse.vin);
-  dfree(c->coarse.vout);
+  CoarseSolver &C = c->coarse;
+  if(C.side)
+    cudaStreamSynchronize(C.side); // a lagged factorization may still run
+  for(int b = 0; b < 2; b++)
+  {
+    if(C.setup[b])
+      cudaGraphExecDestroy(C.setup[b]);
+    if(C.factor[b])
+      cudaGraphExecDestroy(C.factor[b]);
+    if(C.ev_factor[b])
+      cudaEventDestroy(C.ev_factor[b]);
+    dfree(C.A[b]);
+    dfree(C.W[b]);
+    dfree(C.work[b]);
+  }
+  if(C.levels)
+    cudaGraphExecDestroy(C.levels);
+  if(C.ev_levels)
+    cudaEventDestroy(C.ev_levels);
+  if(C.side)
+    cudaStreamDestroy(C.side);
+  dfree(C.map);
+  dfree(C.vin);
+  dfree(C.vout);
   c->coarse = CoarseSolver{};
   c->mg_built_levels = 0;
 }
@@ -438,18 +454,17 @@ static void allocate_levels(icarat_ctx *c, int levels)
                    cudaMemcpyHostToDevice));
   ICK(cudaMemcpy(c->coarse.map + nf, colmap.data(), sizeof(int) * colmap.size(),
                  cudaMemcpyHostToDevice));
-  c->coarse.A = dalloc((size_t)nf * nf);
-  c->coarse.W = dalloc((size_t)nf * nf);
-  c->coarse.work = dalloc((size_t)nf * nf);
+  c->coarse.A[0] = dalloc((size_t)nf * nf);
+  c->coarse.W[0] = dalloc((size_t)nf * nf);
+  c->coarse.work[0] = dalloc((size_t)nf * nf);
   c->coarse.vin = dalloc(nf);
   c->coarse.vout = dalloc(nf);
   c->mg_built_levels = levels;
 }
 
-// Everything that depends on the design: coarse moduli, Jacobi diagonals (and
-// their FP32 copies), the dense coarsest matrix and W = L^-1 of its Cholesky
-// factor.
-static void enqueue_mg_setup(icarat_ctx *c, int levels)
+// Everything on the levels that depends on the design: coarse moduli and
+// Jacobi diagonals (and their FP32 copies).
+static void enqueue_levels(icarat_ctx *c, int levels, cudaStream_t st)
 {
   for(int l = 0; l < levels; l++)
   {
@@ -458,30 +473,35 @@ static void enqueue_mg_setup(icarat_ctx *c, int levels)
     {
       const MgLevel &F = c->mg[l - 1];
       note_launch();
-      k_coarsen_E<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>(F.g, L.g, F.E, L.E);
+      k_coarsen_E<<<blocks_for(L.g.nelx, 256), 256, 0, st>>>(F.g, L.g, F.E, L.E);
     }
-    launch_diag(c, L.g, L.E, L.fix, L.invd);
+    launch_diag(c, L.g, L.E, L.fix, L.invd, st);
     if(l > 0) // the finest FP32 moduli come with the design
     {
       note_launch();
-      k_cast<<<blocks_for(L.g.nelx, 256), 256, 0, c->stream>>>((long)L.g.nelx, L.E, L.E32);
+      k_cast<<<blocks_for(L.g.nelx, 256), 256, 0, st>>>((long)L.g.nelx, L.E, L.E32);
     }
     note_launch();
-    k_cast<<<blocks_for(3L * L.g.numnp, 256), 256, 0, c->stream>>>(3L * L.g.numnp, L.invd,
-                                                                   L.invd32);
+    k_cast<<<blocks_for(3L * L.g.numnp, 256), 256, 0, st>>>(3L * L.g.numnp, L.invd,
+                                                           L.invd32);
   }
-  const MgLevel &C = c->mg[levels - 1];
+}
+
+// The dense coarsest matrix of the current coarsest moduli and W = L^-1 of
+// its Cholesky factor, into factor buffer b.
+static void enqueue_factor(icarat_ctx *c, int b, cudaStream_t st)
+{
+  const MgLevel &C = c->mg.back();
   const int n = c->coarse.n;
-  if(n > 0)
-  {
-    ICK(cudaMemsetAsync(c->coarse.A, 0, sizeof(double) * (size_t)n * n, c->stream));
-    note_launch();
-    k_coarse_assemble<<<blocks_for(n, 64), 64, 0, c->stream>>>(
-        C.g, c->ke0, C.E, c->coarse.map, c->coarse.map + n, n, c->coarse.A);
-    ICK(cudaGetLastError());
-    dense_spd_inverse_factor(c->stream, c->coarse.A, c->coarse.W, c->coarse.work, n,
-                             c->coarse.bw);
-  }
+  if(n == 0)
+    return;
+  ICK(cudaMemsetAsync(c->coarse.A[b], 0, sizeof(double) * (size_t)n * n, st));
+  note_launch();
+  k_coarse_assemble<<<blocks_for(n, 64), 64, 0, st>>>(C.g, c->ke0, C.E, c->coarse.map,
+                                                     c->coarse.map + n, n, c->coarse.A[b]);
+  ICK(cudaGetLastError());
+  dense_spd_inverse_factor(st, c->coarse.A[b], c->coarse.W[b], c->coarse.work[b], n,
+                           c->coarse.bw);
 }
 
 // ||b - K_c x|| / ||b|| of the coarsest dense solve for a fixed right-hand
@@ -505,8 +525,8 @@ double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
   ICK(cudaMemcpy(rowmap.data(), c->coarse.map, sizeof(int) * n, cudaMemcpyDeviceToHost));
   ICK(cudaMemcpy(c->coarse.vin, b.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
   ICK(cudaMemsetAsync(C.x, 0, sizeof(double) * nv, c->stream));
-  dense_spd_solve(c->stream, c->coarse.W, c->coarse.work, n, c->coarse.vin, c->coarse.vout,
-                  c->coarse.map, C.x);
+  dense_spd_solve(c->stream, c->coarse.W[c->coarse.cur], c->coarse.work[c->coarse.cur], n,
+                  c->coarse.vin, c->coarse.vout, c->coarse.map, C.x);
   launch_apply_K(c, C.g, C.E, C.fix, C.x, C.t, nullptr);
   ICK(cudaMemcpyAsync(y.data(), C.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
   ICK(cudaStreamSynchronize(c->stream));
@@ -520,50 +540,128 @@ double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
   return std::sqrt(rr / bb);
 }
 
+// Captures what f enqueues on stream st into an instantiated graph.
+template <typename F>
+static cudaGraphExec_t capture(cudaStream_t st, int &kernels, F f)
+{
+  cudaGraph_t graph;
+  ICK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  set_capturing(true);
+  try
+  {
+    f();
+  }
+  catch(...)
+  {
+    set_capturing(false);
+    cudaStreamEndCapture(st, &graph);
+    throw;
+  }
+  set_capturing(false);
+  ICK(cudaStreamEndCapture(st, &graph));
+  size_t nn = 0;
+  ICK(cudaGraphGetNodes(graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  ICK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+  kernels = 0;
+  for(auto nd : nodes)
+  {
+    cudaGraphNodeType t;
+    ICK(cudaGraphNodeGetType(nd, &t));
+    kernels += (t == cudaGraphNodeTypeKernel) ? 1 : 0;
+  }
+  cudaGraphExec_t exec;
+  ICK(cudaGraphInstantiate(&exec, graph, 0));
+  cudaGraphDestroy(graph);
+  return exec;
+}
+
 // Coarse operators and the dense inverse for the current design.  The fixed
-// launch sequence is captured once per hierarchy into a CUDA graph and
+// launch sequences are captured once per hierarchy into CUDA graphs and
 // replayed for every new design.
-void mg_setup(icarat_ctx *c, int levels)
+//
+// Lagged set-up (factor reuse across design iterations): the levels of the
+// new design are built on the context's stream as usual, but its coarsest
+// factor goes into the other buffer on a side stream, overlapped with the
+// solve, which keeps the factor of the previous design; the next set-up
+// waits for it and switches buffers.  The coarse correction then belongs to
+// a slightly different operator, which costs at most a few iterations while
+// the design changes slowly; the solve's stopping test is unchanged.
+void mg_setup(icarat_ctx *c, int levels, bool lag)
 {
   IREQUIRE(levels >= 2 && levels <= 12, ICARAT_ERR_ARG, "mg_levels must be in [2, 12]");
   if((int)c->mg.size() != levels)
     allocate_levels(c, levels);
   else if(c->mg_version == c->design_version)
-    return; // operators of this design are built already
-  c->mg_version = c->design_version;
-  if(!c->coarse.setup)
   {
-    cudaGraph_t graph;
-    ICK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    set_capturing(true);
-    try
+    // operators of this design are built; its lagged factor replaces the
+    // previous design's once it has finished (a synchronous request waits
+    // for it)
+    CoarseSolver &C = c->coarse;
+    if(C.pending >= 0 && (!lag || cudaEventQuery(C.ev_factor[C.pending]) == cudaSuccess))
     {
-      enqueue_mg_setup(c, levels);
+      ICK(cudaStreamWaitEvent(c->stream, C.ev_factor[C.pending], 0));
+      C.cur = C.pending;
+      C.pending = -1;
     }
-    catch(...)
-    {
-      set_capturing(false);
-      cudaStreamEndCapture(c->stream, &graph);
-      throw;
-    }
-    set_capturing(false);
-    ICK(cudaStreamEndCapture(c->stream, &graph));
-    size_t nn = 0;
-    ICK(cudaGraphGetNodes(graph, nullptr, &nn));
-    std::vector<cudaGraphNode_t> nodes(nn);
-    ICK(cudaGraphGetNodes(graph, nodes.data(), &nn));
-    c->coarse.setup_kernels = 0;
-    for(auto nd : nodes)
-    {
-      cudaGraphNodeType t;
-      ICK(cudaGraphNodeGetType(nd, &t));
-      c->coarse.setup_kernels += (t == cudaGraphNodeTypeKernel) ? 1 : 0;
-    }
-    ICK(cudaGraphInstantiate(&c->coarse.setup, graph, 0));
-    cudaGraphDestroy(graph);
+    return;
   }
-  ICK(cudaGraphLaunch(c->coarse.setup, c->stream));
-  note_launch(c->coarse.setup_kernels);
+  c->mg_version = c->design_version;
+  CoarseSolver &C = c->coarse;
+  if(C.pending >= 0)
+  {
+    // the previous design's factor (lagged) is needed now, and its inputs
+    // (the coarsest moduli) are about to be overwritten
+    ICK(cudaStreamWaitEvent(c->stream, C.ev_factor[C.pending], 0));
+    C.cur = C.pending;
+    C.pending = -1;
+  }
+  if(!lag || !C.have || C.n == 0)
+  {
+    const int b = C.cur;
+    if(!C.setup[b])
+      C.setup[b] = capture(c->stream, C.setup_kernels, [&] {
+        enqueue_levels(c, levels, c->stream);
+        enqueue_factor(c, b, c->stream);
+      });
+    ICK(cudaGraphLaunch(C.setup[b], c->stream));
+    note_launch(C.setup_kernels);
+    C.have = true;
+    return;
+  }
+  const int nb = 1 - C.cur;
+  if(!C.A[nb])
+  {
+    const size_t nn = (size_t)C.n * C.n;
+    C.A[nb] = dalloc(nn);
+    C.W[nb] = dalloc(nn);
+    C.work[nb] = dalloc(nn);
+  }
+  if(!C.side)
+  {
+    ICK(cudaStreamCreateWithFlags(&C.side, cudaStreamNonBlocking));
+    ICK(cudaEventCreateWithFlags(&C.ev_levels, cudaEventDisableTiming));
+    for(int b = 0; b < 2; b++)
+      ICK(cudaEventCreateWithFlags(&C.ev_factor[b], cudaEventDisableTiming));
+  }
+  if(!C.levels)
+    C.levels = capture(c->stream, C.levels_kernels, [&] { enqueue_levels(c, levels, c->stream); });
+  if(!C.factor[nb])
+    C.factor[nb] = capture(C.side, C.factor_kernels, [&] { enqueue_factor(c, nb, C.side); });
+  ICK(cudaGraphLaunch(C.levels, c->stream));
+  note_launch(C.levels_kernels);
+  ICK(cudaEventRecord(C.ev_levels, c->stream));
+  ICK(cudaStreamWaitEvent(C.side, C.ev_levels, 0));
+  ICK(cudaGraphLaunch(C.factor[nb], C.side));
+  note_launch(C.factor_kernels);
+  ICK(cudaEventRecord(C.ev_factor[nb], C.side));
+  C.pending = nb;
+}
+
+void mg_join(icarat_ctx *c)
+{
+  if(c->coarse.pending >= 0)
+    ICK(cudaStreamWaitEvent(c->stream, c->coarse.ev_factor[c->coarse.pending], 0));
 }
 
 // the finest level of the FP32 V-cycle may run on the tensor-core operator
@@ -705,8 +803,8 @@ template <typename T> static void vcycle(icarat_ctx *c, int l, const T *b, int d
       note_launch();
       k_coarse_gather<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, c->coarse.map, b,
                                                                  c->coarse.vin);
-      dense_spd_solve(c->stream, c->coarse.W, c->coarse.work, n, c->coarse.vin,
-                      c->coarse.vout, c->coarse.map, L.x);
+      dense_spd_solve(c->stream, c->coarse.W[c->coarse.cur], c->coarse.work[c->coarse.cur],
+                      n, c->coarse.vin, c->coarse.vout, c->coarse.map, L.x);
     }
     if(!std::is_same<T, double>::value)
     {

@@ -346,7 +346,7 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   {
     levels = o->mg_levels > 0 ? o->mg_levels : 4;
     smooth = o->mg_smooth > 0 ? o->mg_smooth : 2;
-    mg_setup(c, levels);
+    mg_setup(c, levels, o->coarse_lag != 0);
   }
   else
     launch_diag(c, g, c->d_E, c->d_fix, c->d_invd);
@@ -368,7 +368,8 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                         cudaMemcpyDeviceToDevice, c->stream));
   }
   const auto key =
-      std::make_tuple(method + 4096 * (c->fp64_tc + 1), levels, smooth, chunk, (const void *)d_x);
+      std::make_tuple(method + 4096 * (c->fp64_tc + 1), levels + 32 * c->coarse.cur, smooth,
+                      chunk, (const void *)d_x);
   auto it = c->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
   if(it == c->graphs.end())
@@ -421,6 +422,8 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
     ICK(cudaGraphLaunch(exec, c->stream));
     note_launch(graph_kernels);
   }
+  if(method == ICARAT_SOLVER_MG_PCG)
+    mg_join(c);
   ICK(cudaMemcpyAsync(c->h_cg, c->d_cg, sizeof(CgScalars),
                       cudaMemcpyDeviceToHost, c->stream));
   ICK(cudaStreamSynchronize(c->stream));

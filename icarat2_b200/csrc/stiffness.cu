@@ -213,10 +213,10 @@ void launch_apply_K_f32(icarat_ctx *c, const GridDev &g, const float *E,
 }
 
 void launch_diag(icarat_ctx *c, const GridDev &g, const double *E,
-                 const uint8_t *fix, double *invd)
+                 const uint8_t *fix, double *invd, cudaStream_t st)
 {
   note_launch();
-  k_inv_diag<<<node_blocks(g, 256), 256, 0, c->stream>>>(g, c->ke0, E, fix, invd);
+  k_inv_diag<<<node_blocks(g, 256), 256, 0, st ? st : c->stream>>>(g, c->ke0, E, fix, invd);
   ICK(cudaGetLastError());
 }
 

@@ -110,6 +110,12 @@ typedef struct
                      1 = tensor cores on every level of 32k nodes and more,
                      -1 = node stencil only.  Also the operator of later
                      icarat_apply_K calls on the context. */
+  int coarse_lag; /* MG_PCG, MIXED_IR: 1 = the V-cycle keeps the coarsest-level
+                     factor of the previous design while this design's factor
+                     is computed on a second stream, overlapped with the solve
+                     (factor reuse across design iterations; every solve still
+                     meets rtol on the current operator).  The first solve on a
+                     new hierarchy factors synchronously. */
 } icarat_solve_opts;
 
 typedef struct
