@@ -12,6 +12,11 @@ set-up.
         `reps` launches of K u with operator 0 FP64, 1 FP32, 2 tensor cores
         BF16x3, 3 tensor cores BF16, 4 FP64 tensor cores (after one warm-up
         launch)
+    python -m icarat2_b200.profile_cases headline 5
+        one design iteration of the bench's headline loop (128x64x64,
+        uniform start density 0.3, filter radius 2.5, MMA move 0.2, 4-level
+        MG-PCG to 1e-8 with the coarse factor reused) after `warm` warm-up
+        iterations
     python -m icarat2_b200.profile_cases loop 256x128x128 mixed 6 1e-6 3
         one design iteration of the MMA loop (densities U[0.1, 0.5], seed 0,
         filter radius 3, move 0.2) after `warm` warm-up iterations; methods
@@ -87,11 +92,29 @@ def loop(grid, method, levels, rtol, warm):
                                                          info.status))
 
 
+def headline(warm):
+    G = gpu.Context(128, 64, 64)
+    o = gpu.solve_opts(gpu.MG_PCG, rtol=1e-8, mg_levels=4, coarse_lag=1)
+    G.loop_init(0.3, method="mma", filter_radius=2.5, move=0.2, solve=o)
+    for _ in range(int(warm)):
+        G.loop_step()
+    G.synchronize()
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    info = G.loop_step()
+    G.synchronize()
+    rt.cudaProfilerStop()
+    print("cg iterations %d compliance %.6g status %d" % (info.cg_iterations, info.compliance,
+                                                         info.status))
+
+
 def main(argv):
     if len(argv) >= 5 and argv[0] == "solve":
         solve(*argv[1:5])
     elif len(argv) >= 6 and argv[0] == "loop":
         loop(*argv[1:6])
+    elif len(argv) >= 2 and argv[0] == "headline":
+        headline(argv[1])
     elif len(argv) >= 4 and argv[0] == "operator":
         operator(*argv[1:4])
     else:
