@@ -345,10 +345,17 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
 // net.cu: z = s net(r / s) on ctx's grid and current design
 template <typename T>
 void net_apply(icarat_net *N, icarat_ctx *c, const T *r, double s, T *z);
+// reports (ICARAT_ERR_CUDA) a tensor-core wait of the net that ran out
+void net_check(icarat_net *N, cudaStream_t st);
 
 // tc_stencil.cu
 void launch_ku_tc(icarat_ctx *c, int op, int terms, TcArgs a, cudaStream_t st);
 int pick_layers(long tiles, int NZ, long slots, long max_ctas);
+// net_tc.cu: tensor-core forward 3x3x3 convolution of the U-net (BF16 bits)
+long conv3_tc_packed_size(int cin, int cout);
+void conv3_tc_pack(const uint16_t *W, int cin, int cout, uint16_t *wpk, cudaStream_t st);
+void conv3_tc_fwd(int X, int Y, int Z, long V, const uint16_t *x, int cin, const uint16_t *wpk,
+                  const float *bias, int cout, uint16_t *y, int *err, cudaStream_t st);
 // dmma_stencil.cu
 bool dmma_fits(const GridDev &g);
 void launch_ku_dmma(icarat_ctx *c, int op, DmArgs a, cudaStream_t st);

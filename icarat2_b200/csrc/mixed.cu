@@ -632,6 +632,7 @@ void mixed_begin(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, d
         }
       }
     }
+    net_check(c->net, c->stream);
   }
   else
     enqueue_precondition(c, smooth, 1);

@@ -18,9 +18,11 @@
 // the node grid zero-padded to multiples of 8 (three 2x poolings).
 // Layout: tensor [channel][z][y][x] over the padded grid.
 //
-// Kernels (CUDA cores, FP32 FMA on BF16 operands):
+// Kernels: the forward 3x3x3 convolutions run on the tensor cores
+// (k_conv3_tc in net_tc.cu: implicit GEMM, tcgen05, FP32 accumulation in
+// TMEM); the backward pass on the CUDA cores (FP32 FMA on BF16 operands):
 //   k_conv3        one voxel x 16 output channels per thread, the weights of
-//                  a 16-input-channel chunk staged in shared memory; also the
+//                  a 16-input-channel chunk staged in shared memory: the
 //                  data gradient (input: ReLU-masked FP32 output gradient,
 //                  weights transposed and flipped)
 //   k_conv3_wgrad  per 256-voxel chunk and 16 output channels, every
@@ -523,6 +525,11 @@ struct icarat_net
   long np = 0;
   float *w = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
   bf16 *wb = nullptr, *wt = nullptr;
+  // conv3 weights packed for the tensor-core forward (net_tc.cu) and its
+  // error flag (an mbarrier wait that ran out)
+  bf16 *wpk = nullptr;
+  long wpk_off[15] = {};
+  int *tc_err = nullptr;
   long step = 0;
   bool wdirty = true;
   // activations of the current padded grid
@@ -636,18 +643,34 @@ void refresh_weights(icarat_net *N, cudaStream_t st)
   note_launch();
   k_net_weights<<<nb(N->np), 256, 0, st>>>(N->np, N->lt, N->w, N->wb, N->wt);
   ICK(cudaGetLastError());
+  for(int l = 0; l < 15; l++)
+    if(N->L[l].k == 3)
+      conv3_tc_pack(reinterpret_cast<const uint16_t *>(N->wb + N->L[l].woff), N->L[l].cin,
+                    N->L[l].cout, reinterpret_cast<uint16_t *>(N->wpk + N->wpk_off[l]), st);
   N->wdirty = false;
 }
 
+// the tensor-core convolution reports a wait that ran out through a flag
+void check_tc_conv(icarat_net *N, cudaStream_t st)
+{
+  int e = 0;
+  ICK(cudaMemcpyAsync(&e, N->tc_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ICK(cudaStreamSynchronize(st));
+  if(e)
+  {
+    ICK(cudaMemsetAsync(N->tc_err, 0, sizeof(int), st));
+    throw Error{ICARAT_ERR_CUDA, "tensor-core convolution: an mbarrier wait ran out"};
+  }
+}
+
+// forward conv3 + bias + ReLU on the tensor cores (net_tc.cu)
 void conv_fwd(icarat_net *N, cudaStream_t st, int li, int lvl, const bf16 *x, bf16 *y)
 {
   const NetLayer &Ly = N->L[li];
   const Dims &d = N->d[lvl];
-  dim3 grid((unsigned)((d.V + 127) / 128), (unsigned)((Ly.cout + 15) / 16));
-  note_launch();
-  k_conv3<bf16, false, true><<<grid, 128, 0, st>>>(d, x, nullptr, Ly.cin, N->wb + Ly.woff,
-                                                   N->w + Ly.boff, Ly.cout, y, nullptr, 1);
-  ICK(cudaGetLastError());
+  conv3_tc_fwd(d.X, d.Y, d.Z, d.V, reinterpret_cast<const uint16_t *>(x), Ly.cin,
+               reinterpret_cast<const uint16_t *>(N->wpk + N->wpk_off[li]), N->w + Ly.boff,
+               Ly.cout, reinterpret_cast<uint16_t *>(y), N->tc_err, st);
 }
 
 void forward(icarat_net *N, cudaStream_t st)
@@ -782,6 +805,8 @@ void net_apply(icarat_net *N, icarat_ctx *c, const T *r, double s, T *z)
   k_net_output<T><<<nb(c->numnp), 256, 0, c->stream>>>(N->d[0], g, N->out, c->d_fix, s, z);
   ICK(cudaGetLastError());
 }
+void net_check(icarat_net *N, cudaStream_t st) { check_tc_conv(N, st); }
+
 template void net_apply<float>(icarat_net *, icarat_ctx *, const float *, double, float *);
 template void net_apply<double>(icarat_net *, icarat_ctx *, const double *, double, double *);
 } // namespace icarat_b200
@@ -834,6 +859,16 @@ int icarat_net_create(int device, unsigned long long seed, icarat_net **out)
     N->g = alloc_n<float>(o);
     N->wb = alloc_n<bf16>(o);
     N->wt = alloc_n<bf16>(o);
+    long po = 0;
+    for(int l = 0; l < 15; l++)
+      if(N->L[l].k == 3)
+      {
+        N->wpk_off[l] = po;
+        po += conv3_tc_packed_size(N->L[l].cin, N->L[l].cout);
+      }
+    N->wpk = alloc_n<bf16>(po);
+    N->tc_err = alloc_n<int>(1);
+    ICK(cudaMemset(N->tc_err, 0, sizeof(int)));
     ICK(cudaMemcpy(N->w, w.data(), sizeof(float) * o, cudaMemcpyHostToDevice));
     ICK(cudaMemset(N->m, 0, sizeof(float) * o));
     ICK(cudaMemset(N->v, 0, sizeof(float) * o));
@@ -858,7 +893,7 @@ int icarat_net_destroy(icarat_net *N)
   cudaDeviceSynchronize();
   free_acts(N);
   for(void *p : {(void *)N->w, (void *)N->m, (void *)N->v, (void *)N->g, (void *)N->wb,
-                 (void *)N->wt})
+                 (void *)N->wt, (void *)N->wpk, (void *)N->tc_err})
     if(p)
       cudaFree(p);
   if(N->h_lpart)
@@ -967,7 +1002,7 @@ int icarat_net_train_step(icarat_net *N, icarat_ctx *c, const double *rho, const
                                       (float)b2, (float)c1, (float)c2, 1e-8f);
     N->wdirty = true;
   }
-  ICK(cudaStreamSynchronize(st));
+  check_tc_conv(N, st);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -981,6 +1016,7 @@ int icarat_net_infer(icarat_net *N, icarat_ctx *c, const double *f, double *u)
   const double s = host_norm_free(c, f);
   to_full(c, f, c->d_Ap, true);
   net_apply<double>(N, c, c->d_Ap, s, c->d_z);
+  check_tc_conv(N, c->stream);
   from_full(c, c->d_z, u, true);
   return ICARAT_OK;
   ICARAT_API_END

@@ -17,6 +17,9 @@ set-up.
         uniform start density 0.3, filter radius 2.5, MMA move 0.2, 4-level
         MG-PCG to 1e-8 with the coarse factor reused) after `warm` warm-up
         iterations
+    python -m icarat2_b200.profile_cases net 256x128x128
+        one inference of the U-net (random weights, seed 1) on the load of
+        the cantilever, after one warm-up inference
     python -m icarat2_b200.profile_cases loop 256x128x128 mixed 6 1e-6 3
         one design iteration of the MMA loop (densities U[0.1, 0.5], seed 0,
         filter radius 3, move 0.2) after `warm` warm-up iterations; methods
@@ -108,6 +111,22 @@ def headline(warm):
                                                          info.status))
 
 
+def net(grid):
+    nx, ny, nz = _grid(grid)
+    G = gpu.Context(nx, ny, nz)
+    G.set_design(np.full(G.nelx, 0.5))
+    N = gpu.Net(seed=1)
+    f = G.fext()
+    N.infer(G, f)
+    G.synchronize()
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    u = N.infer(G, f)
+    G.synchronize()
+    rt.cudaProfilerStop()
+    print("|u| %.6g" % float(np.linalg.norm(u)))
+
+
 def main(argv):
     if len(argv) >= 5 and argv[0] == "solve":
         solve(*argv[1:5])
@@ -115,6 +134,8 @@ def main(argv):
         loop(*argv[1:6])
     elif len(argv) >= 2 and argv[0] == "headline":
         headline(argv[1])
+    elif len(argv) >= 2 and argv[0] == "net":
+        net(argv[1])
     elif len(argv) >= 4 and argv[0] == "operator":
         operator(*argv[1:4])
     else:
