@@ -155,8 +155,18 @@ __global__ void __launch_bounds__(128)
 {
   constexpr int CH = 256;
   __shared__ float dys[16][CH];
+  __shared__ int vxyz[CH][3]; // coordinates of the chunk's voxels (one division each)
   const int chunk = blockIdx.x, co0 = blockIdx.y * 16;
   const long v0 = (long)chunk * CH;
+  for(int i = threadIdx.x; i < CH; i += blockDim.x)
+  {
+    const long v = v0 + i;
+    const int vx = (int)(v % d.X);
+    const long r = v / d.X;
+    vxyz[i][0] = vx;
+    vxyz[i][1] = (int)(r % d.Y);
+    vxyz[i][2] = (int)(r / d.Y);
+  }
   for(int q = threadIdx.x; q < 16 * CH; q += blockDim.x)
   {
     const int co = q / CH, i = q % CH;
@@ -185,8 +195,7 @@ __global__ void __launch_bounds__(128)
       const long v = v0 + i;
       if(v >= d.V)
         break;
-      const int vx = (int)(v % d.X), vy = (int)((v / d.X) % d.Y), vz = (int)(v / ((long)d.X * d.Y));
-      const int xx = vx + ox, yy = vy + oy, zz = vz + oz;
+      const int xx = vxyz[i][0] + ox, yy = vxyz[i][1] + oy, zz = vxyz[i][2] + oz;
       if(xx < 0 || xx >= d.X || yy < 0 || yy >= d.Y || zz < 0 || zz >= d.Z)
         continue;
       const float xv = bfv(xc[v + ox + (long)oy * d.X + (long)oz * d.X * d.Y]);
@@ -234,21 +243,28 @@ __global__ void k_bias_grad(Dims d, const float *__restrict__ dy, const bf16 *__
     db[co] = (float)a[0];
 }
 
+// The grid transfers run one block per x-line (channel, z, y) of the grid
+// they write, threads along x: no 64-bit index division per element.
+// Blocks for the x-lines of ch channels of level d.
+static inline int line_blocks(int ch, int Z, int Y) { return std::min(ch * Z * Y, 148 * 16); }
+
 // coarse[c][V] = mean of the 8 children
 __global__ void k_pool(Dims f, Dims c, int ch, const bf16 *__restrict__ in, bf16 *__restrict__ out)
 {
-  const long n = (long)ch * c.V;
-  for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-      i += (long)gridDim.x * blockDim.x)
+  const int lines = ch * c.Z * c.Y;
+  for(int L = blockIdx.x; L < lines; L += gridDim.x)
   {
-    const int k = (int)(i / c.V);
-    const long v = i % c.V;
-    const int X = (int)(v % c.X), Y = (int)((v / c.X) % c.Y), Z = (int)(v / ((long)c.X * c.Y));
-    float s = 0.0f;
-    for(int q = 0; q < 8; q++)
-      s += bfv(in[(long)k * f.V + (2 * X + (q & 1)) + (long)(2 * Y + ((q >> 1) & 1)) * f.X +
-                  (long)(2 * Z + (q >> 2)) * f.X * f.Y]);
-    out[i] = __float2bfloat16_rn(s * 0.125f);
+    const int Y = L % c.Y, Z = (L / c.Y) % c.Z, k = L / (c.Y * c.Z);
+    const bf16 *src = in + (long)k * f.V + (long)(2 * Z) * f.X * f.Y + (long)(2 * Y) * f.X;
+    bf16 *dst = out + (long)k * c.V + (long)Z * c.X * c.Y + (long)Y * c.X;
+    for(int X = threadIdx.x; X < c.X; X += blockDim.x)
+    {
+      float s = 0.0f;
+      for(int q = 0; q < 8; q++)
+        s += bfv(src[(2 * X + (q & 1)) + (long)((q >> 1) & 1) * f.X +
+                     (long)(q >> 2) * f.X * f.Y]);
+      dst[X] = __float2bfloat16_rn(s * 0.125f);
+    }
   }
 }
 
@@ -256,28 +272,41 @@ __global__ void k_pool(Dims f, Dims c, int ch, const bf16 *__restrict__ in, bf16
 __global__ void k_pool_back_add(Dims f, Dims c, int ch, const float *__restrict__ dc,
                                 float *__restrict__ df)
 {
-  const long n = (long)ch * f.V;
-  for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-      i += (long)gridDim.x * blockDim.x)
+  const int lines = ch * f.Z * f.Y;
+  for(int L = blockIdx.x; L < lines; L += gridDim.x)
   {
-    const int k = (int)(i / f.V);
-    const long v = i % f.V;
-    const int x = (int)(v % f.X), y = (int)((v / f.X) % f.Y), z = (int)(v / ((long)f.X * f.Y));
-    df[i] += 0.125f * dc[(long)k * c.V + x / 2 + (long)(y / 2) * c.X + (long)(z / 2) * c.X * c.Y];
+    const int y = L % f.Y, z = (L / f.Y) % f.Z, k = L / (f.Y * f.Z);
+    const float *src = dc + (long)k * c.V + (long)(z / 2) * c.X * c.Y + (long)(y / 2) * c.X;
+    float *dst = df + (long)k * f.V + (long)z * f.X * f.Y + (long)y * f.X;
+    for(int x = threadIdx.x; x < f.X; x += blockDim.x)
+      dst[x] += 0.125f * src[x / 2];
   }
 }
 
 // fine[c][v] = coarse (nearest)
 __global__ void k_up(Dims f, Dims c, int ch, const bf16 *__restrict__ in, bf16 *__restrict__ out)
 {
-  const long n = (long)ch * f.V;
-  for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-      i += (long)gridDim.x * blockDim.x)
+  const int lines = ch * f.Z * f.Y;
+  for(int L = blockIdx.x; L < lines; L += gridDim.x)
   {
-    const int k = (int)(i / f.V);
-    const long v = i % f.V;
-    const int x = (int)(v % f.X), y = (int)((v / f.X) % f.Y), z = (int)(v / ((long)f.X * f.Y));
-    out[i] = in[(long)k * c.V + x / 2 + (long)(y / 2) * c.X + (long)(z / 2) * c.X * c.Y];
+    const int y = L % f.Y, z = (L / f.Y) % f.Z, k = L / (f.Y * f.Z);
+    const bf16 *src = in + (long)k * c.V + (long)(z / 2) * c.X * c.Y + (long)(y / 2) * c.X;
+    bf16 *dst = out + (long)k * f.V + (long)z * f.X * f.Y + (long)y * f.X;
+    if(f.X % 8 == 0 && c.X % 4 == 0)
+    {
+      // 8 outputs from 4 inputs per thread: 16-byte stores, 8-byte loads
+      // (every line starts on those boundaries when the extents divide)
+      for(int x = 8 * threadIdx.x; x < f.X; x += 8 * blockDim.x)
+      {
+        const uint2 s4 = *reinterpret_cast<const uint2 *>(src + x / 2);
+        const uint32_t a = s4.x & 0xFFFFu, b = s4.x >> 16, cc = s4.y & 0xFFFFu, dd = s4.y >> 16;
+        *reinterpret_cast<uint4 *>(dst + x) =
+            make_uint4(a | (a << 16), b | (b << 16), cc | (cc << 16), dd | (dd << 16));
+      }
+    }
+    else
+      for(int x = threadIdx.x; x < f.X; x += blockDim.x)
+        dst[x] = src[x / 2];
   }
 }
 
@@ -285,18 +314,19 @@ __global__ void k_up(Dims f, Dims c, int ch, const bf16 *__restrict__ in, bf16 *
 __global__ void k_up_back(Dims f, Dims c, int ch, const float *__restrict__ df,
                           float *__restrict__ dc)
 {
-  const long n = (long)ch * c.V;
-  for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-      i += (long)gridDim.x * blockDim.x)
+  const int lines = ch * c.Z * c.Y;
+  for(int L = blockIdx.x; L < lines; L += gridDim.x)
   {
-    const int k = (int)(i / c.V);
-    const long v = i % c.V;
-    const int X = (int)(v % c.X), Y = (int)((v / c.X) % c.Y), Z = (int)(v / ((long)c.X * c.Y));
-    float s = 0.0f;
-    for(int q = 0; q < 8; q++)
-      s += df[(long)k * f.V + (2 * X + (q & 1)) + (long)(2 * Y + ((q >> 1) & 1)) * f.X +
-              (long)(2 * Z + (q >> 2)) * f.X * f.Y];
-    dc[i] = s;
+    const int Y = L % c.Y, Z = (L / c.Y) % c.Z, k = L / (c.Y * c.Z);
+    const float *src = df + (long)k * f.V + (long)(2 * Z) * f.X * f.Y + (long)(2 * Y) * f.X;
+    float *dst = dc + (long)k * c.V + (long)Z * c.X * c.Y + (long)Y * c.X;
+    for(int X = threadIdx.x; X < c.X; X += blockDim.x)
+    {
+      float s = 0.0f;
+      for(int q = 0; q < 8; q++)
+        s += src[(2 * X + (q & 1)) + (long)((q >> 1) & 1) * f.X + (long)(q >> 2) * f.X * f.Y];
+      dst[X] = s;
+    }
   }
 }
 
@@ -680,25 +710,25 @@ void forward(icarat_net *N, cudaStream_t st)
   conv_fwd(N, st, 0, 0, N->in, N->a0);
   conv_fwd(N, st, 1, 0, N->a0, N->c0 + 32 * V0); // S0 into the skip slice
   note_launch(3);
-  k_pool<<<nb(16 * d[1].V), 256, 0, st>>>(d[0], d[1], 16, N->c0 + 32 * V0, N->p1);
+  k_pool<<<line_blocks(16, d[1].Z, d[1].Y), 128, 0, st>>>(d[0], d[1], 16, N->c0 + 32 * V0, N->p1);
   conv_fwd(N, st, 2, 1, N->p1, N->a1);
   conv_fwd(N, st, 3, 1, N->a1, N->c1 + 64 * V1);
-  k_pool<<<nb(32 * d[2].V), 256, 0, st>>>(d[1], d[2], 32, N->c1 + 64 * V1, N->p2);
+  k_pool<<<line_blocks(32, d[2].Z, d[2].Y), 128, 0, st>>>(d[1], d[2], 32, N->c1 + 64 * V1, N->p2);
   conv_fwd(N, st, 4, 2, N->p2, N->a2);
   conv_fwd(N, st, 5, 2, N->a2, N->c2 + 128 * V2);
-  k_pool<<<nb(64 * d[3].V), 256, 0, st>>>(d[2], d[3], 64, N->c2 + 128 * V2, N->p3);
+  k_pool<<<line_blocks(64, d[3].Z, d[3].Y), 128, 0, st>>>(d[2], d[3], 64, N->c2 + 128 * V2, N->p3);
   conv_fwd(N, st, 6, 3, N->p3, N->a3);
   conv_fwd(N, st, 7, 3, N->a3, N->b3);
   note_launch();
-  k_up<<<nb(128 * V2), 256, 0, st>>>(d[2], d[3], 128, N->b3, N->c2);
+  k_up<<<line_blocks(128, d[2].Z, d[2].Y), 128, 0, st>>>(d[2], d[3], 128, N->b3, N->c2);
   conv_fwd(N, st, 8, 2, N->c2, N->e2);
   conv_fwd(N, st, 9, 2, N->e2, N->d2);
   note_launch();
-  k_up<<<nb(64 * V1), 256, 0, st>>>(d[1], d[2], 64, N->d2, N->c1);
+  k_up<<<line_blocks(64, d[1].Z, d[1].Y), 128, 0, st>>>(d[1], d[2], 64, N->d2, N->c1);
   conv_fwd(N, st, 10, 1, N->c1, N->e1);
   conv_fwd(N, st, 11, 1, N->e1, N->d1);
   note_launch();
-  k_up<<<nb(32 * V0), 256, 0, st>>>(d[0], d[1], 32, N->d1, N->c0);
+  k_up<<<line_blocks(32, d[0].Z, d[0].Y), 128, 0, st>>>(d[0], d[1], 32, N->d1, N->c0);
   conv_fwd(N, st, 12, 0, N->c0, N->e0);
   conv_fwd(N, st, 13, 0, N->e0, N->d0);
   note_launch();
@@ -746,32 +776,32 @@ void backward(icarat_net *N, cudaStream_t st)
   conv_back(N, st, 12, 0, N->c0, N->e0, N->gB[0], N->gA[0]);
   // dD1 = up^T(dC0[0:32]) -> gA[1]; dS0 (skip) stays in gA[0] + 32 V0
   note_launch();
-  k_up_back<<<nb(32 * V1), 256, 0, st>>>(d[0], d[1], 32, N->gA[0], N->gA[1]);
+  k_up_back<<<line_blocks(32, d[1].Z, d[1].Y), 128, 0, st>>>(d[0], d[1], 32, N->gA[0], N->gA[1]);
   conv_back(N, st, 11, 1, N->e1, N->d1, N->gA[1], N->gB[1]);
   conv_back(N, st, 10, 1, N->c1, N->e1, N->gB[1], N->gA[1]); // dC1 (96 ch)
   note_launch();
-  k_up_back<<<nb(64 * V2), 256, 0, st>>>(d[1], d[2], 64, N->gA[1], N->gA[2]);
+  k_up_back<<<line_blocks(64, d[2].Z, d[2].Y), 128, 0, st>>>(d[1], d[2], 64, N->gA[1], N->gA[2]);
   conv_back(N, st, 9, 2, N->e2, N->d2, N->gA[2], N->gB[2]);
   conv_back(N, st, 8, 2, N->c2, N->e2, N->gB[2], N->gA[2]); // dC2 (192 ch)
   note_launch();
-  k_up_back<<<nb(128 * d[3].V), 256, 0, st>>>(d[2], d[3], 128, N->gA[2], N->gA[3]);
+  k_up_back<<<line_blocks(128, d[3].Z, d[3].Y), 128, 0, st>>>(d[2], d[3], 128, N->gA[2], N->gA[3]);
   // bottom: dB3 = gA[3] -> dA3 = gB[3] -> dP3 = gA[3]
   conv_back(N, st, 7, 3, N->a3, N->b3, N->gA[3], N->gB[3]);
   conv_back(N, st, 6, 3, N->p3, N->a3, N->gB[3], N->gA[3]);
   // dS2 = dC2[128:192] + pool^T(dP3)
   float *dS2 = N->gA[2] + 128 * V2;
   note_launch();
-  k_pool_back_add<<<nb(64 * V2), 256, 0, st>>>(d[2], d[3], 64, N->gA[3], dS2);
+  k_pool_back_add<<<line_blocks(64, d[2].Z, d[2].Y), 128, 0, st>>>(d[2], d[3], 64, N->gA[3], dS2);
   conv_back(N, st, 5, 2, N->a2, N->c2 + 128 * V2, dS2, N->gB[2]);
   conv_back(N, st, 4, 2, N->p2, N->a2, N->gB[2], N->gA[2]); // dP2 (32 ch) overwrites
   float *dS1 = N->gA[1] + 64 * V1;
   note_launch();
-  k_pool_back_add<<<nb(32 * V1), 256, 0, st>>>(d[1], d[2], 32, N->gA[2], dS1);
+  k_pool_back_add<<<line_blocks(32, d[1].Z, d[1].Y), 128, 0, st>>>(d[1], d[2], 32, N->gA[2], dS1);
   conv_back(N, st, 3, 1, N->a1, N->c1 + 64 * V1, dS1, N->gB[1]);
   conv_back(N, st, 2, 1, N->p1, N->a1, N->gB[1], N->gA[1]);
   float *dS0 = N->gA[0] + 32 * V0;
   note_launch();
-  k_pool_back_add<<<nb(16 * V0), 256, 0, st>>>(d[0], d[1], 16, N->gA[1], dS0);
+  k_pool_back_add<<<line_blocks(16, d[0].Z, d[0].Y), 128, 0, st>>>(d[0], d[1], 16, N->gA[1], dS0);
   conv_back(N, st, 1, 0, N->a0, N->c0 + 32 * V0, dS0, N->gB[0]);
   conv_back(N, st, 0, 0, N->in, N->a0, N->gB[0], nullptr);
 }
