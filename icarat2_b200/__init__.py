@@ -173,6 +173,7 @@ SIGNATURES = {
     "icarat_net_train_step": (_i, [_vp, _vp, _dp, _dp, _dp, _d, _P(_d)]),
     "icarat_net_get_grads": (_i, [_vp, _vp]),
     "icarat_net_infer": (_i, [_vp, _vp, _dp, _dp]),
+    "icarat_net_infer_dev": (_i, [_vp, _vp, _vp, _vp]),
     "icarat_ctx_set_net": (_i, [_vp, _vp]),
     "icarat_batch_create": (_i, [_vp, _vp, _i, _P(Material), _i, _P(_vp)]),
     "icarat_batch_destroy": (_i, [_vp]),
@@ -745,3 +746,9 @@ class Net:
         u = np.zeros(max(ctx.numeq, 1))
         _check(self.lib.icarat_net_infer(self.h, ctx.h, _f64(f), u), "infer")
         return u[:ctx.numeq]
+
+    def infer_dev(self, ctx, f_ptr, u_ptr):
+        """infer() on device pointers (numeq doubles each, e.g. torch
+        tensors' data_ptr()), enqueued on the context's stream."""
+        _check(self.lib.icarat_net_infer_dev(self.h, ctx.h, C.c_void_p(f_ptr), C.c_void_p(u_ptr)),
+               "infer_dev")

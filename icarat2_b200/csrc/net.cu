@@ -1052,6 +1052,21 @@ int icarat_net_infer(icarat_net *N, icarat_ctx *c, const double *f, double *u)
   ICARAT_API_END
 }
 
+int icarat_net_infer_dev(icarat_net *N, icarat_ctx *c, const double *f, double *u)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(N && c && f && u, ICARAT_ERR_ARG, "null argument");
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  ICK(cudaSetDevice(c->device));
+  to_full(c, f, c->d_Ap, false);
+  const double bb = device_dot(c, c->d_Ap, c->d_Ap, c->neq);
+  net_apply<double>(N, c, c->d_Ap, bb > 0.0 ? std::sqrt(bb) : 1.0, c->d_z);
+  check_tc_conv(N, c->stream);
+  from_full(c, c->d_z, u, false);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
 int icarat_ctx_set_net(icarat_ctx *c, icarat_net *N)
 {
   ICARAT_API_BEGIN

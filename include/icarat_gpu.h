@@ -391,6 +391,10 @@ int icarat_net_get_grads(icarat_net *net, float *g);
 /* s net(f / s) on ctx's current design (numeq in and out): a vector along
    the net's estimate of K^-1 f (its scale is not fitted) */
 int icarat_net_infer(icarat_net *net, icarat_ctx *ctx, const double *f, double *u);
+/* icarat_net_infer with device pointers (numeq vectors on the context's
+   device); enqueued on the context's stream, which it synchronizes once to
+   read the norm of f and once at the end to check the net's status */
+int icarat_net_infer_dev(icarat_net *net, icarat_ctx *ctx, const double *f, double *u);
 /* the net used by ICARAT_SOLVER_LEARNED_FPCG on this context (NULL: none) */
 int icarat_ctx_set_net(icarat_ctx *ctx, icarat_net *net);
 

@@ -206,3 +206,20 @@ def test_learned_solver_needs_a_net(gpu):
     with pytest.raises(gpu.IcaratError) as e:
         G.solve(gpu.solve_opts(gpu.LEARNED_FPCG, rtol=1e-8, mg_levels=2))
     assert e.value.status == gpu.ERR_STATE
+
+
+def test_device_inference_matches_host_inference(gpu):
+    torch = pytest.importorskip("torch")
+    G = gpu.Context(24, 12, 12)
+    G.set_design(np.random.default_rng(41).uniform(0.1, 1.0, G.nelx))
+    N = gpu.Net(seed=3)
+    f = G.fext()
+    u_host = N.infer(G, f)
+    fd = torch.tensor(f, dtype=torch.float64, device="cuda")
+    ud = torch.zeros_like(fd)
+    N.infer_dev(G, fd.data_ptr(), ud.data_ptr())
+    torch.cuda.synchronize()
+    u_dev = ud.cpu().numpy()
+    # the two compute the scale |f| in different summation orders; the net's
+    # BF16 input rounding may then differ in the last bit
+    assert np.abs(u_dev - u_host).max() <= 1e-2 * np.abs(u_host).max()
