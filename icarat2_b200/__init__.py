@@ -215,6 +215,14 @@ def _check(status, what):
     return status
 
 
+def _out(a, n):
+    """A caller's output array: contiguous float64 with at least n entries."""
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+            and a.size >= max(n, 1)):
+        raise ValueError("out must be a contiguous float64 array of %d entries" % n)
+    return a
+
+
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
@@ -360,10 +368,13 @@ class Context:
         _check(self.lib.icarat_apply_K_dev(self.h, C.c_void_p(uptr), C.c_void_p(yptr)),
                "apply_K_dev")
 
-    def solve(self, opts=None, want_val=True):
-        """LinearAnalysis::solve: returns (value.val, SolveInfo)."""
+    def solve(self, opts=None, want_val=True, out=None):
+        """LinearAnalysis::solve: returns (value.val, SolveInfo); out: an
+        optional float64 array of numeq entries (e.g. in pinned memory) that
+        receives value.val."""
         info = SolveInfo()
-        val = np.zeros(max(self.numeq, 1)) if want_val else None
+        val = (_out(out, self.numeq) if out is not None else np.zeros(max(self.numeq, 1))) \
+            if want_val else None
         st = self.lib.icarat_solve(self.h, C.byref(opts) if opts is not None else None,
                                    val.ctypes.data if want_val else None, C.byref(info))
         _check(st, "solve")
@@ -397,9 +408,11 @@ class Context:
         _check(self.lib.icarat_compliance(self.h, C.byref(c)), "compliance")
         return c.value
 
-    def sensitivity(self, dgds_scale=1.0):
-        dfds = np.zeros(self.nelx)
-        dgds = np.zeros(self.nelx)
+    def sensitivity(self, dgds_scale=1.0, out=None):
+        """(dfds, dgds); out: an optional pair of float64 arrays of nelx
+        entries that receive them."""
+        dfds = _out(out[0], self.nelx) if out is not None else np.zeros(self.nelx)
+        dgds = _out(out[1], self.nelx) if out is not None else np.zeros(self.nelx)
         _check(self.lib.icarat_sensitivity(self.h, dgds_scale, dfds.ctypes.data,
                                            dgds.ctypes.data), "sensitivity")
         return dfds, dgds
@@ -408,8 +421,8 @@ class Context:
     def filter_setup(self, radius):
         _check(self.lib.icarat_filter_setup(self.h, radius), "filter_setup")
 
-    def density_filter(self, x, is_sens=False):
-        out = np.zeros(self.nelx)
+    def density_filter(self, x, is_sens=False, out=None):
+        out = _out(out, self.nelx) if out is not None else np.zeros(self.nelx)
         _check(self.lib.icarat_density_filter(self.h, _f64(x), out, 1 if is_sens else 0),
                "density_filter")
         return out

@@ -1,6 +1,6 @@
 """Mixed-precision solver (FP32 multigrid-PCG refined by FP64 residuals).
 
-The solver has no reference counterpart; it is judged against the FP64 paths:
+The solver has no reference counterpart; it is checked against the FP64 paths:
   - displacements against the CPU oracle (FP64, rtol 1e-12) at small sizes:
     <= 1e-6 relative (the tolerance stated for the mixed path);
   - at larger sizes against the library's own FP64 multigrid-PCG solve
