@@ -391,7 +391,7 @@ int icarat_ctx_destroy_impl(icarat_ctx *c)
   if(c->loop.mma)
     icarat_mma_destroy(c->loop.mma);
   for(double *p : {c->loop.x, c->loop.xfil, c->loop.xthr, c->loop.thrd,
-                   c->loop.dfds, c->loop.dgds, c->loop.tmp, c->loop.xmin,
+                   c->loop.dfds, c->loop.dgds, c->loop.tmp, c->loop.tmp2, c->loop.xmin,
                    c->loop.xmax})
     dfree(p);
   dfree(c->d_free);

@@ -87,6 +87,34 @@ __global__ void k_filter_trans(ElemGrid g, int nofs, const int *__restrict__ ofs
   }
 }
 
+// the transposed filter of two inputs in one pass (the loop's objective and
+// volume sensitivities): neighbour offsets, weights and a_j read once, each
+// output summed in the order and with the operations of k_filter_trans
+__global__ void k_filter_trans2(ElemGrid g, int nofs, const int *__restrict__ ofs,
+                                const double *__restrict__ w, const double *__restrict__ aa,
+                                const double *__restrict__ in1, const double *__restrict__ in2,
+                                double *__restrict__ out1, double *__restrict__ out2)
+{
+  for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelx;
+      e += gridDim.x * blockDim.x)
+  {
+    const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
+    double s1 = 0.0, s2 = 0.0;
+    for(int q = 0; q < nofs; q++)
+    {
+      const int ii = i + ofs[3 * q], jj = j + ofs[3 * q + 1], kk = k + ofs[3 * q + 2];
+      if(ii < 0 || ii >= g.nx || jj < 0 || jj >= g.ny || kk < 0 || kk >= g.nz)
+        continue;
+      const long f = ii + (long)jj * g.nx + (long)kk * g.nx * g.ny;
+      const double wq = w[q], af = __ldg(aa + f);
+      s1 = __dadd_rn(s1, __ddiv_rn(__dmul_rn(wq, __ldg(in1 + f)), af));
+      s2 = __dadd_rn(s2, __ddiv_rn(__dmul_rn(wq, __ldg(in2 + f)), af));
+    }
+    out1[e] = s1;
+    out2[e] = s2;
+  }
+}
+
 // sensitivityFilter (filter.hpp:77-104)
 __global__ void k_sens_filter(ElemGrid g, int nofs, const int *__restrict__ ofs,
                               const double *__restrict__ w, double vol,
@@ -208,6 +236,20 @@ void filter_apply(icarat_ctx *c, const double *in, double *out, bool is_sens)
     k_filter_trans<<<eblocks(c), 256, 0, c->stream>>>(egrid(c), F.nofs, F.d_ofs,
                                                       F.d_w, F.d_aa, in, out);
   }
+  ICK(cudaGetLastError());
+}
+
+// transposed filter of in1 and in2 (a forward call must have come first)
+void filter_trans2(icarat_ctx *c, const double *in1, const double *in2, double *out1,
+                   double *out2)
+{
+  FilterState &F = c->filt;
+  IREQUIRE(F.d_w != nullptr, ICARAT_ERR_STATE, "filter not set up");
+  IREQUIRE(F.have_forward, ICARAT_ERR_STATE,
+           "transposed filter needs a forward call first (filter.hpp:140-153)");
+  note_launch();
+  k_filter_trans2<<<eblocks(c), 256, 0, c->stream>>>(egrid(c), F.nofs, F.d_ofs, F.d_w, F.d_aa,
+                                                     in1, in2, out1, out2);
   ICK(cudaGetLastError());
 }
 

@@ -223,8 +223,8 @@ struct LoopState
   int optstep = 0;
   double V0 = 0.0;
   double *x = nullptr, *xfil = nullptr, *xthr = nullptr, *thrd = nullptr,
-         *dfds = nullptr, *dgds = nullptr, *tmp = nullptr, *xmin = nullptr,
-         *xmax = nullptr;
+         *dfds = nullptr, *dgds = nullptr, *tmp = nullptr, *tmp2 = nullptr,
+         *xmin = nullptr, *xmax = nullptr;
   icarat_mma *mma = nullptr;
 };
 
@@ -402,6 +402,8 @@ void mg_free(icarat_ctx *c);
 void filter_setup(icarat_ctx *c, double radius);
 void filter_apply(icarat_ctx *c, const double *d_in, double *d_out,
                   bool is_sens);
+void filter_trans2(icarat_ctx *c, const double *in1, const double *in2, double *out1,
+                   double *out2);
 void filter_free(icarat_ctx *c);
 void threshold_dev(icarat_ctx *c, const double *d_in, double beta, double T,
                    double *d_out, bool derivative);

@@ -67,7 +67,7 @@ int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
   const int n = c->nelx;
   if(!L.x)
   {
-    for(double **p : {&L.x, &L.xfil, &L.xthr, &L.thrd, &L.dfds, &L.dgds, &L.tmp,
+    for(double **p : {&L.x, &L.xfil, &L.xthr, &L.thrd, &L.dfds, &L.dgds, &L.tmp, &L.tmp2,
                       &L.xmin, &L.xmax})
       *p = dalloc(n);
   }
@@ -154,12 +154,11 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
   sensitivity_dev(c, o.method == 1 ? 1.0 / L.V0 : 1.0, L.dfds, L.dgds);
   note_launch();
   k_mul2<<<eb(n), 256, 0, c->stream>>>(n, L.thrd, L.dfds, L.dgds);
-  filter_apply(c, L.dfds, L.tmp, true);
-  ICK(cudaMemcpyAsync(L.dfds, L.tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice,
-                      c->stream));
-  filter_apply(c, L.dgds, L.tmp, true);
-  ICK(cudaMemcpyAsync(L.dgds, L.tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice,
-                      c->stream));
+  // both transposed filters in one pass, into the spare buffers, which then
+  // become the sensitivities
+  filter_trans2(c, L.dfds, L.dgds, L.tmp, L.tmp2);
+  std::swap(L.dfds, L.tmp);
+  std::swap(L.dgds, L.tmp2);
   // update
   int ust = ICARAT_OK, usteps = 0;
   if(o.method == 1)
