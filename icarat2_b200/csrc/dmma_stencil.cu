@@ -367,14 +367,16 @@ __global__ void __launch_bounds__(dm::kThreads, 2) k_ku_dmma(DmArgs a)
 // ---------------------------------------------------------------- host side
 template <int OP> static int dm_prepare()
 {
-  static int occ = 0;
+  static int occ_of[kMaxDevices] = {};
+  int &occ = occ_of[device_slot()];
   if(!occ)
   {
     ICK(cudaFuncSetAttribute(k_ku_dmma<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(dm::Smem)));
-    ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ku_dmma<OP>, dm::kThreads,
+    int o = 0;
+    ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_ku_dmma<OP>, dm::kThreads,
                                                       sizeof(dm::Smem)));
-    occ = occ < 1 ? 1 : occ;
+    occ = o < 1 ? 1 : o;
   }
   return occ;
 }

@@ -160,6 +160,17 @@ struct DmArgs
   int tiles_x = 0, tiles = 0, kc = 0; // tiles along x, tiles, node layers per CTA
 };
 
+// Kernel attributes (the dynamic shared-memory limit) and occupancies are per
+// device: launch set-up that is done once keeps one slot per device index.
+constexpr int kMaxDevices = 64;
+inline int device_slot()
+{
+  int d = 0;
+  ICK(cudaGetDevice(&d));
+  IREQUIRE(d >= 0 && d < kMaxDevices, ICARAT_ERR_UNSUPPORTED, "device index above 63");
+  return d;
+}
+
 // Reduction geometry: every grid-stride reduction kernel runs on
 // kRedBlocks blocks of kRedThreads threads so that partial sums are summed
 // in one fixed order (bit-reproducible on a given GPU).

@@ -267,12 +267,13 @@ void conv3_tc_fwd(int X, int Y, int Z, long V, const uint16_t *x, int cin, const
   IREQUIRE(cout % 16 == 0 && cout >= 16 && cout <= 128, ICARAT_ERR_ARG,
            "tensor-core convolution needs 16..128 output channels in steps of 16");
   constexpr size_t kMaxSmem = 2 * ctc::kActHalf + 27 * 2 * 128 * 16;
-  static bool configured = false;
-  if(!configured)
+  static bool configured[kMaxDevices] = {};
+  bool &done = configured[device_slot()];
+  if(!done)
   {
     ICK(cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kMaxSmem));
-    configured = true;
+    done = true;
   }
   const size_t smem = 2 * ctc::kActHalf + 27u * 2u * (size_t)cout * 16u;
   int cols = 32;

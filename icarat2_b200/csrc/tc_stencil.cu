@@ -525,14 +525,16 @@ template <int TERMS> static size_t tc_smem_bytes() { return sizeof(tc::Smem<TERM
 
 template <int OP, int TERMS> static int tc_prepare()
 {
-  static int occ = 0;
+  static int occ_of[kMaxDevices] = {};
+  int &occ = occ_of[device_slot()];
   if(!occ)
   {
     ICK(cudaFuncSetAttribute(k_ku_tc<OP, TERMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)tc_smem_bytes<TERMS>()));
-    ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ku_tc<OP, TERMS>, tc::kThreads,
+    int o = 0;
+    ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_ku_tc<OP, TERMS>, tc::kThreads,
                                                       tc_smem_bytes<TERMS>()));
-    occ = occ < 1 ? 1 : occ;
+    occ = o < 1 ? 1 : o;
   }
   return occ;
 }
