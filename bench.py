@@ -254,6 +254,7 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
     level) at the same residual, compliance and dc error of one solve
     against an FP64 solve at rtol 1e-12, and K u GDOF/s of every operator
     on the same design."""
+    from icarat2_b200.replicas import job_rate
     nx, ny, nz = (int(v) for v in a.mixed_grid.split("x"))
     nelx, nd = nx * ny * nz, 3 * (nx + 1) * (ny + 1) * (nz + 1)
     rho0 = np.random.default_rng(0).uniform(0.1, 0.5, nelx)
@@ -281,12 +282,9 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
             with torch.cuda.stream(s):
                 flush.zero_()
         torch.cuda.synchronize()
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        value, ms = job_rate(ms, a.mixed_steps, world, dist, dev)
         c.close()
-        return {"value": world * a.mixed_steps / (float(t.item()) / 1000.0),
-                "unit": "design-iter/s", "ms_per_step": float(t.item()) / a.mixed_steps,
+        return {"value": value, "unit": "design-iter/s", "ms_per_step": ms / a.mixed_steps,
                 "cg_iterations_per_step": its}
 
     for rtol in (1e-6, 1e-8):
@@ -545,6 +543,7 @@ def gpu_arm(a):
     import torch
     import torch.distributed as dist
     import icarat2_b200 as G
+    from icarat2_b200.replicas import job_rate
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -602,12 +601,7 @@ def gpu_arm(a):
     barrier()
     clk = clocks.stop()
     ms_steps = [e0.elapsed_time(e1) for e0, e1 in evs]
-    total_ms = sum(ms_steps)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * a.steps / (total_ms / 1000.0)
+    value, total_ms = job_rate(sum(ms_steps), a.steps, world, dist, dev)
 
     def alt_loop(levels, lag):
         ca = make_ctx()
@@ -629,13 +623,10 @@ def gpu_arm(a):
             with torch.cuda.stream(sa):
                 flush.zero_()
         torch.cuda.synchronize()
-        ta = torch.tensor([alt_ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(ta, op=dist.ReduceOp.MAX)
+        v, alt_ms = job_rate(alt_ms, a.steps, world, dist, dev)
         ca.close()
-        return {"mg_levels": levels, "coarse_lag": lag,
-                "value": world * a.steps / (float(ta.item()) / 1000.0),
-                "unit": "design-iter/s", "ms_per_step": float(ta.item()) / a.steps,
+        return {"mg_levels": levels, "coarse_lag": lag, "value": v,
+                "unit": "design-iter/s", "ms_per_step": alt_ms / a.steps,
                 "cg_iterations_per_step": its}
 
     # ---------------- the same loop with the coarsest factor of each design
@@ -724,10 +715,7 @@ def gpu_arm(a):
             with torch.cuda.stream(s2):
                 flush.zero_()
             torch.cuda.synchronize()
-        te = torch.tensor([e_ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * a.steps / (float(te.item()) / 1000.0), "unit": "design-iter/s",
+        e2e = {"value": job_rate(e_ms, a.steps, world, dist, dev)[0], "unit": "design-iter/s",
                "h2d_bytes_per_step": state["h2d"], "d2h_bytes_per_step": state["d2h"],
                "host_memory": "pinned"}
         del mma
