@@ -45,7 +45,7 @@ def test_job_rate_single_rank():
 
 def test_job_rate_is_the_slowest_rank_over_two_gloo_ranks():
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank_main, args=(world, free_port(), out), nprocs=world, join=True)
         res = dict(out)
