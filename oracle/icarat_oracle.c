@@ -1767,3 +1767,193 @@ void or_loop_scalars(const or_loop *L, double *d, int *iv)
   iv[2] = L->oc_steps;
   iv[3] = L->mma_outloops;
 }
+
+/* ------------------------------------------------------------------------ */
+/* 9. Helmholtz PDE filter (FilterHelmholtz, src/optimization/filter_helm.hpp)*/
+/*    makeKeFint (:179-223): per element and Gauss point                      */
+/*      Ke += (N N^T + B^T (R / (2 sqrt 3))^2 I B) jac,  fe += s N jac,       */
+/*    fe /= ipmax for the sensitivity call; densityFilter (:76-138):          */
+/*    assemble the nodal scalar system, solve K val = F (Jacobi-PCG here, as  */
+/*    "Eigen_CG"), divideToElement (:225-257): sum_gp N . val_e, divided by    */
+/*    ipmax for the density call.                                             */
+/* ------------------------------------------------------------------------ */
+static void or_helm_element(const double *X, double R, double Ke[64], double Nj[8],
+                            double Ns[8])
+{
+  const double g = 1.0 / sqrt(3.0);
+  const double c = pow(R / (2 * sqrt(3.0)), 2);
+  for(int i = 0; i < 64; i++)
+    Ke[i] = 0.0;
+  for(int n = 0; n < 8; n++)
+    Nj[n] = Ns[n] = 0.0;
+  for(int ip = 0; ip < 8; ip++)
+  {
+    double r[3] = {or_gauss_sign[ip][0] * g, or_gauss_sign[ip][1] * g,
+                   or_gauss_sign[ip][2] * g};
+    double N[8];
+    for(int n = 0; n < 8; n++)
+      N[n] = 0.125 * (1.0 + or_gauss_sign[n][0] * r[0]) * (1.0 + or_gauss_sign[n][1] * r[1]) *
+             (1.0 + or_gauss_sign[n][2] * r[2]);
+    double dN[3][8];
+    or_dNdr(r, dN);
+    double J[3][3];
+    for(int a = 0; a < 3; a++)
+      for(int b = 0; b < 3; b++)
+      {
+        double s = 0.0;
+        for(int n = 0; n < 8; n++)
+          s += dN[a][n] * X[3 * n + b];
+        J[a][b] = s;
+      }
+    double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                 J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                 J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+    double inv[3][3];
+    inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+    inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+    inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+    inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+    inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+    inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+    inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+    inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+    inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+    double B[3][8];
+    for(int a = 0; a < 3; a++)
+      for(int n = 0; n < 8; n++)
+      {
+        double s = 0.0;
+        for(int b = 0; b < 3; b++)
+          s += inv[a][b] * dN[b][n];
+        B[a][n] = s;
+      }
+    const double jac = det * 1.0;
+    for(int a = 0; a < 8; a++)
+      for(int b = 0; b < 8; b++)
+      {
+        double s = 0.0;
+        for(int d = 0; d < 3; d++)
+          s += B[d][a] * c * B[d][b];
+        Ke[8 * a + b] += (N[a] * N[b] + s) * jac;
+      }
+    for(int n = 0; n < 8; n++)
+    {
+      Nj[n] += N[n] * jac;
+      Ns[n] += N[n];
+    }
+  }
+}
+
+/* out[nelx] = Helmholtz filter of in[nelx] on the nx x ny x nz box of size
+   lx x ly x lz, radius R; sens != 0: the sensitivity call.  Jacobi-PCG from
+   zero to ||r|| < tol ||F||. */
+int or_helmholtz_filter(int nx, int ny, int nz, double lx, double ly, double lz, double R,
+                        const double *in, double *out, int sens, double tol, int maxit,
+                        int *iters_out)
+{
+  if(nx < 1 || ny < 1 || nz < 1 || R <= 0.0)
+    return OR_ERR_ARG;
+  const long NX = nx + 1, NY = ny + 1, NZ = nz + 1, numnp = NX * NY * NZ;
+  const long nelx = (long)nx * ny * nz;
+  double *xyz = (double *)malloc(sizeof(double) * 3 * numnp);
+  int *conn = (int *)malloc(sizeof(int) * 8 * nelx);
+  or_mesh_box(nx, ny, nz, lx, ly, lz, xyz, conn);
+  double *K = (double *)calloc(27 * numnp, sizeof(double)); /* [node][neighbour slot] */
+  double *F = (double *)calloc(numnp, sizeof(double));
+  double Ke[64], Nj[8], Ns[8];
+  for(long e = 0; e < nelx; e++)
+  {
+    double X[24];
+    for(int a = 0; a < 8; a++)
+      for(int d = 0; d < 3; d++)
+        X[3 * a + d] = xyz[3 * (long)conn[8 * e + a] + d];
+    or_helm_element(X, R, Ke, Nj, Ns);
+    for(int a = 0; a < 8; a++)
+    {
+      const long na = conn[8 * e + a];
+      const long ia = na % NX, ja = (na / NX) % NY, ka = na / (NX * NY);
+      for(int b = 0; b < 8; b++)
+      {
+        const long nb = conn[8 * e + b];
+        const long ib = nb % NX, jb = (nb / NX) % NY, kb = nb / (NX * NY);
+        const int slot = (int)((kb - ka + 1) * 9 + (jb - ja + 1) * 3 + (ib - ia + 1));
+        K[27 * na + slot] += Ke[8 * a + b];
+      }
+      double fe = in[e] * Nj[a];
+      if(sens)
+        fe = fe / 8.0;
+      F[na] += fe;
+    }
+  }
+  /* Jacobi-PCG */
+  double *val = (double *)calloc(numnp, sizeof(double));
+  double *r = (double *)malloc(sizeof(double) * numnp);
+  double *z = (double *)malloc(sizeof(double) * numnp);
+  double *p = (double *)malloc(sizeof(double) * numnp);
+  double *Ap = (double *)malloc(sizeof(double) * numnp);
+  for(long n = 0; n < numnp; n++)
+  {
+    r[n] = F[n];
+    z[n] = r[n] / K[27 * n + 13];
+    p[n] = z[n];
+  }
+  double bnorm = sqrt(or_dot(F, F, numnp)), zr = or_dot(z, r, numnp);
+  int iter = 0;
+  while(bnorm > 0.0)
+  {
+    iter++;
+    for(long n = 0; n < numnp; n++)
+    {
+      const long i = n % NX, j = (n / NX) % NY, k = n / (NX * NY);
+      double s = 0.0;
+      for(int slot = 0; slot < 27; slot++)
+      {
+        const double kv = K[27 * n + slot];
+        if(kv == 0.0)
+          continue;
+        const long m = (i + slot % 3 - 1) + (j + (slot / 3) % 3 - 1) * NX +
+                       (k + slot / 9 - 1) * NX * NY;
+        s += kv * p[m];
+      }
+      Ap[n] = s;
+    }
+    const double alpha = zr / or_dot(p, Ap, numnp);
+    for(long n = 0; n < numnp; n++)
+    {
+      val[n] += alpha * p[n];
+      r[n] -= alpha * Ap[n];
+      z[n] = r[n] / K[27 * n + 13];
+    }
+    const double zr1 = or_dot(z, r, numnp);
+    const double beta = zr1 / zr;
+    for(long n = 0; n < numnp; n++)
+      p[n] = beta * p[n] + z[n];
+    zr = zr1;
+    if(sqrt(or_dot(r, r, numnp)) < tol * bnorm || iter > maxit)
+      break;
+  }
+  for(long e = 0; e < nelx; e++)
+  {
+    double X[24];
+    for(int a = 0; a < 8; a++)
+      for(int d = 0; d < 3; d++)
+        X[3 * a + d] = xyz[3 * (long)conn[8 * e + a] + d];
+    or_helm_element(X, R, Ke, Nj, Ns);
+    double s = 0.0;
+    for(int a = 0; a < 8; a++)
+      s += Ns[a] * val[conn[8 * e + a]];
+    out[e] = sens ? s : s / 8.0;
+  }
+  if(iters_out)
+    *iters_out = iter;
+  free(xyz);
+  free(conn);
+  free(K);
+  free(F);
+  free(val);
+  free(r);
+  free(z);
+  free(p);
+  free(Ap);
+  return OR_OK;
+}

@@ -76,6 +76,9 @@ def _load():
         "or_filter_density": (C.c_int, [_vp, _dp, _dp, C.c_int]),
         "or_filter_sensitivity": (None, [_vp, _dp, _dp, _dp, _dp]),
         "or_threshold": (None, [C.c_int, _dp, C.c_double, C.c_double, _dp]),
+        "or_helmholtz_filter": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, _dp, _dp, C.c_int,
+                                          C.c_double, C.c_int, C.POINTER(C.c_int)]),
         "or_threshold_deriv": (None, [C.c_int, _dp, C.c_double, C.c_double, _dp]),
         "or_oc_update": (C.c_int, [C.c_int, _dp, _dp, C.c_double, _dp, _dp, _dp,
                                    C.POINTER(_OCParams), VOLUME_FN, C.c_void_p,
@@ -288,6 +291,22 @@ class Filter:
         out = np.zeros(self.n)
         lib.or_filter_sensitivity(self.h, _f64(design_s), _f64(dfds), _f64(volume), out)
         return out
+
+
+def helmholtz_filter(nx, ny, nz, R, x, is_sens=False, tol=1e-14, lx=None, ly=None, lz=None,
+                     maxit=100000):
+    """FilterHelmholtz::densityFilter (filter_helm.hpp:76-138) on the box;
+    returns (filtered, PCG iterations)."""
+    x = _f64(x)
+    out = np.zeros(nx * ny * nz)
+    it = C.c_int()
+    st = lib.or_helmholtz_filter(nx, ny, nz, float(nx if lx is None else lx),
+                                 float(ny if ly is None else ly),
+                                 float(nz if lz is None else lz), R, x, out,
+                                 1 if is_sens else 0, tol, maxit, C.byref(it))
+    if st != 0:
+        raise RuntimeError("or_helmholtz_filter: status %d" % st)
+    return out, it.value
 
 
 def threshold(x, beta, T):

@@ -3,6 +3,7 @@
 reference_tests.json holds the known answers of the reference's own unit tests
 for this path, read as text from the reference tree (sample/test/...):
   - FilterTest          test-optimization/test_filter.cpp:63-124
+  - FilterHelmholtzTest test-optimization/test_filter.cpp:126-175
   - MMASolverTest.toy   test-optimization/test_opt_solver.cpp:17-73
   - BmatrixTest.cubic8  test-basis/test_bmatrix.cpp:123-146
 oracle_trajectory.json is a short OC and MMA design trajectory of the CPU
@@ -55,6 +56,15 @@ def reference_known_answers(ref):
     g_lt = float(re.search(r"EXPECT_LT\(abs\(constraints\[0\]\), ([0-9.e-]+)\);", mblock).group(1))
     smax = float(re.search(r"smax = vector<double>\(n, ([0-9.]+)\)", mblock).group(1))
 
+    hblock = filt[filt.index("TEST(FilterHelmholtzTest"):]
+    hblock = hblock[:hblock.index("\n}\n") + 3]
+    h_radius = float(re.search(r"double radius = ([0-9.]+);", hblock).group(1))
+    h_answer = [float(v) for _, v in sorted(
+        (int(i), v) for i, v in re.findall(r"answer\[(\d)\] = ([0-9.]+);", hblock))]
+    h_s = [float(v) for _, v in sorted(
+        (int(i), v) for i, v in re.findall(r"\bs\[(\d)\] = ([0-9.e-]+);", hblock))]
+    h_tol = float(re.search(r"EXPECT_LT\(norm, ([0-9.e-]+)\);", hblock).group(1))
+
     bm = _read(ref, "sample/test/test-basis/test_bmatrix.cpp")
     bblock = bm[bm.index("TEST(BmatrixTest, cubic8)"):bm.index("TEST(BmatrixTest, cubic20)")]
     vol_tol = float(re.search(r"EXPECT_LT\(abs\(volume - 1.0\), ([0-9.e-]+)\);", bblock).group(1))
@@ -75,6 +85,13 @@ def reference_known_answers(ref):
             "n": int(nm.group(1)), "m": int(nm.group(2)), "x0": x0, "xmin": 0.0,
             "xmax": smax, "move": move, "albefa": osc, "asymptotes": asym,
             "iterations": iters, "objective_lt": obj_lt, "constraint_abs_lt": g_lt,
+        },
+        "helmholtz_2x2": {
+            "source": "sample/test/test-optimization/test_filter.cpp:126-175",
+            "mesh": "2 x 2 unit quad4 (as a 2 x 2 x 1 hexa8 slab: z-independent data give "
+                    "the same nodal system scaled by the layer)",
+            "radius": h_radius, "design_s": h_s, "answer": h_answer,
+            "answer_sens": h_answer, "norm2_tol": h_tol,
         },
         "hexa8_volume": {
             "source": "sample/test/test-basis/test_bmatrix.cpp:123-146",
