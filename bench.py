@@ -75,6 +75,14 @@ def parse():
     p.add_argument("--learned-train", type=int, default=64,
                    help="training samples generated by the plain solver")
     p.add_argument("--learned-epochs", type=int, default=3)
+    p.add_argument("--helm-grid", default="256x128x128",
+                   help="Helmholtz PDE filter measurement grid ('' skips it)")
+    p.add_argument("--helm-radius", type=float, default=2.0,
+                   help="Helmholtz filter radius (element lengths)")
+    p.add_argument("--helm-sample", default="128x64x64",
+                   help="grid of the oracle's timed Helmholtz call")
+    p.add_argument("--cpu-helm", action="store_true",
+                   help="(internal) time the oracle's Helmholtz filter and exit")
     return p.parse_args()
 
 
@@ -150,6 +158,20 @@ def reference_arm(a):
             "e2e": {"value": value, "unit": "design-iter/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_helm(a):
+    """The oracle's Helmholtz filter (assembly, Jacobi-PCG to 1e-10, readout)
+    on the sample grid, one call, one thread."""
+    from oracle import oracle as O
+
+    nx, ny, nz = (int(v) for v in a.helm_sample.split("x"))
+    x = np.random.default_rng(0).uniform(0.0, 1.0, nx * ny * nz)
+    t0 = time.perf_counter()
+    _, its = O.helmholtz_filter(nx, ny, nz, a.helm_radius, x, tol=1e-10, maxit=10000)
+    t = time.perf_counter() - t0
+    print(json.dumps({"t": t, "iters": its, "threads": 1, "grid": a.helm_sample}), flush=True)
     return 0
 
 
@@ -329,6 +351,127 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
                                flops / (ku["tc_fp64"]["ms"] * 1e-3) / 1e12, "unit": "TFLOP/s",
                                "flops_per_launch": flops}
     c.close()
+    return out
+
+
+def helmholtz_section(a, G, torch, dev, flush, world, dist):
+    """Helmholtz PDE filter (densityFilter of FilterHelmholtz) of a U[0, 1]
+    design (seed 0) on the helm grid, CG to the reference's 1e-10: device
+    call, host-pointer call, the CG iteration's bytes against HBM and the
+    oracle's call on a smaller grid."""
+    from icarat2_b200.replicas import job_rate
+
+    nx, ny, nz = (int(v) for v in a.helm_grid.split("x"))
+    c = G.Context(nx, ny, nz, dirichlet=[], loads=[], device=dev.index)
+    c.helmholtz_setup(a.helm_radius)
+    nelx, numnp = c.nelx, c.numnp
+    x = np.random.default_rng(0).uniform(0.0, 1.0, nelx)
+    xd = torch.tensor(x, dtype=torch.float64, device=dev)
+    od = torch.empty_like(xd)
+    st = torch.cuda.ExternalStream(c.stream_ptr(), device=dev)
+    for _ in range(a.warmup):
+        c.helmholtz_filter_dev(xd.data_ptr(), od.data_ptr())
+    torch.cuda.synchronize()
+    l0 = G.kernel_launches()
+    ms, its = 0.0, []
+    for _ in range(a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        its.append(c.helmholtz_filter_dev(xd.data_ptr(), od.data_ptr()).iterations)
+        e1.record(st)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        with torch.cuda.stream(st):
+            flush.zero_()
+        torch.cuda.synchronize()
+    launches = G.kernel_launches() - l0
+    value, total = job_rate(ms, a.steps, world, dist, dev)
+    ms_call = total / a.steps
+    it = sum(its) / len(its)
+    # per node and CG iteration: K p (read p, write Ap: 16 B), the Jacobi
+    # update (read x p r Ap invd, write x r z: 64 B), p = z + beta p (24 B);
+    # per call: right-hand side, CG start and readout
+    bytes_call = numnp * (104.0 * it + 8 + 48 + 8) + 16.0 * nelx
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    gbs = bytes_call / (ms_call * 1e-3) / 1e9
+    # host-pointer call: pinned input and output, copies inside the events
+    xh = torch.empty(nelx, dtype=torch.float64, pin_memory=True).numpy()
+    oh = torch.empty(nelx, dtype=torch.float64, pin_memory=True).numpy()
+    xh[:] = x
+    e_ms = 0.0
+    for k in range(a.warmup + a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        c.helmholtz_filter(xh, out=oh)
+        e1.record(st)
+        e1.synchronize()
+        if k >= a.warmup:
+            e_ms += e0.elapsed_time(e1)
+        with torch.cuda.stream(st):
+            flush.zero_()
+        torch.cuda.synchronize()
+    e2e_v = job_rate(e_ms, a.steps, world, dist, dev)[0]
+    ok = bool(np.allclose(oh, od.cpu().numpy(), rtol=0, atol=1e-12))
+    c.close()
+    # the MMA loop of opt_mma_Helmholtz.cpp (Helmholtz filter R = 2 elements,
+    # threshold, move 0.2) on the headline grid and solver
+    gx, gy, gz = grid_of(a)
+    cl = G.Context(gx, gy, gz, device=dev.index)
+    cl.loop_init(0.3, method="mma", filter_radius=2.0, move=0.2, use_threshold=True,
+                 solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth,
+                                    coarse_lag=a.coarse_lag), filter="helmholtz")
+    sl = torch.cuda.ExternalStream(cl.stream_ptr(), device=dev)
+    for _ in range(a.warmup):
+        cl.loop_step()
+    torch.cuda.synchronize()
+    l_ms = 0.0
+    for _ in range(a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(sl)
+        cl.loop_step()
+        e1.record(sl)
+        e1.synchronize()
+        l_ms += e0.elapsed_time(e1)
+        with torch.cuda.stream(sl):
+            flush.zero_()
+        torch.cuda.synchronize()
+    loop_v, loop_total = job_rate(l_ms, a.steps, world, dist, dev)
+    cl.close()
+    out = {"grid": a.helm_grid, "radius": a.helm_radius, "rtol": 1e-10,
+           "value": value, "unit": "filter-calls/s", "ms_per_call": ms_call,
+           "cg_iterations": its, "gpu_launches_per_call": launches / a.steps,
+           "e2e": {"value": e2e_v, "unit": "filter-calls/s", "h2d_bytes_per_step": 8 * nelx,
+                   "d2h_bytes_per_step": 8 * nelx, "host_memory": "pinned",
+                   "matches_device_call": ok},
+           "roofline": {"bound": "hbm", "kernel": "Jacobi-PCG iteration (k_helm_spmv, "
+                        "k_cg_update_jacobi, k_cg_pupdate) + rhs/readout",
+                        "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                        "bytes_per_call": bytes_call},
+           "mma_loop": {"grid": a.grid, "value": loop_v, "unit": "design-iter/s",
+                        "ms_per_step": loop_total / a.steps,
+                        "workload": "opt_mma_Helmholtz loop: Helmholtz filter R = 2, "
+                                    "threshold, MMA move 0.2, MG-PCG %g" % a.rtol}}
+    if not a.no_cpu_baseline and world == 1:
+        r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--cpu-helm",
+                            "--helm-sample", a.helm_sample, "--helm-radius",
+                            str(a.helm_radius)], capture_output=True, text=True)
+        if r.returncode == 0:
+            cl = json.loads(r.stdout.strip().splitlines()[-1])
+            sx, sy, sz = (int(v) for v in a.helm_sample.split("x"))
+            s_np = (sx + 1) * (sy + 1) * (sz + 1)
+            rate = s_np * cl["iters"] / cl["t"]  # node-iterations/s
+            out["cpu_baseline"] = {
+                "value": rate / (numnp * it), "unit": "filter-calls/s", "cores": 1,
+                "kind": "port",
+                "sample": "oracle Helmholtz filter (assembly, Jacobi-PCG to 1e-10, readout) "
+                          "on %s: %.3f s, %d iterations; scaled to the measured grid by "
+                          "node-iterations" % (a.helm_sample, cl["t"], cl["iters"])}
     return out
 
 
@@ -730,6 +873,9 @@ def gpu_arm(a):
     learned = None
     if a.learned_grid:
         learned = learned_section(a, G, torch)
+    helm = None
+    if a.helm_grid:
+        helm = helmholtz_section(a, G, torch, dev, flush, world, dist)
 
     if rank == 0:
         cg = [i.cg_iterations for i in infos]
@@ -759,6 +905,7 @@ def gpu_arm(a):
             "mixed_256x128x128": mixed,
             "batched_80_designs": batched,
             "learned": learned,
+            "helmholtz_filter": helm,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }
@@ -781,6 +928,8 @@ def main():
     a = parse()
     if a.cpu_sample:
         return cpu_sample(a)
+    if a.cpu_helm:
+        return cpu_helm(a)
     if a.impl == "reference":
         return reference_arm(a)
     return gpu_arm(a)

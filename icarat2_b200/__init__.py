@@ -98,7 +98,8 @@ class OcOpts(C.Structure):
 class LoopOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("use_threshold", C.c_int), ("T", C.c_double),
                 ("move", C.c_double), ("xmin", C.c_double), ("xmax", C.c_double),
-                ("filter_radius", C.c_double), ("solve", SolveOpts)]
+                ("filter_radius", C.c_double), ("solve", SolveOpts),
+                ("filter_kind", C.c_int)]
 
 
 class BatchOpts(C.Structure):
@@ -148,6 +149,9 @@ SIGNATURES = {
     "icarat_density_filter": (_i, [_vp, _dp, _dp, _i]),
     "icarat_density_filter_dev": (_i, [_vp, _vp, _vp, _i]),
     "icarat_sensitivity_filter": (_i, [_vp, _dp, _dp, _dp]),
+    "icarat_helmholtz_setup": (_i, [_vp, _d]),
+    "icarat_helmholtz_filter": (_i, [_vp, _dp, _dp, _i, _d, _i, _P(SolveInfo)]),
+    "icarat_helmholtz_filter_dev": (_i, [_vp, _vp, _vp, _i, _d, _i, _P(SolveInfo)]),
     "icarat_threshold": (_i, [_vp, _dp, _d, _d, _dp]),
     "icarat_threshold_derivative": (_i, [_vp, _dp, _d, _d, _dp]),
     "icarat_oc_update": (_i, [_vp, _dp, _dp, _d, _dp, _dp, _dp, _P(OcOpts), _P(_i)]),
@@ -427,6 +431,27 @@ class Context:
                "density_filter")
         return out
 
+    def helmholtz_setup(self, radius):
+        _check(self.lib.icarat_helmholtz_setup(self.h, radius), "helmholtz_setup")
+
+    def helmholtz_filter(self, x, is_sens=False, rtol=0.0, maxit=0, out=None):
+        """FilterHelmholtz::densityFilter: returns (filtered, SolveInfo of the
+        nodal CG); rtol <= 0 / maxit <= 0 take 1e-10 / 10000."""
+        out = _out(out, self.nelx) if out is not None else np.zeros(self.nelx)
+        info = SolveInfo()
+        _check(self.lib.icarat_helmholtz_filter(self.h, _f64(x), out, 1 if is_sens else 0,
+                                                rtol, maxit, C.byref(info)),
+               "helmholtz_filter")
+        return out, info
+
+    def helmholtz_filter_dev(self, in_ptr, out_ptr, is_sens=False, rtol=0.0, maxit=0):
+        info = SolveInfo()
+        _check(self.lib.icarat_helmholtz_filter_dev(self.h, C.c_void_p(in_ptr),
+                                                    C.c_void_p(out_ptr), 1 if is_sens else 0,
+                                                    rtol, maxit, C.byref(info)),
+               "helmholtz_filter_dev")
+        return info
+
     def sensitivity_filter(self, design_s, dfds):
         out = np.zeros(self.nelx)
         _check(self.lib.icarat_sensitivity_filter(self.h, _f64(design_s), _f64(dfds), out),
@@ -458,13 +483,18 @@ class Context:
 
     # --- design loop -------------------------------------------------------------
     def loop_init(self, x0, method="mma", filter_radius=1.5, move=None, xmin=1e-4,
-                  xmax=1.0, use_threshold=False, T=0.5, solve=None):
+                  xmax=1.0, use_threshold=False, T=0.5, solve=None, filter="radius"):
+        """filter: "radius" (Filter, filter.hpp) or "helmholtz" (FilterHelmholtz,
+        filter_helm.hpp, as opt_macro_oc.cpp / opt_mma_Helmholtz.cpp use)."""
+        if filter not in ("radius", "helmholtz"):
+            raise ValueError("filter must be 'radius' or 'helmholtz'")
         if move is None:
             move = 0.2 if method == "mma" else 0.15
         if np.isscalar(x0):
             x0 = np.full(self.nelx, float(x0))
         o = LoopOpts(1 if method == "mma" else 0, 1 if use_threshold else 0, T, move, xmin,
-                     xmax, filter_radius, solve if solve is not None else solve_opts())
+                     xmax, filter_radius, solve if solve is not None else solve_opts(),
+                     1 if filter == "helmholtz" else 0)
         _check(self.lib.icarat_loop_init(self.h, C.byref(o), _f64(x0)), "loop_init")
 
     def coarse_check(self, mg_levels=4):
@@ -552,6 +582,37 @@ class Filter:
 
     def thresholdDerivative(self, d, beta, T):
         return self.ctx.threshold_derivative(d, beta, T)
+
+
+class FilterHelmholtz:
+    """FilterHelmholtz<E,N> (src/optimization/filter_helm.hpp:16-65) on the
+    voxel grid: densityFilter (:75-138) solves the nodal Helmholtz system on
+    the GPU; "Eigen_CG" is the solver the samples name."""
+
+    def __init__(self, ctx, radious):
+        self.ctx = ctx
+        ctx.helmholtz_setup(radious)
+        self.info = None
+
+    def densityFilter(self, design_s, solvName="Eigen_CG", log=0, sensFlag=False):
+        if solvName not in _SOLVER_NAMES:
+            # Solvers::solve exits on an unknown name (solvers.cpp:56-60)
+            raise IcaratError(ERR_UNSUPPORTED, "Solver type name is wrong: %s" % solvName)
+        if _SOLVER_NAMES[solvName] != JACOBI_PCG:
+            raise IcaratError(ERR_UNSUPPORTED, "the Helmholtz system is solved by Jacobi-PCG "
+                              "(Eigen_CG / Scaling_CG), not %s" % solvName)
+        out, self.info = self.ctx.helmholtz_filter(design_s, is_sens=sensFlag)
+        if log == 1:
+            print("Helmholtz filtering...")
+            print("#iterations:     %d" % self.info.iterations)
+            print("estimated error: %g" % self.info.rel_residual)
+        return out
+
+    def threshold(self, design_filtered, beta, T):
+        return self.ctx.threshold(design_filtered, beta, T)
+
+    def thresholdDerivative(self, design_filtered, beta, T):
+        return self.ctx.threshold_derivative(design_filtered, beta, T)
 
 
 class OC:

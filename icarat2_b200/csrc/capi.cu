@@ -481,6 +481,39 @@ int icarat_density_filter_dev(icarat_ctx *c, const double *in, double *out,
   ICARAT_API_END
 }
 
+int icarat_helmholtz_setup(icarat_ctx *c, double radius)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  helm_setup(c, radius);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_helmholtz_filter(icarat_ctx *c, const double *in, double *out, int is_sens,
+                            double rtol, int maxit, icarat_solve_info *info)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(in && out, ICARAT_ERR_ARG, "null argument");
+  double *a = stage(c, 0), *b = stage(c, 1);
+  h2d(c, a, in, c->nelx);
+  const int st = helm_filter(c, a, b, is_sens != 0, rtol, maxit, info);
+  d2h(c, out, b, c->nelx);
+  return st;
+  ICARAT_API_END
+}
+
+int icarat_helmholtz_filter_dev(icarat_ctx *c, const double *in, double *out, int is_sens,
+                                double rtol, int maxit, icarat_solve_info *info)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(in && out && in != out, ICARAT_ERR_ARG, "need distinct in/out");
+  return helm_filter(c, in, out, is_sens != 0, rtol, maxit, info);
+  ICARAT_API_END
+}
+
 int icarat_sensitivity_filter(icarat_ctx *c, const double *design_s,
                               const double *dfds, double *out)
 {

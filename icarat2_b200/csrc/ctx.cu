@@ -388,6 +388,7 @@ int icarat_ctx_destroy_impl(icarat_ctx *c)
   mg_free(c);
   mixed_free(c);
   filter_free(c);
+  helm_free(c);
   if(c->loop.mma)
     icarat_mma_destroy(c->loop.mma);
   for(double *p : {c->loop.x, c->loop.xfil, c->loop.xthr, c->loop.thrd,

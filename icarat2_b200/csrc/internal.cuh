@@ -225,6 +225,19 @@ struct FilterState
   bool have_forward = false;
 };
 
+// Helmholtz PDE filter: element matrix, the 27 x 27 node-class stencil
+// table and the CG work vectors (numnp each), allocated by helm_setup
+struct HelmState
+{
+  double radius = 0.0;
+  double ke[64] = {}, nj[8] = {}, ns[8] = {};
+  double *d_coef = nullptr;
+  double *d_invd = nullptr, *d_F = nullptr, *d_val = nullptr, *d_r = nullptr,
+         *d_z = nullptr, *d_p = nullptr, *d_Ap = nullptr, *d_partials = nullptr;
+  CgScalars *d_cg = nullptr;
+  cudaGraphExec_t exec = nullptr; // kHelmChunk iterations
+};
+
 struct MmaDev;
 
 struct LoopState
@@ -305,6 +318,7 @@ struct icarat_ctx
   icarat_b200::CoarseSolver coarse;
   // filter
   icarat_b200::FilterState filt;
+  icarat_b200::HelmState helm;
   // loop
   icarat_b200::LoopState loop;
   // instantiated solver graphs: (method, levels, smooth, chunk, x) -> exec
@@ -419,6 +433,14 @@ void filter_free(icarat_ctx *c);
 void threshold_dev(icarat_ctx *c, const double *d_in, double beta, double T,
                    double *d_out, bool derivative);
 
+// helmholtz.cu
+void helm_element(double hx, double hy, double hz, double R, double *ke, double *nj,
+                  double *ns);
+void helm_setup(icarat_ctx *c, double radius);
+int helm_filter(icarat_ctx *c, const double *d_in, double *d_out, bool is_sens,
+                double rtol, int maxit, icarat_solve_info *info);
+void helm_free(icarat_ctx *c);
+
 // sens.cu
 void node_values_dev(icarat_ctx *c, double *d_node_val);
 double compliance_dev(icarat_ctx *c);
@@ -429,6 +451,10 @@ void sensitivity_dev(icarat_ctx *c, double dgds_scale, double *d_dfds,
 int oc_update_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
                   const double *dgdx, const double *xmin, const double *xmax,
                   const icarat_oc_opts *o, int *steps);
+int oc_update_helm_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
+                       const double *dgdx, const double *xmin, const double *xmax,
+                       const icarat_oc_opts *o, int *steps, double *fil, double *thr,
+                       const double *vol);
 
 // device reductions shared by several kernels
 template <int NV>

@@ -1,7 +1,9 @@
 // One design iteration with every array resident on the device: the loop body
 // of sample/algorithm/opt-macro-oc/opt_macro_oc.cpp:83-172 (OC) and
 // sample/algorithm/opt-macro-mma-nondesign/opt_macro_mma_nondesign.cpp:90-178
-// (MMA), with the radius Filter and an optional Heaviside threshold.
+// (MMA), with the radius Filter or the Helmholtz PDE filter of
+// opt_macro_oc.cpp:73-74 / opt_mma_Helmholtz.cpp:70-72 and an optional
+// Heaviside threshold.
 #include <cmath>
 
 #include "internal.cuh"
@@ -63,6 +65,8 @@ static int eb(int n) { return (n + 255) / 256 > 0 ? (n + 255) / 256 : 1; }
 int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
 {
   IREQUIRE(o->method == 0 || o->method == 1, ICARAT_ERR_ARG, "method must be 0 (OC) or 1 (MMA)");
+  IREQUIRE(o->filter_kind == 0 || o->filter_kind == 1, ICARAT_ERR_ARG,
+           "filter_kind must be 0 (radius) or 1 (Helmholtz)");
   LoopState &L = c->loop;
   const int n = c->nelx;
   if(!L.x)
@@ -79,7 +83,10 @@ int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
   L.opts = *o;
   L.optstep = 0;
   L.V0 = 0.0;
-  filter_setup(c, o->filter_radius);
+  if(o->filter_kind == 1)
+    helm_setup(c, o->filter_radius);
+  else
+    filter_setup(c, o->filter_radius);
   ICK(cudaMemcpyAsync(L.x, x0, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
   note_launch();
   k_fill<<<eb(n), 256, 0, c->stream>>>(n, o->xmin, L.xmin);
@@ -107,7 +114,13 @@ double loop_pre(icarat_ctx *c)
   const icarat_loop_opts &o = L.opts;
   L.optstep++;
   // filter -> threshold -> element design
-  filter_apply(c, L.x, L.xfil, false);
+  if(o.filter_kind == 1)
+  {
+    const int st = helm_filter(c, L.x, L.xfil, false, 0.0, 0, nullptr);
+    IREQUIRE(st >= 0, st, "Helmholtz filter failed");
+  }
+  else
+    filter_apply(c, L.x, L.xfil, false);
   double beta = std::pow(2.0, (int)(L.optstep / 40));
   beta = beta < 16.0 ? beta : 16.0;
   if(o.use_threshold)
@@ -156,7 +169,15 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
   k_mul2<<<eb(n), 256, 0, c->stream>>>(n, L.thrd, L.dfds, L.dgds);
   // both transposed filters in one pass, into the spare buffers, which then
   // become the sensitivities
-  filter_trans2(c, L.dfds, L.dgds, L.tmp, L.tmp2);
+  if(o.filter_kind == 1)
+  {
+    // densityFilter(dfds / dgds, .., true) (opt_mma_Helmholtz.cpp:150-151)
+    int st1 = helm_filter(c, L.dfds, L.tmp, true, 0.0, 0, nullptr);
+    int st2 = helm_filter(c, L.dgds, L.tmp2, true, 0.0, 0, nullptr);
+    IREQUIRE(st1 >= 0 && st2 >= 0, st1 < 0 ? st1 : st2, "Helmholtz filter failed");
+  }
+  else
+    filter_trans2(c, L.dfds, L.dgds, L.tmp, L.tmp2);
   std::swap(L.dfds, L.tmp);
   std::swap(L.dgds, L.tmp2);
   // update
@@ -170,7 +191,19 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
   else
   {
     icarat_oc_opts oc{o.move, 0.5, 0.0, 1.0e4, 1.0e-5, 100, o.use_threshold, beta, o.T};
-    ust = oc_update_dev(c, L.x, L.dfds, L.V0, L.dgds, L.xmin, L.xmax, &oc, &usteps);
+    if(o.filter_kind == 1)
+    {
+      // after the swap L.tmp / L.tmp2 hold the unfiltered sensitivities, no
+      // longer needed: they take the filtered and thresholded trials; the
+      // element volumes go to c->d_e1
+      note_launch();
+      k_fill<<<eb(n), 256, 0, c->stream>>>(n, c->vol0, c->d_e1);
+      ICK(cudaGetLastError());
+      ust = oc_update_helm_dev(c, L.x, L.dfds, L.V0, L.dgds, L.xmin, L.xmax, &oc, &usteps,
+                               L.tmp, L.tmp2, c->d_e1);
+    }
+    else
+      ust = oc_update_dev(c, L.x, L.dfds, L.V0, L.dgds, L.xmin, L.xmax, &oc, &usteps);
   }
   ICK(cudaStreamSynchronize(c->stream));
   if(info)

@@ -112,6 +112,14 @@ __global__ void __launch_bounds__(256) k_oc_bisect(OcArgs a)
   }
 }
 
+// one trial design of the bisection (the Helmholtz volume functor's input)
+__global__ void k_oc_trial(OcArgs a, double lambda)
+{
+  for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < a.nelx;
+      e += gridDim.x * blockDim.x)
+    a.xk[e] = oc_trial(a, e, lambda);
+}
+
 // x <- last trial (zeros when no step ran, like the reference's xkp1)
 __global__ void k_oc_finish(int n, const double *__restrict__ xk, int steps,
                             double *__restrict__ x)
@@ -183,6 +191,64 @@ int oc_update_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
   if(steps)
     *steps = nsteps;
   return nsteps >= o->maxiter ? ICARAT_WARN_MAXITER : ICARAT_OK;
+}
+
+// The same bisection with the volume functor of opt_macro_oc.cpp:153-164 on
+// the Helmholtz filter: g(x) = sum_i thr(H(x))_i v_i needs a nodal solve
+// per step, so the host drives the steps (trial kernel, Helmholtz filter,
+// threshold, volume dot) and takes each lambda decision.  fil and thr are
+// nelx work vectors, vol the element volumes (nelx).
+int oc_update_helm_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
+                       const double *dgdx, const double *xmin, const double *xmax,
+                       const icarat_oc_opts *o, int *steps, double *fil, double *thr,
+                       const double *vol)
+{
+  IREQUIRE(c->helm.d_coef != nullptr, ICARAT_ERR_STATE,
+           "the Helmholtz OC volume functor needs the Helmholtz filter set up");
+  IREQUIRE(o->maxiter >= 0 && o->lambda_max + o->lambda_min > 0, ICARAT_ERR_ARG,
+           "bad OC parameters");
+  OcArgs a{};
+  a.nelx = c->nelx;
+  a.x = x;
+  a.dfdx = dfdx;
+  a.dgdx = dgdx;
+  a.xmin = xmin;
+  a.xmax = xmax;
+  a.xk = c->d_e2;
+  a.move = o->move;
+  a.iota = o->iota;
+  const int n = c->nelx;
+  const int blocks = (n + 255) / 256 > 4 * c->sm_count ? 4 * c->sm_count : (n + 255) / 256;
+  double l0 = o->lambda_min, l1 = o->lambda_max;
+  int counter = 0;
+  while((l1 - l0) / (l1 + l0) > o->lambda_eps && o->maxiter > counter)
+  {
+    const double lambda = 0.5 * (l1 + l0);
+    note_launch();
+    k_oc_trial<<<blocks, 256, 0, c->stream>>>(a, lambda);
+    ICK(cudaGetLastError());
+    const int st = helm_filter(c, a.xk, fil, false, 0.0, 0, nullptr);
+    if(st < 0)
+      return st;
+    const double *t = fil;
+    if(o->use_threshold)
+    {
+      threshold_dev(c, fil, o->beta, o->T, thr, false);
+      t = thr;
+    }
+    if(device_dot(c, t, vol, n) - g > 0.0)
+      l0 = lambda;
+    else
+      l1 = lambda;
+    counter++;
+  }
+  note_launch();
+  k_oc_finish<<<blocks, 256, 0, c->stream>>>(n, c->d_e2, counter, x);
+  ICK(cudaGetLastError());
+  ICK(cudaStreamSynchronize(c->stream));
+  if(steps)
+    *steps = counter;
+  return counter >= o->maxiter ? ICARAT_WARN_MAXITER : ICARAT_OK;
 }
 
 } // namespace icarat_b200

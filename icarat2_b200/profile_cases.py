@@ -24,6 +24,9 @@ set-up.
         one design iteration of the MMA loop (densities U[0.1, 0.5], seed 0,
         filter radius 3, move 0.2) after `warm` warm-up iterations; methods
         mg, mixed (warm-started), jacobi
+    python -m icarat2_b200.profile_cases helm 256x128x128 2.0
+        one Helmholtz PDE filter call (design U[0, 1], seed 0, CG to 1e-10)
+        after one warm-up call
 """
 import ctypes as C
 import sys
@@ -127,6 +130,22 @@ def net(grid):
     print("|u| %.6g" % float(np.linalg.norm(u)))
 
 
+def helm(grid, radius):
+    nx, ny, nz = _grid(grid)
+    G = gpu.Context(nx, ny, nz, dirichlet=[], loads=[])
+    G.helmholtz_setup(float(radius))
+    x = np.random.default_rng(0).uniform(0.0, 1.0, G.nelx)
+    G.helmholtz_filter(x)
+    G.synchronize()
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    out, info = G.helmholtz_filter(x)
+    G.synchronize()
+    rt.cudaProfilerStop()
+    print("cg iterations %d rel_residual %.3g sum %.12g" % (info.iterations,
+                                                           info.rel_residual, out.sum()))
+
+
 def main(argv):
     if len(argv) >= 5 and argv[0] == "solve":
         solve(*argv[1:5])
@@ -134,6 +153,8 @@ def main(argv):
         loop(*argv[1:6])
     elif len(argv) >= 2 and argv[0] == "headline":
         headline(argv[1])
+    elif len(argv) >= 3 and argv[0] == "helm":
+        helm(argv[1], argv[2])
     elif len(argv) >= 2 and argv[0] == "net":
         net(argv[1])
     elif len(argv) >= 4 and argv[0] == "operator":

@@ -214,6 +214,24 @@ int icarat_threshold(icarat_ctx *ctx, const double *in, double beta, double T,
 int icarat_threshold_derivative(icarat_ctx *ctx, const double *in, double beta,
                                 double T, double *out);
 
+/* ---- Helmholtz PDE filter (FilterHelmholtz<E,N>,
+ *      src/optimization/filter_helm.hpp) ------------------------------------
+ * setup: the constructor (:67-73) for radius R >= 0.  filter: densityFilter
+ * (:75-138) with solvName "Eigen_CG": the nodal system K val = F solved by
+ * Jacobi-PCG from zero to ||r|| < rtol ||F|| (rtol <= 0: 1e-10, maxit <= 0:
+ * 10000, the Solvers defaults of solvers.hpp:89-90); is_sens != 0 is the
+ * sensitivity call (sensFlag).  Returns ICARAT_WARN_MAXITER when the CG
+ * stopped at its cap; info (may be NULL) gets the iterations and the final
+ * ||r|| / ||F||.  threshold / thresholdDerivative (:140-174) are the same
+ * maps as icarat_threshold / icarat_threshold_derivative. */
+int icarat_helmholtz_setup(icarat_ctx *ctx, double radius);
+int icarat_helmholtz_filter(icarat_ctx *ctx, const double *in, double *out,
+                            int is_sens, double rtol, int maxit,
+                            icarat_solve_info *info);
+int icarat_helmholtz_filter_dev(icarat_ctx *ctx, const double *in, double *out,
+                                int is_sens, double rtol, int maxit,
+                                icarat_solve_info *info);
+
 /* ---- OC (src/optimization/opt-solver/OCSolver.hpp:21-68) ----------------
  * x is updated in place; g is the reference volume (the driver's V0); the
  * volume functor runs on the GPU with the filter of icarat_filter_setup. */
@@ -247,8 +265,12 @@ int icarat_mma_last_loops(const icarat_mma *mma, int *outer, int *newton);
 
 /* ---- one design iteration, device resident --------------------------------
  * The loop body of the sample drivers (opt_macro_oc.cpp:83-172,
- * opt_macro_mma_nondesign.cpp:90-178): filter -> (threshold) -> solve ->
- * compliance/volume -> sensitivity -> filter^T -> OC or MMA update. */
+ * opt_macro_mma_nondesign.cpp:90-178, opt_mma_Helmholtz.cpp:86-170): filter
+ * -> (threshold) -> solve -> compliance/volume -> sensitivity -> filter^T ->
+ * OC or MMA update.  filter_kind 0 is the radius Filter (filter.hpp), 1 the
+ * Helmholtz PDE filter (filter_helm.hpp, CG to the "Eigen_CG" default 1e-10)
+ * that opt_macro_oc.cpp:73-74 and opt_mma_Helmholtz.cpp:70-72 use -- for OC
+ * also inside the volume functor of the bisection (:153-164). */
 typedef struct
 {
   int method;        /* 0 = OC, 1 = MMA */
@@ -258,6 +280,7 @@ typedef struct
   double xmin, xmax;
   double filter_radius;
   icarat_solve_opts solve;
+  int filter_kind; /* 0 radius filter, 1 Helmholtz PDE filter */
 } icarat_loop_opts;
 
 typedef struct

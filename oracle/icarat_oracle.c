@@ -1104,8 +1104,13 @@ int or_oc_update(int n, double *x, const double *dfdx, double g,
   return counter >= prm->maxiter ? 1 : OR_OK;
 }
 
+int or_helmholtz_filter(int nx, int ny, int nz, double lx, double ly, double lz, double R,
+                        const double *in, double *out, int sens, double tol, int maxit,
+                        int *iters_out);
+
 /* Volume functor of the sample drivers (opt_macro_oc.cpp:153-164):
-   g(x) = sum_i thr(filter(x))_i v_i. */
+   g(x) = sum_i thr(filter(x))_i v_i, with the radius filter F or, when
+   helm_R > 0, the Helmholtz filter of the box (nx, ny, nz, lx, ly, lz). */
 typedef struct
 {
   or_filter *F;
@@ -1113,13 +1118,21 @@ typedef struct
   double beta, T;
   const double *vol;
   double *tmp, *tmp2;
+  int n;
+  double helm_R, helm_tol;
+  int nx, ny, nz;
+  double lx, ly, lz;
 } or_filter_volume;
 
 static double or_filter_volume_fn(const double *x, void *user)
 {
   or_filter_volume *fv = (or_filter_volume *)user;
-  int n = fv->F->n;
-  or_filter_density(fv->F, x, fv->tmp, 0);
+  int n = fv->n;
+  if(fv->helm_R > 0.0)
+    or_helmholtz_filter(fv->nx, fv->ny, fv->nz, fv->lx, fv->ly, fv->lz, fv->helm_R, x,
+                        fv->tmp, 0, fv->helm_tol, 10000, NULL);
+  else
+    or_filter_density(fv->F, x, fv->tmp, 0);
   const double *t = fv->tmp;
   if(fv->use_threshold)
   {
@@ -1548,6 +1561,9 @@ void or_mma_update(or_mma *M, double *xval, const double *dfdx,
 /*     sample/algorithm/opt-macro-mma-nondesign/opt_macro_mma_nondesign.cpp: */
 /*     90-178 (MMA), with the radius Filter and an optional threshold (the   */
 /*     drivers always apply it with beta = min(2^(step/40), 16), T = 0.5).   */
+/*     or_loop_set_helmholtz switches to the Helmholtz filter of             */
+/*     opt_macro_oc.cpp:73-74 / opt_mma_Helmholtz.cpp:70-72 (solved to tol,   */
+/*     the "Eigen_CG" default being 1e-10), also inside the OC functor.       */
 /* ------------------------------------------------------------------------ */
 typedef struct
 {
@@ -1568,7 +1584,26 @@ typedef struct
   int cg_iters, oc_steps, mma_outloops;
   double cg_relres;
   double t_filter, t_solve, t_sens, t_update, t_pcg;
+  double helm_R, helm_tol; /* helm_R > 0: Helmholtz filter */
 } or_loop;
+
+void or_loop_set_helmholtz(or_loop *L, double R, double tol)
+{
+  L->helm_R = R;
+  L->helm_tol = tol;
+}
+
+static int or_loop_filter(or_loop *L, const double *in, double *out, int sens)
+{
+  const or_problem *P = L->P;
+  if(L->helm_R > 0.0)
+  {
+    int st = or_helmholtz_filter(P->nx, P->ny, P->nz, P->lx, P->ly, P->lz, L->helm_R, in,
+                                 out, sens, L->helm_tol, 10000, NULL);
+    return st == OR_OK ? OR_OK : st;
+  }
+  return or_filter_density(L->F, in, out, sens);
+}
 
 or_loop *or_loop_create(or_problem *P, or_filter *F, int method,
                         int use_threshold, double move, double xmin,
@@ -1647,7 +1682,7 @@ int or_loop_step(or_loop *L)
   const int n = P->nelx;
   double t0 = or_now();
   L->optstep++;
-  int st = or_filter_density(L->F, L->x, L->xfil, 0);
+  int st = or_loop_filter(L, L->x, L->xfil, 0);
   if(st != OR_OK)
     return st;
   double beta = pow(2, (int)(L->optstep / 40));
@@ -1706,9 +1741,9 @@ int or_loop_step(or_loop *L)
     L->dfds[e] *= L->thrd[e];
     L->dgds[e] *= L->thrd[e];
   }
-  or_filter_density(L->F, L->dfds, L->tmp, 1);
+  or_loop_filter(L, L->dfds, L->tmp, 1);
   memcpy(L->dfds, L->tmp, sizeof(double) * n);
-  or_filter_density(L->F, L->dgds, L->tmp, 1);
+  or_loop_filter(L, L->dgds, L->tmp, 1);
   memcpy(L->dgds, L->tmp, sizeof(double) * n);
   double t3 = or_now();
   if(L->method == 1)
@@ -1719,8 +1754,9 @@ int or_loop_step(or_loop *L)
   }
   else
   {
-    or_filter_volume fv = {L->F, L->use_threshold, beta, L->T, L->vol, L->tmp,
-                           L->tmp2};
+    or_filter_volume fv = {L->F, L->use_threshold, beta, L->T, L->vol, L->tmp, L->tmp2,
+                           n, L->helm_R, L->helm_tol, P->nx, P->ny, P->nz, P->lx, P->ly,
+                           P->lz};
     or_oc_update(n, L->x, L->dfds, L->V0, L->dgds, L->xmin, L->xmax, &L->oc,
                  or_filter_volume_fn, &fv, &L->oc_steps);
   }

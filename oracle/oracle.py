@@ -92,6 +92,7 @@ def _load():
         "or_mma_outloops": (C.c_int, [_vp]),
         "or_mma_inner_total": (C.c_int, [_vp]),
         "or_mma_state": (None, [_vp, _dp, _dp, _dp, _dp]),
+        "or_loop_set_helmholtz": (None, [_vp, C.c_double, C.c_double]),
         "or_loop_create": (_vp, [_vp, _vp, C.c_int, C.c_int, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_int, _dp]),
         "or_loop_destroy": (None, [_vp]),
@@ -381,14 +382,19 @@ class Loop:
 
     def __init__(self, problem, filt, method="mma", x0=0.3, move=None,
                  use_threshold=False, xmin=1e-4, xmax=1.0, cg_tol=1e-10,
-                 cg_maxit=10000):
+                 cg_maxit=10000, helmholtz_R=None, helmholtz_tol=1e-10):
+        """filt: a radius Filter, or None with helmholtz_R: the Helmholtz
+        filter of radius helmholtz_R solved to helmholtz_tol."""
         self.P, self.F = problem, filt
         if move is None:
             move = 0.15
         x0 = np.full(problem.nelx, x0) if np.isscalar(x0) else _f64(x0)
-        self.h = lib.or_loop_create(problem.h, filt.h, 1 if method == "mma" else 0,
+        self.h = lib.or_loop_create(problem.h, filt.h if filt is not None else None,
+                                    1 if method == "mma" else 0,
                                     1 if use_threshold else 0, move, xmin, xmax,
                                     cg_tol, cg_maxit, _f64(x0))
+        if helmholtz_R is not None:
+            lib.or_loop_set_helmholtz(self.h, helmholtz_R, helmholtz_tol)
 
     def __del__(self):
         if getattr(self, "h", None):

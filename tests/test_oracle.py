@@ -366,3 +366,21 @@ def test_helmholtz_filter_properties(oracle):
     # stretched elements (lx != nx) keep both properties
     c2, _ = oracle.helmholtz_filter(nx, ny, nz, R, np.full(n, 0.5), lx=2.0 * nx)
     assert np.abs(c2 - 0.5).max() < 1e-12
+
+
+def test_helmholtz_loop_oracle(oracle):
+    # the loop with the Helmholtz filter (opt_macro_oc.cpp:73-74): step 1
+    # filters the start design with the same map as helmholtz_filter, and
+    # OC (Helmholtz volume functor) and MMA steps run and lower compliance
+    nx, ny, nz, R = 8, 4, 4, 1.5
+    for method in ("oc", "mma"):
+        P = oracle.Problem(nx, ny, nz)
+        L = oracle.Loop(P, None, method=method, x0=0.3, use_threshold=True,
+                        cg_tol=1e-12, helmholtz_R=R)
+        L.step()
+        ref, _ = oracle.helmholtz_filter(nx, ny, nz, R, np.full(P.nelx, 0.3), tol=1e-10)
+        assert np.abs(L.get("xfil") - ref).max() < 1e-12
+        c1 = L.scalars()["compliance"]
+        for _ in range(3):
+            L.step()
+        assert L.scalars()["compliance"] < c1
