@@ -14,9 +14,9 @@
 // which of the node's 8 neighbouring elements exist: 3 x 3 x 3 node classes
 // (lower face, interior, upper face per axis).  The table of 27 classes x 27
 // neighbour slots is assembled once on the host in the reference's order
-// (ascending element id) and the solve runs matrix-free: Ap = K p reads the
-// class row from shared memory and p from a register window of 3 planes
-// that marches along z.  The CG iteration
+// (ascending element id) for the Jacobi diagonal; the solve runs
+// matrix-free with the same operator in sum-factorised form (k_helm_spmv).
+// The CG iteration
 // reuses the device-resident scalar kernels of the elasticity solve (one
 // stop-flag read per graph replay of `kHelmChunk` iterations).
 #include <cmath>
@@ -113,86 +113,200 @@ __global__ void k_helm_invd(HelmGrid g, const double *__restrict__ coef,
   }
 }
 
-// Ap = K p and alpha = zr / (p . Ap).
+// Ap = K p and alpha = zr / (p . Ap), by sum factorisation.
 //
-// A block of 32 x 8 threads owns a tile of 32 x 8 node columns and marches
-// through kHelmTz planes of it: each thread keeps p of its 3 x 3 neighbour
-// columns on planes k-1, k, k+1 in registers and loads one new plane (9
-// values) per node instead of 27.  Neighbour slot q = (dk+1) 9 + (dj+1) 3 +
-// (di+1) is also the window index; values outside the box are held as 0
-// and their class coefficients are 0 (no element reaches them), so no read
-// leaves the box.
-constexpr int kHelmTx = 32, kHelmTy = 8, kHelmTz = 16;
+// With trilinear shape functions and exact 2-point Gauss rules the element
+// matrix is a tensor product, Ke = Mx (x) My (x) Mz + c (Sx (x) My (x) Mz +
+// Mx (x) Sy (x) Mz + Mx (x) My (x) Sz), c = (R / (2 sqrt 3))^2, with the 1-D
+// element mass h/6 [2 1; 1 2] and stiffness 1/h [1 -1; -1 1]; assembled on
+// the box it stays one, with the 3-point 1-D stencils m, s of each node
+// class (lower face, inside, upper face).  So every plane of p contributes
+// through two in-plane sums per node, A = (mx my + c (sx my + mx sy)) p and
+// B = mx my p, and Ap(k) = sum_dz mz A(k+dz) + c sz B(k+dz).
+//
+// A block of 8 warps owns 32 x 8 kHelmRows node columns (a warp kHelmRows
+// rows of 32 nodes along x) and marches through kHelmTz planes, holding A
+// and B of planes k-1, k, k+1 in registers.  The planes of p come through
+// shared memory: a ring of kHelmDepth halo tiles filled by cp.async,
+// kHelmDepth - 1 planes ahead of the plane being reduced, so later planes
+// are in flight without holding registers.  Positions outside the box are
+// stored as 0 (their stencil weights are 0 as well).  Measured on the B200
+// at 257 x 129 x 129 nodes: about 50 us per launch, like a variant with a
+// one-plane register lookahead and one with two rows per thread; the limit
+// is dependent-latency (FP64 FMA chains, barriers), not DRAM.
+constexpr int kHelmTx = 32, kHelmWarps = 8, kHelmRows = 1, kHelmTz = 16, kHelmDepth = 4;
+constexpr int kHelmTy = kHelmWarps * kHelmRows;
+constexpr int kHaloX = kHelmTx + 2, kHaloY = kHelmTy + 2, kHalo = kHaloX * kHaloY;
+constexpr int kStage = (kHalo + kHelmTx * kHelmWarps - 1) / (kHelmTx * kHelmWarps);
 
-__device__ __forceinline__ void helm_load_plane(double (&d)[9], const double *__restrict__ col,
-                                                int k, int NZ, long plane, int NX, bool xm,
-                                                bool xp, bool ym, bool yp)
+// 1-D stencils [axis][class][d + 1] and the diffusion coefficient c
+struct HelmAxes
 {
-  const bool in = k >= 0 && k < NZ;
-  const double *q = col + (long)k * plane;
-#pragma unroll
-  for(int dy = -1; dy <= 1; dy++)
-#pragma unroll
-    for(int dx = -1; dx <= 1; dx++)
-    {
-      const bool ok = in && (dx >= 0 || xm) && (dx <= 0 || xp) && (dy >= 0 || ym) &&
-                      (dy <= 0 || yp);
-      d[(dy + 1) * 3 + dx + 1] = ok ? __ldg(q + dx + (long)dy * NX) : 0.0;
-    }
+  double m[3][3][3], s[3][3][3];
+  double c;
+};
+
+// 8-byte global -> shared copies (cp.async), one commit group per staged
+// plane, and a wait for all but the newest kHelmDepth - 1 groups
+__device__ __forceinline__ void cp_async8(double *dst, const double *src)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit()
+{
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_ring()
+{
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(kHelmDepth - 1) : "memory");
 }
 
-__global__ void __launch_bounds__(kHelmTx * kHelmTy)
-    k_helm_spmv(HelmGrid g, const double *__restrict__ coef, const double *__restrict__ p,
+// this thread's staged halo positions: in-plane offset (or -1 outside)
+struct HelmStage
+{
+  long off[kStage];
+};
+
+// halo tile of plane kk (rows j0-1 .. j0+kHelmTy, columns i0-1 .. i0+32)
+// into buf; one commit group per call, empty when the plane is not needed
+__device__ __forceinline__ void helm_stage(double *buf, const double *__restrict__ p,
+                                          const HelmStage &st, int NZ, long plane, int kk,
+                                          bool needed)
+{
+  if(needed)
+  {
+    const bool inz = kk >= 0 && kk < NZ;
+#pragma unroll
+    for(int q = 0; q < kStage; q++)
+    {
+      const int e = threadIdx.x + q * kHelmTx * kHelmWarps;
+      if(e < kHalo)
+      {
+        if(inz && st.off[q] >= 0)
+          cp_async8(buf + e, p + st.off[q] + kk * plane);
+        else
+          buf[e] = 0.0;
+      }
+    }
+  }
+  cp_async_commit();
+}
+
+__global__ void __launch_bounds__(kHelmTx * kHelmWarps)
+    k_helm_spmv(HelmGrid g, HelmAxes ax, const double *__restrict__ p,
                 double *__restrict__ Ap, double *__restrict__ partials, CgScalars *s)
 {
-  __shared__ double cs[kHelmClasses * 27];
+  __shared__ double ring[kHelmDepth][kHalo];
   __shared__ double sh[64];
   if(s->done)
     return;
-  for(int t = threadIdx.x; t < kHelmClasses * 27; t += blockDim.x)
-    cs[t] = coef[t];
-  __syncthreads();
   const int NZ = g.nz + 1;
   const long plane = (long)g.NX * g.NY;
   const int tiles_x = (g.NX + kHelmTx - 1) / kHelmTx, tiles_y = (g.NY + kHelmTy - 1) / kHelmTy;
   const int tiles = tiles_x * tiles_y * ((NZ + kHelmTz - 1) / kHelmTz);
+  const double c = ax.c;
+  const int lx = threadIdx.x & 31, ly = (threadIdx.x >> 5) * kHelmRows;
   double dot = 0.0;
   for(int t = blockIdx.x; t < tiles; t += gridDim.x)
   {
-    const int i = (t % tiles_x) * kHelmTx + (threadIdx.x & 31);
-    const int j = (t / tiles_x % tiles_y) * kHelmTy + (threadIdx.x >> 5);
+    const int i0 = (t % tiles_x) * kHelmTx, j0 = (t / tiles_x % tiles_y) * kHelmTy;
     const int k0 = t / (tiles_x * tiles_y) * kHelmTz;
     const int k1 = min(k0 + kHelmTz, NZ);
-    if(i >= g.NX || j >= g.NY)
-      continue;
-    const bool xm = i > 0, xp = i < g.NX - 1, ym = j > 0, yp = j < g.NY - 1;
-    const int cxy = node_class(i, g.NX) + 3 * node_class(j, g.NY);
-    const long c0 = i + (long)j * g.NX;
-    const double *col = p + c0;
-    double w0[9], w1[9], w2[9];
-    helm_load_plane(w0, col, k0 - 1, NZ, plane, g.NX, xm, xp, ym, yp);
-    helm_load_plane(w1, col, k0, NZ, plane, g.NX, xm, xp, ym, yp);
-    for(int k = k0; k < k1; k++)
+    const int i = i0 + lx;
+    HelmStage st;
+#pragma unroll
+    for(int q = 0; q < kStage; q++)
     {
-      helm_load_plane(w2, col, k + 1, NZ, plane, g.NX, xm, xp, ym, yp);
-      const double *cf = cs + 27 * (cxy + 9 * node_class(k, NZ));
-      double acc = 0.0;
+      const int e = threadIdx.x + q * kHelmTx * kHelmWarps;
+      const int x = i0 - 1 + e % kHaloX, y = j0 - 1 + e / kHaloX;
+      st.off[q] = (x >= 0 && x < g.NX && y >= 0 && y < g.NY) ? x + (long)y * g.NX : -1;
+    }
+    double mx[3], sx[3], my[kHelmRows][3], sy[kHelmRows][3];
+    const int cx = node_class(min(i, g.NX - 1), g.NX);
 #pragma unroll
-      for(int q = 0; q < 9; q++)
-        acc += cf[q] * w0[q];
+    for(int d = 0; d < 3; d++)
+    {
+      mx[d] = ax.m[0][cx][d];
+      sx[d] = ax.s[0][cx][d];
+    }
 #pragma unroll
-      for(int q = 0; q < 9; q++)
-        acc += cf[9 + q] * w1[q];
+    for(int r = 0; r < kHelmRows; r++)
+    {
+      const int cy = node_class(min(j0 + ly + r, g.NY - 1), g.NY);
 #pragma unroll
-      for(int q = 0; q < 9; q++)
-        acc += cf[18 + q] * w2[q];
-      Ap[c0 + k * plane] = acc;
-      dot += w1[4] * acc;
-#pragma unroll
-      for(int q = 0; q < 9; q++)
+      for(int d = 0; d < 3; d++)
       {
-        w0[q] = w1[q];
-        w1[q] = w2[q];
+        my[r][d] = ax.m[1][cy][d];
+        sy[r][d] = ax.s[1][cy][d];
+      }
+    }
+    // planes k0-1 .. k1 are reduced, plane m in ring slot (m - k0 + 1) % depth;
+    // the ring of the previous tile is no longer read past this barrier, and
+    // every copy of that tile has landed (its groups past plane k1 were empty)
+    __syncthreads();
+#pragma unroll
+    for(int q = 0; q < kHelmDepth; q++)
+      helm_stage(ring[q], p, st, NZ, plane, k0 - 1 + q, k0 - 1 + q <= k1);
+    double A0[kHelmRows], B0[kHelmRows], A1[kHelmRows], B1[kHelmRows], A2[kHelmRows],
+        B2[kHelmRows], P1[kHelmRows], P2[kHelmRows];
+    for(int m = k0 - 1; m <= k1; m++)
+    {
+      const int slot = (m - k0 + 1) % kHelmDepth;
+      cp_async_wait_ring();
+      __syncthreads();
+      {
+        const double *buf = ring[slot] + ly * kHaloX + lx;
+        double rm[kHelmRows + 2], rs[kHelmRows + 2];
+#pragma unroll
+        for(int q = 0; q < kHelmRows + 2; q++)
+        {
+          const double vl = buf[q * kHaloX], v0 = buf[q * kHaloX + 1], vr = buf[q * kHaloX + 2];
+          rm[q] = mx[0] * vl + mx[1] * v0 + mx[2] * vr;
+          rs[q] = sx[0] * vl + sx[1] * v0 + sx[2] * vr;
+          if(q >= 1 && q <= kHelmRows)
+            P2[q - 1] = v0;
+        }
+#pragma unroll
+        for(int r = 0; r < kHelmRows; r++)
+        {
+          const double pm = my[r][0] * rm[r] + my[r][1] * rm[r + 1] + my[r][2] * rm[r + 2];
+          const double ps = my[r][0] * rs[r] + my[r][1] * rs[r + 1] + my[r][2] * rs[r + 2] +
+                            sy[r][0] * rm[r] + sy[r][1] * rm[r + 1] + sy[r][2] * rm[r + 2];
+          A2[r] = pm + c * ps;
+          B2[r] = pm;
+        }
+      }
+      __syncthreads(); // every thread has read the slot: refill it
+      helm_stage(ring[slot], p, st, NZ, plane, m + kHelmDepth, m + kHelmDepth <= k1);
+      if(m >= k0 + 1)
+      {
+        // output plane k = m - 1 from planes k-1, k, k+1
+        const int k = m - 1;
+        const int cz = node_class(k, NZ);
+        const double mz0 = ax.m[2][cz][0], mz1 = ax.m[2][cz][1], mz2 = ax.m[2][cz][2];
+        const double sz0 = ax.s[2][cz][0], sz1 = ax.s[2][cz][1], sz2 = ax.s[2][cz][2];
+#pragma unroll
+        for(int r = 0; r < kHelmRows; r++)
+        {
+          const double y = mz0 * A0[r] + mz1 * A1[r] + mz2 * A2[r] +
+                           c * (sz0 * B0[r] + sz1 * B1[r] + sz2 * B2[r]);
+          const int j = j0 + ly + r;
+          if(i < g.NX && j < g.NY)
+          {
+            Ap[i + (long)j * g.NX + (long)k * plane] = y;
+            dot += P1[r] * y;
+          }
+        }
+      }
+#pragma unroll
+      for(int r = 0; r < kHelmRows; r++)
+      {
+        A0[r] = A1[r];
+        B0[r] = B1[r];
+        A1[r] = A2[r];
+        B1[r] = B2[r];
+        P1[r] = P2[r];
       }
     }
   }
@@ -333,6 +447,30 @@ static void helm_class_table(const double *ke, double *coef)
       }
 }
 
+// the assembled 1-D stencils of each axis: element mass h/6 [2 1; 1 2] and
+// stiffness 1/h [1 -1; -1 1] summed over the one (face) or two (inside)
+// elements of a node
+static HelmAxes helm_axes(const icarat_ctx *c)
+{
+  HelmAxes a{};
+  const double h[3] = {c->hx, c->hy, c->hz};
+  for(int d = 0; d < 3; d++)
+  {
+    const double md = h[d] / 3.0, mo = h[d] / 6.0, sd = 1.0 / h[d], so = -1.0 / h[d];
+    // class 0: only the element above; 1: both; 2: only the element below
+    const double m[3][3] = {{0.0, md, mo}, {mo, md + md, mo}, {mo, md, 0.0}};
+    const double s[3][3] = {{0.0, sd, so}, {so, sd + sd, so}, {so, sd, 0.0}};
+    for(int k = 0; k < 3; k++)
+      for(int q = 0; q < 3; q++)
+      {
+        a.m[d][k][q] = m[k][q];
+        a.s[d][k][q] = s[k][q];
+      }
+  }
+  a.c = std::pow(c->helm.radius / (2.0 * std::sqrt(3.0)), 2);
+  return a;
+}
+
 void helm_free(icarat_ctx *c)
 {
   HelmState &H = c->helm;
@@ -373,18 +511,26 @@ void helm_setup(icarat_ctx *c, double R)
   ICK(cudaGetLastError());
 }
 
+// grid of the streaming CG kernels: 8 blocks of 256 threads per SM (full
+// occupancy; 4 per SM left them at 3-4 TB/s on the B200)
+static int helm_red_blocks(const icarat_ctx *c)
+{
+  return 8 * c->sm_count < kMaxRedBlocks ? 8 * c->sm_count : kMaxRedBlocks;
+}
+
 static void helm_iteration(icarat_ctx *c)
 {
   HelmState &H = c->helm;
   const int n = c->numnp;
+  const int rb = helm_red_blocks(c);
   const long tiles = (long)((c->NX + kHelmTx - 1) / kHelmTx) *
                     ((c->NY + kHelmTy - 1) / kHelmTy) * ((c->NZ + kHelmTz - 1) / kHelmTz);
   note_launch(3);
-  k_helm_spmv<<<blocks_for(tiles, 1, kMaxRedBlocks), kHelmTx * kHelmTy, 0, c->stream>>>(
-      hgrid(c), H.d_coef, H.d_p, H.d_Ap, H.d_partials, H.d_cg);
-  k_cg_update_jacobi<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
-      n, H.d_invd, H.d_val, H.d_r, H.d_z, H.d_p, H.d_Ap, H.d_partials, H.d_cg);
-  k_cg_pupdate<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, H.d_z, H.d_p, H.d_cg);
+  k_helm_spmv<<<blocks_for(tiles, 1, kMaxRedBlocks), kHelmTx * kHelmWarps, 0, c->stream>>>(
+      hgrid(c), helm_axes(c), H.d_p, H.d_Ap, H.d_partials, H.d_cg);
+  k_cg_update_jacobi<<<rb, kRedThreads, 0, c->stream>>>(n, H.d_invd, H.d_val, H.d_r, H.d_z,
+                                                        H.d_p, H.d_Ap, H.d_partials, H.d_cg);
+  k_cg_pupdate<<<rb, kRedThreads, 0, c->stream>>>(n, H.d_z, H.d_p, H.d_cg);
   ICK(cudaGetLastError());
 }
 
@@ -411,7 +557,7 @@ int helm_filter(icarat_ctx *c, const double *in, double *out, bool is_sens, doub
   note_launch(2);
   k_helm_rhs<<<eb, kHelmThreads, 0, c->stream>>>(hgrid(c), w, in, H.d_F, is_sens ? 1 : 0);
   ICK(cudaGetLastError());
-  k_cg_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, H.d_F, H.d_invd, H.d_val,
+  k_cg_init<<<helm_red_blocks(c), kRedThreads, 0, c->stream>>>(n, H.d_F, H.d_invd, H.d_val,
                                                           H.d_r, H.d_z, H.d_p, H.d_partials,
                                                           H.d_cg, rtol, maxit, 1);
   ICK(cudaGetLastError());
