@@ -183,6 +183,51 @@ private:
   Model &m_;
 };
 
+// FilterHelmholtz<E,N> (src/optimization/filter_helm.hpp:16-65): the nodal
+// Helmholtz system solved on the GPU by Jacobi-PCG ("Eigen_CG" and
+// "Scaling_CG"; other solver names are rejected), CG tolerance 1e-10
+class FilterHelmholtz
+{
+public:
+  FilterHelmholtz(Model &m, double radious) : m_(m)
+  {
+    check(icarat_helmholtz_setup(m.ctx(), radious), "FilterHelmholtz");
+  }
+  std::vector<double> densityFilter(const std::vector<double> &design_s,
+                                    const std::string &solvName, int log, bool sensFlag)
+  {
+    if(solvName != "Eigen_CG" && solvName != "Scaling_CG")
+      throw Error(ICARAT_ERR_UNSUPPORTED,
+                  "FilterHelmholtz: solver " + solvName + " is not offered");
+    std::vector<double> out(m_.nelx);
+    icarat_solve_info info{};
+    check(icarat_helmholtz_filter(m_.ctx(), design_s.data(), out.data(), sensFlag ? 1 : 0,
+                                  0.0, 0, &info),
+          "densityFilter");
+    if(log == 1)
+      std::printf("Helmholtz filtering...\n#iterations:     %d\nestimated error: %g\n",
+                  info.iterations, info.rel_residual);
+    return out;
+  }
+  std::vector<double> threshold(const std::vector<double> &d, double beta, double T)
+  {
+    std::vector<double> out(m_.nelx);
+    check(icarat_threshold(m_.ctx(), d.data(), beta, T, out.data()), "threshold");
+    return out;
+  }
+  std::vector<double> thresholdDerivative(const std::vector<double> &d, double beta,
+                                          double T)
+  {
+    std::vector<double> out(m_.nelx);
+    check(icarat_threshold_derivative(m_.ctx(), d.data(), beta, T, out.data()),
+          "thresholdDerivative");
+    return out;
+  }
+
+private:
+  Model &m_;
+};
+
 // OC (src/optimization/opt-solver/OCSolver.hpp:13-80).  The reference takes
 // the volume functor as a lambda; here it is the sample drivers' functor,
 // g(x) = sum thr(filter(x)) v, evaluated on the GPU with the Model's Filter

@@ -42,3 +42,28 @@ def test_cpp_driver_rejects_unknown_solver():
     out = subprocess.run([EXE, "4", "2", "2", "1", "1.5", "mma", "Eigen_LDLT"],
                          capture_output=True, text=True, timeout=120)
     assert out.returncode == 2 and "Solver type name is wrong" in out.stdout
+
+
+def test_cpp_helmholtz_driver_trajectory(oracle):
+    """examples/opt_mma_helmholtz.cpp (the opt_mma_Helmholtz.cpp loop through
+    FilterHelmholtz of include/icarat_b200.hpp) against the oracle's loop with
+    the Helmholtz filter (MMA, threshold; both Helmholtz CGs at the reference's
+    1e-10, elasticity CG at 1e-12): compliance <= 1e-7 relative."""
+    exe = os.path.join(ROOT, "icarat2_b200", "examples", "opt_mma_helmholtz")
+    if not os.path.exists(exe):
+        from icarat2_b200 import build
+        build.build()
+    nx, ny, nz, steps, R = 16, 8, 8, 4, 2.0
+    out = subprocess.run([exe, str(nx), str(ny), str(nz), str(steps), str(R), "MG_CG"],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    comp = [float(l.split()[2]) for l in out.stdout.splitlines() if l.startswith("step")]
+    assert len(comp) == steps
+    P = oracle.Problem(nx, ny, nz)
+    L = oracle.Loop(P, None, method="mma", x0=0.3, move=0.2, use_threshold=True,
+                    cg_tol=1e-12, helmholtz_R=R)
+    ref = []
+    for _ in range(steps):
+        L.step()
+        ref.append(L.scalars()["compliance"])
+    assert np.allclose(comp, ref, rtol=1e-7, atol=0)
