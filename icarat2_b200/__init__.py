@@ -149,6 +149,8 @@ SIGNATURES = {
     "icarat_density_filter": (_i, [_vp, _dp, _dp, _i]),
     "icarat_density_filter_dev": (_i, [_vp, _vp, _vp, _i]),
     "icarat_sensitivity_filter": (_i, [_vp, _dp, _dp, _dp]),
+    "icarat_set_load_cases": (_i, [_vp, _i, _vp]),
+    "icarat_loop_set_domains": (_i, [_vp, _vp, _i, _vp, _i]),
     "icarat_helmholtz_setup": (_i, [_vp, _d]),
     "icarat_helmholtz_filter": (_i, [_vp, _dp, _dp, _i, _d, _i, _P(SolveInfo)]),
     "icarat_helmholtz_filter_dev": (_i, [_vp, _vp, _vp, _i, _d, _i, _P(SolveInfo)]),
@@ -236,6 +238,45 @@ def _box(b):
     for a in range(3):
         arr[a][0], arr[a][1] = float(b[a][0]), float(b[a][1])
     return arr
+
+
+def nondesign_boxes(nx, ny, nz, boxes, designs_0, lx=None, ly=None, lz=None):
+    """getDesignNonDesignIDs of opt_macro_mma_nondesign.cpp:247-317 on the
+    voxel box: boxes is a list of (value, ((x0, x1), (y0, y1), (z0, z1))); an
+    element whose centroid lies strictly inside a box is non-design and
+    starts at that box's value.  As in the reference, each box adds every
+    element outside it to the design IDs, so with two or more disjoint boxes
+    every element counts in the volume.  Returns (x0, design_ids,
+    nondesign_ids)."""
+    lx = float(nx if lx is None else lx)
+    ly = float(ny if ly is None else ly)
+    lz = float(nz if lz is None else lz)
+    hx, hy, hz = lx / nx, ly / ny, lz / nz
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    # centroid as the mean of the 8 corner coordinates, corner by corner
+    cx = sum(((i + a) * hx) / 8.0 for a in (0, 1, 1, 0, 0, 1, 1, 0)).ravel()
+    cy = sum(((j + b) * hy) / 8.0 for b in (0, 0, 1, 1, 0, 0, 1, 1)).ravel()
+    cz = sum(((k + c) * hz) / 8.0 for c in (0, 0, 0, 0, 1, 1, 1, 1)).ravel()
+    x0 = np.full(nx * ny * nz, float(designs_0))
+    design, nondesign = [], []
+    for value, ((x_0, x_1), (y_0, y_1), (z_0, z_1)) in boxes:
+        inside = (x_0 < cx) & (cx < x_1) & (y_0 < cy) & (cy < y_1) & (z_0 < cz) & (cz < z_1)
+        nondesign.append(np.nonzero(inside)[0])
+        design.append(np.nonzero(~inside)[0])
+        x0[inside] = value
+    if not boxes:
+        design = [np.arange(nx * ny * nz)]
+    d = np.unique(np.concatenate(design)) if design else np.zeros(0, np.int64)
+    nd = np.unique(np.concatenate(nondesign)) if nondesign else np.zeros(0, np.int64)
+    return x0, d.astype(np.int32), nd.astype(np.int32)
+
+
+def design_nondesign_ids(nelx, nondesign_ids):
+    """getDesignNonDesignIDs of src/misc/non_design_domain.hpp:9-53 from
+    element ID lists: (all minus the sorted unique non-design IDs, those IDs)."""
+    nd = np.unique(np.asarray(nondesign_ids, dtype=np.int64))
+    d = np.setdiff1d(np.arange(nelx), nd)
+    return d.astype(np.int32), nd.astype(np.int32)
 
 
 def cantilever_bc(nx, ny, nz, lx=None, ly=None, lz=None, load_node=None, load=(0.0, 0.0, -1.0)):
@@ -528,6 +569,31 @@ class Context:
         info = StepInfo()
         _check(self.lib.icarat_loop_step(self.h, C.byref(info)), "loop_step")
         return info
+
+    def set_load_cases(self, fext_cases):
+        """the load cases of a multi-load loop: an (ncases, numeq) array of
+        icarat_fext-layout vectors; None or an empty array returns to the
+        context's own load"""
+        if fext_cases is None or len(fext_cases) == 0:
+            _check(self.lib.icarat_set_load_cases(self.h, 0, None), "set_load_cases")
+            return
+        F = np.ascontiguousarray(fext_cases, dtype=np.float64)
+        if F.ndim != 2 or F.shape[1] != self.numeq:
+            raise ValueError("load cases must be (ncases, %d)" % self.numeq)
+        _check(self.lib.icarat_set_load_cases(self.h, F.shape[0], F.ctypes.data),
+               "set_load_cases")
+
+    def loop_set_domains(self, design_ids=None, nondesign_ids=()):
+        """volume over design_ids (None: all elements), sensitivities zeroed on
+        nondesign_ids; after loop_init"""
+        nd = np.ascontiguousarray(nondesign_ids, dtype=np.int32)
+        if design_ids is None:
+            dp, dn = None, 0
+        else:
+            d = np.ascontiguousarray(design_ids, dtype=np.int32)
+            dp, dn = d.ctypes.data, d.size
+        _check(self.lib.icarat_loop_set_domains(self.h, dp, dn, nd.ctypes.data if nd.size
+                                                else None, nd.size), "loop_set_domains")
 
     def loop_get(self, which):
         idx = {"x": 0, "xfil": 1, "xthr": 2, "dfds": 3, "dgds": 4}[which]

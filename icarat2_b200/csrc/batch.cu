@@ -936,6 +936,9 @@ int icarat_batch_loop_step(icarat_batch *B, const icarat_batch_opts *opts,
   IREQUIRE(B, ICARAT_ERR_ARG, "null batch");
   ICK(cudaSetDevice(B->device));
   const size_t n = B->ctx.size();
+  for(size_t d = 0; d < n; d++)
+    IREQUIRE(B->ctx[d]->loop.ncases == 0, ICARAT_ERR_UNSUPPORTED,
+             "batch members take one load case each (icarat_loop_step runs several)");
   std::vector<double> beta(n);
   for(size_t d = 0; d < n; d++)
     beta[d] = loop_pre(B->ctx[d]); // filter, design, right-hand side

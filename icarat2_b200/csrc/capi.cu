@@ -29,6 +29,9 @@ void build_rhs(icarat_ctx *c);
 int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0);
 int loop_step(icarat_ctx *c, icarat_step_info *info);
 int loop_get(icarat_ctx *c, int which, double *out);
+int set_load_cases(icarat_ctx *c, int ncases, const double *fext);
+int loop_set_domains(icarat_ctx *c, const int *design_ids, int n_design,
+                     const int *nondesign_ids, int n_nondesign);
 void sensitivity_filter_dev(icarat_ctx *c, const double *s, const double *df,
                             double *out);
 
@@ -606,6 +609,23 @@ int icarat_loop_step(icarat_ctx *c, icarat_step_info *info)
   ICARAT_API_BEGIN
   check_ctx(c);
   return loop_step(c, info);
+  ICARAT_API_END
+}
+
+int icarat_set_load_cases(icarat_ctx *c, int ncases, const double *fext)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  return set_load_cases(c, ncases, fext);
+  ICARAT_API_END
+}
+
+int icarat_loop_set_domains(icarat_ctx *c, const int *design_ids, int n_design,
+                            const int *nondesign_ids, int n_nondesign)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  return loop_set_domains(c, design_ids, n_design, nondesign_ids, n_nondesign);
   ICARAT_API_END
 }
 

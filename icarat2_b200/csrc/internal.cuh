@@ -250,6 +250,11 @@ struct LoopState
          *dfds = nullptr, *dgds = nullptr, *tmp = nullptr, *tmp2 = nullptr,
          *xmin = nullptr, *xmax = nullptr;
   icarat_mma *mma = nullptr;
+  // load cases (ncases x neq, node layout) and design domains
+  int ncases = 0;
+  double *d_cases = nullptr;
+  double *d_volw = nullptr;   // element volume on design IDs, 0 elsewhere
+  uint8_t *d_fixed = nullptr; // 1 on non-design IDs
 };
 
 } // namespace icarat_b200

@@ -62,6 +62,8 @@ void build_rhs(icarat_ctx *c)
 
 static int eb(int n) { return (n + 255) / 256 > 0 ? (n + 255) / 256 : 1; }
 
+void loop_free_domains(icarat_ctx *c);
+
 int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
 {
   IREQUIRE(o->method == 0 || o->method == 1, ICARAT_ERR_ARG, "method must be 0 (OC) or 1 (MMA)");
@@ -83,6 +85,7 @@ int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
   L.opts = *o;
   L.optstep = 0;
   L.V0 = 0.0;
+  loop_free_domains(c);
   if(o->filter_kind == 1)
     helm_setup(c, o->filter_radius);
   else
@@ -140,35 +143,58 @@ double loop_pre(icarat_ctx *c)
   return beta;
 }
 
-// Rest of a design iteration after the solve (status st, info si):
-// compliance, volume, sensitivities, transposed filter and the update.
-int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
-              icarat_step_info *info)
+__global__ void k_add(int n, const double *__restrict__ a, double *__restrict__ b)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+    b[i] += a[i];
+}
+
+// dfds = dgds = 0 on non-design elements (opt_macro_mma_nondesign.cpp:161-166)
+__global__ void k_zero_fixed(int n, const uint8_t *__restrict__ fixed, double *__restrict__ a,
+                             double *__restrict__ b)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+    if(fixed[i])
+    {
+      a[i] = 0.0;
+      b[i] = 0.0;
+    }
+}
+
+// volume of the thresholded design over the design IDs (all elements without
+// domains) and the constraint of this step; sets V0 on the first step
+static double loop_constraint(icarat_ctx *c)
+{
+  LoopState &L = c->loop;
+  const int n = c->nelx;
+  const double *w = L.d_volw;
+  if(!w)
+  {
+    note_launch();
+    k_fill<<<eb(n), 256, 0, c->stream>>>(n, c->vol0, L.tmp);
+    w = L.tmp;
+  }
+  const double vol = device_dot(c, L.xthr, w, n);
+  const bool mma = L.opts.method == 1;
+  if(L.optstep == 1)
+  {
+    L.V0 = vol;
+    return mma ? 0.0 : vol;
+  }
+  return mma ? vol / L.V0 - 1.0 : vol;
+}
+
+// threshold chain rule, transposed filter, non-design zeroing and the OC or
+// MMA update; returns the update's status
+static int loop_finish(icarat_ctx *c, double beta, double constraint, int *usteps)
 {
   LoopState &L = c->loop;
   const int n = c->nelx;
   const icarat_loop_opts &o = L.opts;
-  c->solved = true;
-  c->last_info = si;
-  // objective and constraint
-  const double compliance = compliance_dev(c);
-  note_launch();
-  k_fill<<<eb(n), 256, 0, c->stream>>>(n, c->vol0, L.tmp);
-  const double vol = device_dot(c, L.xthr, L.tmp, n);
-  double constraint;
-  if(L.optstep == 1)
-  {
-    L.V0 = vol;
-    constraint = (o.method == 1) ? 0.0 : vol;
-  }
-  else
-    constraint = (o.method == 1) ? vol / L.V0 - 1.0 : vol;
-  // sensitivities, threshold chain rule, transposed filter
-  sensitivity_dev(c, o.method == 1 ? 1.0 / L.V0 : 1.0, L.dfds, L.dgds);
   note_launch();
   k_mul2<<<eb(n), 256, 0, c->stream>>>(n, L.thrd, L.dfds, L.dgds);
-  // both transposed filters in one pass, into the spare buffers, which then
-  // become the sensitivities
   if(o.filter_kind == 1)
   {
     // densityFilter(dfds / dgds, .., true) (opt_mma_Helmholtz.cpp:150-151)
@@ -177,16 +203,24 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
     IREQUIRE(st1 >= 0 && st2 >= 0, st1 < 0 ? st1 : st2, "Helmholtz filter failed");
   }
   else
+    // both transposed filters in one pass, into the spare buffers
     filter_trans2(c, L.dfds, L.dgds, L.tmp, L.tmp2);
+  // the spare buffers become the sensitivities
   std::swap(L.dfds, L.tmp);
   std::swap(L.dgds, L.tmp2);
-  // update
-  int ust = ICARAT_OK, usteps = 0;
+  if(L.d_fixed)
+  {
+    note_launch();
+    k_zero_fixed<<<eb(n), 256, 0, c->stream>>>(n, L.d_fixed, L.dfds, L.dgds);
+  }
+  ICK(cudaGetLastError());
+  int ust = ICARAT_OK;
+  *usteps = 0;
   if(o.method == 1)
   {
     double g = constraint;
     ust = mma_update_device(L.mma, L.x, L.dfds, &g, L.dgds, L.xmin, L.xmax);
-    usteps = mma_last_newton(L.mma);
+    *usteps = mma_last_newton(L.mma);
   }
   else
   {
@@ -199,13 +233,35 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
       note_launch();
       k_fill<<<eb(n), 256, 0, c->stream>>>(n, c->vol0, c->d_e1);
       ICK(cudaGetLastError());
-      ust = oc_update_helm_dev(c, L.x, L.dfds, L.V0, L.dgds, L.xmin, L.xmax, &oc, &usteps,
+      ust = oc_update_helm_dev(c, L.x, L.dfds, L.V0, L.dgds, L.xmin, L.xmax, &oc, usteps,
                                L.tmp, L.tmp2, c->d_e1);
     }
     else
-      ust = oc_update_dev(c, L.x, L.dfds, L.V0, L.dgds, L.xmin, L.xmax, &oc, &usteps);
+      ust = oc_update_dev(c, L.x, L.dfds, L.V0, L.dgds, L.xmin, L.xmax, &oc, usteps);
   }
   ICK(cudaStreamSynchronize(c->stream));
+  return ust;
+}
+
+static int step_status(int st, int ust)
+{
+  return st < 0 ? st : (ust < 0 ? ust : (st != ICARAT_OK ? st : ust));
+}
+
+// Rest of a design iteration after the solve (status st, info si):
+// compliance, volume, sensitivities, transposed filter and the update.
+int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
+              icarat_step_info *info)
+{
+  LoopState &L = c->loop;
+  const icarat_loop_opts &o = L.opts;
+  c->solved = true;
+  c->last_info = si;
+  const double compliance = compliance_dev(c);
+  const double constraint = loop_constraint(c);
+  sensitivity_dev(c, o.method == 1 ? 1.0 / L.V0 : 1.0, L.dfds, L.dgds);
+  int usteps = 0;
+  const int ust = loop_finish(c, beta, constraint, &usteps);
   if(info)
   {
     info->step = L.optstep;
@@ -216,15 +272,146 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
     info->update_steps = usteps;
     info->status = st != ICARAT_OK ? st : ust;
   }
-  return st < 0 ? st : (ust < 0 ? ust : (st != ICARAT_OK ? st : ust));
+  return step_status(st, ust);
+}
+
+// A design iteration over several load cases (opt_multi_load.cpp:100-200):
+// one solve per case on the same design (the multigrid hierarchy is built
+// once), object_f = sum_lc u_lc . f_lc and dfds = sum_lc -(E'/E) u_lc Ke u_lc
+// accumulated in case order, then the shared tail.  The constraint is the
+// design-domain volume, as in that driver.
+static int loop_step_cases(icarat_ctx *c, double beta, icarat_step_info *info)
+{
+  LoopState &L = c->loop;
+  const int n = c->nelx;
+  const double constraint = loop_constraint(c);
+  double compliance = 0.0, relres = 0.0;
+  int iterations = 0, st = ICARAT_OK;
+  double *own = c->d_fext;
+  try
+  {
+    for(int lc = 0; lc < L.ncases; lc++)
+    {
+      c->d_fext = L.d_cases + (size_t)lc * c->neq;
+      build_rhs(c);
+      icarat_solve_info si{};
+      const int s1 = solve_full(c, &L.opts.solve, c->d_rhs, c->d_u, &si);
+      if(s1 < 0 || (st >= 0 && s1 != ICARAT_OK))
+        st = s1;
+      c->solved = true;
+      c->last_info = si;
+      iterations += si.iterations;
+      relres = relres > si.rel_residual ? relres : si.rel_residual;
+      compliance += compliance_dev(c);
+      // first case into dfds, later cases through the spare buffer
+      sensitivity_dev(c, 1.0 / L.V0, lc == 0 ? L.dfds : L.tmp2, L.dgds);
+      if(lc > 0)
+      {
+        note_launch();
+        k_add<<<eb(n), 256, 0, c->stream>>>(n, L.tmp2, L.dfds);
+        ICK(cudaGetLastError());
+      }
+    }
+  }
+  catch(...)
+  {
+    c->d_fext = own;
+    throw;
+  }
+  c->d_fext = own;
+  int usteps = 0;
+  const int ust = loop_finish(c, beta, constraint, &usteps);
+  if(info)
+  {
+    info->step = L.optstep;
+    info->compliance = compliance;
+    info->constraint = constraint;
+    info->cg_iterations = iterations;
+    info->cg_rel_residual = relres;
+    info->update_steps = usteps;
+    info->status = st != ICARAT_OK ? st : ust;
+  }
+  return step_status(st, ust);
 }
 
 int loop_step(icarat_ctx *c, icarat_step_info *info)
 {
+  const LoopState &L = c->loop;
+  IREQUIRE(!L.init || L.opts.method == 1 || (L.ncases == 0 && !L.d_volw),
+           ICARAT_ERR_UNSUPPORTED,
+           "load cases and design domains take the MMA update (opt_multi_load.cpp, "
+           "opt_macro_mma_nondesign.cpp)");
   const double beta = loop_pre(c);
+  if(c->loop.ncases > 0)
+    return loop_step_cases(c, beta, info);
   icarat_solve_info si{};
   const int st = solve_full(c, &c->loop.opts.solve, c->d_rhs, c->d_u, &si);
   return loop_post(c, st, si, beta, info);
+}
+
+// Load cases of a multi-load loop: ncases x numeq host vectors (the layout of
+// icarat_fext), kept on the device in node layout; ncases = 0 returns to the
+// context's own load.
+int set_load_cases(icarat_ctx *c, int ncases, const double *fext)
+{
+  LoopState &L = c->loop;
+  IREQUIRE(ncases >= 0 && (ncases == 0 || fext), ICARAT_ERR_ARG, "bad load cases");
+  dfree(L.d_cases);
+  L.d_cases = nullptr;
+  L.ncases = 0;
+  if(ncases == 0)
+    return ICARAT_OK;
+  L.d_cases = dalloc((size_t)ncases * c->neq);
+  for(int lc = 0; lc < ncases; lc++)
+    to_full(c, fext + (size_t)lc * c->numeq, L.d_cases + (size_t)lc * c->neq, true);
+  ICK(cudaStreamSynchronize(c->stream));
+  L.ncases = ncases;
+  return ICARAT_OK;
+}
+
+// Design / non-design element IDs of the loop (the pair returned by
+// getDesignNonDesignIDs, non_design_domain.hpp:9-53 and
+// opt_macro_mma_nondesign.cpp:247-317): the volume constraint sums over the
+// design IDs (NULL: every element), sensitivities are zeroed on the
+// non-design IDs after the transposed filter.  Cleared by icarat_loop_init.
+int loop_set_domains(icarat_ctx *c, const int *design_ids, int n_design,
+                     const int *nondesign_ids, int n_nondesign)
+{
+  LoopState &L = c->loop;
+  IREQUIRE(L.init, ICARAT_ERR_STATE, "icarat_loop_init first");
+  IREQUIRE(n_design >= 0 && n_nondesign >= 0 && (n_design == 0 || design_ids) &&
+               (n_nondesign == 0 || nondesign_ids),
+           ICARAT_ERR_ARG, "bad domain lists");
+  const int n = c->nelx;
+  std::vector<double> w(n, design_ids ? 0.0 : c->vol0);
+  for(int q = 0; q < n_design; q++)
+  {
+    IREQUIRE(design_ids[q] >= 0 && design_ids[q] < n, ICARAT_ERR_ARG, "design ID out of range");
+    w[design_ids[q]] = c->vol0;
+  }
+  std::vector<uint8_t> f(n, 0);
+  for(int q = 0; q < n_nondesign; q++)
+  {
+    IREQUIRE(nondesign_ids[q] >= 0 && nondesign_ids[q] < n, ICARAT_ERR_ARG,
+             "non-design ID out of range");
+    f[nondesign_ids[q]] = 1;
+  }
+  if(!L.d_volw)
+    L.d_volw = dalloc(n);
+  if(!L.d_fixed)
+    ICK(cudaMalloc(&L.d_fixed, n));
+  ICK(cudaMemcpy(L.d_volw, w.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  ICK(cudaMemcpy(L.d_fixed, f.data(), n, cudaMemcpyHostToDevice));
+  return ICARAT_OK;
+}
+
+void loop_free_domains(icarat_ctx *c)
+{
+  LoopState &L = c->loop;
+  dfree(L.d_volw);
+  dfree(L.d_fixed);
+  L.d_volw = nullptr;
+  L.d_fixed = nullptr;
 }
 
 int loop_get(icarat_ctx *c, int which, double *out)

@@ -444,6 +444,21 @@ int icarat_loop_init(icarat_ctx *ctx, const icarat_loop_opts *opts,
 int icarat_loop_step(icarat_ctx *ctx, icarat_step_info *info);
 /* which: 0 x, 1 filtered, 2 thresholded, 3 dfds, 4 dgds (nelx each) */
 int icarat_loop_get(icarat_ctx *ctx, int which, double *out);
+/* Load cases (the vector<Force> of opt_multi_load.cpp:68-80): fext holds
+ * ncases load vectors of numeq entries (the layout of icarat_fext), case
+ * after case.  With ncases >= 1 icarat_loop_step solves every case on the
+ * same design and sums the compliances and the sensitivities in case order
+ * (opt_multi_load.cpp:114-174); ncases = 0 returns to the context's own
+ * load.  MMA loops only; batch members take one case. */
+int icarat_set_load_cases(icarat_ctx *ctx, int ncases, const double *fext);
+/* Design / non-design element IDs of the loop (getDesignNonDesignIDs,
+ * src/misc/non_design_domain.hpp:9-53, and its box form in
+ * opt_macro_mma_nondesign.cpp:247-317): the volume constraint sums over
+ * design_ids (NULL: every element), dfds and dgds are zeroed on
+ * nondesign_ids after the transposed filter (:161-166).  Call after
+ * icarat_loop_init, which clears them; MMA loops only. */
+int icarat_loop_set_domains(icarat_ctx *ctx, const int *design_ids, int n_design,
+                            const int *nondesign_ids, int n_nondesign);
 
 #ifdef __cplusplus
 }

@@ -426,6 +426,75 @@ class Loop:
         return out
 
 
+class CaseLoop:
+    """MMA design loop over several load cases with design / non-design
+    element IDs, composed from the primitives above (test infrastructure):
+    the loop body of sample/software/opt-multi-load/opt_multi_load.cpp:100-200
+    (per case: solve, object_f += u.f, dfds += -(E'/E) u Ke u; volume
+    constraint over the design IDs, V0 on step 1) and of
+    sample/algorithm/opt-macro-mma-nondesign/opt_macro_mma_nondesign.cpp:
+    90-178 (threshold, filter^T, sensitivities zeroed on the non-design IDs
+    :161-166, MMA).  problems: one Problem per load case (same mesh and
+    Dirichlet boxes); filt: a radius Filter, or None with helmholtz_R."""
+
+    def __init__(self, problems, filt=None, helmholtz_R=None, x0=0.3, design_ids=None,
+                 nondesign_ids=(), use_threshold=True, move=0.2, xmin=1e-4, xmax=1.0,
+                 cg_tol=1e-12, helmholtz_tol=1e-10):
+        self.P = problems
+        self.F, self.R, self.htol = filt, helmholtz_R, helmholtz_tol
+        n = problems[0].nelx
+        self.x = np.full(n, x0) if np.isscalar(x0) else _f64(x0).copy()
+        self.design = np.arange(n) if design_ids is None else np.asarray(design_ids)
+        self.nondesign = np.asarray(nondesign_ids, dtype=np.int64)
+        self.use_thr, self.cg_tol = use_threshold, cg_tol
+        self.xmin, self.xmax = np.full(n, xmin), np.full(n, xmax)
+        self.mma = MMA(n, 1)
+        self.mma.set_move_limit(move)
+        self.vol = problems[0].ke0()[1]
+        self.optstep, self.V0 = 0, 0.0
+
+    def _filter(self, v, sens):
+        if self.R is not None:
+            P = self.P[0]
+            return helmholtz_filter(P.nx, P.ny, P.nz, self.R, v, is_sens=sens, tol=self.htol,
+                                    lx=self.lx, ly=self.ly, lz=self.lz)[0]
+        return self.F.density_filter(v, sens)
+
+    lx = ly = lz = None
+
+    def step(self):
+        self.optstep += 1
+        xfil = self._filter(self.x, False)
+        beta = min(2.0 ** int(self.optstep / 40), 16.0)
+        if self.use_thr:
+            thr, thrd = threshold(xfil, beta, 0.5), threshold_derivative(xfil, beta, 0.5)
+        else:
+            thr, thrd = xfil.copy(), np.ones_like(xfil)
+        const = 0.0
+        if self.optstep == 1:
+            self.V0 = 0.0
+            for e in self.design:
+                self.V0 += thr[e] * self.vol
+        else:
+            for e in self.design:
+                const += thr[e] * self.vol / self.V0
+            const += -1.0
+        comp, dfds, dgds, its = 0.0, np.zeros_like(xfil), None, 0
+        for P in self.P:
+            val, it, _ = P.solve(thr, tol=self.cg_tol)
+            its += it
+            comp += P.compliance(val)
+            df, dgds = P.sensitivity(thr, P.node_values(val), 1.0 / self.V0)
+            dfds += df
+        dfds, dgds = dfds * thrd, dgds * thrd
+        dfds, dgds = self._filter(dfds, True), self._filter(dgds, True)
+        dfds[self.nondesign] = 0.0
+        dgds[self.nondesign] = 0.0
+        self.x = self.mma.update(self.x, dfds, [const], dgds, self.xmin, self.xmax)
+        self.xfil, self.dfds, self.dgds = xfil, dfds, dgds
+        return comp, const, its
+
+
 def ref_available():
     return os.path.exists(_REFLIB)
 

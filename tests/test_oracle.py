@@ -384,3 +384,43 @@ def test_helmholtz_loop_oracle(oracle):
         for _ in range(3):
             L.step()
         assert L.scalars()["compliance"] < c1
+
+
+def test_case_loop_matches_c_loop(oracle):
+    # the composed multi-case loop with one case and no domains is the C
+    # loop (MMA, threshold on and off)
+    nx, ny, nz = 8, 4, 4
+    for thr in (False, True):
+        P = oracle.Problem(nx, ny, nz)
+        F = oracle.Filter(P, 1.5)
+        L = oracle.Loop(P, F, method="mma", x0=0.3, move=0.2, use_threshold=thr, cg_tol=1e-12)
+        P2 = oracle.Problem(nx, ny, nz)
+        F2 = oracle.Filter(P2, 1.5)
+        M = oracle.CaseLoop([P2], F2, use_threshold=thr)
+        for _ in range(3):
+            L.step()
+            comp, const, _ = M.step()
+            s = L.scalars()
+            assert abs(comp - s["compliance"]) <= 1e-12 * s["compliance"]
+            assert abs(const - s["constraint"]) <= 1e-12
+        assert np.abs(M.x - L.get("x")).max() <= 1e-12
+
+
+def test_case_loop_domains_and_cases(oracle):
+    # zeroed sensitivities stay zero on the non-design IDs, and two load
+    # cases give the sum of the two single-case compliances on step 1
+    nx, ny, nz = 8, 4, 4
+    loads = [[((0.0, 0.0, -1.0), ((nx, nx), (2, 2), (0, 0)))],
+             [((0.0, -1.0, 0.0), ((nx, nx), (4, 4), (4, 4)))]]
+    dirich = [((1, 1, 1), (0.0, 0.0, 0.0), ((0, 0), (0, ny), (0, nz)))]
+    Ps = [oracle.Problem(nx, ny, nz, dirichlet=dirich, loads=l) for l in loads]
+    nd = np.arange(0, 32)
+    M = oracle.CaseLoop(Ps, oracle.Filter(Ps[0], 1.5), nondesign_ids=nd,
+                        design_ids=np.arange(32, Ps[0].nelx))
+    comp, _, _ = M.step()
+    assert not M.dfds[nd].any() and not M.dgds[nd].any()
+    singles = []
+    for l in loads:
+        P = oracle.Problem(nx, ny, nz, dirichlet=dirich, loads=l)
+        singles.append(oracle.CaseLoop([P], oracle.Filter(P, 1.5)).step()[0])
+    assert abs(comp - sum(singles)) <= 1e-12 * comp
