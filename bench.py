@@ -81,6 +81,8 @@ def parse():
                    help="Helmholtz filter radius (element lengths)")
     p.add_argument("--helm-sample", default="128x64x64",
                    help="grid of the oracle's timed Helmholtz call")
+    p.add_argument("--multi-load", type=int, default=1,
+                   help="measure the 3-case multi-load loop (0 skips it)")
     p.add_argument("--cpu-helm", action="store_true",
                    help="(internal) time the oracle's Helmholtz filter and exit")
     return p.parse_args()
@@ -473,6 +475,50 @@ def helmholtz_section(a, G, torch, dev, flush, world, dist):
                           "on %s: %.3f s, %d iterations; scaled to the measured grid by "
                           "node-iterations" % (a.helm_sample, cl["t"], cl["iters"])}
     return out
+
+
+def multi_load_section(a, G, torch, dev, flush, world, dist):
+    """The opt_multi_load loop on the headline grid: 3 point-load cases (tip
+    down, tip sideways at the top edge, tip up at the far edge), Helmholtz
+    filter R = 2, threshold, MMA move 0.2, the headline solver per case."""
+    from icarat2_b200.replicas import job_rate
+
+    nx, ny, nz = grid_of(a)
+    dirich = [((1, 1, 1), (0.0, 0.0, 0.0), ((0, 0), (0, ny), (0, nz)))]
+    cases = [[((0.0, 0.0, -1.0), ((nx, nx), (ny // 2, ny // 2), (0, 0)))],
+             [((0.0, -1.0, 0.0), ((nx, nx), (ny, ny), (nz, nz)))],
+             [((0.0, 0.0, 1.0), ((nx, nx), (0, 0), (nz, nz)))]]
+    F = []
+    for loads in cases:
+        c = G.Context(nx, ny, nz, dirichlet=dirich, loads=loads, device=dev.index)
+        F.append(c.fext())
+        c.close()
+    c = G.Context(nx, ny, nz, dirichlet=dirich, loads=cases[0], device=dev.index)
+    c.loop_init(0.3, method="mma", filter_radius=2.0, move=0.2, use_threshold=True,
+                solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth,
+                                   coarse_lag=a.coarse_lag), filter="helmholtz")
+    c.set_load_cases(np.array(F))
+    st = torch.cuda.ExternalStream(c.stream_ptr(), device=dev)
+    for _ in range(a.warmup):
+        c.loop_step()
+    torch.cuda.synchronize()
+    ms, its = 0.0, []
+    for _ in range(a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        its.append(c.loop_step().cg_iterations)
+        e1.record(st)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        with torch.cuda.stream(st):
+            flush.zero_()
+        torch.cuda.synchronize()
+    v, total = job_rate(ms, a.steps, world, dist, dev)
+    c.close()
+    return {"grid": a.grid, "load_cases": len(cases), "value": v, "unit": "design-iter/s",
+            "ms_per_step": total / a.steps, "cg_iterations_per_step": its,
+            "workload": "opt_multi_load loop: 3 load cases, Helmholtz filter R = 2, "
+                        "threshold, MMA move 0.2, MG-PCG %g per case" % a.rtol}
 
 
 def batch_problems(G, seed=1):
@@ -876,6 +922,9 @@ def gpu_arm(a):
     helm = None
     if a.helm_grid:
         helm = helmholtz_section(a, G, torch, dev, flush, world, dist)
+    multi = None
+    if a.multi_load:
+        multi = multi_load_section(a, G, torch, dev, flush, world, dist)
 
     if rank == 0:
         cg = [i.cg_iterations for i in infos]
@@ -906,6 +955,7 @@ def gpu_arm(a):
             "batched_80_designs": batched,
             "learned": learned,
             "helmholtz_filter": helm,
+            "multi_load": multi,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }
