@@ -150,6 +150,10 @@ SIGNATURES = {
     "icarat_density_filter_dev": (_i, [_vp, _vp, _vp, _i]),
     "icarat_sensitivity_filter": (_i, [_vp, _dp, _dp, _dp]),
     "icarat_set_load_cases": (_i, [_vp, _i, _vp]),
+    "icarat_mises": (_i, [_vp, _dp]),
+    "icarat_mises_dev": (_i, [_vp, _vp]),
+    "icarat_write_vtk": (_i, [_vp, C.c_char_p, _i]),
+    "icarat_write_vtk_arrays": (_i, [C.c_char_p, _i, _i, _i, _i, _d, _d, _d, _vp, _vp, _vp]),
     "icarat_loop_set_domains": (_i, [_vp, _vp, _i, _vp, _i]),
     "icarat_helmholtz_setup": (_i, [_vp, _d]),
     "icarat_helmholtz_filter": (_i, [_vp, _dp, _dp, _i, _d, _i, _P(SolveInfo)]),
@@ -269,6 +273,30 @@ def nondesign_boxes(nx, ny, nz, boxes, designs_0, lx=None, ly=None, lz=None):
     d = np.unique(np.concatenate(design)) if design else np.zeros(0, np.int64)
     nd = np.unique(np.concatenate(nondesign)) if nondesign else np.zeros(0, np.int64)
     return x0, d.astype(np.int32), nd.astype(np.int32)
+
+
+def write_vtk_arrays(path, nx, ny, nz, node_val=None, density=None, mises=None, binary=False,
+                     lx=None, ly=None, lz=None):
+    """icarat_write_vtk_arrays: the VTK writer on host arrays (no GPU work)."""
+    L = load_library()
+    lx = float(nx if lx is None else lx)
+    ly = float(ny if ly is None else ly)
+    lz = float(nz if lz is None else lz)
+    keep = []
+
+    def ptr(a, n):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+        if a.size != n:
+            raise ValueError("array of %d values expected" % n)
+        keep.append(a)
+        return a.ctypes.data
+
+    numnp, nelx = (nx + 1) * (ny + 1) * (nz + 1), nx * ny * nz
+    _check(L.icarat_write_vtk_arrays(os.fsencode(path), 1 if binary else 0, nx, ny, nz, lx, ly,
+                                     lz, ptr(node_val, 3 * numnp), ptr(density, nelx),
+                                     ptr(mises, nelx)), "write_vtk_arrays")
 
 
 def design_nondesign_ids(nelx, nondesign_ids):
@@ -569,6 +597,17 @@ class Context:
         info = StepInfo()
         _check(self.lib.icarat_loop_step(self.h, C.byref(info)), "loop_step")
         return info
+
+    def mises(self):
+        """element von Mises stress of the last solve (nelx)"""
+        out = np.zeros(max(self.nelx, 1))
+        _check(self.lib.icarat_mises(self.h, out), "mises")
+        return out[:self.nelx]
+
+    def write_vtk(self, path, binary=False):
+        """the sample drivers' output(): displacement, density, mises"""
+        _check(self.lib.icarat_write_vtk(self.h, os.fsencode(path), 1 if binary else 0),
+               "write_vtk")
 
     def set_load_cases(self, fext_cases):
         """the load cases of a multi-load loop: an (ncases, numeq) array of

@@ -417,6 +417,57 @@ int icarat_node_values(icarat_ctx *c, double *node_val)
   ICARAT_API_END
 }
 
+int icarat_mises(icarat_ctx *c, double *mises)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(mises, ICARAT_ERR_ARG, "null argument");
+  double *a = stage(c, 0);
+  mises_dev(c, a);
+  d2h(c, mises, a, c->nelx);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_mises_dev(icarat_ctx *c, double *mises)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(mises, ICARAT_ERR_ARG, "null argument");
+  mises_dev(c, mises);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_write_vtk_arrays(const char *path, int binary, int nx, int ny, int nz, double lx,
+                            double ly, double lz, const double *node_val,
+                            const double *density, const double *mises)
+{
+  ICARAT_API_BEGIN
+  write_vtk(path, binary != 0, nx, ny, nz, lx, ly, lz, node_val, density, mises);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_write_vtk(icarat_ctx *c, const char *path, int binary)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(path, ICARAT_ERR_ARG, "null argument");
+  IREQUIRE(c->solved, ICARAT_ERR_STATE, "solve first");
+  std::vector<double> nv((size_t)c->neq), rho((size_t)c->nelx), mis((size_t)c->nelx);
+  node_values_dev(c, c->d_v1);
+  d2h(c, nv.data(), c->d_v1, c->neq);
+  d2h(c, rho.data(), c->d_rho, c->nelx);
+  double *a = stage(c, 0);
+  mises_dev(c, a);
+  d2h(c, mis.data(), a, c->nelx);
+  write_vtk(path, binary != 0, c->nx, c->ny, c->nz, c->lx, c->ly, c->lz, nv.data(),
+            rho.data(), mis.data());
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
 int icarat_compliance(icarat_ctx *c, double *compliance)
 {
   ICARAT_API_BEGIN

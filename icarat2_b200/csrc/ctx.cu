@@ -286,6 +286,7 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     c->neq = 3 * c->numnp;
     c->mat = *mat;
     hexa8_stiffness(c->hx, c->hy, c->hz, mat->poisson, c->ke0.k, &c->vol0);
+    hexa8_stress_operator(c->hx, c->hy, c->hz, mat->poisson, c->sb0.s);
     for(int q = 0; q < 576; q++)
       c->ke0f.k[q] = (float)c->ke0.k[q];
     c->ke_diag_max = 0.0;

@@ -86,6 +86,11 @@ struct KeParamF
 {
   float k[576];
 };
+// Gauss-averaged stress operator at E = 1 (6 x 24, Voigt rows)
+struct StressParam
+{
+  double s[144];
+};
 
 // Structured grid of one level.
 struct GridDev
@@ -269,6 +274,7 @@ struct icarat_ctx
   icarat_material mat;
   icarat_b200::KeParam ke0;
   icarat_b200::KeParamF ke0f; // ke0 rounded to FP32
+  icarat_b200::StressParam sb0; // stress operator at E = 1
   double vol0;
   double ke_diag_max; // max_a Ke0[a][a]
   double lam_max_dk;  // bound on lambda_max(D^-1 K) from the element matrix
@@ -338,6 +344,7 @@ struct icarat_ctx
 namespace icarat_b200
 {
 // ke0.cpp
+void hexa8_stress_operator(double hx, double hy, double hz, double nu, double *s);
 void hexa8_stiffness(double hx, double hy, double hz, double nu, double *ke,
                      double *volume);
 double jacobi_bound(const double *ke);
@@ -448,6 +455,11 @@ void helm_free(icarat_ctx *c);
 
 // sens.cu
 void node_values_dev(icarat_ctx *c, double *d_node_val);
+void mises_dev(icarat_ctx *c, double *d_mises);
+
+// vtk.cu
+void write_vtk(const char *path, bool binary, int nx, int ny, int nz, double lx, double ly,
+               double lz, const double *node_val, const double *density, const double *mises);
 double compliance_dev(icarat_ctx *c);
 void sensitivity_dev(icarat_ctx *c, double dgds_scale, double *d_dfds,
                      double *d_dgds);

@@ -82,6 +82,66 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// von Mises stress of the last solve per element (Elastic::makeMisesStress,
+// src/problem/elasticity.cpp:166-207): sigma = E(rho) S u_e with the
+// Gauss-averaged stress operator S and the truncated nodal values,
+// mises = sqrt(sigma^T V sigma), V = [1 -1/2 -1/2; ..] (+) 3 I on the shears
+__global__ void __launch_bounds__(128)
+    k_mises(GridDev g, StressParam sp, const double *__restrict__ rho,
+            const double *__restrict__ u, const double *__restrict__ uD,
+            const uint8_t *__restrict__ fix, double e1, double e2, double p,
+            double *__restrict__ out)
+{
+  for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelx;
+      e += gridDim.x * blockDim.x)
+  {
+    const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
+    double ue[24];
+#pragma unroll
+    for(int bz = 0; bz < 2; bz++)
+#pragma unroll
+      for(int by = 0; by < 2; by++)
+#pragma unroll
+        for(int bx = 0; bx < 2; bx++)
+        {
+          const int b = local_node(bx, by, bz);
+          const long m = (i + bx) + (long)(j + by) * g.NX + (long)(k + bz) * g.NX * g.NY;
+          const unsigned f = fix[m];
+#pragma unroll
+          for(int q = 0; q < 3; q++)
+            ue[3 * b + q] = node_value(u, uD, f, (long)q * g.numnp + m, q);
+        }
+    const double dens = rho[e];
+    const double young = (1.0 - pow(dens, p)) * e1 + pow(dens, p) * e2;
+    double sg[6];
+#pragma unroll
+    for(int r = 0; r < 6; r++)
+    {
+      double t = 0.0;
+#pragma unroll
+      for(int c = 0; c < 24; c++)
+        t = fma(sp.s[24 * r + c], ue[c], t);
+      sg[r] = young * t;
+    }
+    const double q = sg[0] * (sg[0] - 0.5 * sg[1] - 0.5 * sg[2]) +
+                     sg[1] * (sg[1] - 0.5 * sg[0] - 0.5 * sg[2]) +
+                     sg[2] * (sg[2] - 0.5 * sg[0] - 0.5 * sg[1]) +
+                     3.0 * (sg[3] * sg[3] + sg[4] * sg[4] + sg[5] * sg[5]);
+    out[e] = sqrt(fmax(q, 0.0)); // V is positive semidefinite: q < 0 is rounding
+  }
+}
+
+void mises_dev(icarat_ctx *c, double *out)
+{
+  IREQUIRE(c->solved, ICARAT_ERR_STATE, "Mises stress needs a solve first");
+  GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
+  note_launch();
+  k_mises<<<(c->nelx + 127) / 128, 128, 0, c->stream>>>(g, c->sb0, c->d_rho, c->d_u, c->d_uD,
+                                                        c->d_fix, c->mat.young_min,
+                                                        c->mat.young_max, c->mat.penalty, out);
+  ICK(cudaGetLastError());
+}
+
 void node_values_dev(icarat_ctx *c, double *out)
 {
   note_launch();

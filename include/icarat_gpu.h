@@ -187,6 +187,23 @@ int icarat_solve_rhs(icarat_ctx *ctx, const icarat_solve_opts *opts,
 /* node.val after divideValIntoNode (analysis_utility.hpp:9-31): numnp x 3,
    prescribed values on constrained DOFs, |v| < 1e-15 -> 0 */
 int icarat_node_values(icarat_ctx *ctx, double *node_val);
+/* element von Mises stress of the last solve (Elastic::makeMisesStress,
+   src/problem/elasticity.cpp:166-207: Gauss-averaged De B u_e of the
+   truncated nodal values, sqrt(sigma^T V sigma)); nelx values */
+int icarat_mises(icarat_ctx *ctx, double *mises);
+int icarat_mises_dev(icarat_ctx *ctx, double *mises);
+/* Legacy VTK file of the box as the sample drivers' output()
+   (opt_macro_mma_nondesign.cpp:220-242 with src/io/export_vtk.hpp): points,
+   hexa8 cells, point vectors "displacement" (node values of the last solve),
+   cell scalars "density" (the element design) and "mises".  binary = 0
+   writes the reference's ASCII format byte for byte, 1 the same sections as
+   legacy BINARY (big-endian float32 / int32). */
+int icarat_write_vtk(icarat_ctx *ctx, const char *path, int binary);
+/* The same writer on host arrays (no device work): node_val numnp x 3,
+   density and mises nelx each; any of the three may be NULL (omitted). */
+int icarat_write_vtk_arrays(const char *path, int binary, int nx, int ny, int nz,
+                            double lx, double ly, double lz, const double *node_val,
+                            const double *density, const double *mises);
 /* object_f = value.val . fext (opt_macro_oc.cpp:110) of the last solve */
 int icarat_compliance(icarat_ctx *ctx, double *compliance);
 /* driver sensitivity() (opt_macro_oc.cpp:182-212): dfds = -(dE/E) u_e^T Ke

@@ -495,6 +495,94 @@ class CaseLoop:
         return comp, const, its
 
 
+def hexa8_gauss_B(h):
+    """Voigt B (6 x 24) at the 8 Gauss points of an h[0] x h[1] x h[2] voxel
+    (src/basis/bmatrix.hpp:125-140 with shape_function.cpp:422-447 and the
+    Gauss8Cubic order of gauss_integration.cpp:268-289), and det J."""
+    corner = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1),
+              (0, 1, 1)]
+    g = 1.0 / np.sqrt(3.0)
+    Bs = []
+    for sx, sy, sz in [(-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1), (-1, -1, 1),
+                       (1, -1, 1), (1, 1, 1), (-1, 1, 1)]:
+        r = np.array([sx, sy, sz]) * g
+        B = np.zeros((6, 24))
+        for a, c in enumerate(corner):
+            s = [1.0 if v else -1.0 for v in c]
+            f = [1 + s[d] * r[d] for d in range(3)]
+            dx = 0.125 * s[0] * f[1] * f[2] * 2.0 / h[0]
+            dy = 0.125 * s[1] * f[0] * f[2] * 2.0 / h[1]
+            dz = 0.125 * s[2] * f[0] * f[1] * 2.0 / h[2]
+            B[0, 3 * a], B[1, 3 * a + 1], B[2, 3 * a + 2] = dx, dy, dz
+            B[3, 3 * a], B[3, 3 * a + 1] = dy, dx
+            B[4, 3 * a + 1], B[4, 3 * a + 2] = dz, dy
+            B[5, 3 * a], B[5, 3 * a + 2] = dz, dx
+        Bs.append(B)
+    return Bs
+
+
+def mises(P, design_s, node_val, lx=None, ly=None, lz=None):
+    """Elastic::makeMisesStress (src/problem/elasticity.cpp:166-207) per
+    element: stress = sum_ip De B(ip) u_e / ipmax with De of E(rho) (SIMP)
+    and the truncated nodal values, mises = sqrt(stress^T V stress)."""
+    h = [(lx or P.nx) / P.nx, (ly or P.ny) / P.ny, (lz or P.nz) / P.nz]
+    Bs = hexa8_gauss_B(h)
+    nu = P.nu
+    lam = nu / ((1 + nu) * (1 - 2 * nu))
+    mu = 1.0 / (2 * (1 + nu))
+    D0 = np.zeros((6, 6))
+    D0[:3, :3] = lam
+    D0[[0, 1, 2], [0, 1, 2]] = lam + 2 * mu
+    D0[[3, 4, 5], [3, 4, 5]] = mu
+    V = np.array([[1, -.5, -.5, 0, 0, 0], [-.5, 1, -.5, 0, 0, 0], [-.5, -.5, 1, 0, 0, 0],
+                  [0, 0, 0, 3, 0, 0], [0, 0, 0, 0, 3, 0], [0, 0, 0, 0, 0, 3]])
+    conn = P.conn()
+    nv = np.asarray(node_val).reshape(-1, 3)
+    rho = np.asarray(design_s)
+    E = (1 - rho ** P.penal) * P.E1 + rho ** P.penal * P.E2
+    out = np.zeros(P.nelx)
+    for e in range(P.nelx):
+        ue = nv[conn[e]].ravel()
+        st = sum((E[e] * D0) @ (B @ ue) for B in Bs) / 8.0
+        out[e] = np.sqrt(max(st @ V @ st, 0.0))
+    return out
+
+
+def vtk_ascii(nx, ny, nz, node_val=None, density=None, mises=None, lx=None, ly=None, lz=None):
+    """The bytes the reference's sample output() writes for the box
+    (src/io/export_vtk.hpp: makeHeaderVTK :47-53, setPointVTK :67-79,
+    setElementVTK :82-101, setElementTypeVTK :104-112, addPointVectorVTK
+    :134-151, addElementScalarVTK :153-170); numbers through an ostream's
+    default formatting, which is printf %g."""
+    lx = float(nx if lx is None else lx)
+    ly = float(ny if ly is None else ly)
+    lz = float(nz if lz is None else lz)
+    xyz = np.zeros(3 * (nx + 1) * (ny + 1) * (nz + 1))
+    conn = np.zeros(8 * nx * ny * nz, np.int32)
+    lib.or_mesh_box(nx, ny, nz, lx, ly, lz, xyz, conn)
+    xyz, conn = xyz.reshape(-1, 3), conn.reshape(-1, 8)
+    out = ["# vtk DataFile Version 4.1\nvtk output\nASCII\nDATASET UNSTRUCTURED_GRID\n"]
+    out.append("\nPOINTS\t%d\tfloat\n" % len(xyz))
+    out += ["".join("%g\t" % v for v in p) + "\n" for p in xyz]
+    out.append("\nCELLS %d\t%d\n" % (len(conn), 9 * len(conn)))
+    out += ["8\t" + "".join("%d\t" % v for v in c) + "\n" for c in conn]
+    out.append("\nCELL_TYPES\t%d\n" % len(conn))
+    out += ["12\n"] * len(conn)
+    if node_val is not None:
+        out.append("\nPOINT_DATA\t%d\nVECTORS displacement float\n" % len(xyz))
+        out += ["".join("%g\t" % v for v in p) + "\n" for p in np.asarray(node_val).reshape(-1, 3)]
+    first = True
+    for name, f in (("density", density), ("mises", mises)):
+        if f is None:
+            continue
+        if first:
+            out.append("\nCELL_DATA\t%d\n" % len(conn))
+            first = False
+        out.append("SCALARS %s float\nLOOKUP_TABLE default\n" % name)
+        out += ["%g\n" % v for v in f]
+    return "".join(out).encode()
+
+
 def ref_available():
     return os.path.exists(_REFLIB)
 
