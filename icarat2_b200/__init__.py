@@ -153,6 +153,7 @@ SIGNATURES = {
     "icarat_mises": (_i, [_vp, _dp]),
     "icarat_mises_dev": (_i, [_vp, _vp]),
     "icarat_write_vtk": (_i, [_vp, C.c_char_p, _i]),
+    "icarat_voxelize": (_i, [_i, _dp, _i, _i, _i, _i, _dp, _dp, _vp]),
     "icarat_write_vtk_arrays": (_i, [C.c_char_p, _i, _i, _i, _i, _d, _d, _d, _vp, _vp, _vp]),
     "icarat_loop_set_domains": (_i, [_vp, _vp, _i, _vp, _i]),
     "icarat_helmholtz_setup": (_i, [_vp, _d]),
@@ -297,6 +298,49 @@ def write_vtk_arrays(path, nx, ny, nz, node_val=None, density=None, mises=None, 
     _check(L.icarat_write_vtk_arrays(os.fsencode(path), 1 if binary else 0, nx, ny, nz, lx, ly,
                                      lz, ptr(node_val, 3 * numnp), ptr(density, nelx),
                                      ptr(mises, nelx)), "write_vtk_arrays")
+
+
+def read_stl(path):
+    """Triangles of a binary or ASCII STL file as an (ntri, 9) float64 array
+    (three xyz vertices per row)."""
+    data = open(path, "rb").read()
+    if len(data) >= 84:
+        n = int(np.frombuffer(data[80:84], "<u4")[0])
+        if len(data) == 84 + 50 * n:
+            rec = np.frombuffer(data[84:], np.dtype([("n", "<f4", 3), ("v", "<f4", 9),
+                                                     ("a", "<u2")]), count=n)
+            return rec["v"].astype(np.float64)
+    verts = [list(map(float, ln.split()[1:4])) for ln in data.decode(errors="replace").splitlines()
+             if ln.strip().startswith("vertex")]
+    if not verts or len(verts) % 3:
+        raise ValueError("%s: not an STL file" % path)
+    return np.array(verts, dtype=np.float64).reshape(-1, 9)
+
+
+def voxelize(tri, dims, origin, pitch, device=0):
+    """icarat_voxelize: inside (1) / outside (0) of the closed surface tri
+    for the voxel centres of the grid; flat uint8 array, x fastest."""
+    L = load_library()
+    tri = np.ascontiguousarray(tri, dtype=np.float64).reshape(-1, 9)
+    nx, ny, nz = (int(v) for v in dims)
+    mask = np.zeros(nx * ny * nz, np.uint8)
+    _check(L.icarat_voxelize(device, tri.ravel(), tri.shape[0], nx, ny, nz,
+                             _f64(origin), _f64(pitch), mask.ctypes.data), "voxelize")
+    return mask
+
+
+def voxelize_stl(stl, mesh_size=100, cubic=False, device=0):
+    """The grid of scripts/stl_to_vtk_voxel.py: mesh_size cells per axis over
+    the surface's bounding box, pitch (max - min) / mesh_size per axis
+    ("rect") or the largest extent / mesh_size on every axis ("cubic"); stl
+    is a path or an (ntri, 9) array.  Returns (mask, dims, origin, pitch)."""
+    tri = read_stl(stl) if isinstance(stl, (str, bytes, os.PathLike)) else np.asarray(stl)
+    v = tri.reshape(-1, 3)
+    lo, hi = v.min(axis=0), v.max(axis=0)
+    ext = hi - lo
+    pitch = np.full(3, ext.max() / mesh_size) if cubic else ext / mesh_size
+    dims = (mesh_size, mesh_size, mesh_size)
+    return voxelize(tri, dims, lo, pitch, device), dims, lo, pitch
 
 
 def design_nondesign_ids(nelx, nondesign_ids):

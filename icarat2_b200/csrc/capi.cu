@@ -449,6 +449,15 @@ int icarat_write_vtk_arrays(const char *path, int binary, int nx, int ny, int nz
   ICARAT_API_END
 }
 
+int icarat_voxelize(int device, const double *tri, int ntri, int nx, int ny, int nz,
+                    const double *origin, const double *pitch, unsigned char *mask)
+{
+  ICARAT_API_BEGIN
+  voxelize(device, tri, ntri, nx, ny, nz, origin, pitch, mask);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
 int icarat_write_vtk(icarat_ctx *c, const char *path, int binary)
 {
   ICARAT_API_BEGIN

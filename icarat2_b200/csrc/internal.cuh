@@ -457,6 +457,10 @@ void helm_free(icarat_ctx *c);
 void node_values_dev(icarat_ctx *c, double *d_node_val);
 void mises_dev(icarat_ctx *c, double *d_mises);
 
+// voxel.cu
+void voxelize(int device, const double *tri, int ntri, int nx, int ny, int nz,
+              const double *origin, const double *pitch, uint8_t *mask);
+
 // vtk.cu
 void write_vtk(const char *path, bool binary, int nx, int ny, int nz, double lx, double ly,
                double lz, const double *node_val, const double *density, const double *mises);

@@ -204,6 +204,15 @@ int icarat_write_vtk(icarat_ctx *ctx, const char *path, int binary);
 int icarat_write_vtk_arrays(const char *path, int binary, int nx, int ny, int nz,
                             double lx, double ly, double lz, const double *node_val,
                             const double *density, const double *mises);
+/* STL surface -> voxel design domain (the job of scripts/stl_to_vtk_voxel.py,
+   vtkSelectEnclosedPoints on the voxel centres): mask[i + nx (j + ny k)] = 1
+   when the centre origin + (i+1/2, j+1/2, k+1/2) * pitch lies inside the
+   closed surface of ntri triangles (tri: 9 doubles each, three xyz
+   vertices), by ray parity along +z on the GPU.  mask is a host array of
+   nx ny nz bytes.  More than 256 crossings of one voxel column return
+   ICARAT_ERR_UNSUPPORTED. */
+int icarat_voxelize(int device, const double *tri, int ntri, int nx, int ny, int nz,
+                    const double *origin, const double *pitch, unsigned char *mask);
 /* object_f = value.val . fext (opt_macro_oc.cpp:110) of the last solve */
 int icarat_compliance(icarat_ctx *ctx, double *compliance);
 /* driver sensitivity() (opt_macro_oc.cpp:182-212): dfds = -(dE/E) u_e^T Ke

@@ -583,6 +583,52 @@ def vtk_ascii(nx, ny, nz, node_val=None, density=None, mises=None, lx=None, ly=N
     return "".join(out).encode()
 
 
+def voxelize(tri, dims, origin, pitch):
+    """Ray-parity voxelisation along +z (test infrastructure, the algorithm of
+    the library's voxel.cu restated in numpy): per column centre, crossings
+    with counter-clockwise-normalised projected triangles under a top-left
+    rule, edge functions from the smaller endpoint; odd crossings below a
+    centre = inside."""
+    tri = np.asarray(tri, dtype=np.float64).reshape(-1, 3, 3)
+    nx, ny, nz = dims
+    ox, oy, oz = origin
+    px, py, pz = pitch
+
+    def efn(ax, ay, bx, by, x, y):
+        return (bx - ax) * (y - ay) - (by - ay) * (x - ax)
+
+    def canon(ax, ay, bx, by, x, y):
+        sw = (bx < ax) | ((bx == ax) & (by < ay))
+        return np.where(sw, -efn(bx, by, ax, ay, x, y), efn(ax, ay, bx, by, x, y))
+
+    def tl(ax, ay, bx, by):
+        return ((ay == by) & (bx < ax)) | (by < ay)
+
+    a, b, c = tri[:, 0].copy(), tri[:, 1].copy(), tri[:, 2].copy()
+    area = efn(a[:, 0], a[:, 1], b[:, 0], b[:, 1], c[:, 0], c[:, 1])
+    keep = area != 0
+    a, b, c, area = a[keep], b[keep], c[keep], area[keep]
+    neg = area < 0
+    b[neg], c[neg] = c[neg].copy(), b[neg].copy()
+    area = np.abs(area)
+    t0, t1, t2 = tl(b[:, 0], b[:, 1], c[:, 0], c[:, 1]), tl(c[:, 0], c[:, 1], a[:, 0], a[:, 1]), \
+        tl(a[:, 0], a[:, 1], b[:, 0], b[:, 1])
+    zc = oz + (np.arange(nz) + 0.5) * pz
+    mask = np.zeros((nz, ny, nx), np.uint8)
+    for j in range(ny):
+        for i in range(nx):
+            x, y = ox + (i + 0.5) * px, oy + (j + 0.5) * py
+            w0 = canon(b[:, 0], b[:, 1], c[:, 0], c[:, 1], x, y)
+            w1 = canon(c[:, 0], c[:, 1], a[:, 0], a[:, 1], x, y)
+            w2 = canon(a[:, 0], a[:, 1], b[:, 0], b[:, 1], x, y)
+            ins = ((w0 > 0) | ((w0 == 0) & t0)) & ((w1 > 0) | ((w1 == 0) & t1)) & \
+                  ((w2 > 0) | ((w2 == 0) & t2))
+            z = (w0 * a[:, 2] + w1 * b[:, 2] + w2 * c[:, 2])[ins] / area[ins]
+            below = np.searchsorted(np.sort(z), zc, side="left")
+            mask[:, j, i] = below & 1
+    return mask.ravel()
+
+
 def ref_available():
     return os.path.exists(_REFLIB)
 
