@@ -521,6 +521,30 @@ def multi_load_section(a, G, torch, dev, flush, world, dist):
                         "threshold, MMA move 0.2, MG-PCG %g per case" % a.rtol}
 
 
+def voxel_section(a, G, dev):
+    """STL -> voxel design domain: a UV sphere of 2 x 256 x 128 triangles
+    voxelised on a 256^3 grid over its bounding box, host arrays in and out
+    (one blocking call, wall clock over 5 calls after a warm-up)."""
+    nu, nv = 256, 128
+    u = np.linspace(0, 2 * np.pi, nu, endpoint=False)
+    w = np.linspace(0, np.pi, nv + 1)
+    P = np.stack([np.outer(np.sin(w), np.cos(u)), np.outer(np.sin(w), np.sin(u)),
+                  np.outer(np.cos(w), np.ones(nu))], -1)  # (nv+1, nu, 3)
+    a00, a01 = P[:-1, :], np.roll(P[:-1, :], -1, axis=1)
+    a10, a11 = P[1:, :], np.roll(P[1:, :], -1, axis=1)
+    tri = np.concatenate([np.concatenate([a00, a10, a11], -1).reshape(-1, 9),
+                          np.concatenate([a00, a11, a01], -1).reshape(-1, 9)])
+    G.voxelize_stl(tri, 64, device=dev.index)
+    ts = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        mask, dims, lo, pitch = G.voxelize_stl(tri, 256, device=dev.index)
+        ts.append(time.perf_counter() - t0)
+    return {"triangles": int(tri.shape[0]), "grid": "256^3", "ms_per_call": 1e3 * min(ts),
+            "inside_fraction": float(mask.mean()),
+            "timing": "host wall clock of the blocking call (triangles in, 16.8 MB mask out)"}
+
+
 def batch_problems(G, seed=1):
     """64 cantilevers 64x32x32 and 16 of nx in {32, 48, 64, 80, 96} (2:1:1,
     cycled); load node uniform over the right-face nodes, volume fraction
@@ -925,6 +949,7 @@ def gpu_arm(a):
     multi = None
     if a.multi_load:
         multi = multi_load_section(a, G, torch, dev, flush, world, dist)
+    vox = voxel_section(a, G, dev) if a.multi_load else None
 
     if rank == 0:
         cg = [i.cg_iterations for i in infos]
@@ -956,6 +981,7 @@ def gpu_arm(a):
             "learned": learned,
             "helmholtz_filter": helm,
             "multi_load": multi,
+            "voxelize": vox,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }
