@@ -136,6 +136,79 @@ void set_design_device(icarat_ctx *c, const double *d_rho)
   c->design_version++;
 }
 
+
+// hexa8 faces as SurfaceLoad numbers them (sides 1..6,
+// boundary_condition_base.cpp:313-336): local nodes of each face
+static const int kFaceNodes[7][4] = {{0, 0, 0, 0}, {0, 1, 2, 3}, {3, 0, 4, 7}, {0, 1, 5, 4},
+                                     {1, 2, 6, 5}, {2, 3, 7, 6}, {4, 5, 6, 7}};
+
+// SurfaceLoad::judgeLine for hexa8 (:58-76): the face from the local index k
+// of the 4th node inside the load box and the local indices found so far;
+// as there, nodes 4,5,6,7 give side 2 (hits[2] - hits[1] == 1 is tested
+// first)
+static int judge_face(int k, const int *hits)
+{
+  if(k == 3)
+    return 1;
+  if(k == 5)
+    return 3;
+  if(k == 6)
+    return 4;
+  if(hits[2] - hits[1] == 1)
+    return 2;
+  if(hits[1] - hits[0] == 1)
+    return 5;
+  return 6;
+}
+
+// equivalent nodal forces of a uniform traction val on a quad4 face X
+// (SurfaceLoad::generate :143-187 with snmatrix2d, nmatrix_surface.hpp:60-89):
+// fe = sum over the 2 x 2 Gauss points of N^T val |dX/dr1 x dX/dr2|
+static void face_load(const double X[4][3], const double *val, double fe[12])
+{
+  const double g = 1.0 / std::sqrt(3.0);
+  const double pts[4][2] = {{-g, -g}, {g, -g}, {-g, g}, {g, g}};
+  for(int i = 0; i < 12; i++)
+    fe[i] = 0.0;
+  for(int ip = 0; ip < 4; ip++)
+  {
+    const double r0 = pts[ip][0], r1 = pts[ip][1];
+    const double N[4] = {0.25 * (1.0 - r0) * (1.0 - r1), 0.25 * (1.0 + r0) * (1.0 - r1),
+                         0.25 * (1.0 + r0) * (1.0 + r1), 0.25 * (1.0 - r0) * (1.0 + r1)};
+    const double dN[2][4] = {{-0.25 * (1.0 - r1), 0.25 * (1.0 - r1), 0.25 * (1.0 + r1),
+                              -0.25 * (1.0 + r1)},
+                             {-0.25 * (1.0 - r0), -0.25 * (1.0 + r0), 0.25 * (1.0 + r0),
+                              0.25 * (1.0 - r0)}};
+    double J[2][3];
+    for(int a = 0; a < 2; a++)
+      for(int d = 0; d < 3; d++)
+      {
+        double t = 0.0;
+        for(int n = 0; n < 4; n++)
+          t += dN[a][n] * X[n][d];
+        J[a][d] = t;
+      }
+    const double cx = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+    const double cy = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+    const double cz = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    const double jac = std::sqrt(cx * cx + cy * cy + cz * cz) * 1.0;
+    for(int n = 0; n < 4; n++)
+      for(int d = 0; d < 3; d++)
+        fe[3 * n + d] += (N[n] * val[d]) * jac;
+  }
+}
+
+// global node numbers of element e in the mesher's local order
+static void element_nodes(const icarat_ctx *c, long e, long en[8])
+{
+  const long NX = c->NX, NY = c->NY;
+  const long i = e % c->nx, j = (e / c->nx) % c->ny, k = e / ((long)c->nx * c->ny);
+  const long b = NX * NY * k + NX * j + i;
+  const long o[8] = {0, 1, 1 + NX, NX, NX * NY, 1 + NX * NY, 1 + NX + NX * NY, NX + NX * NY};
+  for(int a = 0; a < 8; a++)
+    en[a] = b + o[a];
+}
+
 // Mesh + BC on the host, mirroring MeshIcarat/BCIcarat:
 //  node coordinates x = (L / div) * index (mesh_icarat.hpp:468-476);
 //  Dirichlet boxes widened by 1e-7, flags kept once 1, values overwritten
@@ -219,27 +292,58 @@ static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
           if(c->uD_h[3 * n + q] != 0.0)
             c->has_uD = true;
         }
-  // point loads
+  // Neumann loads in input order (generateLoadMain,
+  // boundary_condition_icarat.hpp:271-410)
   c->fext_h.assign(c->numeq, 0.0);
   for(int l = 0; l < (bc ? bc->n_loads : 0); l++)
   {
     const icarat_load &L = bc->loads[l];
-    IREQUIRE(L.box[0][0] == L.box[0][1] && L.box[1][0] == L.box[1][1] &&
-                 L.box[2][0] == L.box[2][1],
-             ICARAT_ERR_UNSUPPORTED,
-             "only point loads (degenerate neumann boxes) are supported");
-    for(long n = 0; n < c->numnp; n++)
+    auto inside = [&](long n) {
+      const double x = coord(n, 0), y = coord(n, 1), z = coord(n, 2);
+      return L.box[0][0] - tol <= x && x <= L.box[0][1] + tol && L.box[1][0] - tol <= y &&
+             y <= L.box[1][1] + tol && L.box[2][0] - tol <= z && z <= L.box[2][1] + tol;
+    };
+    if(L.box[0][0] == L.box[0][1] && L.box[1][0] == L.box[1][1] && L.box[2][0] == L.box[2][1])
     {
-      double x = coord(n, 0), y = coord(n, 1), z = coord(n, 2);
-      if(L.box[0][0] - tol <= x && x <= L.box[0][1] + tol &&
-         L.box[1][0] - tol <= y && y <= L.box[1][1] + tol &&
-         L.box[2][0] - tol <= z && z <= L.box[2][1] + tol)
-        for(int q = 0; q < 3; q++)
-        {
-          int d = c->dof[3 * n + q];
-          if(d < c->numeq)
-            c->fext_h[d] += L.val[q];
-        }
+      // point load (:380-396)
+      for(long n = 0; n < c->numnp; n++)
+        if(inside(n))
+          for(int q = 0; q < 3; q++)
+          {
+            int d = c->dof[3 * n + q];
+            if(d < c->numeq)
+              c->fext_h[d] += L.val[q];
+          }
+      continue;
+    }
+    // distributed load (:336-378): the face of each element found by its
+    // nodes inside the box, equivalent nodal forces of the traction L.val
+    for(long e = 0; e < c->nelx; e++)
+    {
+      long en[8];
+      element_nodes(c, e, en);
+      int hits[8], count = 0;
+      for(int k = 0; k < 8; k++)
+      {
+        if(!inside(en[k]))
+          continue;
+        hits[count++] = k;
+        if(count != 4)
+          continue;
+        const int *fn = kFaceNodes[judge_face(k, hits)];
+        double X[4][3], fe[12];
+        for(int i = 0; i < 4; i++)
+          for(int d = 0; d < 3; d++)
+            X[i][d] = coord(en[fn[i]], d);
+        face_load(X, L.val, fe);
+        for(int i = 0; i < 4; i++)
+          for(int q = 0; q < 3; q++)
+          {
+            int d = c->dof[3 * en[fn[i]] + q];
+            if(d < c->numeq)
+              c->fext_h[d] += fe[3 * i + q];
+          }
+      }
     }
   }
 }

@@ -62,8 +62,12 @@ typedef struct
   double box[3][2];
 } icarat_dirichlet;
 
-/* one [boundary_condition] neumann entry; only degenerate (point) boxes are
-   supported (boundary_condition_icarat.hpp:231-239, 380-396) */
+/* one [boundary_condition] neumann entry (boundary_condition_icarat.hpp:
+   213-264): a box degenerate in all three ranges is a point load (val added
+   to every node inside, :380-396); any other box is a distributed load, the
+   traction val integrated over the face of each element that has 4 nodes
+   inside the box (:336-378, SurfaceLoad in boundary_condition_base.cpp:
+   16-187, including its face choice: nodes 4-7 select the x-min face). */
 typedef struct
 {
   double val[3];

@@ -173,36 +173,131 @@ int or_count_dof(int numnp, const double *xyz, int ndir, const int *dflag,
 }
 
 /* ------------------------------------------------------------------------ */
-/* 3. Point loads: BCIcarat::input_neumann (boundary_condition_icarat.hpp:   */
+/* 3. Neumann loads: BCIcarat::input_neumann (boundary_condition_icarat.hpp: */
 /*    213-264) marks a box whose three ranges are all degenerate as a point   */
-/*    load; generateLoadMain's point branch (:380-396) adds val[c] to        */
-/*    fext_org[dof] of every free component of every node inside the box     */
-/*    widened by 1e-7.  Distributed (non-degenerate) loads are not covered.  */
+/*    load, anything else as distributed; both are widened by 1e-7.          */
+/*    generateLoadMain (:271-410), loads in input order:                     */
+/*    point (:380-396): val[c] to fext_org[dof] of every free component of   */
+/*    every node inside the box;                                            */
+/*    distributed (:336-378): per element, nodes tested in local order; when */
+/*    the 4th one inside is found at local index k, SurfaceLoad::judgeLine   */
+/*    (boundary_condition_base.cpp:58-76) picks the face from k and the hit  */
+/*    list, resizeSurfaceParameter (:313-336) its 4 nodes, and generate       */
+/*    (:143-187) adds fe = sum_ip N^T val |dX/dr1 x dX/dr2| over the 2 x 2    */
+/*    Gauss points of the quad4 face (snmatrix2d, nmatrix_surface.hpp:60-89; */
+/*    Gauss4Square gauss_integration.cpp:72-88; ShapeFunction4Square        */
+/*    shape_function.cpp:97-119) to the face nodes' free components.  As in */
+/*    the reference, hits at local nodes 4,5,6,7 (the z-max face) select     */
+/*    face 2 (nodes 3,0,4,7): judgeLine tests hitpoints[2] - hitpoints[1]    */
+/*    == 1 first.                                                            */
 /* ------------------------------------------------------------------------ */
-int or_point_loads(int numnp, const double *xyz, const int *dof, int numeq,
-                   int nload, const double *lval, const double *lbox,
+static const int or_face_nodes[7][4] = {{0, 0, 0, 0}, {0, 1, 2, 3}, {3, 0, 4, 7}, {0, 1, 5, 4},
+                                        {1, 2, 6, 5}, {2, 3, 7, 6}, {4, 5, 6, 7}};
+
+static int or_judge_face(int counter, const int *hits)
+{
+  if(counter == 3)
+    return 1;
+  if(counter == 5)
+    return 3;
+  if(counter == 6)
+    return 4;
+  if(hits[2] - hits[1] == 1)
+    return 2;
+  if(hits[1] - hits[0] == 1)
+    return 5;
+  return 6;
+}
+
+static void or_surface_fe(const double X[4][3], const double *val, double fe[12])
+{
+  const double g = 1.0 / sqrt(3.0);
+  const double pts[4][2] = {{-g, -g}, {g, -g}, {-g, g}, {g, g}};
+  for(int i = 0; i < 12; i++)
+    fe[i] = 0.0;
+  for(int ip = 0; ip < 4; ip++)
+  {
+    const double r0 = pts[ip][0], r1 = pts[ip][1];
+    const double N[4] = {0.25 * (1.0 - r0) * (1.0 - r1), 0.25 * (1.0 + r0) * (1.0 - r1),
+                         0.25 * (1.0 + r0) * (1.0 + r1), 0.25 * (1.0 - r0) * (1.0 + r1)};
+    const double dN[2][4] = {{-0.25 * (1.0 - r1), 0.25 * (1.0 - r1), 0.25 * (1.0 + r1),
+                              -0.25 * (1.0 + r1)},
+                             {-0.25 * (1.0 - r0), -0.25 * (1.0 + r0), 0.25 * (1.0 + r0),
+                              0.25 * (1.0 - r0)}};
+    double J[2][3];
+    for(int a = 0; a < 2; a++)
+      for(int d = 0; d < 3; d++)
+      {
+        double t = 0.0;
+        for(int n = 0; n < 4; n++)
+          t += dN[a][n] * X[n][d];
+        J[a][d] = t;
+      }
+    const double cx = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+    const double cy = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+    const double cz = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    const double jac = sqrt(cx * cx + cy * cy + cz * cz) * 1.0;
+    for(int n = 0; n < 4; n++)
+      for(int d = 0; d < 3; d++)
+        fe[3 * n + d] += (N[n] * val[d]) * jac;
+  }
+}
+
+int or_point_loads(int numnp, const double *xyz, const int *dof, int numeq, int nelx,
+                   const int *conn, int nload, const double *lval, const double *lbox,
                    double *fext)
 {
   const double tol = 1.0e-7;
+  (void)numnp;
   for(int i = 0; i < numeq; i++)
     fext[i] = 0.0;
   for(int l = 0; l < nload; l++)
   {
     const double *b = lbox + 6 * l;
-    if(!(b[0] == b[1] && b[2] == b[3] && b[4] == b[5]))
-      return OR_ERR_UNSUPPORTED;
-    for(int n = 0; n < numnp; n++)
+    const double *v = lval + 3 * l;
+#define OR_IN_BOX(x)                                                                         \
+  (b[0] - tol <= (x)[0] && (x)[0] <= b[1] + tol && b[2] - tol <= (x)[1] &&                   \
+   (x)[1] <= b[3] + tol && b[4] - tol <= (x)[2] && (x)[2] <= b[5] + tol)
+    if(b[0] == b[1] && b[2] == b[3] && b[4] == b[5])
     {
-      const double *x = xyz + 3 * n;
-      if(b[0] - tol <= x[0] && x[0] <= b[1] + tol && b[2] - tol <= x[1] &&
-         x[1] <= b[3] + tol && b[4] - tol <= x[2] && x[2] <= b[5] + tol)
-        for(int c = 0; c < 3; c++)
-        {
-          int d = dof[3 * n + c];
-          if(d < numeq)
-            fext[d] += lval[3 * l + c];
-        }
+      for(int n = 0; n < numnp; n++)
+        if(OR_IN_BOX(xyz + 3 * n))
+          for(int c = 0; c < 3; c++)
+          {
+            int d = dof[3 * n + c];
+            if(d < numeq)
+              fext[d] += v[c];
+          }
+      continue;
     }
+    for(long e = 0; e < nelx; e++)
+    {
+      const int *ce = conn + 8 * e;
+      int hits[8], count = 0;
+      for(int k = 0; k < 8; k++)
+      {
+        if(!OR_IN_BOX(xyz + 3 * (long)ce[k]))
+          continue;
+        hits[count++] = k;
+        if(count == 4)
+        {
+          const int *fn = or_face_nodes[or_judge_face(k, hits)];
+          double X[4][3], fe[12];
+          for(int i = 0; i < 4; i++)
+            for(int d = 0; d < 3; d++)
+              X[i][d] = xyz[3 * (long)ce[fn[i]] + d];
+          or_surface_fe(X, v, fe);
+          for(int i = 0; i < 4; i++)
+            for(int c = 0; c < 3; c++)
+            {
+              int d = dof[3 * (long)ce[fn[i]] + c];
+              if(d < numeq)
+                fext[d] += fe[3 * i + c];
+            }
+        }
+      }
+    }
+#undef OR_IN_BOX
   }
   return OR_OK;
 }
@@ -452,7 +547,7 @@ or_problem *or_problem_create(int nx, int ny, int nz, double lx, double ly,
       P->node_dval[i] = 0.0;
   P->fext = (double *)calloc(P->numeq > 0 ? P->numeq : 1, sizeof(double));
   P->fint = (double *)calloc(P->numeq > 0 ? P->numeq : 1, sizeof(double));
-  int st = or_point_loads(P->numnp, P->xyz, P->dof, P->numeq, nload, lval,
+  int st = or_point_loads(P->numnp, P->xyz, P->dof, P->numeq, P->nelx, P->conn, nload, lval,
                           lbox, P->fext);
   if(st != OR_OK)
   {

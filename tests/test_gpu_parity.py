@@ -53,10 +53,27 @@ def test_element_matrix_bit_exact(oracle, gpu):
     assert np.array_equal(a, b) and va == vb
 
 
-def test_unsupported_distributed_load(gpu):
-    with pytest.raises(gpu.IcaratError) as e:
-        gpu.Context(4, 2, 2, dirichlet=[], loads=[((0, 0, -1.0), ((4, 4), (0, 2), (0, 2)))])
-    assert e.value.status == gpu.ERR_UNSUPPORTED
+DIST_LOADS = [
+    ("xmax face", (7.0, 3.0, 5.0), ((0.0, 0.0, -1.0), ((7, 7), (0, 3), (0, 5)))),
+    ("zmin face", (7.0, 3.0, 5.0), ((0.0, 0.5, -1.0), ((0, 7), (0, 3), (0, 0)))),
+    ("zmax face", (7.0, 3.0, 5.0), ((1.0, 0.0, 0.0), ((0, 7), (0, 3), (5, 5)))),
+    ("ymin patch", (7.0, 3.0, 5.0), ((0.0, 0.0, -2.0), ((2, 5), (0, 0), (1, 4)))),
+    ("ymax face", (7.0, 3.0, 5.0), ((0.0, -1.0, 0.0), ((0, 7), (3, 3), (0, 5)))),
+    ("thick box", (7.0, 3.0, 5.0), ((0.3, -0.2, 1.0), ((1, 4.5), (0, 2), (0, 2.5)))),
+    ("xmax stretched", (3.5, 3.0, 7.5), ((0.0, 0.0, -1.0), ((3.5, 3.5), (0, 3), (0, 7.5)))),
+]
+
+
+@pytest.mark.parametrize("name,lengths,load", DIST_LOADS, ids=[d[0] for d in DIST_LOADS])
+def test_distributed_loads_bit_exact(oracle, gpu, name, lengths, load):
+    """distributed Neumann boxes (generateLoadMain, SurfaceLoad) followed by a
+    point load, on a 7 x 3 x 5 box"""
+    lx, ly, lz = lengths
+    d = [((1, 1, 1), (0.0, 0.0, 0.0), ((0, 0), (0, ly), (0, lz)))]
+    loads = [load, ((0.0, 0.0, -1.0), ((lx, lx), (1.2, 1.2), (0, 0)))]
+    P, G = pair(oracle, gpu, 7, 3, 5, lx=lx, ly=ly, lz=lz, dirichlet=d, loads=loads)
+    assert np.array_equal(P.fext(), G.fext())
+    assert np.count_nonzero(G.fext()) > 4
 
 
 # ------------------------------------------------------------------ K u

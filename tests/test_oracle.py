@@ -424,3 +424,23 @@ def test_case_loop_domains_and_cases(oracle):
         P = oracle.Problem(nx, ny, nz, dirichlet=dirich, loads=l)
         singles.append(oracle.CaseLoop([P], oracle.Filter(P, 1.5)).step()[0])
     assert abs(comp - sum(singles)) <= 1e-12 * comp
+
+
+def test_distributed_load_totals(oracle):
+    # a traction on a whole free face sums to traction x area (Gauss rule
+    # exact for the bilinear face); a z-max box goes to the x-min faces of
+    # the top elements as SurfaceLoad::judgeLine picks them
+    nx, ny, nz = 6, 4, 3
+    free = [((1, 1, 1), (0.0, 0.0, 0.0), ((0, 0), (0, 0), (0, 0)))]  # one corner node
+    P = oracle.Problem(nx, ny, nz, lx=3.0, ly=2.0, lz=6.0, dirichlet=free,
+                       loads=[((0.0, 0.0, -2.0), ((3, 3), (0, 2), (0, 6)))])
+    assert abs(P.fext().sum() + 2.0 * 2.0 * 6.0) < 1e-12
+    P = oracle.Problem(nx, ny, nz, dirichlet=free,
+                       loads=[((0.0, 0.0, 1.0), ((0, nx), (0, ny), (nz, nz)))])
+    f = P.fext()
+    assert abs(f.sum() - nx * ny * 1.0) < 1e-12  # 24 unit x-min faces of the top layer
+    # the x-min face of a top element spans z = nz - 1 .. nz: the layer below
+    # the loaded face receives half of the load
+    d, z = P.dof(), P.xyz()[:, 2]
+    below = [d[n, 2] for n in range(P.numnp) if z[n] == nz - 1 and d[n, 2] < P.numeq]
+    assert abs(f[below].sum() - nx * ny * 0.5) < 1e-12
