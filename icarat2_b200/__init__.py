@@ -687,7 +687,15 @@ class Context:
 
 # ---- reference-named mirrors ------------------------------------------------------
 _SOLVER_NAMES = {"Eigen_CG": JACOBI_PCG, "Scaling_CG": JACOBI_PCG, "MG_CG": MG_PCG,
-                 "Mixed_MG_CG": MIXED_IR}
+                 "Mixed_MG_CG": MIXED_IR,
+                 # the reference's other names (Solvers::solve, solvers.cpp:27-61):
+                 # plain CG as Jacobi-PCG, the other preconditioned Krylov
+                 # solvers as MG-PCG (same solution to the tolerance, other
+                 # iteration counts), the direct solvers as MG-PCG to 1e-12
+                 "CG": JACOBI_PCG, "ICCG": MG_PCG, "Eigen_ICCG": MG_PCG,
+                 "Eigen_BiCGSTAB": MG_PCG, "Eigen_SparseLU": MG_PCG, "Eigen_LDLT": MG_PCG,
+                 "Pardiso_LDLT": MG_PCG, "Pardiso_LLT": MG_PCG, "Pardiso_LU": MG_PCG}
+_DIRECT_NAMES = ("Eigen_SparseLU", "Eigen_LDLT", "Pardiso_LDLT", "Pardiso_LLT", "Pardiso_LU")
 
 
 class LinearAnalysis:
@@ -704,7 +712,8 @@ class LinearAnalysis:
         if solvName not in _SOLVER_NAMES:
             # Solvers::solve exits on an unknown name (solvers.cpp:56-60)
             raise IcaratError(ERR_UNSUPPORTED, "Solver type name is wrong: %s" % solvName)
-        o = solve_opts(_SOLVER_NAMES[solvName], self.rtol, self.maxit, self.mg_levels,
+        rtol = min(self.rtol, 1e-12) if solvName in _DIRECT_NAMES else self.rtol
+        o = solve_opts(_SOLVER_NAMES[solvName], rtol, self.maxit, self.mg_levels,
                        self.mg_smooth)
         self.val, self.info = self.ctx.solve(o)
         if log:
@@ -747,9 +756,6 @@ class FilterHelmholtz:
         if solvName not in _SOLVER_NAMES:
             # Solvers::solve exits on an unknown name (solvers.cpp:56-60)
             raise IcaratError(ERR_UNSUPPORTED, "Solver type name is wrong: %s" % solvName)
-        if _SOLVER_NAMES[solvName] != JACOBI_PCG:
-            raise IcaratError(ERR_UNSUPPORTED, "the Helmholtz system is solved by Jacobi-PCG "
-                              "(Eigen_CG / Scaling_CG), not %s" % solvName)
         out, self.info = self.ctx.helmholtz_filter(design_s, is_sens=sensFlag)
         if log == 1:
             print("Helmholtz filtering...")

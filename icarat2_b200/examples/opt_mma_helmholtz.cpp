@@ -5,7 +5,8 @@
 // constraint, sensitivity times the threshold derivative, the two
 // sensitivity calls of the Helmholtz filter, MMA.
 //
-// usage: opt_mma_helmholtz <nx> <ny> <nz> <steps> <radius> [MG_CG|Eigen_CG]
+// usage: opt_mma_helmholtz <nx> <ny> <nz> <steps> <radius> [solver name]
+// (default "Eigen_LDLT", the reference driver's choice at :99)
 // prints "step <k> <compliance> <constraint> <cg iterations>" per iteration.
 #include <algorithm>
 #include <cmath>
@@ -22,13 +23,13 @@ int main(int argc, char **argv)
 {
   if(argc < 6)
   {
-    std::printf("usage: %s nx ny nz steps radius [MG_CG|Eigen_CG]\n", argv[0]);
+    std::printf("usage: %s nx ny nz steps radius [solver name]\n", argv[0]);
     return 1;
   }
   const int nx = std::atoi(argv[1]), ny = std::atoi(argv[2]), nz = std::atoi(argv[3]);
   const int steps = std::atoi(argv[4]);
   const double filterR = std::atof(argv[5]);
-  const std::string solver = argc > 6 ? argv[6] : "MG_CG";
+  const std::string solver = argc > 6 ? argv[6] : "Eigen_LDLT";
   try
   {
     // x = 0 face clamped, unit load at (nx, ny/2, 0)

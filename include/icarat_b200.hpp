@@ -92,17 +92,29 @@ class LinearAnalysis
 {
 public:
   explicit LinearAnalysis(Model &m) : m_(m), val(m.numeq) {}
-  // solvName: "Eigen_CG" / "Scaling_CG" (Jacobi-PCG), "MG_CG" (multigrid) or
-  // "Mixed_MG_CG" (FP32 multigrid-PCG refined by FP64 residuals)
+  // solvName: "Eigen_CG" / "Scaling_CG" / "CG" (Jacobi-PCG), "MG_CG"
+  // (multigrid), "Mixed_MG_CG" (FP32 multigrid-PCG refined by FP64
+  // residuals); the reference's other names (Solvers::solve,
+  // solvers.cpp:27-61) run multigrid-PCG: "ICCG", "Eigen_ICCG",
+  // "Eigen_BiCGSTAB" at tol, the direct "Eigen_SparseLU", "Eigen_LDLT",
+  // "Pardiso_*" to 1e-12
   void solve(const std::string &solvName, bool log)
   {
     icarat_solve_opts o{ICARAT_SOLVER_JACOBI_PCG, tol, maxIter, mg_levels, mg_smooth, 0, 0.0};
-    if(solvName == "MG_CG")
+    static const char *direct[] = {"Eigen_SparseLU", "Eigen_LDLT", "Pardiso_LDLT",
+                                   "Pardiso_LLT", "Pardiso_LU"};
+    bool is_direct = false;
+    for(const char *d : direct)
+      is_direct = is_direct || solvName == d;
+    if(solvName == "MG_CG" || solvName == "ICCG" || solvName == "Eigen_ICCG" ||
+       solvName == "Eigen_BiCGSTAB" || is_direct)
       o.method = ICARAT_SOLVER_MG_PCG;
     else if(solvName == "Mixed_MG_CG")
       o.method = ICARAT_SOLVER_MIXED_IR;
-    else if(solvName != "Eigen_CG" && solvName != "Scaling_CG")
+    else if(solvName != "Eigen_CG" && solvName != "Scaling_CG" && solvName != "CG")
       throw Error(ICARAT_ERR_UNSUPPORTED, "Solver type name is wrong: " + solvName);
+    if(is_direct && o.rtol > 1e-12)
+      o.rtol = 1e-12;
     check(icarat_solve(m_.ctx(), &o, val.data(), &info), "LinearAnalysis::solve");
     if(log)
       printf("iteration: %d\nresidual: %g\n", info.iterations, info.rel_residual);
@@ -184,8 +196,9 @@ private:
 };
 
 // FilterHelmholtz<E,N> (src/optimization/filter_helm.hpp:16-65): the nodal
-// Helmholtz system solved on the GPU by Jacobi-PCG ("Eigen_CG" and
-// "Scaling_CG"; other solver names are rejected), CG tolerance 1e-10
+// Helmholtz system solved on the GPU by Jacobi-PCG to 1e-10 for any of the
+// reference's solver names (a well-conditioned mass + diffusion system: the
+// name selects nothing else); unknown names throw as Solvers::solve exits
 class FilterHelmholtz
 {
 public:
@@ -196,9 +209,14 @@ public:
   std::vector<double> densityFilter(const std::vector<double> &design_s,
                                     const std::string &solvName, int log, bool sensFlag)
   {
-    if(solvName != "Eigen_CG" && solvName != "Scaling_CG")
-      throw Error(ICARAT_ERR_UNSUPPORTED,
-                  "FilterHelmholtz: solver " + solvName + " is not offered");
+    static const char *names[] = {"Eigen_CG", "Scaling_CG", "CG", "ICCG", "Eigen_ICCG",
+                                  "Eigen_BiCGSTAB", "Eigen_SparseLU", "Eigen_LDLT",
+                                  "Pardiso_LDLT", "Pardiso_LLT", "Pardiso_LU"};
+    bool known = false;
+    for(const char *nm : names)
+      known = known || solvName == nm;
+    if(!known)
+      throw Error(ICARAT_ERR_UNSUPPORTED, "Solver type name is wrong: " + solvName);
     std::vector<double> out(m_.nelx);
     icarat_solve_info info{};
     check(icarat_helmholtz_filter(m_.ctx(), design_s.data(), out.data(), sensFlag ? 1 : 0,

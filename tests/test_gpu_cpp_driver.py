@@ -39,9 +39,31 @@ def test_cpp_driver_rejects_unknown_solver():
     if not os.path.exists(EXE):
         from icarat2_b200 import build
         build.build()
-    out = subprocess.run([EXE, "4", "2", "2", "1", "1.5", "mma", "Eigen_LDLT"],
+    out = subprocess.run([EXE, "4", "2", "2", "1", "1.5", "mma", "No_Such_Solver"],
                          capture_output=True, text=True, timeout=120)
     assert out.returncode == 2 and "Solver type name is wrong" in out.stdout
+
+
+def test_cpp_driver_direct_solver_names(oracle):
+    """the reference's direct solver names ("Eigen_LDLT", opt_mma_Helmholtz.cpp:99)
+    run multigrid-PCG to 1e-12: the trajectory matches the oracle's loop"""
+    if not os.path.exists(EXE):
+        from icarat2_b200 import build
+        build.build()
+    nx, ny, nz, steps = 16, 8, 8, 3
+    for name in ("Eigen_LDLT", "Eigen_SparseLU", "Eigen_ICCG"):
+        out = subprocess.run([EXE, str(nx), str(ny), str(nz), str(steps), "1.5", "mma", name],
+                             capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stdout + out.stderr
+        comp = [float(l.split()[2]) for l in out.stdout.splitlines() if l.startswith("step")]
+        P = oracle.Problem(nx, ny, nz)
+        L = oracle.Loop(P, oracle.Filter(P, 1.5), method="mma", x0=0.3, move=0.2,
+                        cg_tol=1e-12)
+        ref = []
+        for _ in range(steps):
+            L.step()
+            ref.append(L.scalars()["compliance"])
+        assert np.allclose(comp, ref, rtol=1e-9, atol=0)
 
 
 def test_cpp_helmholtz_driver_trajectory(oracle):
