@@ -92,7 +92,7 @@ class OcOpts(C.Structure):
     _fields_ = [("move", C.c_double), ("iota", C.c_double), ("lambda_min", C.c_double),
                 ("lambda_max", C.c_double), ("lambda_eps", C.c_double),
                 ("maxiter", C.c_int), ("use_threshold", C.c_int), ("beta", C.c_double),
-                ("T", C.c_double)]
+                ("T", C.c_double), ("filter_kind", C.c_int)]
 
 
 class LoopOpts(C.Structure):
@@ -584,10 +584,14 @@ class Context:
 
     def oc_update(self, x, dfdx, g, dgdx, xmin, xmax, move=0.15, iota=0.5,
                   lambda_min=0.0, lambda_max=1.0e4, lambda_eps=1.0e-5, maxiter=100,
-                  use_threshold=False, beta=1.0, T=0.5):
+                  use_threshold=False, beta=1.0, T=0.5, filter="radius"):
+        """OC::UpdateVariables with the drivers' volume functor over the
+        context's radius filter or (filter="helmholtz") its Helmholtz filter"""
+        if filter not in ("radius", "helmholtz"):
+            raise ValueError("filter must be 'radius' or 'helmholtz'")
         x = _f64(x).copy()
         o = OcOpts(move, iota, lambda_min, lambda_max, lambda_eps, maxiter,
-                   1 if use_threshold else 0, beta, T)
+                   1 if use_threshold else 0, beta, T, 1 if filter == "helmholtz" else 0)
         steps = C.c_int()
         _check(self.lib.icarat_oc_update(self.h, x, _f64(dfdx), g, _f64(dgdx), _f64(xmin),
                                          _f64(xmax), C.byref(o), C.byref(steps)),
@@ -772,12 +776,14 @@ class FilterHelmholtz:
 
 class OC:
     """OC (OCSolver.hpp:13-80); the volume functor is the drivers' filtered
-    volume, evaluated on the GPU with the context's filter."""
+    volume, evaluated on the GPU with the context's radius filter or, with
+    filter="helmholtz", its Helmholtz filter (opt_macro_oc.cpp:153-164)."""
 
-    def __init__(self, ctx, use_threshold=False, beta=1.0, T=0.5):
+    def __init__(self, ctx, use_threshold=False, beta=1.0, T=0.5, filter="radius"):
         self.ctx = ctx
         self.movelimit = 0.15
         self.use_threshold, self.beta, self.T = use_threshold, beta, T
+        self.filter = filter
         self.steps = 0
 
     def setMoveLimit(self, m):
@@ -787,7 +793,7 @@ class OC:
         x, self.steps = self.ctx.oc_update(xk, dfdx, g, dgdx, xmin, xmax,
                                            move=self.movelimit,
                                            use_threshold=self.use_threshold,
-                                           beta=self.beta, T=self.T)
+                                           beta=self.beta, T=self.T, filter=self.filter)
         xk[:] = x
         return xk
 

@@ -620,7 +620,7 @@ int icarat_threshold_derivative(icarat_ctx *c, const double *in, double beta, do
   ICARAT_API_END
 }
 
-static const icarat_oc_opts kDefaultOc = {0.15, 0.5, 0.0, 1.0e4, 1.0e-5, 100, 0, 1.0, 0.5};
+static const icarat_oc_opts kDefaultOc = {0.15, 0.5, 0.0, 1.0e4, 1.0e-5, 100, 0, 1.0, 0.5, 0};
 
 int icarat_oc_update(icarat_ctx *c, double *x, const double *dfdx, double g,
                      const double *dgdx, const double *xmin, const double *xmax,

@@ -477,7 +477,7 @@ void helm_free(icarat_ctx *c)
   if(H.exec)
     cudaGraphExecDestroy(H.exec);
   for(double *p : {H.d_coef, H.d_invd, H.d_F, H.d_val, H.d_r, H.d_z, H.d_p, H.d_Ap,
-                   H.d_partials})
+                   H.d_partials, H.d_oc})
     dfree(p);
   dfree(H.d_cg);
   H = HelmState{};
@@ -503,6 +503,7 @@ void helm_setup(icarat_ctx *c, double R)
   H.d_p = dalloc(n);
   H.d_Ap = dalloc(n);
   H.d_partials = dalloc((size_t)kMaxRedBlocks * 2);
+  H.d_oc = dalloc(3 * (size_t)c->nelx);
   ICK(cudaMalloc(&H.d_cg, sizeof(CgScalars)));
   ICK(cudaMemsetAsync(H.d_cg, 0, sizeof(CgScalars), c->stream));
   note_launch();

@@ -241,6 +241,7 @@ struct HelmState
          *d_z = nullptr, *d_p = nullptr, *d_Ap = nullptr, *d_partials = nullptr;
   CgScalars *d_cg = nullptr;
   cudaGraphExec_t exec = nullptr; // kHelmChunk iterations
+  double *d_oc = nullptr;         // 3 nelx: work of the OC volume functor
 };
 
 struct MmaDev;

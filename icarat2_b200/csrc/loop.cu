@@ -224,7 +224,7 @@ static int loop_finish(icarat_ctx *c, double beta, double constraint, int *ustep
   }
   else
   {
-    icarat_oc_opts oc{o.move, 0.5, 0.0, 1.0e4, 1.0e-5, 100, o.use_threshold, beta, o.T};
+    icarat_oc_opts oc{o.move, 0.5, 0.0, 1.0e4, 1.0e-5, 100, o.use_threshold, beta, o.T, 0};
     if(o.filter_kind == 1)
     {
       // after the swap L.tmp / L.tmp2 hold the unfiltered sensitivities, no

@@ -120,6 +120,12 @@ __global__ void k_oc_trial(OcArgs a, double lambda)
     a.xk[e] = oc_trial(a, e, lambda);
 }
 
+__global__ void k_oc_fill(int n, double v, double *__restrict__ out)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = v;
+}
+
 // x <- last trial (zeros when no step ran, like the reference's xkp1)
 __global__ void k_oc_finish(int n, const double *__restrict__ xk, int steps,
                             double *__restrict__ x)
@@ -133,6 +139,22 @@ int oc_update_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
                   const double *dgdx, const double *xmin, const double *xmax,
                   const icarat_oc_opts *o, int *steps)
 {
+  IREQUIRE(o->filter_kind == 0 || o->filter_kind == 1, ICARAT_ERR_ARG,
+           "filter_kind must be 0 (radius) or 1 (Helmholtz)");
+  if(o->filter_kind == 1)
+  {
+    // the Helmholtz functor of opt_macro_oc.cpp:153-164 on the set-up's
+    // work vectors: filtered trial, thresholded trial, element volumes
+    HelmState &H = c->helm;
+    IREQUIRE(H.d_oc != nullptr, ICARAT_ERR_STATE,
+             "the OC volume functor needs icarat_helmholtz_setup");
+    const int n = c->nelx;
+    note_launch();
+    k_oc_fill<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->vol0, H.d_oc + 2L * n);
+    ICK(cudaGetLastError());
+    return oc_update_helm_dev(c, x, dfdx, g, dgdx, xmin, xmax, o, steps, H.d_oc, H.d_oc + n,
+                              H.d_oc + 2L * n);
+  }
   IREQUIRE(c->filt.d_w != nullptr, ICARAT_ERR_STATE,
            "the OC volume functor needs icarat_filter_setup");
   IREQUIRE(c->filt.radius >= 1.0e-10, ICARAT_ERR_FILTER,

@@ -258,10 +258,12 @@ public:
   void UpdateVariables(std::vector<double> &xk, std::vector<double> &dfdx, double g,
                        std::vector<double> &dgdx, std::vector<double> &xmin,
                        std::vector<double> &xmax, bool useThreshold = false,
-                       double beta = 1.0, double T = 0.5)
+                       double beta = 1.0, double T = 0.5, bool helmholtz = false)
   {
+    // helmholtz: the volume functor filters by FilterHelmholtz, as
+    // opt_macro_oc.cpp:153-164 does
     icarat_oc_opts o{movelimit, 0.5, 0.0, 1.0e4, 1.0e-5, 100, useThreshold ? 1 : 0,
-                     beta, T};
+                     beta, T, helmholtz ? 1 : 0};
     int steps = 0;
     check(icarat_oc_update(m_.ctx(), xk.data(), dfdx.data(), g, dgdx.data(), xmin.data(),
                            xmax.data(), &o, &steps),

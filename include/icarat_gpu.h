@@ -134,13 +134,16 @@ typedef struct
 
 /* OC::UpdateVariables parameters (OCSolver.hpp:73-79) and the volume functor
    of the sample drivers: g(x) = sum_i thr(filter(x))_i v_i
-   (opt_macro_oc.cpp:153-164), thr only when use_threshold != 0. */
+   (opt_macro_oc.cpp:153-164), thr only when use_threshold != 0; filter is
+   the radius filter of icarat_filter_setup (filter_kind 0) or the Helmholtz
+   filter of icarat_helmholtz_setup (1, as opt_macro_oc.cpp:158). */
 typedef struct
 {
   double move, iota, lambda_min, lambda_max, lambda_eps;
   int maxiter;
   int use_threshold;
   double beta, T;
+  int filter_kind;
 } icarat_oc_opts;
 
 /* ---- library ---------------------------------------------------------- */

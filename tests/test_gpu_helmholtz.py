@@ -159,3 +159,38 @@ def test_helmholtz_loop_matches_oracle(oracle, gpu, method, R, thr):
         assert abs(info.constraint - s["constraint"]) <= 1e-7 * max(1.0, abs(s["constraint"]))
     for which in ("xfil", "x", "dfds", "dgds"):
         assert rel(G.loop_get(which), L.get(which)) <= 1e-6, which
+
+
+@pytest.mark.parametrize("use_thr", [False, True])
+def test_oc_update_with_helmholtz_functor(oracle, gpu, use_thr):
+    """OC::UpdateVariables with the volume functor of opt_macro_oc.cpp:153-164
+    over the Helmholtz filter (icarat_oc_update, filter_kind 1) against the
+    oracle's OC with that functor built from its Helmholtz restatement (both
+    filters' CGs at the reference's 1e-10): same bisection steps, x to 1e-8."""
+    nx, ny, nz, R = 10, 5, 5, 1.0
+    G = gpu.Context(nx, ny, nz)
+    G.helmholtz_setup(R)
+    rng = np.random.default_rng(31)
+    n = G.nelx
+    x = rng.uniform(0.2, 0.6, n)
+    dfdx = -rng.uniform(0.1, 2.0, n)
+    dgdx = np.full(n, 1.0)
+    xmin, xmax = np.full(n, 1e-4), np.ones(n)
+    vol = G.element_stiffness()[1]
+    beta, T = 2.0, 0.5
+    g0 = 0.35 * n * vol
+
+    def volume(xk):
+        f, _ = oracle.helmholtz_filter(nx, ny, nz, R, xk, tol=1e-10)
+        t = oracle.threshold(f, beta, T) if use_thr else f
+        return float(np.sum(t * vol))
+
+    ref, steps_ref = oracle.oc_update(x, dfdx, g0, dgdx, xmin, xmax, volume)
+    got, steps = G.oc_update(x, dfdx, g0, dgdx, xmin, xmax, use_threshold=use_thr, beta=beta,
+                             T=T, filter="helmholtz")
+    assert steps == steps_ref
+    assert np.abs(got - ref).max() <= 1e-8
+    with pytest.raises(gpu.IcaratError) as e:
+        gpu.Context(4, 2, 2).oc_update(x[:16], dfdx[:16], 1.0, dgdx[:16], xmin[:16],
+                                       xmax[:16], filter="helmholtz")
+    assert e.value.status == gpu.ERR_STATE
