@@ -66,7 +66,8 @@ def test_cpp_driver_direct_solver_names(oracle):
         assert np.allclose(comp, ref, rtol=1e-9, atol=0)
 
 
-def test_cpp_helmholtz_driver_trajectory(oracle):
+@pytest.mark.parametrize("method", ["mma", "oc"])
+def test_cpp_helmholtz_driver_trajectory(oracle, method):
     """examples/opt_mma_helmholtz.cpp (the opt_mma_Helmholtz.cpp loop through
     FilterHelmholtz of include/icarat_b200.hpp) against the oracle's loop with
     the Helmholtz filter (MMA, threshold; both Helmholtz CGs at the reference's
@@ -76,14 +77,14 @@ def test_cpp_helmholtz_driver_trajectory(oracle):
         from icarat2_b200 import build
         build.build()
     nx, ny, nz, steps, R = 16, 8, 8, 4, 2.0
-    out = subprocess.run([exe, str(nx), str(ny), str(nz), str(steps), str(R), "MG_CG"],
+    out = subprocess.run([exe, str(nx), str(ny), str(nz), str(steps), str(R), "MG_CG", method],
                          capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     comp = [float(l.split()[2]) for l in out.stdout.splitlines() if l.startswith("step")]
     assert len(comp) == steps
     P = oracle.Problem(nx, ny, nz)
-    L = oracle.Loop(P, None, method="mma", x0=0.3, move=0.2, use_threshold=True,
-                    cg_tol=1e-12, helmholtz_R=R)
+    L = oracle.Loop(P, None, method=method, x0=0.3, move=0.2 if method == "mma" else 0.15,
+                    use_threshold=True, cg_tol=1e-12, helmholtz_R=R)
     ref = []
     for _ in range(steps):
         L.step()
