@@ -391,9 +391,10 @@ def helmholtz_section(a, G, torch, dev, flush, world, dist):
     ms_call = total / a.steps
     it = sum(its) / len(its)
     # per node and CG iteration: K p (read p, write Ap: 16 B), the Jacobi
-    # update (read x p r Ap invd, write x r z: 64 B), p = z + beta p (24 B);
-    # per call: right-hand side, CG start and readout
-    bytes_call = numnp * (104.0 * it + 8 + 48 + 8) + 16.0 * nelx
+    # update (read x p r Ap, write x r: 48 B; the diagonal comes from the node
+    # class), p = D^-1 r + beta p (read r p, write p: 24 B); per call:
+    # right-hand side, CG start and readout
+    bytes_call = numnp * (88.0 * it + 8 + 48 + 8) + 16.0 * nelx
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -451,7 +452,7 @@ def helmholtz_section(a, G, torch, dev, flush, world, dist):
                    "d2h_bytes_per_step": 8 * nelx, "host_memory": "pinned",
                    "matches_device_call": ok},
            "roofline": {"bound": "hbm", "kernel": "Jacobi-PCG iteration (k_helm_spmv, "
-                        "k_cg_update_jacobi, k_cg_pupdate) + rhs/readout",
+                        "k_helm_update, k_helm_pupdate) + rhs/readout",
                         "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                         "bytes_per_call": bytes_call},

@@ -17,7 +17,7 @@
 // (ascending element id) for the Jacobi diagonal; the solve runs
 // matrix-free with the same operator in sum-factorised form (k_helm_spmv).
 // The CG iteration
-// reuses the device-resident scalar kernels of the elasticity solve (one
+// keeps the device-resident scalar logic of the elasticity solve (one
 // stop-flag read per graph replay of `kHelmChunk` iterations).
 #include <cmath>
 
@@ -26,20 +26,12 @@
 namespace icarat_b200
 {
 
-// the generic CG kernels of pcg.cu
+// the CG start of pcg.cu
 __global__ void k_cg_init(int n, const double *__restrict__ b,
                           const double *__restrict__ invd, double *__restrict__ x,
                           double *__restrict__ r, double *__restrict__ z,
                           double *__restrict__ p, double *__restrict__ partials,
                           CgScalars *s, double tol, int maxit, int jacobi);
-__global__ void k_cg_update_jacobi(int n, const double *__restrict__ invd,
-                                   double *__restrict__ x, double *__restrict__ r,
-                                   double *__restrict__ z,
-                                   const double *__restrict__ p,
-                                   const double *__restrict__ Ap,
-                                   double *__restrict__ partials, CgScalars *s);
-__global__ void k_cg_pupdate(int n, const double *__restrict__ z,
-                             double *__restrict__ p, const CgScalars *s);
 
 namespace
 {
@@ -327,6 +319,78 @@ __global__ void __launch_bounds__(kHelmTx * kHelmWarps)
   }
 }
 
+// Jacobi inverse diagonal per node class (27 values, 1 / centre coefficient
+// of the class row)
+struct HelmInvd
+{
+  double v[kHelmClasses];
+};
+
+__device__ __forceinline__ int helm_class(const HelmGrid &g, int n)
+{
+  const int i = n % g.NX, rest = n / g.NX, j = rest % g.NY, k = rest / g.NY;
+  return node_class(i, g.NX) + 3 * node_class(j, g.NY) + 9 * node_class(k, g.nz + 1);
+}
+
+// The Jacobi CG update of k_cg_update_jacobi (x += alpha p, r -= alpha Ap,
+// z = D^-1 r, beta, stop test) with D^-1 taken from the node's class instead
+// of a vector and z not stored: k_helm_pupdate forms it again from r, with
+// the same operations, so the iterates are those of the generic kernels on
+// 16 bytes per node less.
+__global__ void k_helm_update(HelmGrid g, HelmInvd iv, double *__restrict__ x,
+                              double *__restrict__ r, const double *__restrict__ p,
+                              const double *__restrict__ Ap, double *__restrict__ partials,
+                              CgScalars *s)
+{
+  __shared__ double sh[64];
+  if(s->done)
+    return;
+  const double alpha = s->alpha;
+  double zr = 0.0, rr = 0.0;
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+  {
+    x[n] += alpha * p[n];
+    const double ri = r[n] - alpha * Ap[n];
+    r[n] = ri;
+    const double zi = ri * iv.v[helm_class(g, n)];
+    zr += zi * ri;
+    rr += ri * ri;
+  }
+  double v[2] = {zr, rr};
+  block_sum<2>(v, sh);
+  if(threadIdx.x == 0)
+  {
+    partials[blockIdx.x] = v[0];
+    partials[gridDim.x + blockIdx.x] = v[1];
+  }
+  if(last_block(&s->counter))
+  {
+    double t[2];
+    sum_partials<2>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      s->zr_new = t[0];
+      s->beta = t[0] / s->zr;
+      s->zr = t[0];
+      cg_check(s, t[1]);
+      s->counter = 0;
+    }
+  }
+}
+
+// p = z + beta p with z = D^-1 r
+__global__ void k_helm_pupdate(HelmGrid g, HelmInvd iv, const double *__restrict__ r,
+                               double *__restrict__ p, const CgScalars *s)
+{
+  if(s->done)
+    return;
+  const double beta = s->beta;
+  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
+      n += gridDim.x * blockDim.x)
+    p[n] = beta * p[n] + r[n] * iv.v[helm_class(g, n)];
+}
+
 // out_e = sum_a ns[a] val[node_a] (/8 for the density call)
 __global__ void k_helm_out(HelmGrid g, HelmWeights w, const double *__restrict__ val,
                            double *__restrict__ out, int sens)
@@ -492,6 +556,8 @@ void helm_setup(icarat_ctx *c, double R)
   helm_element(c->hx, c->hy, c->hz, R, H.ke, H.nj, H.ns);
   double coef[kHelmClasses * 27];
   helm_class_table(H.ke, coef);
+  for(int q = 0; q < kHelmClasses; q++)
+    H.invd_cls[q] = 1.0 / coef[27 * q + 13];
   const size_t n = (size_t)c->numnp;
   H.d_coef = dalloc(kHelmClasses * 27);
   ICK(cudaMemcpy(H.d_coef, coef, sizeof(coef), cudaMemcpyHostToDevice));
@@ -529,9 +595,13 @@ static void helm_iteration(icarat_ctx *c)
   note_launch(3);
   k_helm_spmv<<<blocks_for(tiles, 1, kMaxRedBlocks), kHelmTx * kHelmWarps, 0, c->stream>>>(
       hgrid(c), helm_axes(c), H.d_p, H.d_Ap, H.d_partials, H.d_cg);
-  k_cg_update_jacobi<<<rb, kRedThreads, 0, c->stream>>>(n, H.d_invd, H.d_val, H.d_r, H.d_z,
-                                                        H.d_p, H.d_Ap, H.d_partials, H.d_cg);
-  k_cg_pupdate<<<rb, kRedThreads, 0, c->stream>>>(n, H.d_z, H.d_p, H.d_cg);
+  HelmInvd iv;
+  for(int q = 0; q < kHelmClasses; q++)
+    iv.v[q] = H.invd_cls[q];
+  (void)n;
+  k_helm_update<<<rb, kRedThreads, 0, c->stream>>>(hgrid(c), iv, H.d_val, H.d_r, H.d_p, H.d_Ap,
+                                                   H.d_partials, H.d_cg);
+  k_helm_pupdate<<<rb, kRedThreads, 0, c->stream>>>(hgrid(c), iv, H.d_r, H.d_p, H.d_cg);
   ICK(cudaGetLastError());
 }
 

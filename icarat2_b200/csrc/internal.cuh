@@ -242,6 +242,7 @@ struct HelmState
   CgScalars *d_cg = nullptr;
   cudaGraphExec_t exec = nullptr; // kHelmChunk iterations
   double *d_oc = nullptr;         // 3 nelx: work of the OC volume functor
+  double invd_cls[27] = {};       // Jacobi inverse diagonal per node class
 };
 
 struct MmaDev;
@@ -503,6 +504,30 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sh)
       for(int o = 16; o > 0; o >>= 1)
         v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
     }
+  }
+}
+
+// Stop test of the CG iterations (ScalingCG, CG.cpp:56-99): count the
+// iteration, keep ||r||, stop on NaN, on ||r|| < tol ||b|| or past maxit.
+__device__ __forceinline__ void cg_check(CgScalars *s, double rr)
+{
+  s->iter += 1;
+  s->rr = rr;
+  s->rnorm = sqrt(rr);
+  if(!(rr == rr))
+  {
+    s->done = 1;
+    s->status = ICARAT_ERR_NAN;
+  }
+  else if(s->rnorm < s->tol * s->bnorm)
+  {
+    s->done = 1;
+    s->status = ICARAT_OK;
+  }
+  else if(s->iter > s->maxit)
+  {
+    s->done = 1;
+    s->status = ICARAT_WARN_MAXITER;
   }
 }
 

@@ -118,27 +118,6 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-__device__ __forceinline__ void cg_check(CgScalars *s, double rr)
-{
-  s->iter += 1;
-  s->rr = rr;
-  s->rnorm = sqrt(rr);
-  if(!(rr == rr))
-  {
-    s->done = 1;
-    s->status = ICARAT_ERR_NAN;
-  }
-  else if(s->rnorm < s->tol * s->bnorm)
-  {
-    s->done = 1;
-    s->status = ICARAT_OK;
-  }
-  else if(s->iter > s->maxit)
-  {
-    s->done = 1;
-    s->status = ICARAT_WARN_MAXITER;
-  }
-}
 
 // Jacobi: x += alpha p, r -= alpha Ap, z = invd r; beta, ||r||, stop test.
 __global__ void k_cg_update_jacobi(int n, const double *__restrict__ invd,
