@@ -90,3 +90,29 @@ def test_cpp_helmholtz_driver_trajectory(oracle, method):
         L.step()
         ref.append(L.scalars()["compliance"])
     assert np.allclose(comp, ref, rtol=1e-7, atol=0)
+
+
+def test_cpp_multi_load_driver(oracle):
+    """examples/opt_multi_load.cpp (the opt_multi_load.cpp loop through the C
+    ABI: 3 load cases, design / non-design IDs, Helmholtz filter, MMA) against
+    oracle.CaseLoop: compliance sums <= 1e-7 relative over 3 iterations."""
+    exe = os.path.join(ROOT, "icarat2_b200", "examples", "opt_multi_load")
+    if not os.path.exists(exe):
+        from icarat2_b200 import build
+        build.build()
+    nx, ny, nz, steps, R = 16, 8, 8, 3, 2.0
+    out = subprocess.run([exe, str(nx), str(ny), str(nz), str(steps), str(R)],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    comp = [float(l.split()[2]) for l in out.stdout.splitlines() if l.startswith("step")]
+    assert len(comp) == steps
+    d = [((1, 1, 1), (0.0, 0.0, 0.0), ((0, 0), (0, ny), (0, nz)))]
+    cases = [[((0, 0, -1.0), ((nx, nx), (ny // 2, ny // 2), (0, 0)))],
+             [((0, -1.0, 0), ((nx, nx), (ny, ny), (nz, nz)))],
+             [((0, 0, 1.0), ((nx, nx), (0, 0), (nz, nz)))]]
+    Ps = [oracle.Problem(nx, ny, nz, dirichlet=d, loads=c) for c in cases]
+    e = np.arange(nx * ny * nz)
+    M = oracle.CaseLoop(Ps, None, helmholtz_R=R, design_ids=e[e % nx < nx - 2],
+                        nondesign_ids=e[e % nx >= nx - 2])
+    ref = [M.step()[0] for _ in range(steps)]
+    assert np.allclose(comp, ref, rtol=1e-7, atol=0)
