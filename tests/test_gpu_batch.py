@@ -240,3 +240,28 @@ def test_batch_rejects_unknown_method(gpu):
         with pytest.raises(gpu.IcaratError) as e:
             B.solve(o)
         assert e.value.status == gpu.ERR_ARG
+
+
+def test_batch_design_loop_with_helmholtz_filter(gpu):
+    """members looping with the Helmholtz filter (opt_mma_Helmholtz.cpp) in
+    the interleaved batch mode track standalone loops to 1e-6"""
+    prs = problems(gpu, [(16, 8, 8), (24, 12, 12)], 18)
+    B = gpu.Batch(prs)
+    solo = []
+    for i, (nx, ny, nz, d, lo) in enumerate(prs):
+        B[i].loop_init(0.3, method="mma", filter_radius=2.0, move=0.2, use_threshold=True,
+                       filter="helmholtz")
+        G = gpu.Context(nx, ny, nz, dirichlet=d, loads=lo)
+        G.loop_init(0.3, method="mma", filter_radius=2.0, move=0.2, use_threshold=True,
+                    solve=gpu.solve_opts(gpu.MG_PCG, rtol=1e-12, mg_levels=2),
+                    filter="helmholtz")
+        solo.append(G)
+    o = B.opts(rtol=1e-10, method=gpu.MIXED_IR, warm_start=True)
+    for _ in range(3):
+        infos = B.loop_step(o)
+        for i, G in enumerate(solo):
+            ref = G.loop_step()
+            assert infos[i].status == gpu.OK
+            assert abs(infos[i].compliance - ref.compliance) <= 1e-6 * ref.compliance
+    for i, G in enumerate(solo):
+        assert rel(B[i].loop_get("x"), G.loop_get("x")) <= 1e-6
