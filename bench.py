@@ -54,6 +54,9 @@ def parse():
                    help="1: reuse the previous design's coarsest factor while this "
                         "design's is computed on a second stream")
     p.add_argument("--smooth", type=int, default=2)
+    p.add_argument("--warm-start", type=int, default=1,
+                   help="headline FP64 MG-PCG starts from the previous design's solution "
+                        "(stop test unchanged: ||r|| < rtol ||b||)")
     p.add_argument("--rtol", type=float, default=1e-8)
     p.add_argument("--cpu-sample", action="store_true",
                    help="internal: time one full CPU design iteration and print it")
@@ -106,6 +109,8 @@ def config(a, extra=None):
     if a.impl == "ours":
         c["coarse_factor"] = ("previous design's, this design's computed on a second stream "
                               "during the solve" if a.coarse_lag else "this design's")
+        c["initial_guess"] = ("the previous design's solution (stop test ||r|| < rtol ||b||)"
+                              if a.warm_start else "zero")
     if extra:
         c.update(extra)
     return c
@@ -427,7 +432,8 @@ def helmholtz_section(a, G, torch, dev, flush, world, dist):
     cl = G.Context(gx, gy, gz, device=dev.index)
     cl.loop_init(0.3, method="mma", filter_radius=2.0, move=0.2, use_threshold=True,
                  solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth,
-                                    coarse_lag=a.coarse_lag), filter="helmholtz")
+                                    coarse_lag=a.coarse_lag, warm_start=a.warm_start),
+                 filter="helmholtz")
     sl = torch.cuda.ExternalStream(cl.stream_ptr(), device=dev)
     for _ in range(a.warmup):
         cl.loop_step()
@@ -497,7 +503,8 @@ def multi_load_section(a, G, torch, dev, flush, world, dist):
     c = G.Context(nx, ny, nz, dirichlet=dirich, loads=cases[0], device=dev.index)
     c.loop_init(0.3, method="mma", filter_radius=2.0, move=0.2, use_threshold=True,
                 solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth,
-                                   coarse_lag=a.coarse_lag), filter="helmholtz")
+                                   coarse_lag=a.coarse_lag, warm_start=a.warm_start),
+                filter="helmholtz")
     c.set_load_cases(np.array(F))
     st = torch.cuda.ExternalStream(c.stream_ptr(), device=dev)
     for _ in range(a.warmup):
@@ -783,7 +790,8 @@ def gpu_arm(a):
             cpu_line = json.loads(r.stdout.strip().splitlines()[-1])
 
     nx, ny, nz = grid_of(a)
-    opts = G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth, coarse_lag=a.coarse_lag)
+    opts = G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth, coarse_lag=a.coarse_lag,
+                        warm_start=a.warm_start)
 
     def make_ctx():
         return G.Context(nx, ny, nz, device=local)
@@ -817,11 +825,12 @@ def gpu_arm(a):
     ms_steps = [e0.elapsed_time(e1) for e0, e1 in evs]
     value, total_ms = job_rate(sum(ms_steps), a.steps, world, dist, dev)
 
-    def alt_loop(levels, lag):
+    def alt_loop(levels, lag, warm=None):
+        warm = a.warm_start if warm is None else warm
         ca = make_ctx()
         ca.loop_init(0.3, method="mma", filter_radius=a.radius, move=0.2,
                      solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, levels, a.smooth,
-                                        coarse_lag=lag))
+                                        coarse_lag=lag, warm_start=warm))
         sa = torch.cuda.ExternalStream(ca.stream_ptr(), device=dev)
         for _ in range(a.warmup):
             ca.loop_step()
@@ -839,7 +848,7 @@ def gpu_arm(a):
         torch.cuda.synchronize()
         v, alt_ms = job_rate(alt_ms, a.steps, world, dist, dev)
         ca.close()
-        return {"mg_levels": levels, "coarse_lag": lag, "value": v,
+        return {"mg_levels": levels, "coarse_lag": lag, "warm_start": warm, "value": v,
                 "unit": "design-iter/s", "ms_per_step": alt_ms / a.steps,
                 "cg_iterations_per_step": its}
 
@@ -847,6 +856,7 @@ def gpu_arm(a):
     # computed before its solve, and with one more multigrid level (coarsest
     # level 8x4x4 instead of 16x8x8: a 600-DOF dense solve instead of 3,888)
     other_coarse = alt_loop(a.levels, 1 - a.coarse_lag) if a.alt_levels else None
+    other_warm = alt_loop(a.levels, a.coarse_lag, 1 - a.warm_start) if a.alt_levels else None
     alt = alt_loop(a.alt_levels, a.coarse_lag) if a.alt_levels else None
 
     # ---------------- dominant kernel: FP64 stencil K u on the final design
@@ -977,6 +987,7 @@ def gpu_arm(a):
             "cg_iterations_per_step": cg,
             "alt_levels": alt,
             "alt_coarse_lag": other_coarse,
+            "alt_warm_start": other_warm,
             "mixed_256x128x128": mixed,
             "batched_80_designs": batched,
             "learned": learned,

@@ -667,6 +667,7 @@ static void note_result(icarat_ctx *c, const icarat_solve_info &si, icarat_solve
                         int &worst)
 {
   c->solved = true;
+  c->have_u = true;
   c->last_info = si;
   if(out)
     *out = si;
@@ -704,7 +705,7 @@ static int batch_solve_concurrent(icarat_batch *B, const icarat_batch_opts *o, d
     so.refresh = refresh;
     so.fine_op = ICARAT_OP_FP32;
     so.krylov_op = ICARAT_OP_FP32;
-    so.warm_start = (o->warm_start && c->solved) ? 1 : 0;
+    so.warm_start = (o->warm_start && c->have_u) ? 1 : 0;
     mixed_begin(c, &so, c->d_rhs, c->d_u, run[d]);
     ICK(cudaEventRecord(B->ev[d], c->stream));
   }

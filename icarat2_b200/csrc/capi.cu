@@ -375,6 +375,7 @@ int icarat_solve(icarat_ctx *c, const icarat_solve_opts *opts, double *val,
   icarat_solve_info si{};
   int st = solve_full(c, &o, c->d_rhs, c->d_u, &si);
   c->solved = true;
+  c->have_u = true;
   c->last_info = si;
   if(info)
     *info = si;
@@ -396,6 +397,7 @@ int icarat_solve_rhs(icarat_ctx *c, const icarat_solve_opts *opts, const double 
   icarat_solve_info si{};
   int st = solve_full(c, &o, c->d_rhs, c->d_u, &si);
   c->solved = true;
+  c->have_u = true;
   c->last_info = si;
   if(info)
     *info = si;

@@ -500,7 +500,7 @@ int icarat_ctx_destroy_impl(icarat_ctx *c)
     icarat_mma_destroy(c->loop.mma);
   for(double *p : {c->loop.x, c->loop.xfil, c->loop.xthr, c->loop.thrd,
                    c->loop.dfds, c->loop.dgds, c->loop.tmp, c->loop.tmp2, c->loop.xmin,
-                   c->loop.xmax, c->loop.d_cases, c->loop.d_volw})
+                   c->loop.xmax, c->loop.d_cases, c->loop.d_cases_u, c->loop.d_volw})
     dfree(p);
   dfree(c->loop.d_fixed);
   dfree(c->d_free);

@@ -260,6 +260,8 @@ struct LoopState
   // load cases (ncases x neq, node layout) and design domains
   int ncases = 0;
   double *d_cases = nullptr;
+  double *d_cases_u = nullptr;      // ncases x neq: each case's last solution
+  std::vector<uint8_t> cases_have;  // a case's last solution is held
   double *d_volw = nullptr;   // element volume on design IDs, 0 elsewhere
   uint8_t *d_fixed = nullptr; // 1 on non-design IDs
 };
@@ -324,6 +326,9 @@ struct icarat_ctx
   // learned preconditioner attached by icarat_ctx_set_net (not owned)
   icarat_net *net = nullptr;
   bool design_set = false, solved = false;
+  // d_u holds the solution of an earlier system (kept across design
+  // changes): a warm start may begin from it
+  bool have_u = false;
   icarat_solve_info last_info{};
   // multigrid
   std::vector<icarat_b200::MgLevel> mg;

@@ -256,6 +256,7 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
   LoopState &L = c->loop;
   const icarat_loop_opts &o = L.opts;
   c->solved = true;
+  c->have_u = true;
   c->last_info = si;
   const double compliance = compliance_dev(c);
   const double constraint = loop_constraint(c);
@@ -294,11 +295,29 @@ static int loop_step_cases(icarat_ctx *c, double beta, icarat_step_info *info)
     {
       c->d_fext = L.d_cases + (size_t)lc * c->neq;
       build_rhs(c);
+      // a warm start begins from this case's own last solution
+      double *ucase = L.d_cases_u + (size_t)lc * c->neq;
+      if(L.opts.solve.warm_start)
+      {
+        if(L.cases_have[lc])
+          ICK(cudaMemcpyAsync(c->d_u, ucase, sizeof(double) * c->neq,
+                              cudaMemcpyDeviceToDevice, c->stream));
+        else
+          ICK(cudaMemsetAsync(c->d_u, 0, sizeof(double) * c->neq, c->stream));
+        c->have_u = L.cases_have[lc] != 0;
+      }
       icarat_solve_info si{};
       const int s1 = solve_full(c, &L.opts.solve, c->d_rhs, c->d_u, &si);
+      if(L.opts.solve.warm_start)
+      {
+        ICK(cudaMemcpyAsync(ucase, c->d_u, sizeof(double) * c->neq, cudaMemcpyDeviceToDevice,
+                            c->stream));
+        L.cases_have[lc] = 1;
+      }
       if(s1 < 0 || (st >= 0 && s1 != ICARAT_OK))
         st = s1;
       c->solved = true;
+      c->have_u = true;
       c->last_info = si;
       iterations += si.iterations;
       relres = relres > si.rel_residual ? relres : si.rel_residual;
@@ -357,11 +376,15 @@ int set_load_cases(icarat_ctx *c, int ncases, const double *fext)
   LoopState &L = c->loop;
   IREQUIRE(ncases >= 0 && (ncases == 0 || fext), ICARAT_ERR_ARG, "bad load cases");
   dfree(L.d_cases);
-  L.d_cases = nullptr;
+  dfree(L.d_cases_u);
+  L.d_cases = L.d_cases_u = nullptr;
+  L.cases_have.clear();
   L.ncases = 0;
   if(ncases == 0)
     return ICARAT_OK;
   L.d_cases = dalloc((size_t)ncases * c->neq);
+  L.d_cases_u = dalloc((size_t)ncases * c->neq);
+  L.cases_have.assign(ncases, 0);
   for(int lc = 0; lc < ncases; lc++)
     to_full(c, fext + (size_t)lc * c->numeq, L.d_cases + (size_t)lc * c->neq, true);
   ICK(cudaStreamSynchronize(c->stream));

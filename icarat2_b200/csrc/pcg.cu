@@ -76,6 +76,68 @@ __global__ void k_cg_init(int n, const double *__restrict__ b,
   }
 }
 
+// Warm start from the solution x of a previous system (Ax = K x given):
+// r = b - Ax, z = invd r (Jacobi only), zr, ||b|| and ||r||.  The stop test
+// stays ||r|| < tol ||b||; a start that already meets it is done after 0
+// iterations (Eigen's solveWithGuess checks the initial residual too).
+__global__ void k_cg_init_warm(int n, const double *__restrict__ b,
+                               const double *__restrict__ Ax,
+                               const double *__restrict__ invd, double *__restrict__ r,
+                               double *__restrict__ z, double *__restrict__ p,
+                               double *__restrict__ partials, CgScalars *s, double tol,
+                               int maxit, int jacobi)
+{
+  __shared__ double sh[96];
+  double zr = 0.0, bb = 0.0, rr = 0.0;
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+  {
+    const double bi = b[i];
+    const double ri = bi - Ax[i];
+    r[i] = ri;
+    if(jacobi)
+    {
+      const double zi = ri * invd[i];
+      z[i] = zi;
+      p[i] = zi;
+      zr += zi * ri;
+    }
+    bb += bi * bi;
+    rr += ri * ri;
+  }
+  double v[3] = {zr, bb, rr};
+  block_sum<3>(v, sh);
+  if(threadIdx.x == 0)
+  {
+    partials[blockIdx.x] = v[0];
+    partials[gridDim.x + blockIdx.x] = v[1];
+    partials[2 * gridDim.x + blockIdx.x] = v[2];
+  }
+  if(last_block(&s->counter))
+  {
+    double t[3];
+    sum_partials<3>(partials, gridDim.x, t, sh);
+    if(threadIdx.x == 0)
+    {
+      s->zr = t[0];
+      s->bnorm = sqrt(t[1]);
+      s->rnorm = sqrt(t[2]);
+      s->rr = t[2];
+      s->tol = tol;
+      s->maxit = maxit;
+      s->iter = 0;
+      s->status = ICARAT_OK;
+      s->done = (t[1] == 0.0 || s->rnorm < tol * s->bnorm) ? 1 : 0;
+      if(!(t[1] == t[1]) || !(t[2] == t[2]))
+      {
+        s->done = 1;
+        s->status = ICARAT_ERR_NAN;
+      }
+      s->counter = 0;
+    }
+  }
+}
+
 // Ap = K p, alpha = zr / (p . Ap)
 __global__ void __launch_bounds__(128)
     k_cg_spmv(GridDev g, KeParam ke, const double *__restrict__ E,
@@ -331,10 +393,23 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
     launch_diag(c, g, c->d_E, c->d_fix, c->d_invd);
   int chunk = o->chunk > 0 ? o->chunk : (method == ICARAT_SOLVER_MG_PCG ? 4 : 16);
 
-  note_launch();
-  k_cg_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
-      n, d_b, c->d_invd, d_x, c->d_r, c->d_z, c->d_p, c->d_partials, c->d_cg,
-      o->rtol, o->maxit, method == ICARAT_SOLVER_JACOBI_PCG ? 1 : 0);
+  // warm start: the context's own solution buffer holds a previous solution
+  const bool warm = o->warm_start != 0 && c->have_u && d_x == c->d_u;
+  if(warm)
+  {
+    launch_apply_K(c, g, c->d_E, c->d_fix, d_x, c->d_Ap, nullptr);
+    note_launch();
+    k_cg_init_warm<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
+        n, d_b, c->d_Ap, c->d_invd, c->d_r, c->d_z, c->d_p, c->d_partials, c->d_cg, o->rtol,
+        o->maxit, method == ICARAT_SOLVER_JACOBI_PCG ? 1 : 0);
+  }
+  else
+  {
+    note_launch();
+    k_cg_init<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
+        n, d_b, c->d_invd, d_x, c->d_r, c->d_z, c->d_p, c->d_partials, c->d_cg,
+        o->rtol, o->maxit, method == ICARAT_SOLVER_JACOBI_PCG ? 1 : 0);
+  }
   ICK(cudaGetLastError());
   if(method == ICARAT_SOLVER_MG_PCG)
   {

@@ -105,8 +105,11 @@ typedef struct
   int fine_op;    /* MIXED_IR: ICARAT_OP_* of the finest-level smoothing and
                      residual in the V-cycle (0 = default) */
   int krylov_op;  /* MIXED_IR: ICARAT_OP_* of K p in the Krylov loop (0 = default) */
-  int warm_start; /* MIXED_IR: start from the solution held by the context (the
-                     previous solve, e.g. of the previous design) instead of 0 */
+  int warm_start; /* start from the solution held by the context (the previous
+                     solve, e.g. of the previous design; the loop keeps one per
+                     load case) instead of 0; MIXED_IR, and JACOBI_PCG / MG_PCG
+                     when the solve writes the context's own solution (icarat_solve,
+                     the loop): r0 = b - K x0, same stop test ||r|| < rtol ||b|| */
   int fp64_tc;    /* JACOBI_PCG, MG_PCG: FP64 products K u element by element
                      on the FP64 tensor cores (ICARAT_OP_TC_FP64) or by the
                      node stencil on the CUDA cores: 0 (default) = by grid
