@@ -15,8 +15,8 @@ set-up.
     python -m icarat2_b200.profile_cases headline 5
         one design iteration of the bench's headline loop (128x64x64,
         uniform start density 0.3, filter radius 2.5, MMA move 0.2, 4-level
-        MG-PCG to 1e-8 with the coarse factor reused) after `warm` warm-up
-        iterations
+        MG-PCG to 1e-8 with the coarse factor reused and the solve started
+        from the previous design's solution) after `warm` warm-up iterations
     python -m icarat2_b200.profile_cases net 256x128x128
         one inference of the U-net (random weights, seed 1) on the load of
         the cantilever, after one warm-up inference
@@ -100,7 +100,7 @@ def loop(grid, method, levels, rtol, warm):
 
 def headline(warm):
     G = gpu.Context(128, 64, 64)
-    o = gpu.solve_opts(gpu.MG_PCG, rtol=1e-8, mg_levels=4, coarse_lag=1)
+    o = gpu.solve_opts(gpu.MG_PCG, rtol=1e-8, mg_levels=4, coarse_lag=1, warm_start=1)
     G.loop_init(0.3, method="mma", filter_radius=2.5, move=0.2, solve=o)
     for _ in range(int(warm)):
         G.loop_step()
