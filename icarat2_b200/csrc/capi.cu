@@ -68,7 +68,8 @@ using namespace icarat_b200;
 
 extern "C" {
 
-int icarat_version(void) { return 10000; }
+// ICARAT_ABI_VERSION of the header the library was built with
+int icarat_version(void) { return ICARAT_ABI_VERSION; }
 
 int icarat_kernel_launches(unsigned long long *count)
 {

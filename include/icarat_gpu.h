@@ -150,6 +150,11 @@ typedef struct
 } icarat_oc_opts;
 
 /* ---- library ---------------------------------------------------------- */
+/* 10100: icarat_loop_opts.filter_kind and icarat_oc_opts.filter_kind
+   appended (Helmholtz filter); callers built against 10000 headers pass the
+   shorter structs and must be rebuilt.  A caller checks
+   icarat_version() == ICARAT_ABI_VERSION before passing option structs. */
+#define ICARAT_ABI_VERSION 10100
 int icarat_version(void);
 const char *icarat_status_string(int status);
 /* message of the last failed call on this thread */
