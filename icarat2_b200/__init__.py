@@ -118,6 +118,9 @@ class StepInfo(C.Structure):
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _vp = C.c_void_p
+# ICARAT_ABI_VERSION of include/icarat_gpu.h that the structs below mirror
+ABI_VERSION = 10100
+
 _i = C.c_int
 _d = C.c_double
 _P = C.POINTER
@@ -215,6 +218,9 @@ def load_library(path=LIBPATH):
         f = getattr(L, name)
         f.restype = res
         f.argtypes = args
+    if L.icarat_version() != ABI_VERSION:
+        raise ImportError("libicarat_gpu.so has ABI %d, these bindings %d: rebuild with "
+                          "python -m icarat2_b200.build" % (L.icarat_version(), ABI_VERSION))
     _lib = L
     return L
 
