@@ -8,11 +8,11 @@
 //
 // The kernels are the ones of the ordinary solve (pcg.cu, stiffness.cu,
 // ctx.cu); only the work buffers differ.  Host code cannot use the array's
-// name as a device address, so the address is resolved once per device with
-// cudaGetSymbolAddress (on the first call on that device, with that device
-// current) and passed to the kernels.
-#include <mutex>
-
+// name as a device address, so the address is resolved with
+// cudaGetSymbolAddress when a context is created (with its device current)
+// and kept in the context.  Under lazy module loading that call is what loads
+// this file's module and commits the array on the device, so it belongs to
+// context creation, which allocates anyway, and not to the solve.
 #include "internal.cuh"
 
 namespace icarat_b200
@@ -50,24 +50,28 @@ constexpr size_t kNaDoubles = 7 * kNaVec + kNaPartials + kNaScalars;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNaDoubles];
 
-static std::mutex g_noalloc_mutex;
-static double *g_noalloc_addr[128];
-
-// Device address of the static array on the current device (resolved once).
-static double *noalloc_scratch(int device)
+// Device address of the static array on the context's device (current when
+// this runs); every context resolves its own, so an address never outlives
+// the CUDA context it was taken in.
+void noalloc_resolve(icarat_ctx *c)
 {
-  IREQUIRE(device >= 0 && device < 128, ICARAT_ERR_ARG, "device index out of range");
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if(!g_noalloc_addr[device])
+  void *ptr = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  IREQUIRE(e == cudaSuccess && ptr != nullptr, ICARAT_ERR_CUDA,
+           std::string("cudaGetSymbolAddress of the no-allocation solve buffer: ") +
+               cudaGetErrorString(e));
+  c->noalloc_scratch = static_cast<double *>(ptr);
+  // load the kernels the solve launches as well (lazy loading would load
+  // each on its first launch, inside the solve)
+  const void *kernels[] = {(const void *)k_cg_init,          (const void *)k_cg_spmv,
+                           (const void *)k_cg_update_jacobi, (const void *)k_cg_pupdate,
+                           (const void *)k_inv_diag,         (const void *)k_scatter_free,
+                           (const void *)k_gather_free};
+  for(const void *k : kernels)
   {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    IREQUIRE(e == cudaSuccess && ptr != nullptr, ICARAT_ERR_CUDA,
-             std::string("cudaGetSymbolAddress of the solve buffer: ") +
-                 cudaGetErrorString(e));
-    g_noalloc_addr[device] = static_cast<double *>(ptr);
+    cudaFuncAttributes a;
+    ICK(cudaFuncGetAttributes(&a, k));
   }
-  return g_noalloc_addr[device];
 }
 
 static int solve_noalloc(icarat_ctx *c, const icarat_solve_opts *opts, const double *f,
@@ -81,11 +85,18 @@ static int solve_noalloc(icarat_ctx *c, const icarat_solve_opts *opts, const dou
     o = *opts;
   IREQUIRE(o.method == ICARAT_SOLVER_JACOBI_PCG, ICARAT_ERR_UNSUPPORTED,
            "icarat_solve_noalloc runs Jacobi-PCG only");
+  // the node stencil from a zero start is the only form it runs: the FP64
+  // tensor-core operator and warm starts would round differently than asked
+  IREQUIRE(o.fp64_tc == 0 || o.fp64_tc == -1, ICARAT_ERR_UNSUPPORTED,
+           "icarat_solve_noalloc runs the FP64 node stencil only (fp64_tc 0 or -1)");
+  IREQUIRE(o.warm_start == 0, ICARAT_ERR_UNSUPPORTED,
+           "icarat_solve_noalloc starts from zero (warm_start 0)");
   IREQUIRE((size_t)c->neq <= kNaVec, ICARAT_ERR_ARG,
            "grid too large for icarat_solve_noalloc: 3*(nx+1)*(ny+1)*(nz+1) = " +
                std::to_string(c->neq) + " DOFs, limit ICARAT_NOALLOC_MAX_DOFS = " +
                std::to_string(kNaVec));
-  double *S = noalloc_scratch(c->device);
+  double *S = c->noalloc_scratch;
+  IREQUIRE(S != nullptr, ICARAT_ERR_STATE, "no-allocation buffer not resolved");
   double *b = S, *x = S + kNaVec, *r = S + 2 * kNaVec, *p = S + 3 * kNaVec,
          *z = S + 4 * kNaVec, *Ap = S + 5 * kNaVec, *invd = S + 6 * kNaVec;
   double *partials = S + 7 * kNaVec;
