@@ -16,7 +16,8 @@ MMA, exactly the loop body of the reference sample drivers.
           with every host<->device copy inside the timed region, the host
           buffers in pinned memory
   --impl reference : the CPU restatement of the reference path (oracle/,
-          Jacobi-PCG as the reference "Eigen_CG" solver) on all host cores
+          Jacobi-PCG as the reference "Eigen_CG" solver) on the host's physical
+          cores, full design iterations of the same trajectory window
 
 Multi-GPU (torchrun): every rank optimises its own replica (independent
 designs, no data-path collective); value = all ranks' design iterations /
@@ -60,8 +61,9 @@ def parse():
     p.add_argument("--rtol", type=float, default=1e-8)
     p.add_argument("--cpu-sample", action="store_true",
                    help="internal: time one full CPU design iteration and print it")
-    p.add_argument("--cap", type=int, default=100,
-                   help="reference arm: PCG iterations run per timed step")
+    p.add_argument("--ref-budget", type=float, default=120.0,
+                   help="reference arm: seconds of timed design iterations at most "
+                        "(fewer timed steps than requested when they do not fit)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--alt-levels", type=int, default=5,
@@ -117,6 +119,29 @@ def config(a, extra=None):
 
 
 # --------------------------------------------------------------------- CPU arm
+def host_cpu():
+    """(physical cores this process may use, CPU model name) from lscpu."""
+    model, pairs = "unknown", set()
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True).stdout
+        for ln in out.splitlines():
+            if ln.startswith("Model name:"):
+                model = ln.split(":", 1)[1].strip()
+        par = subprocess.run(["lscpu", "-p=CPU,CORE,SOCKET"], capture_output=True,
+                             text=True).stdout
+        allowed = os.sched_getaffinity(0)
+        for ln in par.splitlines():
+            if ln.startswith("#"):
+                continue
+            cpu, core, sock = ln.split(",")[:3]
+            if int(cpu) in allowed:
+                pairs.add((core, sock))
+    except (OSError, ValueError):
+        pass
+    cores = len(pairs) if pairs else (os.cpu_count() or 1)
+    return cores, model
+
+
 def cpu_design_iteration(a, cg_maxit, threads):
     """One first-design iteration of the oracle; returns timings (s) and CG its."""
     from oracle import oracle as O
@@ -133,34 +158,56 @@ def cpu_design_iteration(a, cg_maxit, threads):
 
 
 def reference_arm(a):
+    """The CPU restatement of the reference path, timed in full: W warm-up and
+    then timed design iterations of one trajectory (the GPU arm's window),
+    every solve uncapped to rtol.  The number of timed iterations is cut to
+    what fits a wall-clock budget (--ref-budget seconds for the timed part)
+    and reported as "steps"."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
-    # warm-up: one uncapped design iteration measures the PCG iteration count
-    # N that rtol needs on this design and the per-iteration cost
-    t_full, s_full = cpu_design_iteration(a, 100000, threads)
-    n_full = s_full["cg_iters"]
-    times = []
-    for _ in range(a.steps):
-        t, s = cpu_design_iteration(a, a.cap, threads)
-        t_pcg = s["t_pcg"]
-        it = s["cg_iters"]
-        times.append(t - t_pcg + t_pcg * n_full / max(it, 1))
-    ms = 1000.0 * statistics.mean(times)
+    from oracle import oracle as O
+    cores, model = host_cpu()
+    O.lib.or_set_threads(cores)
+    nx, ny, nz = grid_of(a)
+    t_setup = time.perf_counter()
+    P = O.Problem(nx, ny, nz)
+    F = O.Filter(P, a.radius)
+    L = O.Loop(P, F, method="mma", x0=0.3, move=0.2, cg_tol=a.rtol, cg_maxit=100000)
+    t_setup = time.perf_counter() - t_setup
+    warm = []
+    for _ in range(a.warmup):
+        t0 = time.perf_counter()
+        L.step()
+        warm.append(time.perf_counter() - t0)
+    times, iters = [], []
+    t_begin = time.perf_counter()
+    for k in range(a.steps):
+        t0 = time.perf_counter()
+        L.step()
+        times.append(time.perf_counter() - t0)
+        iters.append(L.scalars()["cg_iters"])
+        spent = time.perf_counter() - t_begin
+        if k + 1 < a.steps and spent + spent / (k + 1) > a.ref_budget:
+            break
+    ms = 1000.0 * sum(times) / len(times)
     value = 1000.0 / ms
-    sample = ("first design iteration of the workload on the CPU restatement "
-              "(oracle/, OpenMP, %d threads): filter, CSR assembly, Jacobi-PCG "
-              "(reference Eigen_CG semantics), sensitivity, filter^T, MMA; each "
-              "timed step runs %d PCG iterations and scales the PCG time to the "
-              "%d iterations the uncapped warm-up solve needed for rtol %g "
-              "(uncapped warm-up step: %.2f s)" % (threads, a.cap + 1, n_full, a.rtol,
-                                                   t_full))
+    sample = ("design iterations %d-%d of the workload's trajectory on the CPU "
+              "restatement (oracle/, OpenMP, %d threads = physical cores of %s): "
+              "filter, CSR assembly, Jacobi-PCG to rtol %g uncapped (reference "
+              "Eigen_CG semantics; %s iterations), sensitivity, filter^T, MMA; %d "
+              "warm-up iterations first (%.1f s), %d of %d requested timed iterations "
+              "within the %g s budget; setup (mesh, CSR pattern, filter lists) %.1f s "
+              "not timed" % (a.warmup + 1, a.warmup + len(times), cores, model, a.rtol,
+                             "/".join(str(i) for i in iters), a.warmup, sum(warm),
+                             len(times), a.steps, a.ref_budget, t_setup))
     line = {"metric": METRIC, "value": value, "unit": "design-iter/s", "impl": "reference",
-            "n_gpus": a.gpus, "steps": a.steps, "warmup": 1, "ms_per_step": ms,
+            "n_gpus": a.gpus, "steps": len(times), "steps_requested": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "config": config(a),
-            "cpu_baseline": {"value": value, "unit": "design-iter/s", "cores": threads,
+            "host_cpu": {"model": model, "physical_cores": cores},
+            "cpu_baseline": {"value": value, "unit": "design-iter/s", "cores": cores,
                              "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "design-iter/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -183,7 +230,7 @@ def cpu_helm(a):
 
 
 def cpu_sample(a):
-    threads = os.cpu_count() or 1
+    threads, _ = host_cpu()
     t, s = cpu_design_iteration(a, 100000, threads)
     print(json.dumps({"t": t, "cg_iters": s["cg_iters"], "threads": threads}), flush=True)
     return 0

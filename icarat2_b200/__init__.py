@@ -119,7 +119,7 @@ _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _vp = C.c_void_p
 # ICARAT_ABI_VERSION of include/icarat_gpu.h that the structs below mirror
-ABI_VERSION = 10100
+ABI_VERSION = 10200
 
 _i = C.c_int
 _d = C.c_double
@@ -201,6 +201,10 @@ SIGNATURES = {
     "icarat_loop_init": (_i, [_vp, _P(LoopOpts), _dp]),
     "icarat_loop_step": (_i, [_vp, _P(StepInfo)]),
     "icarat_loop_get": (_i, [_vp, _i, _dp]),
+    "icarat_loop_is_convergence": (_i, [_vp, _d, _d, _P(_i)]),
+    "icarat_ctx_create_selection": (_i, [_P(Grid), _P(Material), _P(BC), _i, _dp, _i,
+                                         _P(_vp)]),
+    "icarat_selection_ids": (_i, [_vp, _vp, _vp]),
 }
 
 _lib = None
@@ -401,7 +405,11 @@ class Context:
     """A hexa8 voxel box with its boundary conditions, resident on one GPU."""
 
     def __init__(self, nx, ny, nz, lx=None, ly=None, lz=None, young=(1e-9, 1.0),
-                 poisson=0.3, penalty=3.0, dirichlet=None, loads=None, device=0):
+                 poisson=0.3, penalty=3.0, dirichlet=None, loads=None, device=0,
+                 selection=None):
+        """selection: the [mesh] selection boxes, ((x0, x1), (y0, y1), (z0, z1))
+        each (MeshIcarat::modifyMesh); sizes, element and node vectors are then
+        those of the kept mesh."""
         L = load_library()
         lx = float(nx if lx is None else lx)
         ly = float(ny if ly is None else ly)
@@ -414,9 +422,23 @@ class Context:
         grid = Grid(nx, ny, nz, lx, ly, lz)
         mat = Material(young[0], young[1], poisson, penalty)
         h = C.c_void_p()
-        _check(L.icarat_ctx_create(C.byref(grid), C.byref(mat), C.byref(bc), device,
-                                   C.byref(h)), "icarat_ctx_create")
+        if selection is None:
+            _check(L.icarat_ctx_create(C.byref(grid), C.byref(mat), C.byref(bc), device,
+                                       C.byref(h)), "icarat_ctx_create")
+        else:
+            boxes = np.ascontiguousarray(np.asarray(selection, dtype=np.float64).reshape(-1, 6))
+            _check(L.icarat_ctx_create_selection(C.byref(grid), C.byref(mat), C.byref(bc),
+                                                 boxes.shape[0], boxes.ravel(), device,
+                                                 C.byref(h)), "icarat_ctx_create_selection")
         self._adopt(h, L, (nx, ny, nz), young, poisson, penalty, owned=True)
+
+    def selection_ids(self):
+        """(box node id of every node, box element id of every element)"""
+        nodes = np.zeros(max(self.numnp, 1), np.int32)
+        elems = np.zeros(max(self.nelx, 1), np.int32)
+        _check(self.lib.icarat_selection_ids(self.h, nodes.ctypes.data, elems.ctypes.data),
+               "selection_ids")
+        return nodes[:self.numnp], elems[:self.nelx]
 
     def _adopt(self, h, L, dims, young, poisson, penalty, owned):
         self.h = h
@@ -688,6 +710,16 @@ class Context:
         _check(self.lib.icarat_loop_set_domains(self.h, dp, dn, nd.ctypes.data if nd.size
                                                 else None, nd.size), "loop_set_domains")
 
+    def loop_is_convergence(self, epsilon=1.0e-5, minstep=50):
+        """Optimize::isConvergence on the device loop's objective
+        (opt_base.hpp:28-43): 0 when the last step's compliance changed by less
+        than epsilon relative to the one kept at the previous call and the step
+        count exceeds minstep, else 1 (and the compliance is kept)."""
+        conv = C.c_int()
+        _check(self.lib.icarat_loop_is_convergence(self.h, epsilon, minstep, C.byref(conv)),
+               "loop_is_convergence")
+        return conv.value
+
     def loop_get(self, which):
         idx = {"x": 0, "xfil": 1, "xthr": 2, "dfds": 3, "dgds": 4}[which]
         out = np.zeros(self.nelx)
@@ -778,6 +810,34 @@ class FilterHelmholtz:
 
     def thresholdDerivative(self, design_filtered, beta, T):
         return self.ctx.threshold_derivative(design_filtered, beta, T)
+
+
+class Optimize:
+    """Optimize (src/optimization/opt_base.hpp:14-76): the design state of a
+    host-composed loop and its convergence test."""
+
+    def __init__(self, design, constraint, xmin, xmax):
+        self.design_s = np.zeros(design)
+        self.const_h = np.zeros(constraint)
+        self.dfds = np.zeros(design)
+        self.dgds = np.zeros(constraint * design)
+        self.xmin = np.full(design, float(xmin))
+        self.xmax = np.full(design, float(xmax))
+        self.optstep = 0
+        self.object_f = 0.0
+        # uninitialised in the reference; 0 here (the first test then sees a
+        # relative change of 1)
+        self._object_old = 0.0
+
+    def isConvergence(self, epsilon, minstep):
+        """0 when |object_old - object_f| / object_f < epsilon and optstep >
+        minstep, else 1 with object_old = object_f (opt_base.hpp:28-43)."""
+        with np.errstate(divide="ignore", invalid="ignore"):
+            change = np.float64(abs(self._object_old - self.object_f)) / np.float64(self.object_f)
+        if change < epsilon and self.optstep > minstep:
+            return 0
+        self._object_old = self.object_f
+        return 1
 
 
 class OC:

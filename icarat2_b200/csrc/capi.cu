@@ -9,6 +9,9 @@
 
 int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
                            const icarat_bc *bc, int device, icarat_ctx **out);
+int icarat_ctx_create_sel_impl(const icarat_grid *grid, const icarat_material *mat,
+                               const icarat_bc *bc, int nsel, const double *boxes,
+                               int device, icarat_ctx **out);
 int icarat_ctx_destroy_impl(icarat_ctx *c);
 
 namespace icarat_b200
@@ -27,6 +30,7 @@ void set_capturing(bool on) { g_capturing = on; }
 
 void build_rhs(icarat_ctx *c);
 int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0);
+int loop_is_convergence(icarat_ctx *c, double epsilon, double minstep, int *convergence);
 int loop_step(icarat_ctx *c, icarat_step_info *info);
 int loop_get(icarat_ctx *c, int which, double *out);
 int set_load_cases(icarat_ctx *c, int ncases, const double *fext);
@@ -57,6 +61,12 @@ static void check_ctx(const icarat_ctx *c)
 {
   IREQUIRE(c != nullptr, ICARAT_ERR_ARG, "null context");
   ICK(cudaSetDevice(c->device));
+}
+
+static void no_selection(const icarat_ctx *c, const char *what)
+{
+  IREQUIRE(!c->sel, ICARAT_ERR_UNSUPPORTED,
+           std::string(what) + " is not available on a selected (sub-)mesh");
 }
 
 static const icarat_solve_opts kDefaultSolve = {ICARAT_SOLVER_JACOBI_PCG, 1.0e-10,
@@ -146,6 +156,38 @@ int icarat_ctx_create(const icarat_grid *grid, const icarat_material *mat,
   ICARAT_API_END
 }
 
+int icarat_ctx_create_selection(const icarat_grid *grid, const icarat_material *mat,
+                                const icarat_bc *bc, int nsel, const double *boxes,
+                                int device, icarat_ctx **out)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(nsel >= 1 && boxes, ICARAT_ERR_ARG, "a selection needs at least one box");
+  return icarat_ctx_create_sel_impl(grid, mat, bc, nsel, boxes, device, out);
+  ICARAT_API_END
+}
+
+int icarat_selection_ids(const icarat_ctx *c, int *node_ids, int *elem_ids)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(c, ICARAT_ERR_ARG, "null context");
+  if(c->sel)
+  {
+    if(node_ids)
+      std::memcpy(node_ids, c->sel_node_h.data(), sizeof(int) * c->sel_node_h.size());
+    if(elem_ids)
+      std::memcpy(elem_ids, c->sel_elem_h.data(), sizeof(int) * c->sel_elem_h.size());
+  }
+  else
+  {
+    for(int n = 0; node_ids && n < c->numnp; n++)
+      node_ids[n] = n;
+    for(int e = 0; elem_ids && e < c->nelx; e++)
+      elem_ids[e] = e;
+  }
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
 int icarat_ctx_destroy(icarat_ctx *c)
 {
   ICARAT_API_BEGIN
@@ -159,11 +201,11 @@ int icarat_sizes(const icarat_ctx *c, int *numnp, int *nelx, int *neq, int *nume
   ICARAT_API_BEGIN
   IREQUIRE(c, ICARAT_ERR_ARG, "null context");
   if(numnp)
-    *numnp = c->numnp;
+    *numnp = c->sel ? c->numnp_sel : c->numnp;
   if(nelx)
-    *nelx = c->nelx;
+    *nelx = abi_nelx(c);
   if(neq)
-    *neq = c->neq;
+    *neq = c->sel ? 3 * c->numnp_sel : c->neq;
   if(numeq)
     *numeq = c->numeq;
   return ICARAT_OK;
@@ -192,7 +234,12 @@ int icarat_dof_map(const icarat_ctx *c, int *node_dof)
 {
   ICARAT_API_BEGIN
   IREQUIRE(c && node_dof, ICARAT_ERR_ARG, "null argument");
-  std::memcpy(node_dof, c->dof.data(), sizeof(int) * c->dof.size());
+  if(c->sel)
+    for(size_t q = 0; q < c->sel_node_h.size(); q++)
+      for(int d = 0; d < 3; d++)
+        node_dof[3 * q + d] = c->dof[3 * (size_t)c->sel_node_h[q] + d];
+  else
+    std::memcpy(node_dof, c->dof.data(), sizeof(int) * c->dof.size());
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -223,7 +270,7 @@ int icarat_set_design(icarat_ctx *c, const double *design_s)
   ICARAT_API_BEGIN
   check_ctx(c);
   IREQUIRE(design_s, ICARAT_ERR_ARG, "null argument");
-  h2d(c, c->d_rho, design_s, c->nelx);
+  elem_in(c, design_s, true, c->d_rho);
   set_design_device(c, c->d_rho);
   return ICARAT_OK;
   ICARAT_API_END
@@ -234,6 +281,11 @@ int icarat_set_design_dev(icarat_ctx *c, const double *design_s)
   ICARAT_API_BEGIN
   check_ctx(c);
   IREQUIRE(design_s, ICARAT_ERR_ARG, "null argument");
+  if(c->sel)
+  {
+    elem_in(c, design_s, false, c->d_rho);
+    design_s = c->d_rho;
+  }
   set_design_device(c, design_s);
   return ICARAT_OK;
   ICARAT_API_END
@@ -415,7 +467,16 @@ int icarat_node_values(icarat_ctx *c, double *node_val)
   IREQUIRE(node_val, ICARAT_ERR_ARG, "null argument");
   IREQUIRE(c->solved, ICARAT_ERR_STATE, "solve first");
   node_values_dev(c, c->d_v1);
-  d2h(c, node_val, c->d_v1, c->neq);
+  if(c->sel)
+  {
+    std::vector<double> all((size_t)c->neq);
+    d2h(c, all.data(), c->d_v1, c->neq);
+    for(size_t q = 0; q < c->sel_node_h.size(); q++)
+      for(int d = 0; d < 3; d++)
+        node_val[3 * q + d] = all[3 * (size_t)c->sel_node_h[q] + d];
+  }
+  else
+    d2h(c, node_val, c->d_v1, c->neq);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -427,7 +488,7 @@ int icarat_mises(icarat_ctx *c, double *mises)
   IREQUIRE(mises, ICARAT_ERR_ARG, "null argument");
   double *a = stage(c, 0);
   mises_dev(c, a);
-  d2h(c, mises, a, c->nelx);
+  elem_out(c, a, mises, true);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -437,7 +498,14 @@ int icarat_mises_dev(icarat_ctx *c, double *mises)
   ICARAT_API_BEGIN
   check_ctx(c);
   IREQUIRE(mises, ICARAT_ERR_ARG, "null argument");
-  mises_dev(c, mises);
+  if(c->sel)
+  {
+    double *a = stage(c, 0);
+    mises_dev(c, a);
+    elem_out(c, a, mises, false);
+  }
+  else
+    mises_dev(c, mises);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -466,6 +534,7 @@ int icarat_write_vtk(icarat_ctx *c, const char *path, int binary)
   ICARAT_API_BEGIN
   check_ctx(c);
   IREQUIRE(path, ICARAT_ERR_ARG, "null argument");
+  no_selection(c, "icarat_write_vtk");
   IREQUIRE(c->solved, ICARAT_ERR_STATE, "solve first");
   std::vector<double> nv((size_t)c->neq), rho((size_t)c->nelx), mis((size_t)c->nelx);
   node_values_dev(c, c->d_v1);
@@ -498,9 +567,9 @@ int icarat_sensitivity(icarat_ctx *c, double scale, double *dfds, double *dgds)
   double *a = stage(c, 0), *b = stage(c, 1);
   sensitivity_dev(c, scale, dfds ? a : nullptr, dgds ? b : nullptr);
   if(dfds)
-    d2h(c, dfds, a, c->nelx);
+    elem_out(c, a, dfds, true);
   if(dgds)
-    d2h(c, dgds, b, c->nelx);
+    elem_out(c, b, dgds, true);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -509,7 +578,17 @@ int icarat_sensitivity_dev(icarat_ctx *c, double scale, double *dfds, double *dg
 {
   ICARAT_API_BEGIN
   check_ctx(c);
-  sensitivity_dev(c, scale, dfds, dgds);
+  if(c->sel)
+  {
+    double *a = stage(c, 0), *b = stage(c, 1);
+    sensitivity_dev(c, scale, dfds ? a : nullptr, dgds ? b : nullptr);
+    if(dfds)
+      elem_out(c, a, dfds, false);
+    if(dgds)
+      elem_out(c, b, dgds, false);
+  }
+  else
+    sensitivity_dev(c, scale, dfds, dgds);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -529,9 +608,9 @@ int icarat_density_filter(icarat_ctx *c, const double *in, double *out, int is_s
   check_ctx(c);
   IREQUIRE(in && out, ICARAT_ERR_ARG, "null argument");
   double *a = stage(c, 0), *b = stage(c, 1);
-  h2d(c, a, in, c->nelx);
+  elem_in(c, in, true, a);
   filter_apply(c, a, b, is_sens != 0);
-  d2h(c, out, b, c->nelx);
+  elem_out(c, b, out, true);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -542,7 +621,15 @@ int icarat_density_filter_dev(icarat_ctx *c, const double *in, double *out,
   ICARAT_API_BEGIN
   check_ctx(c);
   IREQUIRE(in && out && in != out, ICARAT_ERR_ARG, "need distinct in/out");
-  filter_apply(c, in, out, is_sens != 0);
+  if(c->sel)
+  {
+    double *a = stage(c, 0), *b = stage(c, 1);
+    elem_in(c, in, false, a);
+    filter_apply(c, a, b, is_sens != 0);
+    elem_out(c, b, out, false);
+  }
+  else
+    filter_apply(c, in, out, is_sens != 0);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -551,6 +638,7 @@ int icarat_helmholtz_setup(icarat_ctx *c, double radius)
 {
   ICARAT_API_BEGIN
   check_ctx(c);
+  no_selection(c, "the Helmholtz filter");
   helm_setup(c, radius);
   return ICARAT_OK;
   ICARAT_API_END
@@ -587,10 +675,10 @@ int icarat_sensitivity_filter(icarat_ctx *c, const double *design_s,
   check_ctx(c);
   IREQUIRE(design_s && dfds && out, ICARAT_ERR_ARG, "null argument");
   double *a = stage(c, 0), *b = stage(c, 1), *o = stage(c, 2);
-  h2d(c, a, design_s, c->nelx);
-  h2d(c, b, dfds, c->nelx);
+  elem_in(c, design_s, true, a);
+  elem_in(c, dfds, true, b);
   sensitivity_filter_dev(c, a, b, o);
-  d2h(c, out, o, c->nelx);
+  elem_out(c, o, out, true);
   return ICARAT_OK;
   ICARAT_API_END
 }
@@ -601,9 +689,9 @@ static int threshold_impl(icarat_ctx *c, const double *in, double beta, double T
   check_ctx(c);
   IREQUIRE(in && out, ICARAT_ERR_ARG, "null argument");
   double *a = stage(c, 0), *b = stage(c, 1);
-  h2d(c, a, in, c->nelx);
+  elem_in(c, in, true, a);
   threshold_dev(c, a, beta, T, b, der);
-  d2h(c, out, b, c->nelx);
+  elem_out(c, b, out, true);
   return ICARAT_OK;
 }
 
@@ -634,14 +722,14 @@ int icarat_oc_update(icarat_ctx *c, double *x, const double *dfdx, double g,
   IREQUIRE(x && dfdx && dgdx && xmin && xmax, ICARAT_ERR_ARG, "null argument");
   double *dx = stage(c, 0), *ddf = stage(c, 1), *ddg = stage(c, 2),
          *dmin = stage(c, 3), *dmax = stage(c, 4);
-  h2d(c, dx, x, c->nelx);
-  h2d(c, ddf, dfdx, c->nelx);
-  h2d(c, ddg, dgdx, c->nelx);
-  h2d(c, dmin, xmin, c->nelx);
-  h2d(c, dmax, xmax, c->nelx);
+  elem_in(c, x, true, dx);
+  elem_in(c, dfdx, true, ddf);
+  elem_in(c, dgdx, true, ddg);
+  elem_in(c, xmin, true, dmin);
+  elem_in(c, xmax, true, dmax);
   int st = oc_update_dev(c, dx, ddf, g, ddg, dmin, dmax, opts ? opts : &kDefaultOc,
                          steps);
-  d2h(c, x, dx, c->nelx);
+  elem_out(c, dx, x, true);
   return st;
   ICARAT_API_END
 }
@@ -653,6 +741,20 @@ int icarat_oc_update_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
   ICARAT_API_BEGIN
   check_ctx(c);
   IREQUIRE(x && dfdx && dgdx && xmin && xmax, ICARAT_ERR_ARG, "null argument");
+  if(c->sel)
+  {
+    double *dx = stage(c, 0), *ddf = stage(c, 1), *ddg = stage(c, 2),
+           *dmin = stage(c, 3), *dmax = stage(c, 4);
+    elem_in(c, x, false, dx);
+    elem_in(c, dfdx, false, ddf);
+    elem_in(c, dgdx, false, ddg);
+    elem_in(c, xmin, false, dmin);
+    elem_in(c, xmax, false, dmax);
+    const int st = oc_update_dev(c, dx, ddf, g, ddg, dmin, dmax,
+                                 opts ? opts : &kDefaultOc, steps);
+    elem_out(c, dx, x, false);
+    return st;
+  }
   return oc_update_dev(c, x, dfdx, g, dgdx, xmin, xmax, opts ? opts : &kDefaultOc,
                        steps);
   ICARAT_API_END
@@ -689,6 +791,16 @@ int icarat_loop_set_domains(icarat_ctx *c, const int *design_ids, int n_design,
   ICARAT_API_BEGIN
   check_ctx(c);
   return loop_set_domains(c, design_ids, n_design, nondesign_ids, n_nondesign);
+  ICARAT_API_END
+}
+
+int icarat_loop_is_convergence(icarat_ctx *c, double epsilon, double minstep,
+                               int *convergence)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(convergence, ICARAT_ERR_ARG, "null argument");
+  return loop_is_convergence(c, epsilon, minstep, convergence);
   ICARAT_API_END
 }
 

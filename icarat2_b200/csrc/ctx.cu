@@ -1,8 +1,11 @@
 // Context setup: structured hexa8 box, Dirichlet boxes, DOF numbering, point
 // loads, device arrays, and the numeq <-> node-vector conversions.
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <string>
 
 #include "internal.cuh"
 
@@ -46,19 +49,39 @@ __global__ void k_gather_free(int numeq, const int *__restrict__ free_idx,
 }
 
 // SIMP (src/problem/elasticity.hpp:13-17)
-// (E32: the same moduli rounded to FP32 for the reduced-precision operators)
+// (E32: the same moduli rounded to FP32 for the reduced-precision operators;
+// elements removed by a selection have no stiffness at all: E = 0)
 __global__ void k_simp(int n, const double *__restrict__ rho, double e1,
-                       double e2, double p, double *__restrict__ E,
-                       float *__restrict__ E32)
+                       double e2, double p, const uint8_t *__restrict__ emask,
+                       double *__restrict__ E, float *__restrict__ E32)
 {
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
       i += gridDim.x * blockDim.x)
   {
     double rp = pow(rho[i], p);
-    const double e = (1.0 - rp) * e1 + rp * e2;
+    double e = (1.0 - rp) * e1 + rp * e2;
+    if(emask && !emask[i])
+      e = 0.0;
     E[i] = e;
     E32[i] = (float)e;
   }
+}
+
+// kept -> box element layout (removed elements 0 beforehand) and back
+__global__ void k_sel_scatter(int n, const int *__restrict__ map,
+                              const double *__restrict__ in, double *__restrict__ out)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+    out[map[i]] = in[i];
+}
+
+__global__ void k_sel_gather(int n, const int *__restrict__ map,
+                             const double *__restrict__ in, double *__restrict__ out)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+    out[i] = in[map[i]];
 }
 
 static int grid_for(int n, int threads = 256)
@@ -121,6 +144,62 @@ void from_full(icarat_ctx *c, const double *full_in, double *out, bool host_dst)
   }
 }
 
+int abi_nelx(const icarat_ctx *c) { return c->sel ? c->nelx_sel : c->nelx; }
+
+void elem_in(icarat_ctx *c, const double *src, bool host_src, double *d_box)
+{
+  if(!c->sel)
+  {
+    if(src != d_box)
+      ICK(cudaMemcpyAsync(d_box, src, sizeof(double) * c->nelx,
+                          host_src ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                          c->stream));
+    return;
+  }
+  const double *in = src;
+  if(host_src)
+  {
+    ICK(cudaMemcpyAsync(c->d_sel_buf, src, sizeof(double) * c->nelx_sel,
+                        cudaMemcpyHostToDevice, c->stream));
+    in = c->d_sel_buf;
+  }
+  ICK(cudaMemsetAsync(d_box, 0, sizeof(double) * c->nelx, c->stream));
+  if(c->nelx_sel > 0)
+  {
+    note_launch();
+    k_sel_scatter<<<grid_for(c->nelx_sel), 256, 0, c->stream>>>(c->nelx_sel, c->d_sel_elem,
+                                                                in, d_box);
+  }
+  ICK(cudaGetLastError());
+}
+
+void elem_out(icarat_ctx *c, const double *d_box, double *dst, bool host_dst)
+{
+  if(!c->sel)
+  {
+    if(dst != d_box)
+      ICK(cudaMemcpyAsync(dst, d_box, sizeof(double) * c->nelx,
+                          host_dst ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                          c->stream));
+  }
+  else
+  {
+    double *out = host_dst ? c->d_sel_buf : dst;
+    if(c->nelx_sel > 0)
+    {
+      note_launch();
+      k_sel_gather<<<grid_for(c->nelx_sel), 256, 0, c->stream>>>(c->nelx_sel,
+                                                                 c->d_sel_elem, d_box, out);
+    }
+    ICK(cudaGetLastError());
+    if(host_dst)
+      ICK(cudaMemcpyAsync(dst, c->d_sel_buf, sizeof(double) * c->nelx_sel,
+                          cudaMemcpyDeviceToHost, c->stream));
+  }
+  if(host_dst)
+    ICK(cudaStreamSynchronize(c->stream));
+}
+
 void set_design_device(icarat_ctx *c, const double *d_rho)
 {
   if(d_rho != c->d_rho)
@@ -129,7 +208,7 @@ void set_design_device(icarat_ctx *c, const double *d_rho)
   note_launch();
   k_simp<<<grid_for(c->nelx), 256, 0, c->stream>>>(
       c->nelx, c->d_rho, c->mat.young_min, c->mat.young_max, c->mat.penalty,
-      c->d_E, c->d_E32);
+      c->d_emask, c->d_E, c->d_E32);
   ICK(cudaGetLastError());
   c->design_set = true;
   c->solved = false;
@@ -209,6 +288,77 @@ static void element_nodes(const icarat_ctx *c, long e, long en[8])
     en[a] = b + o[a];
 }
 
+// [mesh] selection (MeshIcarat::modifyMesh, src/io/mesh_icarat.hpp:636-755):
+// a node is kept when it lies in one of the boxes widened by 1e-7, an element
+// when its centroid (the running sum of x / 8 over its local nodes, in that
+// order) does; kept nodes and elements keep their box order.  A kept element
+// with a removed node is the reference's "error in mesh_icarat" (exit(1)); a
+// kept node that no kept element uses would leave a zero stiffness row and is
+// refused as well.
+static void select_mesh(icarat_ctx *c, int nsel, const double *boxes,
+                        std::vector<uint8_t> &keep_node, std::vector<uint8_t> &keep_elem)
+{
+  const double tol = 1.0e-7;
+  const long NX = c->NX, NY = c->NY;
+  auto coord = [&](long n, int d) -> double
+  {
+    long i = n % NX, j = (n / NX) % NY, k = n / (NX * NY);
+    if(d == 0)
+      return (c->lx / c->nx) * i;
+    if(d == 1)
+      return (c->ly / c->ny) * j;
+    return (c->lz / c->nz) * k;
+  };
+  keep_node.assign(c->numnp, 0);
+  keep_elem.assign(c->nelx, 0);
+  for(int b = 0; b < nsel; b++)
+  {
+    const double *B = boxes + 6 * b;
+    const double lo[3] = {B[0] - tol, B[2] - tol, B[4] - tol};
+    const double hi[3] = {B[1] + tol, B[3] + tol, B[5] + tol};
+    for(long n = 0; n < c->numnp; n++)
+    {
+      const double x = coord(n, 0), y = coord(n, 1), z = coord(n, 2);
+      if(x >= lo[0] && x <= hi[0] && y >= lo[1] && y <= hi[1] && z >= lo[2] && z <= hi[2])
+        keep_node[n] = 1;
+    }
+    for(long e = 0; e < c->nelx; e++)
+    {
+      long en[8];
+      element_nodes(c, e, en);
+      double cx = 0.0, cy = 0.0, cz = 0.0;
+      for(int a = 0; a < 8; a++)
+      {
+        cx += coord(en[a], 0) / 8;
+        cy += coord(en[a], 1) / 8;
+        cz += coord(en[a], 2) / 8;
+      }
+      if(cx >= lo[0] && cx <= hi[0] && cy >= lo[1] && cy <= hi[1] && cz >= lo[2] &&
+         cz <= hi[2])
+        keep_elem[e] = 1;
+    }
+  }
+  std::vector<uint8_t> used(c->numnp, 0);
+  for(long e = 0; e < c->nelx; e++)
+  {
+    if(!keep_elem[e])
+      continue;
+    long en[8];
+    element_nodes(c, e, en);
+    for(int a = 0; a < 8; a++)
+    {
+      IREQUIRE(keep_node[en[a]], ICARAT_ERR_ARG,
+               "selection keeps element " + std::to_string(e) + " but not its node " +
+                   std::to_string(en[a]) + " (error in mesh_icarat)");
+      used[en[a]] = 1;
+    }
+  }
+  for(long n = 0; n < c->numnp; n++)
+    IREQUIRE(!keep_node[n] || used[n], ICARAT_ERR_ARG,
+             "selection keeps node " + std::to_string(n) +
+                 " but no element around it (zero stiffness row)");
+}
+
 // Mesh + BC on the host, mirroring MeshIcarat/BCIcarat:
 //  node coordinates x = (L / div) * index (mesh_icarat.hpp:468-476);
 //  Dirichlet boxes widened by 1e-7, flags kept once 1, values overwritten
@@ -216,8 +366,14 @@ static void element_nodes(const icarat_ctx *c, long e, long en[8])
 //  countDOF numbering (boundary_condition_base.hpp:35-95);
 //  point loads on free components of nodes in the widened box
 //  (boundary_condition_icarat.hpp:213-264, 380-396).
-static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
+// With a selection (keep_node / keep_elem non-null) the boundary conditions
+// see the kept nodes and elements only, as they see the reference's
+// modified mesh; removed nodes get every component fixed and no number.
+static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc,
+                          const std::vector<uint8_t> *keep_node = nullptr,
+                          const std::vector<uint8_t> *keep_elem = nullptr)
 {
+  auto kept = [&](long n) { return !keep_node || (*keep_node)[n] != 0; };
   const double tol = 1.0e-7;
   const long NX = c->NX, NY = c->NY;
   auto coord = [&](long n, int d) -> double
@@ -262,6 +418,8 @@ static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
         for(long i = lo[0]; i <= hi[0]; i++)
         {
           long n = i + j * NX + k * NX * NY;
+          if(!kept(n))
+            continue;
           has[n] = 1;
           for(int q = 0; q < 3; q++)
           {
@@ -276,10 +434,19 @@ static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
   c->uD_h.assign(3 * (size_t)c->numnp, 0.0);
   int counter = 0;
   for(long n = 0; n < c->numnp; n++)
-    for(int q = 0; q < 3; q++)
-      if(!has[n] || flag[3 * n + q] == 0)
-        c->dof[3 * n + q] = counter++;
+    if(kept(n))
+      for(int q = 0; q < 3; q++)
+        if(!has[n] || flag[3 * n + q] == 0)
+          c->dof[3 * n + q] = counter++;
   c->numeq = counter;
+  for(long n = 0; n < c->numnp; n++)
+    if(!kept(n))
+    {
+      // removed node: no equation, no number
+      c->fix_h[n] = 7;
+      for(int q = 0; q < 3; q++)
+        c->dof[3 * n + q] = INT32_MAX;
+    }
   for(long n = 0; n < c->numnp; n++)
     if(has[n])
       for(int q = 0; q < 3; q++)
@@ -307,7 +474,7 @@ static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
     {
       // point load (:380-396)
       for(long n = 0; n < c->numnp; n++)
-        if(inside(n))
+        if(kept(n) && inside(n))
           for(int q = 0; q < 3; q++)
           {
             int d = c->dof[3 * n + q];
@@ -320,6 +487,8 @@ static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
     // nodes inside the box, equivalent nodal forces of the traction L.val
     for(long e = 0; e < c->nelx; e++)
     {
+      if(keep_elem && !(*keep_elem)[e])
+        continue;
       long en[8];
       element_nodes(c, e, en);
       int hits[8], count = 0;
@@ -352,10 +521,23 @@ static void build_mesh_bc(icarat_ctx *c, const icarat_bc *bc)
 
 using namespace icarat_b200;
 
+int icarat_ctx_create_sel_impl(const icarat_grid *grid, const icarat_material *mat,
+                               const icarat_bc *bc, int nsel, const double *boxes,
+                               int device, icarat_ctx **out);
+
 int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
                            const icarat_bc *bc, int device, icarat_ctx **out)
 {
+  return icarat_ctx_create_sel_impl(grid, mat, bc, 0, nullptr, device, out);
+}
+
+// nsel > 0: the [mesh] selection boxes (x0, x1, y0, y1, z0, z1 each)
+int icarat_ctx_create_sel_impl(const icarat_grid *grid, const icarat_material *mat,
+                               const icarat_bc *bc, int nsel, const double *boxes,
+                               int device, icarat_ctx **out)
+{
   IREQUIRE(grid && mat && out, ICARAT_ERR_ARG, "null argument");
+  IREQUIRE(nsel >= 0 && (nsel == 0 || boxes), ICARAT_ERR_ARG, "bad selection");
   IREQUIRE(grid->nx >= 1 && grid->ny >= 1 && grid->nz >= 1, ICARAT_ERR_ARG,
            "division must be >= 1");
   IREQUIRE(grid->lx > 0 && grid->ly > 0 && grid->lz > 0, ICARAT_ERR_ARG,
@@ -397,7 +579,30 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     for(int a = 0; a < 24; a++)
       c->ke_diag_max = std::fmax(c->ke_diag_max, c->ke0.k[25 * a]);
     c->lam_max_dk = jacobi_bound(c->ke0.k);
-    build_mesh_bc(c, bc);
+    if(nsel > 0)
+    {
+      std::vector<uint8_t> keep_node, keep_elem;
+      select_mesh(c, nsel, boxes, keep_node, keep_elem);
+      build_mesh_bc(c, bc, &keep_node, &keep_elem);
+      c->sel = true;
+      for(long n = 0; n < c->numnp; n++)
+        if(keep_node[n])
+          c->sel_node_h.push_back((int)n);
+      for(long e = 0; e < c->nelx; e++)
+        if(keep_elem[e])
+          c->sel_elem_h.push_back((int)e);
+      c->numnp_sel = (int)c->sel_node_h.size();
+      c->nelx_sel = (int)c->sel_elem_h.size();
+      IREQUIRE(c->nelx_sel > 0, ICARAT_ERR_ARG, "the selection keeps no element");
+      ICK(cudaMalloc(&c->d_emask, c->nelx));
+      ICK(cudaMemcpy(c->d_emask, keep_elem.data(), c->nelx, cudaMemcpyHostToDevice));
+      ICK(cudaMalloc(&c->d_sel_elem, sizeof(int) * c->nelx_sel));
+      ICK(cudaMemcpy(c->d_sel_elem, c->sel_elem_h.data(), sizeof(int) * c->nelx_sel,
+                     cudaMemcpyHostToDevice));
+      c->d_sel_buf = dalloc(c->nelx_sel);
+    }
+    else
+      build_mesh_bc(c, bc);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     c->sm_count = sms;
@@ -421,6 +626,9 @@ int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
     // streaming CG kernels at full occupancy (8 blocks of 256 threads per
     // SM): with 4 per SM they reached 3-4 TB/s on the B200
     c->red_blocks = sms * 8 > kMaxRedBlocks ? kMaxRedBlocks : sms * 8;
+    // icarat_solve_noalloc's buffer: its address is taken here, where the
+    // context allocates anyway, so that the solve itself never loads a module
+    noalloc_resolve(c);
 
     // free-DOF map: equation number -> 3 node + component
     std::vector<int> freeidx(c->numeq > 0 ? c->numeq : 1);
@@ -503,6 +711,10 @@ int icarat_ctx_destroy_impl(icarat_ctx *c)
                    c->loop.xmax, c->loop.d_cases, c->loop.d_cases_u, c->loop.d_volw})
     dfree(p);
   dfree(c->loop.d_fixed);
+  dfree(c->loop.d_sel);
+  dfree(c->d_emask);
+  dfree(c->d_sel_elem);
+  dfree(c->d_sel_buf);
   dfree(c->d_free);
   dfree(c->d_fix);
   dfree(c->d_uD);

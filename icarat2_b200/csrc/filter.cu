@@ -14,9 +14,12 @@
 namespace icarat_b200
 {
 
+// box elements; mask (null without a selection): 1 on the elements a
+// selection keeps.  Removed elements are no neighbours and get 0.
 struct ElemGrid
 {
   int nx, ny, nz, nelx;
+  const uint8_t *mask;
 };
 
 // dfilters_ds: a_i = sum over valid neighbours of w (geometry only)
@@ -26,12 +29,19 @@ __global__ void k_filter_aa(ElemGrid g, int nofs, const int *__restrict__ ofs,
   for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelx;
       e += gridDim.x * blockDim.x)
   {
+    if(g.mask && !g.mask[e])
+    {
+      aa[e] = 0.0;
+      continue;
+    }
     const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
     double a = 0.0;
     for(int q = 0; q < nofs; q++)
     {
       const int ii = i + ofs[3 * q], jj = j + ofs[3 * q + 1], kk = k + ofs[3 * q + 2];
       if(ii < 0 || ii >= g.nx || jj < 0 || jj >= g.ny || kk < 0 || kk >= g.nz)
+        continue;
+      if(g.mask && !g.mask[ii + (long)jj * g.nx + (long)kk * g.nx * g.ny])
         continue;
       a = __dadd_rn(a, w[q]);
     }
@@ -47,6 +57,11 @@ __global__ void k_filter_fwd(ElemGrid g, int nofs, const int *__restrict__ ofs,
   for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelx;
       e += gridDim.x * blockDim.x)
   {
+    if(g.mask && !g.mask[e])
+    {
+      out[e] = 0.0;
+      continue;
+    }
     const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
     double a = 0.0, b = 0.0;
     for(int q = 0; q < nofs; q++)
@@ -54,10 +69,12 @@ __global__ void k_filter_fwd(ElemGrid g, int nofs, const int *__restrict__ ofs,
       const int ii = i + ofs[3 * q], jj = j + ofs[3 * q + 1], kk = k + ofs[3 * q + 2];
       if(ii < 0 || ii >= g.nx || jj < 0 || jj >= g.ny || kk < 0 || kk >= g.nz)
         continue;
+      const long f = ii + (long)jj * g.nx + (long)kk * g.nx * g.ny;
+      if(g.mask && !g.mask[f])
+        continue;
       const double wq = w[q];
       a = __dadd_rn(a, wq);
-      b = __dadd_rn(b, __dmul_rn(wq, __ldg(in + ii + (long)jj * g.nx +
-                                           (long)kk * g.nx * g.ny)));
+      b = __dadd_rn(b, __dmul_rn(wq, __ldg(in + f)));
     }
     out[e] = __ddiv_rn(b, a);
   }
@@ -73,6 +90,11 @@ __global__ void k_filter_trans(ElemGrid g, int nofs, const int *__restrict__ ofs
   for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelx;
       e += gridDim.x * blockDim.x)
   {
+    if(g.mask && !g.mask[e])
+    {
+      out[e] = 0.0;
+      continue;
+    }
     const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
     double s = 0.0;
     for(int q = 0; q < nofs; q++)
@@ -81,6 +103,8 @@ __global__ void k_filter_trans(ElemGrid g, int nofs, const int *__restrict__ ofs
       if(ii < 0 || ii >= g.nx || jj < 0 || jj >= g.ny || kk < 0 || kk >= g.nz)
         continue;
       const long f = ii + (long)jj * g.nx + (long)kk * g.nx * g.ny;
+      if(g.mask && !g.mask[f])
+        continue;
       s = __dadd_rn(s, __ddiv_rn(__dmul_rn(w[q], __ldg(in + f)), __ldg(aa + f)));
     }
     out[e] = s;
@@ -98,6 +122,12 @@ __global__ void k_filter_trans2(ElemGrid g, int nofs, const int *__restrict__ of
   for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelx;
       e += gridDim.x * blockDim.x)
   {
+    if(g.mask && !g.mask[e])
+    {
+      out1[e] = 0.0;
+      out2[e] = 0.0;
+      continue;
+    }
     const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
     double s1 = 0.0, s2 = 0.0;
     for(int q = 0; q < nofs; q++)
@@ -106,6 +136,8 @@ __global__ void k_filter_trans2(ElemGrid g, int nofs, const int *__restrict__ of
       if(ii < 0 || ii >= g.nx || jj < 0 || jj >= g.ny || kk < 0 || kk >= g.nz)
         continue;
       const long f = ii + (long)jj * g.nx + (long)kk * g.nx * g.ny;
+      if(g.mask && !g.mask[f])
+        continue;
       const double wq = w[q], af = __ldg(aa + f);
       s1 = __dadd_rn(s1, __ddiv_rn(__dmul_rn(wq, __ldg(in1 + f)), af));
       s2 = __dadd_rn(s2, __ddiv_rn(__dmul_rn(wq, __ldg(in2 + f)), af));
@@ -124,6 +156,11 @@ __global__ void k_sens_filter(ElemGrid g, int nofs, const int *__restrict__ ofs,
   for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelx;
       e += gridDim.x * blockDim.x)
   {
+    if(g.mask && !g.mask[e])
+    {
+      out[e] = 0.0;
+      continue;
+    }
     const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
     double a = 0.0, b = 0.0;
     for(int q = 0; q < nofs; q++)
@@ -132,6 +169,8 @@ __global__ void k_sens_filter(ElemGrid g, int nofs, const int *__restrict__ ofs,
       if(ii < 0 || ii >= g.nx || jj < 0 || jj >= g.ny || kk < 0 || kk >= g.nz)
         continue;
       const long f = ii + (long)jj * g.nx + (long)kk * g.nx * g.ny;
+      if(g.mask && !g.mask[f])
+        continue;
       const double wq = w[q], sf = s[f];
       a = __dadd_rn(a, wq);
       b = __dadd_rn(b, __ddiv_rn(__dmul_rn(__dmul_rn(wq, sf), df[f]),
@@ -158,7 +197,7 @@ __global__ void k_threshold(int n, const double *__restrict__ in, double beta,
 
 static ElemGrid egrid(const icarat_ctx *c)
 {
-  return ElemGrid{c->nx, c->ny, c->nz, c->nelx};
+  return ElemGrid{c->nx, c->ny, c->nz, c->nelx, c->d_emask};
 }
 
 static int eblocks(const icarat_ctx *c)

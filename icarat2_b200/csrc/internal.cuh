@@ -253,6 +253,9 @@ struct LoopState
   icarat_loop_opts opts;
   int optstep = 0;
   double V0 = 0.0;
+  // objective of the last step and the one isConvergence last kept
+  // (Optimize::object_f / object_old, opt_base.hpp:73-77)
+  double object_f = 0.0, object_old = 0.0;
   double *x = nullptr, *xfil = nullptr, *xthr = nullptr, *thrd = nullptr,
          *dfds = nullptr, *dgds = nullptr, *tmp = nullptr, *tmp2 = nullptr,
          *xmin = nullptr, *xmax = nullptr;
@@ -264,6 +267,9 @@ struct LoopState
   std::vector<uint8_t> cases_have;  // a case's last solution is held
   double *d_volw = nullptr;   // element volume on design IDs, 0 elsewhere
   uint8_t *d_fixed = nullptr; // 1 on non-design IDs
+  // with a selection, the MMA update runs on the kept elements only:
+  // x, dfds, dgds, xmin, xmax gathered (5 nelx_sel)
+  double *d_sel = nullptr;
 };
 
 } // namespace icarat_b200
@@ -330,6 +336,18 @@ struct icarat_ctx
   // changes): a warm start may begin from it
   bool have_u = false;
   icarat_solve_info last_info{};
+  // [mesh] selection (MeshIcarat::modifyMesh): the kept box elements and
+  // nodes, numbered in ascending box order; every device array stays in box
+  // layout, removed elements have E = 0 and removed nodes are fully fixed
+  bool sel = false;
+  int nelx_sel = 0, numnp_sel = 0;
+  std::vector<int> sel_elem_h, sel_node_h; // kept id -> box id
+  uint8_t *d_emask = nullptr;  // box elements: 1 kept (null without selection)
+  int *d_sel_elem = nullptr;   // kept element id -> box element id
+  double *d_sel_buf = nullptr; // nelx_sel staging of the ABI's element vectors
+  // device address of icarat_solve_noalloc's static work buffer on this
+  // context's device, resolved when the context is created
+  double *noalloc_scratch = nullptr;
   // multigrid
   std::vector<icarat_b200::MgLevel> mg;
   int mg_built_levels = 0;
@@ -356,7 +374,15 @@ void hexa8_stiffness(double hx, double hy, double hz, double nu, double *ke,
                      double *volume);
 double jacobi_bound(const double *ke);
 
+// noalloc.cu: resolves c->noalloc_scratch (context creation)
+void noalloc_resolve(icarat_ctx *c);
+
 // ctx.cu
+// element vectors at the ABI (nelx_sel entries with a selection) <-> box
+// layout on the device (removed elements 0)
+int abi_nelx(const icarat_ctx *c);
+void elem_in(icarat_ctx *c, const double *src, bool host_src, double *d_box);
+void elem_out(icarat_ctx *c, const double *d_box, double *dst, bool host_dst);
 void to_full(icarat_ctx *c, const double *numeq_in, double *full_out,
              bool host_src);
 void from_full(icarat_ctx *c, const double *full_in, double *numeq_out,

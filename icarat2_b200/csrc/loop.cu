@@ -25,6 +25,20 @@ __global__ void k_fill(int n, double v, double *__restrict__ out)
     out[i] = v;
 }
 
+// v on kept elements, 0 on elements a selection removed (mask null: all kept)
+__global__ void k_fill_kept(int n, double v, const uint8_t *__restrict__ emask,
+                            double *__restrict__ out)
+{
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += gridDim.x * blockDim.x)
+    out[i] = (emask && !emask[i]) ? 0.0 : v;
+}
+
+__global__ void k_sel_gather(int n, const int *__restrict__ map,
+                             const double *__restrict__ in, double *__restrict__ out);
+__global__ void k_sel_scatter(int n, const int *__restrict__ map,
+                              const double *__restrict__ in, double *__restrict__ out);
+
 __global__ void k_mul2(int n, const double *__restrict__ s, double *__restrict__ a,
                        double *__restrict__ b)
 {
@@ -69,6 +83,8 @@ int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
   IREQUIRE(o->method == 0 || o->method == 1, ICARAT_ERR_ARG, "method must be 0 (OC) or 1 (MMA)");
   IREQUIRE(o->filter_kind == 0 || o->filter_kind == 1, ICARAT_ERR_ARG,
            "filter_kind must be 0 (radius) or 1 (Helmholtz)");
+  IREQUIRE(!(c->sel && o->filter_kind == 1), ICARAT_ERR_UNSUPPORTED,
+           "the Helmholtz filter is not available on a selected (sub-)mesh");
   LoopState &L = c->loop;
   const int n = c->nelx;
   if(!L.x)
@@ -85,12 +101,16 @@ int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
   L.opts = *o;
   L.optstep = 0;
   L.V0 = 0.0;
+  L.object_f = 0.0;
+  L.object_old = 0.0;
   loop_free_domains(c);
   if(o->filter_kind == 1)
     helm_setup(c, o->filter_radius);
   else
     filter_setup(c, o->filter_radius);
-  ICK(cudaMemcpyAsync(L.x, x0, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  elem_in(c, x0, true, L.x);
+  if(c->sel && !L.d_sel)
+    L.d_sel = dalloc(5 * (size_t)c->nelx_sel);
   note_launch();
   k_fill<<<eb(n), 256, 0, c->stream>>>(n, o->xmin, L.xmin);
   note_launch();
@@ -99,7 +119,9 @@ int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0)
   if(o->method == 1)
   {
     // MMASolver mma(nelx, 1) with SetMoveLimit (opt_mma_Helmholtz.cpp uses 0.2)
-    mma_create(c->device, n, 1, 0.0, 100000.0, 0.0, &L.mma, c->stream);
+    // (on the kept elements of a selection: the reference's MMA has nelx of
+    // the modified mesh variables)
+    mma_create(c->device, abi_nelx(c), 1, 0.0, 100000.0, 0.0, &L.mma, c->stream);
     mma_set_move(L.mma, o->move);
   }
   ICK(cudaStreamSynchronize(c->stream));
@@ -173,7 +195,7 @@ static double loop_constraint(icarat_ctx *c)
   if(!w)
   {
     note_launch();
-    k_fill<<<eb(n), 256, 0, c->stream>>>(n, c->vol0, L.tmp);
+    k_fill_kept<<<eb(n), 256, 0, c->stream>>>(n, c->vol0, c->d_emask, L.tmp);
     w = L.tmp;
   }
   const double vol = device_dot(c, L.xthr, w, n);
@@ -216,7 +238,28 @@ static int loop_finish(icarat_ctx *c, double beta, double constraint, int *ustep
   ICK(cudaGetLastError());
   int ust = ICARAT_OK;
   *usteps = 0;
-  if(o.method == 1)
+  if(o.method == 1 && c->sel)
+  {
+    // MMA over the kept elements: gather, update, scatter the design back
+    const int m = c->nelx_sel;
+    double *sx = L.d_sel, *sdf = sx + m, *sdg = sx + 2L * m, *smin = sx + 3L * m,
+           *smax = sx + 4L * m;
+    const double *src[5] = {L.x, L.dfds, L.dgds, L.xmin, L.xmax};
+    double *dst[5] = {sx, sdf, sdg, smin, smax};
+    for(int q = 0; q < 5; q++)
+    {
+      note_launch();
+      k_sel_gather<<<eb(m), 256, 0, c->stream>>>(m, c->d_sel_elem, src[q], dst[q]);
+    }
+    ICK(cudaGetLastError());
+    double g = constraint;
+    ust = mma_update_device(L.mma, sx, sdf, &g, sdg, smin, smax);
+    *usteps = mma_last_newton(L.mma);
+    note_launch();
+    k_sel_scatter<<<eb(m), 256, 0, c->stream>>>(m, c->d_sel_elem, sx, L.x);
+    ICK(cudaGetLastError());
+  }
+  else if(o.method == 1)
   {
     double g = constraint;
     ust = mma_update_device(L.mma, L.x, L.dfds, &g, L.dgds, L.xmin, L.xmax);
@@ -263,6 +306,7 @@ int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
   sensitivity_dev(c, o.method == 1 ? 1.0 / L.V0 : 1.0, L.dfds, L.dgds);
   int usteps = 0;
   const int ust = loop_finish(c, beta, constraint, &usteps);
+  L.object_f = compliance;
   if(info)
   {
     info->step = L.optstep;
@@ -340,6 +384,7 @@ static int loop_step_cases(icarat_ctx *c, double beta, icarat_step_info *info)
   c->d_fext = own;
   int usteps = 0;
   const int ust = loop_finish(c, beta, constraint, &usteps);
+  L.object_f = compliance;
   if(info)
   {
     info->step = L.optstep;
@@ -405,19 +450,25 @@ int loop_set_domains(icarat_ctx *c, const int *design_ids, int n_design,
   IREQUIRE(n_design >= 0 && n_nondesign >= 0 && (n_design == 0 || design_ids) &&
                (n_nondesign == 0 || nondesign_ids),
            ICARAT_ERR_ARG, "bad domain lists");
-  const int n = c->nelx;
-  std::vector<double> w(n, design_ids ? 0.0 : c->vol0);
+  const int n = c->nelx, na = abi_nelx(c);
+  // IDs are element numbers of the (selected) mesh; box ids inside
+  auto box_id = [&](int id) { return c->sel ? c->sel_elem_h[id] : id; };
+  std::vector<double> w(n, 0.0);
+  if(!design_ids)
+    for(int q = 0; q < na; q++)
+      w[box_id(q)] = c->vol0;
   for(int q = 0; q < n_design; q++)
   {
-    IREQUIRE(design_ids[q] >= 0 && design_ids[q] < n, ICARAT_ERR_ARG, "design ID out of range");
-    w[design_ids[q]] = c->vol0;
+    IREQUIRE(design_ids[q] >= 0 && design_ids[q] < na, ICARAT_ERR_ARG,
+             "design ID out of range");
+    w[box_id(design_ids[q])] = c->vol0;
   }
   std::vector<uint8_t> f(n, 0);
   for(int q = 0; q < n_nondesign; q++)
   {
-    IREQUIRE(nondesign_ids[q] >= 0 && nondesign_ids[q] < n, ICARAT_ERR_ARG,
+    IREQUIRE(nondesign_ids[q] >= 0 && nondesign_ids[q] < na, ICARAT_ERR_ARG,
              "non-design ID out of range");
-    f[nondesign_ids[q]] = 1;
+    f[box_id(nondesign_ids[q])] = 1;
   }
   if(!L.d_volw)
     L.d_volw = dalloc(n);
@@ -437,6 +488,26 @@ void loop_free_domains(icarat_ctx *c)
   L.d_fixed = nullptr;
 }
 
+// Optimize::isConvergence(epsilon, minstep) (src/optimization/opt_base.hpp:28-43)
+// on the loop's objective: 0 when |object_old - object_f| / object_f < epsilon
+// and optstep > minstep, else 1 with object_old = object_f.  The reference
+// leaves object_old uninitialised before the first call; here it starts at 0,
+// so the first call compares against |object_f| / object_f = 1.
+int loop_is_convergence(icarat_ctx *c, double epsilon, double minstep, int *convergence)
+{
+  LoopState &L = c->loop;
+  IREQUIRE(L.init, ICARAT_ERR_STATE, "icarat_loop_init first");
+  IREQUIRE(L.optstep > 0, ICARAT_ERR_STATE, "icarat_loop_step first");
+  if(std::fabs(L.object_old - L.object_f) / L.object_f < epsilon && L.optstep > minstep)
+    *convergence = 0;
+  else
+  {
+    L.object_old = L.object_f;
+    *convergence = 1;
+  }
+  return ICARAT_OK;
+}
+
 int loop_get(icarat_ctx *c, int which, double *out)
 {
   LoopState &L = c->loop;
@@ -451,9 +522,7 @@ int loop_get(icarat_ctx *c, int which, double *out)
   case 4: src = L.dgds; break;
   default: throw Error{ICARAT_ERR_ARG, "which must be 0..4"};
   }
-  ICK(cudaMemcpyAsync(out, src, sizeof(double) * c->nelx, cudaMemcpyDeviceToHost,
-                      c->stream));
-  ICK(cudaStreamSynchronize(c->stream));
+  elem_out(c, src, out, true);
   return ICARAT_OK;
 }
 

@@ -979,6 +979,8 @@ int icarat_net_train_step(icarat_net *N, icarat_ctx *c, const double *rho, const
                           const double *u, double lr, double *loss)
 {
   ICARAT_API_BEGIN
+  IREQUIRE(c == nullptr || !c->sel, ICARAT_ERR_UNSUPPORTED,
+           "the learned preconditioner is not available on a selected (sub-)mesh");
   IREQUIRE(N && c && rho && f && u, ICARAT_ERR_ARG, "null argument");
   IREQUIRE(lr >= 0.0, ICARAT_ERR_ARG, "learning rate must be >= 0");
   ICK(cudaSetDevice(c->device));
@@ -1070,6 +1072,8 @@ int icarat_net_infer_dev(icarat_net *N, icarat_ctx *c, const double *f, double *
 int icarat_ctx_set_net(icarat_ctx *c, icarat_net *N)
 {
   ICARAT_API_BEGIN
+  IREQUIRE(c == nullptr || !c->sel, ICARAT_ERR_UNSUPPORTED,
+           "the learned preconditioner is not available on a selected (sub-)mesh");
   IREQUIRE(c, ICARAT_ERR_ARG, "null context");
   c->net = N;
   return ICARAT_OK;

@@ -31,6 +31,7 @@ struct OcArgs
   double *result;    // [0] steps, [1] lambda
   double move, iota, lmin, lmax, leps, g, vol, beta, T;
   int maxiter, use_thr;
+  const uint8_t *emask; // elements kept by a selection (null: all)
 };
 
 __device__ __forceinline__ double oc_trial(const OcArgs &a, int i, double lambda)
@@ -65,11 +66,13 @@ __global__ void __launch_bounds__(256) k_oc_bisect(OcArgs a)
   {
     lambda = 0.5 * (l1 + l0);
     for(int e = tid; e < a.nelx; e += stride)
-      a.xk[e] = oc_trial(a, e, lambda);
+      a.xk[e] = (a.emask && !a.emask[e]) ? 0.0 : oc_trial(a, e, lambda);
     grid.sync();
     double part = 0.0;
     for(int e = tid; e < a.nelx; e += stride)
     {
+      if(a.emask && !a.emask[e])
+        continue;
       const int i = e % a.nx, j = (e / a.nx) % a.ny, k = e / (a.nx * a.ny);
       double aa = 0.0, bb = 0.0;
       for(int q = 0; q < a.nofs; q++)
@@ -78,11 +81,13 @@ __global__ void __launch_bounds__(256) k_oc_bisect(OcArgs a)
                   kk = k + a.ofs[3 * q + 2];
         if(ii < 0 || ii >= a.nx || jj < 0 || jj >= a.ny || kk < 0 || kk >= a.nz)
           continue;
+        const long f = ii + (long)jj * a.nx + (long)kk * a.nx * a.ny;
+        if(a.emask && !a.emask[f])
+          continue;
         const double wq = a.w[q];
         aa = __dadd_rn(aa, wq);
         // written by other blocks in this launch: bypass L1
-        bb = __dadd_rn(bb, __dmul_rn(wq, __ldcg(a.xk + ii + (long)jj * a.nx +
-                                                  (long)kk * a.nx * a.ny)));
+        bb = __dadd_rn(bb, __dmul_rn(wq, __ldcg(a.xk + f)));
       }
       double rho = __ddiv_rn(bb, aa);
       if(a.use_thr)
@@ -117,7 +122,7 @@ __global__ void k_oc_trial(OcArgs a, double lambda)
 {
   for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < a.nelx;
       e += gridDim.x * blockDim.x)
-    a.xk[e] = oc_trial(a, e, lambda);
+    a.xk[e] = (a.emask && !a.emask[e]) ? 0.0 : oc_trial(a, e, lambda);
 }
 
 __global__ void k_oc_fill(int n, double v, double *__restrict__ out)
@@ -188,6 +193,7 @@ int oc_update_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
   a.T = o->T;
   a.maxiter = o->maxiter;
   a.use_thr = o->use_threshold ? 1 : 0;
+  a.emask = c->d_emask;
   int per_sm = 0, sms = 0;
   ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_oc_bisect, 256, 0));
   ICK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
@@ -239,6 +245,7 @@ int oc_update_helm_dev(icarat_ctx *c, double *x, const double *dfdx, double g,
   a.xk = c->d_e2;
   a.move = o->move;
   a.iota = o->iota;
+  a.emask = c->d_emask;
   const int n = c->nelx;
   const int blocks = (n + 255) / 256 > 4 * c->sm_count ? 4 * c->sm_count : (n + 255) / 256;
   double l0 = o->lambda_min, l1 = o->lambda_max;

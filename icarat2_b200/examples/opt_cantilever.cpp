@@ -3,7 +3,11 @@
 // include/icarat_b200.hpp: same loop body, same call names, GPU underneath.
 //
 // usage: opt_cantilever <nx> <ny> <nz> <steps> <radius> <oc|mma> [MG_CG|Eigen_CG]
-// prints "step <k> <compliance> <constraint>" per design iteration.
+// prints "step <k> <compliance> <constraint> <cg iterations>" per design
+// iteration.  The loop runs while Optimize::isConvergence(1e-5, 50) returns 1
+// (opt_macro_oc.cpp:83,137), at most <steps> iterations, and prints
+// "converged <k>" when the test ended it.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -34,7 +38,9 @@ int main(int argc, char **argv)
     icarat_load load{{0, 0, -1.0}, {{(double)nx, (double)nx}, {py, py}, {0, 0}}};
     Model model(nx, ny, nz, nx, ny, nz, 1e-9, 1.0, 0.3, 3.0, {clamp}, {load});
     const int nelx = model.nelx;
-    std::vector<double> design_s(nelx, 0.3), xmin(nelx, 1e-4), xmax(nelx, 1.0);
+    Optimize optim(nelx, 1, 1e-4, 1.0);
+    std::vector<double> &design_s = optim.design_s, &xmin = optim.xmin, &xmax = optim.xmax;
+    std::fill(design_s.begin(), design_s.end(), 0.3);
     std::vector<double> dfds, dgds;
     double vol = 0.0; // element volume (sum of det J w, elasticity.cpp:249)
     check(icarat_element_stiffness(model.ctx(), nullptr, &vol), "element volume");
@@ -45,12 +51,15 @@ int main(int argc, char **argv)
     mma.SetMoveLimit(0.2);
     OC oc(model, nelx);
     double V0 = 0.0;
-    for(int optstep = 1; optstep <= steps; optstep++)
+    int convergence = 1;
+    while(convergence == 1 && optim.optstep < steps)
     {
+      const int optstep = ++optim.optstep;
       auto design_filtered = filter.densityFilter(design_s, false);
       model.setDesignS(design_filtered);
       compt.solve(solver, false);
       const double object_f = compt.compliance();
+      optim.object_f = object_f;
       double volume = 0.0;
       for(double v : design_filtered)
         volume += v * vol;
@@ -62,6 +71,7 @@ int main(int argc, char **argv)
       }
       else
         const_h = mma_update ? volume / V0 - 1.0 : volume;
+      convergence = optim.isConvergence(1.0e-5, 50);
       compt.sensitivity(dfds, dgds, mma_update ? 1.0 / V0 : 1.0);
       dfds = filter.densityFilter(dfds, true);
       dgds = filter.densityFilter(dgds, true);
@@ -73,6 +83,8 @@ int main(int argc, char **argv)
       std::printf("step %d %.17g %.17g %d\n", optstep, object_f, const_h,
                   compt.info.iterations);
     }
+    if(convergence == 0)
+      std::printf("converged %d\n", optim.optstep);
   }
   catch(const Error &e)
   {

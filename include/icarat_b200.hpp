@@ -10,11 +10,13 @@
 //   Filter::threshold / thresholdDerivative ->   same names
 //   OC::UpdateVariables(x, df, g, dg, ...)  ->   icarat::b200::OC::UpdateVariables
 //   MMASolver::Update(x, df, g, dg, ...)    ->   icarat::b200::MMASolver::Update
+//   Optimize::isConvergence(eps, minstep)    ->   icarat::b200::Optimize::isConvergence
 //
 // Errors: the reference prints and calls exit(1) (solvers.cpp:59,
 // filter.hpp:130-134); here every failing call throws icarat::b200::Error with
 // the library status and message.
 #pragma once
+#include <cmath>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -85,6 +87,35 @@ public:
 
 private:
   icarat_ctx *ctx_ = nullptr;
+};
+
+// Optimize (src/optimization/opt_base.hpp:14-76): the design state of a
+// sample driver's loop and its convergence test.  object_old, which the
+// reference leaves uninitialised, starts at 0.
+class Optimize
+{
+public:
+  Optimize(int design, int constraint, double xmin_, double xmax_)
+      : design_s(design), const_h(constraint), dfds(design),
+        dgds((size_t)constraint * design), xmin(design, xmin_), xmax(design, xmax_)
+  {
+  }
+  // 0 when |object_old - object_f| / object_f < epsilon and optstep >
+  // minstep, else 1 with object_old = object_f
+  int isConvergence(double epsilon, double minstep)
+  {
+    if(std::fabs(object_old - object_f) / object_f < epsilon && optstep > minstep)
+      return 0;
+    object_old = object_f;
+    return 1;
+  }
+
+  std::vector<double> design_s, const_h, dfds, dgds, xmin, xmax;
+  int optstep = 0;
+  double object_f = 0.0;
+
+private:
+  double object_old = 0.0;
 };
 
 // LinearAnalysis<LinearElastic, Node> (src/analysis/linear.hpp:15-41)

@@ -154,7 +154,10 @@ typedef struct
    appended (Helmholtz filter); callers built against 10000 headers pass the
    shorter structs and must be rebuilt.  A caller checks
    icarat_version() == ICARAT_ABI_VERSION before passing option structs. */
-#define ICARAT_ABI_VERSION 10100
+/* 10200: icarat_loop_is_convergence, icarat_ctx_create_selection and
+   icarat_selection_ids added (new functions; the 10100 structs are
+   unchanged). */
+#define ICARAT_ABI_VERSION 10200
 int icarat_version(void);
 const char *icarat_status_string(int status);
 /* message of the last failed call on this thread */
@@ -167,8 +170,27 @@ const char *icarat_last_error(void);
  * constructor (src/analysis/linear.hpp:43-52). */
 int icarat_ctx_create(const icarat_grid *grid, const icarat_material *mat,
                       const icarat_bc *bc, int device, icarat_ctx **out);
+/* [mesh] selection (MeshIcarat::generate -> modifyMesh,
+ * src/io/mesh_icarat.hpp:139-155, 636-755): the box of icarat_ctx_create cut
+ * down to the union of nsel boxes (x0, x1, y0, y1, z0, z1 each, widened by
+ * 1e-7): the nodes inside a box and the elements whose centroid is inside
+ * one are kept and renumbered in ascending box order; the boundary
+ * conditions see the kept mesh only.  Every element / node quantity of the
+ * ABI (sizes, design, filter, sensitivities, DOF map, node values, the
+ * loop's vectors and domain IDs) is then in the kept numbering.  A kept
+ * element with a removed node (the reference's "error in mesh_icarat") and a
+ * kept node without a kept element return ICARAT_ERR_ARG.  Not available on
+ * such a context (ICARAT_ERR_UNSUPPORTED): the Helmholtz filter, the VTK
+ * writer of the box, the learned preconditioner. */
+int icarat_ctx_create_selection(const icarat_grid *grid, const icarat_material *mat,
+                                const icarat_bc *bc, int nsel, const double *boxes,
+                                int device, icarat_ctx **out);
+/* box node id of every kept node (numnp entries) and box element id of every
+ * kept element (nelx entries); either may be NULL; the identity without a
+ * selection */
+int icarat_selection_ids(const icarat_ctx *ctx, int *node_ids, int *elem_ids);
 int icarat_ctx_destroy(icarat_ctx *ctx);
-/* numnp, nelx, neq (= 3 numnp), numeq */
+/* numnp, nelx, neq (= 3 numnp), numeq; of the kept mesh with a selection */
 int icarat_sizes(const icarat_ctx *ctx, int *numnp, int *nelx, int *neq,
                  int *numeq);
 /* the context's cudaStream_t, as void* */
@@ -337,21 +359,24 @@ typedef struct
 
 /* ---- solve without device allocation --------------------------------------
  * No counterpart in the reference.  The Jacobi-PCG solve of
- * icarat_solve_rhs (same kernels, same results) for callers that cannot
- * allocate device memory when they call the solver, e.g. a host application
- * that reserved the whole GPU for its own memory pool at start-up, or a
- * deployment that forbids device allocations after initialisation.  This call
- * allocates nothing: its work vectors live in one static device buffer of
- * the library (about 7.4 MB, held on every GPU that loads the library until
- * the process exits).  f and u are device pointers to numeq vectors (the
- * context's equation numbering); opts may be NULL (rtol 1e-10, maxit 10000)
- * and must select ICARAT_SOLVER_JACOBI_PCG.
+ * icarat_solve_rhs (same kernels: the FP64 node stencil from a zero start)
+ * for callers that cannot allocate device memory when they call the solver,
+ * e.g. a host application that reserved the whole GPU for its own memory pool
+ * at start-up, or a deployment that forbids device allocations after
+ * initialisation.  This call allocates nothing: its work vectors live in one
+ * static device buffer of the library (about 7.4 MB).  The buffer is
+ * committed on a device when the first context of that device is created
+ * (icarat_ctx_create resolves its address; under lazy module loading that is
+ * when the buffer's module is loaded) and is held until the process exits.
+ * f and u are device pointers to numeq vectors (the context's equation
+ * numbering); opts may be NULL (rtol 1e-10, maxit 10000) and must select
+ * ICARAT_SOLVER_JACOBI_PCG with fp64_tc 0 or -1 and warm_start 0 (other
+ * values return ICARAT_ERR_UNSUPPORTED).
  * Limit: 3 (nx+1)(ny+1)(nz+1) <= ICARAT_NOALLOC_MAX_DOFS, larger grids return
- * ICARAT_ERR_ARG.  The first call on a device resolves the buffer's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the one buffer, which keeps the last call's
- * contents (each call clears what must start at zero): calls that overlap on
- * the GPU -- from two threads, or on two contexts of one device -- race. */
+ * ICARAT_ERR_ARG.  All calls share the one buffer, which keeps the last
+ * call's contents (each call clears what must start at zero): calls that
+ * overlap on the GPU -- from two threads, or on two contexts of one device --
+ * race. */
 #define ICARAT_NOALLOC_MAX_DOFS 131072
 int icarat_solve_noalloc(icarat_ctx *ctx, const icarat_solve_opts *opts,
                          const double *f, double *u, icarat_solve_info *info);
@@ -485,6 +510,16 @@ int icarat_loop_init(icarat_ctx *ctx, const icarat_loop_opts *opts,
 int icarat_loop_step(icarat_ctx *ctx, icarat_step_info *info);
 /* which: 0 x, 1 filtered, 2 thresholded, 3 dfds, 4 dgds (nelx each) */
 int icarat_loop_get(icarat_ctx *ctx, int which, double *out);
+/* Optimize::isConvergence(epsilon, minstep) (src/optimization/opt_base.hpp:28-43)
+ * on the loop's objective f, the compliance of the last icarat_loop_step (the
+ * sum over the load cases in a multi-load loop): *convergence = 0 when
+ * |f_old - f| / f < epsilon and the step count > minstep, else 1 and
+ * f_old = f.  f_old starts at 0 at icarat_loop_init (the reference leaves it
+ * uninitialised).  The sample drivers call it once per step after the
+ * objective (opt_macro_oc.cpp:137, with 1e-5 and 50) and leave the loop
+ * after the step in which it returned 0. */
+int icarat_loop_is_convergence(icarat_ctx *ctx, double epsilon, double minstep,
+                               int *convergence);
 /* Load cases (the vector<Force> of opt_multi_load.cpp:68-80): fext holds
  * ncases load vectors of numeq entries (the layout of icarat_fext), case
  * after case.  With ncases >= 1 icarat_loop_step solves every case on the

@@ -693,3 +693,25 @@ def ref_oc_update(x, dfdx, g, dgdx, xmin, xmax, volume_fn, move=0.15):
     L.ref_oc_update(n, x, _f64(dfdx).copy(), g, _f64(dgdx).copy(), _f64(xmin),
                     _f64(xmax), move, fn, None)
     return x
+
+
+class Convergence:
+    """Optimize::isConvergence (src/optimization/opt_base.hpp:28-43): is_convergence
+    returns 0 when |object_old - object_f| / object_f < epsilon and optstep >
+    minstep, else 1 with object_old = object_f.  object_old starts at 0 (the
+    reference leaves it uninitialised)."""
+
+    def __init__(self):
+        self.object_old = 0.0
+
+    def is_convergence(self, object_f, optstep, epsilon, minstep):
+        old, f = float(self.object_old), float(object_f)
+        diff = abs(old - f)
+        if f != 0.0:
+            ratio = diff / f
+        else:
+            ratio = float("nan") if diff == 0.0 else float("inf")
+        if ratio < epsilon and optstep > minstep:
+            return 0
+        self.object_old = f
+        return 1

@@ -11,6 +11,7 @@ restatement (oracle/) on small cantilevers, committed so that a change of the
 oracle itself shows up as a test failure.
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
+(default: the environment variable ICARAT_REFERENCE, else /root/reference)
 """
 import json
 import os
@@ -122,7 +123,8 @@ def oracle_trajectory():
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ICARAT_REFERENCE",
+                                                               "/root/reference")
     with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
         json.dump(reference_known_answers(ref), f, indent=1)
     with open(os.path.join(HERE, "oracle_trajectory.json"), "w") as f:

@@ -91,3 +91,21 @@ def test_mixed_solver_rejects_fp64_operator_choice(gpu):
     with pytest.raises(gpu.IcaratError) as e:
         G.solve(gpu.solve_opts(gpu.MIXED_IR, rtol=1e-8, mg_levels=2, fine_op=9))
     assert e.value.status == gpu.ERR_ARG
+
+
+@pytest.mark.parametrize("grid", [(8, 4, 4), (31, 7, 3), (33, 17, 9), (64, 32, 32)])
+def test_every_operator_matches_oracle_csr(oracle, gpu, grid):
+    """Each operator of icarat_apply_K_op against the oracle's assembled CSR
+    K_ff (triplet assembly of the reference, oracle/icarat_oracle.c), not
+    only against the GPU's own FP64 stencil.  Tolerances as above; both FP64
+    forms (node stencil, FP64 tensor cores) <= 1e-14."""
+    P, G = oracle.Problem(*grid), gpu.Context(*grid)
+    rng = np.random.default_rng(sum(grid))
+    rho = rng.uniform(0.05, 1.0, P.nelx)
+    P.assemble(rho)
+    G.set_design(rho)
+    u = rng.standard_normal(P.numeq)
+    y = P.apply_K(u)
+    tol = {gpu.OP_FP64: 1e-14, gpu.OP_TC_FP64: 1e-14, **TOL}
+    for op, t in tol.items():
+        assert rel(G.apply_K_op(u, op), y) <= t, op
