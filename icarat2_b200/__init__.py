@@ -193,6 +193,7 @@ SIGNATURES = {
     "icarat_batch_destroy": (_i, [_vp]),
     "icarat_batch_ctx": (_i, [_vp, _i, _P(_vp)]),
     "icarat_batch_autotune": (_i, [_vp, _P(_i), _P(_i), _P(_d)]),
+    "icarat_batch_autotune_mg": (_i, [_vp, _i, _P(_i), _P(_i), _P(_d)]),
     "icarat_batch_solve": (_i, [_vp, _P(BatchOpts), _vp]),
     "icarat_batch_solution": (_i, [_vp, _i, _dp]),
     "icarat_batch_loop_step": (_i, [_vp, _P(BatchOpts), _vp]),
@@ -969,6 +970,8 @@ class Batch:
     def opts(rtol=1e-8, maxit=10000, refresh=0.0, tile=0, blocks_per_sm=0, method=0,
              mg_levels=0, chunk=0, warm_start=False):
         """method 0: one persistent Jacobi launch for all designs;
+        MG_PCG: one persistent multigrid-PCG launch for all designs (every
+        design's own hierarchy, the V-cycles of all designs phase by phase);
         MIXED_IR: each design's own mixed-precision multigrid solve,
         interleaved on the designs' streams."""
         return BatchOpts(rtol, maxit, refresh, tile, blocks_per_sm, method, mg_levels, chunk,
@@ -978,6 +981,14 @@ class Batch:
         t, b, ms = C.c_int(), C.c_int(), C.c_double()
         _check(self.lib.icarat_batch_autotune(self.h, C.byref(t), C.byref(b), C.byref(ms)),
                "icarat_batch_autotune")
+        return t.value, b.value, ms.value
+
+    def autotune_mg(self, mg_levels=0):
+        """(tile, CTAs per SM, ms per iteration) of the persistent multigrid
+        launch (method MG_PCG), kept for later MG_PCG solves"""
+        t, b, ms = C.c_int(), C.c_int(), C.c_double()
+        _check(self.lib.icarat_batch_autotune_mg(self.h, mg_levels, C.byref(t), C.byref(b),
+                                                 C.byref(ms)), "icarat_batch_autotune_mg")
         return t.value, b.value, ms.value
 
     def solve(self, opts=None):

@@ -27,7 +27,7 @@
 #include <algorithm>
 #include <cmath>
 
-#include "stencil.cuh"
+#include "batch.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -38,109 +38,6 @@ double loop_pre(icarat_ctx *c);
 int loop_post(icarat_ctx *c, int st, const icarat_solve_info &si, double beta,
               icarat_step_info *info);
 void build_rhs(icarat_ctx *c);
-
-struct BatchDesign
-{
-  GridDev g;
-  const float *E32;
-  const double *E64;
-  const uint8_t *fix;
-  const double *b;
-  double *x64;
-  long off;   // first entry of this design in the FP32 node buffers
-  int item0;  // first work item
-  int nitems; // work items
-};
-
-struct BScal
-{
-  double rz, bb, rr_ref, rr_true, tol2, delta2;
-  int iter, maxit, done, status, refresh, final_, nrefresh, nstall;
-};
-
-struct BatchArgs
-{
-  KeParam ke;
-  KeParamF kef;
-  const BatchDesign *des;
-  int ndes;
-  const int *item_design;
-  int nitems, tile;
-  float *x32, *r, *z, *p, *Ap, *invd;
-  double *part; // 4 per item
-  BScal *s;
-  int *ctl; // [0] designs still iterating, [1], [2] refresh requests by parity
-  int maxit;
-  double tol, delta;
-};
-
-constexpr int kBatchThreads = 128;
-
-// Sum of partial k over the items of design D, in item order; every thread
-// of the block gets the result.
-__device__ double design_sum(const BatchArgs &a, const BatchDesign &D, int k, double *sh,
-                             double *bc)
-{
-  double v = 0.0;
-  for(int i = threadIdx.x; i < D.nitems; i += blockDim.x)
-    v += __ldcg(a.part + 4L * (D.item0 + i) + k);
-  double arr[1] = {v};
-  block_sum<1>(arr, sh);
-  if(threadIdx.x == 0)
-    *bc = arr[0];
-  __syncthreads();
-  const double r = *bc;
-  __syncthreads();
-  return r;
-}
-
-// (K x)_n in FP64 element by element: few live registers, for the refresh
-// phase, which runs rarely and must not raise the register count of the
-// whole persistent kernel.  Coherent (L2) loads: x changes inside the launch.
-__device__ __forceinline__ void node_Ku_lean(const GridDev &g, const KeParam &ke,
-                                             const double *__restrict__ E,
-                                             const double *__restrict__ x, int n,
-                                             double (&acc)[3])
-{
-  const int i = n % g.NX, j = (n / g.NX) % g.NY, k = n / (g.NX * g.NY);
-  acc[0] = acc[1] = acc[2] = 0.0;
-#pragma unroll
-  for(int sz = 0; sz < 2; sz++)
-#pragma unroll
-    for(int sy = 0; sy < 2; sy++)
-#pragma unroll
-      for(int sx = 0; sx < 2; sx++)
-      {
-        const int ei = i - 1 + sx, ej = j - 1 + sy, ek = k - 1 + sz;
-        const double e = load_E(E, g, ei, ej, ek);
-        if(e == 0.0)
-          continue;
-        const int la = local_node(1 - sx, 1 - sy, 1 - sz);
-        double t[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for(int bz = 0; bz < 2; bz++)
-#pragma unroll
-          for(int by = 0; by < 2; by++)
-#pragma unroll
-            for(int bx = 0; bx < 2; bx++)
-            {
-              const int lb = local_node(bx, by, bz);
-              const long m = (long)(ei + bx) + (long)(ej + by) * g.NX +
-                             (long)(ek + bz) * g.NX * g.NY;
-#pragma unroll
-              for(int d = 0; d < 3; d++)
-              {
-                const double u = __ldcg(x + (long)d * g.numnp + m);
-#pragma unroll
-                for(int c = 0; c < 3; c++)
-                  t[c] = fma(ke.k[(3 * la + c) * 24 + 3 * lb + d], u, t[c]);
-              }
-            }
-#pragma unroll
-        for(int c = 0; c < 3; c++)
-          acc[c] = fma(e, t[c], acc[c]);
-      }
-}
 
 __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_pcg(BatchArgs a)
 {
@@ -501,6 +398,19 @@ struct icarat_batch
   std::tuple<int, int, double, int, double> graph_key{};
   std::vector<cudaEvent_t> ev;
   cudaEvent_t done_ev = nullptr;
+  // persistent multigrid launch (method ICARAT_SOLVER_MG_PCG)
+  BmDesign *d_bm = nullptr;
+  std::vector<BmDesign> h_bm;
+  int *d_lv_items[kBmMaxLevels] = {};
+  int lv_nitems[kBmMaxLevels] = {};
+  int *d_citems = nullptr;
+  int c_nitems = 0;
+  double *d_y = nullptr;
+  int mg_levels = 0, mg_tile = 0;         // tables built for these
+  int occ_mg = 0;                         // co-resident CTAs per SM
+  int mg_tuned_tile = 0, mg_tuned_bpsm = 0; // icarat_batch_autotune_mg
+  cudaGraphExec_t mg_graph = nullptr;
+  std::tuple<int, int, double, int, double, int, int> mg_key{};
 };
 
 int icarat_ctx_create_impl(const icarat_grid *grid, const icarat_material *mat,
@@ -548,6 +458,13 @@ static void batch_items(icarat_batch *B, int tile)
     cudaGraphExecDestroy(B->graph);
     B->graph = nullptr;
   }
+  // the multigrid launch's graph and tables hold the old item table too
+  if(B->mg_graph)
+  {
+    cudaGraphExecDestroy(B->mg_graph);
+    B->mg_graph = nullptr;
+  }
+  B->mg_levels = B->mg_tile = 0;
 }
 
 // Right-hand sides of every design, and the batch stream ordered after
@@ -739,6 +656,260 @@ static int batch_solve_concurrent(icarat_batch *B, const icarat_batch_opts *o, d
   return worst;
 }
 
+// ---------------------------------------------------------------- multigrid
+constexpr int kBmCoarseRows = 32; // coarse dense rows per work item
+constexpr int kBmDeg = 2;         // Chebyshev steps per level and direction
+
+// Item tables of the persistent multigrid launch: node tiles of every level
+// of every design, and row blocks of every design's coarsest dense solve.
+// Level 0 uses the batch's own item table (batch_items).
+static void batch_mg_tables(icarat_batch *B, int L, int tile)
+{
+  batch_items(B, tile);
+  const size_t n = B->ctx.size();
+  B->h_bm.assign(n, BmDesign{});
+  std::vector<std::vector<int>> lv(L);
+  std::vector<int> citems;
+  long ylen = 0;
+  for(size_t d = 0; d < n; d++)
+  {
+    icarat_ctx *c = B->ctx[d];
+    BmDesign &M = B->h_bm[d];
+    for(int l = 0; l < L; l++)
+    {
+      const GridDev &g = c->mg[l].g;
+      BmLevel &V = M.lv[l];
+      V.g = g;
+      V.item0 = (int)lv[l].size();
+      V.nitems = (g.numnp + tile - 1) / tile;
+      for(int i = 0; i < V.nitems; i++)
+        lv[l].push_back((int)d);
+    }
+    M.nc = c->coarse.n;
+    M.citem0 = (int)citems.size();
+    M.citems = std::max(1, (M.nc + kBmCoarseRows - 1) / kBmCoarseRows);
+    for(int i = 0; i < M.citems; i++)
+      citems.push_back((int)d);
+    ylen += std::max(1, M.nc);
+  }
+  if(B->mg_levels != L || B->mg_tile != tile)
+  {
+    for(int l = 0; l < kBmMaxLevels; l++)
+    {
+      if(l > 0)
+        dfree(B->d_lv_items[l]);
+      B->d_lv_items[l] = nullptr;
+      B->lv_nitems[l] = 0;
+    }
+    dfree(B->d_citems);
+    dfree(B->d_y);
+    B->d_lv_items[0] = B->d_item_design;
+    B->lv_nitems[0] = B->nitems;
+    for(int l = 1; l < L; l++)
+    {
+      ICK(cudaMalloc(&B->d_lv_items[l], sizeof(int) * lv[l].size()));
+      ICK(cudaMemcpy(B->d_lv_items[l], lv[l].data(), sizeof(int) * lv[l].size(),
+                     cudaMemcpyHostToDevice));
+      B->lv_nitems[l] = (int)lv[l].size();
+    }
+    ICK(cudaMalloc(&B->d_citems, sizeof(int) * citems.size()));
+    ICK(cudaMemcpy(B->d_citems, citems.data(), sizeof(int) * citems.size(),
+                   cudaMemcpyHostToDevice));
+    B->c_nitems = (int)citems.size();
+    B->d_y = dalloc(ylen);
+    B->mg_levels = L;
+    B->mg_tile = tile;
+    if(B->mg_graph)
+    {
+      cudaGraphExecDestroy(B->mg_graph);
+      B->mg_graph = nullptr;
+    }
+  }
+  B->d_lv_items[0] = B->d_item_design; // batch_items may have rebuilt it
+  // per-design pointers (levels and factor buffers of the contexts) and the
+  // Chebyshev coefficients of the smoother (the sequence of smooth() in
+  // multigrid.cu)
+  long yoff = 0;
+  for(size_t d = 0; d < n; d++)
+  {
+    icarat_ctx *c = B->ctx[d];
+    BmDesign &M = B->h_bm[d];
+    for(int l = 0; l < L; l++)
+    {
+      MgLevel &G = c->mg[l];
+      BmLevel &V = M.lv[l];
+      V.E32 = G.E32;
+      V.invd = G.invd32;
+      V.fix = G.fix;
+      V.x = G.x32;
+      V.t = G.t32;
+      V.r = G.r32;
+      V.b = G.b32;
+    }
+    M.W = c->coarse.W[c->coarse.cur];
+    M.WT = c->coarse.work[c->coarse.cur];
+    M.map = c->coarse.map;
+    M.y = B->d_y + yoff;
+    yoff += std::max(1, M.nc);
+    const double lmax = c->lam_max_dk, lmin = 0.1 * lmax;
+    const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+    const double sigma = theta / delta;
+    M.inv_theta = (float)(1.0 / theta);
+    double rho_old = 1.0 / sigma;
+    M.pre_c1[0] = 0.0f;
+    M.pre_c2[0] = (float)(1.0 / theta);
+    for(int k = 1; k < kBmMaxDeg; k++)
+    {
+      const double rho = 1.0 / (2.0 * sigma - rho_old);
+      M.pre_c1[k] = (float)(rho * rho_old);
+      M.pre_c2[k] = (float)(2.0 * rho / delta);
+      rho_old = rho;
+    }
+    for(int k = 0; k < kBmMaxDeg; k++)
+    {
+      M.post_c1[k] = M.pre_c1[k];
+      M.post_c2[k] = M.pre_c2[k];
+    }
+  }
+  if(!B->d_bm)
+    ICK(cudaMalloc(&B->d_bm, sizeof(BmDesign) * n));
+  ICK(cudaStreamSynchronize(B->stream)); // no launch in flight reads the table
+  ICK(cudaMemcpy(B->d_bm, B->h_bm.data(), sizeof(BmDesign) * n, cudaMemcpyHostToDevice));
+}
+
+static void batch_mg_launch(icarat_batch *B, int tile, int bpsm, double rtol, int maxit,
+                            double refresh, int L, int warm)
+{
+  BatchArgs a;
+  a.ke = B->ke;
+  a.kef = B->kef;
+  a.des = B->d_des;
+  a.ndes = (int)B->ctx.size();
+  a.item_design = B->d_item_design;
+  a.nitems = B->nitems;
+  a.tile = tile;
+  const long nv = B->total_nv;
+  a.x32 = B->buf;
+  a.r = B->buf + nv;
+  a.z = B->buf + 2 * nv;
+  a.p = B->buf + 3 * nv;
+  a.Ap = B->buf + 4 * nv;
+  a.invd = B->buf + 5 * nv;
+  a.part = B->d_part;
+  a.s = B->d_s;
+  a.ctl = B->d_ctl;
+  a.maxit = maxit;
+  a.tol = rtol;
+  a.delta = refresh;
+  BmArgs m;
+  m.levels = L;
+  m.deg = kBmDeg;
+  m.ctile = kBmCoarseRows;
+  m.warm = warm;
+  m.bm = B->d_bm;
+  for(int l = 0; l < kBmMaxLevels; l++)
+  {
+    m.lv_item_design[l] = B->d_lv_items[l];
+    m.lv_nitems[l] = B->lv_nitems[l];
+  }
+  m.c_item_design = B->d_citems;
+  m.c_nitems = B->c_nitems;
+  const int sms = B->ctx[0]->sm_count;
+  const int blocks = sms * std::max(1, std::min(bpsm, B->occ_mg));
+  void *args[] = {&a, &m};
+  note_launch();
+  ICK(cudaLaunchCooperativeKernel((void *)k_batch_mg, dim3(blocks), dim3(kBatchThreads), args,
+                                  0, B->stream));
+}
+
+// The multigrid launch as a CUDA graph (one graph per shape and options)
+static void batch_mg_run(icarat_batch *B, int tile, int bpsm, double rtol, int maxit,
+                         double refresh, int L, int warm)
+{
+  const auto key = std::make_tuple(tile, bpsm, rtol, maxit, refresh, L, warm);
+  if(!B->mg_graph || B->mg_key != key)
+  {
+    if(B->mg_graph)
+    {
+      cudaGraphExecDestroy(B->mg_graph);
+      B->mg_graph = nullptr;
+    }
+    cudaGraph_t g;
+    ICK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+    set_capturing(true);
+    try
+    {
+      batch_mg_launch(B, tile, bpsm, rtol, maxit, refresh, L, warm);
+    }
+    catch(...)
+    {
+      set_capturing(false);
+      cudaStreamEndCapture(B->stream, &g);
+      throw;
+    }
+    set_capturing(false);
+    ICK(cudaStreamEndCapture(B->stream, &g));
+    ICK(cudaGraphInstantiate(&B->mg_graph, g, 0));
+    cudaGraphDestroy(g);
+    B->mg_key = key;
+  }
+  ICK(cudaGraphLaunch(B->mg_graph, B->stream));
+  note_launch();
+}
+
+static int design_levels(const icarat_ctx *c, int want);
+
+// Multigrid hierarchies of every design for the current designs (levels:
+// the smallest count every design supports, at most `want`), the tables,
+// and the batch stream ordered after the set-ups; cold starts clear x.
+static int batch_mg_prepare(icarat_batch *B, int want, int tile, bool warm)
+{
+  IREQUIRE(want >= 2 && want <= kBmMaxLevels, ICARAT_ERR_ARG,
+           "mg_levels must be in [2, 8] for the persistent multigrid launch");
+  int L = want;
+  for(icarat_ctx *c : B->ctx)
+    L = std::min(L, design_levels(c, want));
+  for(size_t d = 0; d < B->ctx.size(); d++)
+  {
+    icarat_ctx *c = B->ctx[d];
+    mg_setup(c, L, false);
+    ICK(cudaEventRecord(B->ev[d], c->stream));
+    ICK(cudaStreamWaitEvent(B->stream, B->ev[d], 0));
+  }
+  batch_mg_tables(B, L, tile);
+  for(icarat_ctx *c : B->ctx)
+    if(!warm || !c->have_u)
+      ICK(cudaMemsetAsync(c->d_u, 0, sizeof(double) * c->neq, B->stream));
+  return L;
+}
+
+static int pick_mg_tile(icarat_batch *B, const icarat_batch_opts *o)
+{
+  if(o && o->tile > 0)
+    return o->tile;
+  return B->mg_tuned_tile > 0 ? B->mg_tuned_tile : 256;
+}
+
+static int pick_mg_bpsm(icarat_batch *B, const icarat_batch_opts *o)
+{
+  if(o && o->blocks_per_sm > 0)
+    return std::min(o->blocks_per_sm, B->occ_mg);
+  return B->mg_tuned_bpsm > 0 ? B->mg_tuned_bpsm : B->occ_mg;
+}
+
+static int batch_collect(icarat_batch *B, icarat_solve_info *infos);
+
+static int batch_solve_mg(icarat_batch *B, const icarat_batch_opts *o, double rtol, int maxit,
+                          double refresh, icarat_solve_info *infos)
+{
+  const int tile = pick_mg_tile(B, o), bpsm = pick_mg_bpsm(B, o);
+  IREQUIRE(tile >= 32 && tile <= (1 << 16), ICARAT_ERR_ARG, "tile must be in [32, 65536]");
+  const bool warm = o && o->warm_start;
+  const int L = batch_mg_prepare(B, o && o->mg_levels > 0 ? o->mg_levels : 4, tile, warm);
+  batch_mg_run(B, tile, bpsm, rtol, maxit, refresh, L, warm ? 1 : 0);
+  return batch_collect(B, infos);
+}
+
 static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
                             icarat_solve_info *infos)
 {
@@ -747,13 +918,21 @@ static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
   const double refresh = o && o->refresh > 0.0 ? o->refresh : 1e-2;
   IREQUIRE(rtol >= 0.0 && refresh < 1.0, ICARAT_ERR_ARG, "bad batch options");
   const int method = o ? o->method : 0;
-  IREQUIRE(method == 0 || method == ICARAT_SOLVER_MIXED_IR, ICARAT_ERR_ARG,
-           "batch method must be 0 or ICARAT_SOLVER_MIXED_IR");
+  IREQUIRE(method == 0 || method == ICARAT_SOLVER_MG_PCG || method == ICARAT_SOLVER_MIXED_IR,
+           ICARAT_ERR_ARG, "batch method must be 0, ICARAT_SOLVER_MG_PCG or ICARAT_SOLVER_MIXED_IR");
   if(method == ICARAT_SOLVER_MIXED_IR)
     return batch_solve_concurrent(B, o, rtol, maxit, refresh, infos);
+  if(method == ICARAT_SOLVER_MG_PCG)
+    return batch_solve_mg(B, o, rtol, maxit, refresh, infos);
   const int tile = pick_tile(B, o), bpsm = pick_bpsm(B, o);
   IREQUIRE(tile >= 32 && tile <= (1 << 16), ICARAT_ERR_ARG, "tile must be in [32, 65536]");
   batch_run(B, tile, bpsm, rtol, maxit, refresh);
+  return batch_collect(B, infos);
+}
+
+// per-design results of a persistent launch
+static int batch_collect(icarat_batch *B, icarat_solve_info *infos)
+{
   const size_t n = B->ctx.size();
   ICK(cudaMemcpyAsync(B->h_s, B->d_s, sizeof(BScal) * n, cudaMemcpyDeviceToHost, B->stream));
   ICK(cudaEventRecord(B->done_ev, B->stream));
@@ -817,6 +996,9 @@ int icarat_batch_create(const icarat_grid *grids, const icarat_bc *bcs, int coun
     ICK(cudaMalloc(&B->d_ctl, sizeof(int) * 4));
     ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->occ, k_batch_pcg, kBatchThreads, 0));
     IREQUIRE(B->occ >= 1, ICARAT_ERR_CUDA, "batch kernel cannot be resident");
+    ICK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&B->occ_mg, k_batch_mg, kBatchThreads,
+                                                      0));
+    IREQUIRE(B->occ_mg >= 1, ICARAT_ERR_CUDA, "batch multigrid kernel cannot be resident");
   }
   catch(...)
   {
@@ -837,6 +1019,13 @@ int icarat_batch_destroy(icarat_batch *B)
     cudaStreamSynchronize(B->stream);
   if(B->graph)
     cudaGraphExecDestroy(B->graph);
+  if(B->mg_graph)
+    cudaGraphExecDestroy(B->mg_graph);
+  for(int l = 1; l < kBmMaxLevels; l++)
+    dfree(B->d_lv_items[l]);
+  dfree(B->d_citems);
+  dfree(B->d_y);
+  dfree(B->d_bm);
   for(icarat_ctx *c : B->ctx)
     icarat_ctx_destroy(c);
   for(cudaEvent_t e : B->ev)
@@ -926,6 +1115,54 @@ int icarat_batch_autotune(icarat_batch *B, int *tile, int *bpsm, double *ms_per_
     *bpsm = bb;
   if(ms_per_iteration)
     *ms_per_iteration = best / 10.0;
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
+int icarat_batch_autotune_mg(icarat_batch *B, int mg_levels, int *tile, int *bpsm,
+                             double *ms_per_iteration)
+{
+  ICARAT_API_BEGIN
+  IREQUIRE(B, ICARAT_ERR_ARG, "null batch");
+  ICK(cudaSetDevice(B->device));
+  batch_prepare(B, true);
+  // every candidate runs the same fixed work: 8 multigrid-PCG iterations of
+  // every design (tolerance 0, cap 8) and the final FP64 refresh
+  const int want = mg_levels > 0 ? mg_levels : 4;
+  const int tiles[] = {128, 256, 512, 1024};
+  double best = 1e30;
+  int bt = 256, bb = B->occ_mg;
+  cudaEvent_t e0, e1;
+  ICK(cudaEventCreate(&e0));
+  ICK(cudaEventCreate(&e1));
+  for(int tl : tiles)
+    for(int bp = 1; bp <= B->occ_mg; bp++)
+    {
+      const int L = batch_mg_prepare(B, want, tl, false);
+      batch_mg_launch(B, tl, bp, 0.0, 8, 1e-2, L, 0); // warm-up
+      ICK(cudaEventRecord(e0, B->stream));
+      batch_mg_launch(B, tl, bp, 0.0, 8, 1e-2, L, 0);
+      ICK(cudaEventRecord(e1, B->stream));
+      ICK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      ICK(cudaEventElapsedTime(&ms, e0, e1));
+      if(ms < best)
+      {
+        best = ms;
+        bt = tl;
+        bb = bp;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  B->mg_tuned_tile = bt;
+  B->mg_tuned_bpsm = bb;
+  if(tile)
+    *tile = bt;
+  if(bpsm)
+    *bpsm = bb;
+  if(ms_per_iteration)
+    *ms_per_iteration = best / 8.0;
   return ICARAT_OK;
   ICARAT_API_END
 }

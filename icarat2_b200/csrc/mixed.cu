@@ -142,7 +142,7 @@ __global__ void k_mx_init(int n, const double *__restrict__ b, double *__restric
 
 // Ap = K32 p (constrained rows 0); alpha = zr / (p . Ap).
 __global__ void __launch_bounds__(128)
-    k_mx_spmv(GridDev g, KeParamF ke, const float *__restrict__ E,
+    k_mx_spmv(GridDev g, MarchPlan m, KeParamF ke, const float *__restrict__ E,
               const uint8_t *__restrict__ fix, const float *__restrict__ p,
               float *__restrict__ Ap, double *__restrict__ partials, MxScalars *s)
 {
@@ -150,19 +150,25 @@ __global__ void __launch_bounds__(128)
   if(s->done)
     return;
   double dot = 0.0;
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
-      n += gridDim.x * blockDim.x)
+  for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
+      t += (long)gridDim.x * blockDim.x)
   {
-    float acc[3], uc[3];
-    node_Ku(g, ke, E, p, n, acc, uc);
-    const unsigned f = fix[n];
+    int i, j, k0, k1;
+    if(!march_item(g, m, t, i, j, k0, k1))
+      continue;
+    column_Ku(g, ke, E, p, i, j, k0, k1,
+              [&](int k, const float(&acc)[3], const float(&uc)[3])
+              {
+                const int n = i + j * g.NX + k * g.NX * g.NY;
+                const unsigned f = fix[n];
 #pragma unroll
-    for(int q = 0; q < 3; q++)
-    {
-      const float y = ((f >> q) & 1u) ? 0.0f : acc[q];
-      Ap[(long)q * g.numnp + n] = y;
-      dot += (double)uc[q] * (double)y;
-    }
+                for(int q = 0; q < 3; q++)
+                {
+                  const float y = ((f >> q) & 1u) ? 0.0f : acc[q];
+                  Ap[(long)q * g.numnp + n] = y;
+                  dot += (double)uc[q] * (double)y;
+                }
+              });
   }
   double v[1] = {dot};
   block_sum<1>(v, sh);
@@ -241,7 +247,7 @@ __global__ void k_mx_flush(int n, double *__restrict__ x, float *__restrict__ x3
 
 // Refresh, part 2: r = b - K x in FP64, r32 = (float) r, stop test on ||r||.
 __global__ void __launch_bounds__(128)
-    k_mx_residual(GridDev g, KeParam ke, const double *__restrict__ E,
+    k_mx_residual(GridDev g, MarchPlan m, KeParam ke, const double *__restrict__ E,
                   const uint8_t *__restrict__ fix, const double *__restrict__ b,
                   const double *__restrict__ x, float *__restrict__ r32,
                   double *__restrict__ partials, MxScalars *s)
@@ -250,20 +256,26 @@ __global__ void __launch_bounds__(128)
   if(s->done || !s->refresh)
     return;
   double rr = 0.0;
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
-      n += gridDim.x * blockDim.x)
+  for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
+      t += (long)gridDim.x * blockDim.x)
   {
-    double acc[3], uc[3];
-    node_Ku(g, ke, E, x, n, acc, uc);
-    const unsigned f = fix[n];
+    int i, j, k0, k1;
+    if(!march_item(g, m, t, i, j, k0, k1))
+      continue;
+    column_Ku(g, ke, E, x, i, j, k0, k1,
+              [&](int k, const double(&acc)[3], const double(&)[3])
+              {
+                const int n = i + j * g.NX + k * g.NX * g.NY;
+                const unsigned f = fix[n];
 #pragma unroll
-    for(int q = 0; q < 3; q++)
-    {
-      const long id = (long)q * g.numnp + n;
-      const double r = ((f >> q) & 1u) ? 0.0 : b[id] - acc[q];
-      r32[id] = (float)r;
-      rr += r * r;
-    }
+                for(int q = 0; q < 3; q++)
+                {
+                  const long id = (long)q * g.numnp + n;
+                  const double r = ((f >> q) & 1u) ? 0.0 : b[id] - acc[q];
+                  r32[id] = (float)r;
+                  rr += r * r;
+                }
+              });
   }
   double v[1] = {rr};
   block_sum<1>(v, sh);
@@ -485,9 +497,11 @@ static void enqueue_krylov_step(icarat_ctx *c, int krylov_op, const double *b, d
   const int n = c->neq;
   if(krylov_op == ICARAT_OP_FP32)
   {
+    int blocks;
+    const MarchPlan m = march_launch(L.g, (const void *)k_mx_spmv, 128, c->sm_count, blocks);
     note_launch();
-    k_mx_spmv<<<spmv_blocks(c), 128, 0, c->stream>>>(L.g, c->ke0f, L.E32, L.fix, c->f_p,
-                                                     c->f_Ap, c->d_partials, c->d_mx);
+    k_mx_spmv<<<blocks < kMaxRedBlocks ? blocks : kMaxRedBlocks, 128, 0, c->stream>>>(
+        L.g, m, c->ke0f, L.E32, L.fix, c->f_p, c->f_Ap, c->d_partials, c->d_mx);
   }
   else
   {
@@ -506,8 +520,11 @@ static void enqueue_krylov_step(icarat_ctx *c, int krylov_op, const double *b, d
                                                             c->f_Ap, c->d_partials,
                                                             c->d_mx);
   k_mx_flush<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, x, c->f_x, c->d_mx);
-  k_mx_residual<<<spmv_blocks(c), 128, 0, c->stream>>>(L.g, c->ke0, c->d_E, L.fix, b, x,
-                                                       c->f_r, c->d_partials, c->d_mx);
+  int rblocks;
+  const MarchPlan rm =
+      march_launch(L.g, (const void *)k_mx_residual, 128, c->sm_count, rblocks);
+  k_mx_residual<<<rblocks < kMaxRedBlocks ? rblocks : kMaxRedBlocks, 128, 0, c->stream>>>(
+      L.g, rm, c->ke0, c->d_E, L.fix, b, x, c->f_r, c->d_partials, c->d_mx);
 }
 
 static const MxScalars &read_scalars(icarat_ctx *c)

@@ -65,7 +65,8 @@ __global__ void k_cast(long n, const Tin *__restrict__ in, Tout *__restrict__ ou
 }
 
 // ---------------------------------------------------------------- transfers
-// coarse b = R r  (R = P^T, 27 fine nodes per coarse node, weights 1/2^d)
+// coarse b = R r  (R = P^T, 27 fine nodes per coarse node, weights 1/2^d;
+// restrict_node / prolong_node in stencil.cuh)
 template <typename T>
 __global__ void k_restrict(GridDev f, GridDev c, const T *__restrict__ rf,
                            const uint8_t *__restrict__ fixc, T *__restrict__ bc)
@@ -73,28 +74,12 @@ __global__ void k_restrict(GridDev f, GridDev c, const T *__restrict__ rf,
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.numnp;
       n += gridDim.x * blockDim.x)
   {
-    const int I = n % c.NX, J = (n / c.NX) % c.NY, K = n / (c.NX * c.NY);
-    T s0 = 0, s1 = 0, s2 = 0;
-#pragma unroll
-    for(int dz = -1; dz <= 1; dz++)
-#pragma unroll
-      for(int dy = -1; dy <= 1; dy++)
-#pragma unroll
-        for(int dx = -1; dx <= 1; dx++)
-        {
-          const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
-          if(i < 0 || i >= f.NX || j < 0 || j >= f.NY || k < 0 || k >= f.NZ)
-            continue;
-          const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
-          const long m = i + (long)j * f.NX + (long)k * f.NX * f.NY;
-          s0 += w * rf[m];
-          s1 += w * rf[(long)f.numnp + m];
-          s2 += w * rf[2L * f.numnp + m];
-        }
+    T s[3];
+    restrict_node<T, false>(f, c, rf, n, s);
     const unsigned fx = fixc[n];
-    bc[n] = (fx & 1u) ? T(0) : s0;
-    bc[(long)c.numnp + n] = (fx & 2u) ? T(0) : s1;
-    bc[2L * c.numnp + n] = (fx & 4u) ? T(0) : s2;
+    bc[n] = (fx & 1u) ? T(0) : s[0];
+    bc[(long)c.numnp + n] = (fx & 2u) ? T(0) : s[1];
+    bc[2L * c.numnp + n] = (fx & 4u) ? T(0) : s[2];
   }
 }
 
@@ -106,30 +91,8 @@ __global__ void k_prolong_add(GridDev f, GridDev c, const T *__restrict__ xc,
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < f.numnp;
       n += gridDim.x * blockDim.x)
   {
-    const int i = n % f.NX, j = (n / f.NX) % f.NY, k = n / (f.NX * f.NY);
-    const int I0 = i >> 1, J0 = j >> 1, K0 = k >> 1;
-    const int I1 = I0 + (i & 1), J1 = J0 + (j & 1), K1 = K0 + (k & 1);
-    const T wx = (i & 1) ? T(0.5) : T(1), wy = (j & 1) ? T(0.5) : T(1),
-            wz = (k & 1) ? T(0.5) : T(1);
-    T s[3] = {0, 0, 0};
-#pragma unroll
-    for(int cz = 0; cz < 2; cz++)
-#pragma unroll
-      for(int cy = 0; cy < 2; cy++)
-#pragma unroll
-        for(int cx = 0; cx < 2; cx++)
-        {
-          // odd coordinates take both neighbours with 1/2, even ones the
-          // coincident coarse node once
-          if((cx && !(i & 1)) || (cy && !(j & 1)) || (cz && !(k & 1)))
-            continue;
-          const int I = cx ? I1 : I0, J = cy ? J1 : J0, K = cz ? K1 : K0;
-          const long m = I + (long)J * c.NX + (long)K * c.NX * c.NY;
-          const T w = wx * wy * wz;
-          s[0] += w * xc[m];
-          s[1] += w * xc[(long)c.numnp + m];
-          s[2] += w * xc[2L * c.numnp + m];
-        }
+    T s[3];
+    prolong_node<T, false>(f, c, xc, n, s);
     const unsigned fx = fixf[n];
 #pragma unroll
     for(int q = 0; q < 3; q++)
@@ -157,46 +120,59 @@ __global__ void k_cheb_first(int n, const T *__restrict__ b, const T *__restrict
 // x and xo are distinct buffers (neighbours of x are read by other threads).
 template <typename T, typename KP>
 __global__ void __launch_bounds__(128)
-    k_cheb_step(GridDev g, KP ke, const T *__restrict__ E, const uint8_t *__restrict__ fix,
-                const T *__restrict__ invd, const T *__restrict__ b,
-                const T *__restrict__ x, T *__restrict__ d, T *__restrict__ xo, T c1,
-                T c2)
+    k_cheb_step(GridDev g, MarchPlan m, KP ke, const T *__restrict__ E,
+                const uint8_t *__restrict__ fix, const T *__restrict__ invd,
+                const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ d,
+                T *__restrict__ xo, T c1, T c2)
 {
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
-      n += gridDim.x * blockDim.x)
+  for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
+      t += (long)gridDim.x * blockDim.x)
   {
-    T acc[3], uc[3];
-    node_Ku(g, ke, E, x, n, acc, uc);
-    const unsigned f = fix[n];
+    int i, j, k0, k1;
+    if(!march_item(g, m, t, i, j, k0, k1))
+      continue;
+    column_Ku(g, ke, E, x, i, j, k0, k1,
+              [&](int k, const T(&acc)[3], const T(&uc)[3])
+              {
+                const int n = i + j * g.NX + k * g.NX * g.NY;
+                const unsigned f = fix[n];
 #pragma unroll
-    for(int q = 0; q < 3; q++)
-    {
-      const long id = (long)q * g.numnp + n;
-      T dn = 0;
-      if(!((f >> q) & 1u))
-        dn = (c1 != T(0) ? c1 * d[id] : T(0)) + c2 * invd[id] * (b[id] - acc[q]);
-      d[id] = dn;
-      xo[id] = uc[q] + dn;
-    }
+                for(int q = 0; q < 3; q++)
+                {
+                  const long id = (long)q * g.numnp + n;
+                  T dn = 0;
+                  if(!((f >> q) & 1u))
+                    dn = (c1 != T(0) ? c1 * d[id] : T(0)) + c2 * invd[id] * (b[id] - acc[q]);
+                  d[id] = dn;
+                  xo[id] = uc[q] + dn;
+                }
+              });
   }
 }
 
 // r = b - K x (constrained rows 0)
 template <typename T, typename KP>
 __global__ void __launch_bounds__(128)
-    k_mg_residual(GridDev g, KP ke, const T *__restrict__ E,
+    k_mg_residual(GridDev g, MarchPlan m, KP ke, const T *__restrict__ E,
                   const uint8_t *__restrict__ fix, const T *__restrict__ b,
                   const T *__restrict__ x, T *__restrict__ r)
 {
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
-      n += gridDim.x * blockDim.x)
+  for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
+      t += (long)gridDim.x * blockDim.x)
   {
-    T acc[3], uc[3];
-    node_Ku(g, ke, E, x, n, acc, uc);
-    const unsigned f = fix[n];
+    int i, j, k0, k1;
+    if(!march_item(g, m, t, i, j, k0, k1))
+      continue;
+    column_Ku(g, ke, E, x, i, j, k0, k1,
+              [&](int k, const T(&acc)[3], const T(&)[3])
+              {
+                const int n = i + j * g.NX + k * g.NX * g.NY;
+                const unsigned f = fix[n];
 #pragma unroll
-    for(int c = 0; c < 3; c++)
-      r[(long)c * g.numnp + n] = ((f >> c) & 1u) ? T(0) : b[(long)c * g.numnp + n] - acc[c];
+                for(int c = 0; c < 3; c++)
+                  r[(long)c * g.numnp + n] =
+                      ((f >> c) & 1u) ? T(0) : b[(long)c * g.numnp + n] - acc[c];
+              });
   }
 }
 
@@ -710,9 +686,13 @@ static void cheb_step(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x
       launch_ku_dmma(c, TC_CHEB, a, c->stream);
       return;
     }
+  int blocks;
+  const MarchPlan m =
+      march_launch(L.g, (const void *)k_cheb_step<T, typename KeOf<T>::type>, 128,
+                   c->sm_count, blocks);
   note_launch();
-  k_cheb_step<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(
-      L.g, B::ke(c), B::E(L), L.fix, B::invd(L), b, x, d, xo, T(c1), T(c2));
+  k_cheb_step<<<blocks, 128, 0, c->stream>>>(L.g, m, B::ke(c), B::E(L), L.fix, B::invd(L), b,
+                                             x, d, xo, T(c1), T(c2));
 }
 
 // r = b - K x on level lvl
@@ -745,9 +725,12 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
       launch_ku_dmma(c, TC_RESID, a, c->stream);
       return;
     }
+  int blocks;
+  const MarchPlan m =
+      march_launch(L.g, (const void *)k_mg_residual<T, typename KeOf<T>::type>, 128,
+                   c->sm_count, blocks);
   note_launch();
-  k_mg_residual<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, B::ke(c), B::E(L),
-                                                                  L.fix, b, x, r);
+  k_mg_residual<<<blocks, 128, 0, c->stream>>>(L.g, m, B::ke(c), B::E(L), L.fix, b, x, r);
 }
 
 // Chebyshev smoothing of K x = b on level lvl, deg steps.  from_zero: x = 0

@@ -13,17 +13,18 @@
 // and kept in the context.  Under lazy module loading that call is what loads
 // this file's module and commits the array on the device, so it belongs to
 // context creation, which allocates anyway, and not to the solve.
-#include "internal.cuh"
+#include "stencil.cuh"
 
 namespace icarat_b200
 {
+MarchPlan spmv_plan(const icarat_ctx *c, const GridDev &g, int &blocks);
 // kernels defined in pcg.cu, stiffness.cu and ctx.cu
 __global__ void k_cg_init(int n, const double *__restrict__ b,
                           const double *__restrict__ invd, double *__restrict__ x,
                           double *__restrict__ r, double *__restrict__ z,
                           double *__restrict__ p, double *__restrict__ partials,
                           CgScalars *s, double tol, int maxit, int jacobi);
-__global__ void k_cg_spmv(GridDev g, KeParam ke, const double *__restrict__ E,
+__global__ void k_cg_spmv(GridDev g, MarchPlan m, KeParam ke, const double *__restrict__ E,
                           const uint8_t *__restrict__ fix, const double *__restrict__ p,
                           double *__restrict__ Ap, double *__restrict__ partials,
                           CgScalars *s);
@@ -104,8 +105,8 @@ static int solve_noalloc(icarat_ctx *c, const icarat_solve_opts *opts, const dou
   const GridDev g{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
   const int n = c->neq;
   const int nb_node = (c->numnp + 255) / 256;
-  int nb_spmv = (c->numnp + 127) / 128;
-  nb_spmv = nb_spmv > kMaxRedBlocks ? kMaxRedBlocks : nb_spmv;
+  int nb_spmv;
+  const MarchPlan mp = spmv_plan(c, g, nb_spmv);
   // the buffer keeps the previous call's contents: clear the scalars (their
   // reduction counter must start at 0) and the right-hand side (constrained
   // components stay 0); every other vector is written before it is read
@@ -134,7 +135,7 @@ static int solve_noalloc(icarat_ctx *c, const icarat_solve_opts *opts, const dou
     for(int k = 0; k < chunk; k++)
     {
       note_launch(3);
-      k_cg_spmv<<<nb_spmv, 128, 0, c->stream>>>(g, c->ke0, c->d_E, c->d_fix, p, Ap,
+      k_cg_spmv<<<nb_spmv, 128, 0, c->stream>>>(g, mp, c->ke0, c->d_E, c->d_fix, p, Ap,
                                                  partials, s);
       k_cg_update_jacobi<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
           n, invd, x, r, z, p, Ap, partials, s);

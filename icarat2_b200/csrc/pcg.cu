@@ -140,7 +140,7 @@ __global__ void k_cg_init_warm(int n, const double *__restrict__ b,
 
 // Ap = K p, alpha = zr / (p . Ap)
 __global__ void __launch_bounds__(128)
-    k_cg_spmv(GridDev g, KeParam ke, const double *__restrict__ E,
+    k_cg_spmv(GridDev g, MarchPlan m, KeParam ke, const double *__restrict__ E,
               const uint8_t *__restrict__ fix, const double *__restrict__ p,
               double *__restrict__ Ap, double *__restrict__ partials,
               CgScalars *s)
@@ -149,19 +149,25 @@ __global__ void __launch_bounds__(128)
   if(s->done)
     return;
   double dot = 0.0;
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
-      n += gridDim.x * blockDim.x)
+  for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
+      t += (long)gridDim.x * blockDim.x)
   {
-    double acc[3], uc[3];
-    node_Ku(g, ke, E, p, n, acc, uc);
-    const unsigned f = fix[n];
-    const double y0 = (f & 1u) ? 0.0 : acc[0];
-    const double y1 = (f & 2u) ? 0.0 : acc[1];
-    const double y2 = (f & 4u) ? 0.0 : acc[2];
-    Ap[n] = y0;
-    Ap[(long)g.numnp + n] = y1;
-    Ap[2L * g.numnp + n] = y2;
-    dot += uc[0] * y0 + uc[1] * y1 + uc[2] * y2;
+    int i, j, k0, k1;
+    if(!march_item(g, m, t, i, j, k0, k1))
+      continue;
+    column_Ku(g, ke, E, p, i, j, k0, k1,
+              [&](int k, const double(&acc)[3], const double(&uc)[3])
+              {
+                const int n = i + j * g.NX + k * g.NX * g.NY;
+                const unsigned f = fix[n];
+                const double y0 = (f & 1u) ? 0.0 : acc[0];
+                const double y1 = (f & 2u) ? 0.0 : acc[1];
+                const double y2 = (f & 4u) ? 0.0 : acc[2];
+                Ap[n] = y0;
+                Ap[(long)g.numnp + n] = y1;
+                Ap[2L * g.numnp + n] = y2;
+                dot += uc[0] * y0 + uc[1] * y1 + uc[2] * y2;
+              });
   }
   double v[1] = {dot};
   block_sum<1>(v, sh);
@@ -310,10 +316,14 @@ static GridDev fine_grid(const icarat_ctx *c)
   return GridDev{c->nx, c->ny, c->nz, c->NX, c->NY, c->NZ, c->numnp, c->nelx};
 }
 
-static int spmv_blocks(const icarat_ctx *c)
+// column-march plan and block count of k_cg_spmv (blocks capped at the
+// reduction's partial count; the kernel strides over the rest)
+MarchPlan spmv_plan(const icarat_ctx *c, const GridDev &g, int &blocks)
 {
-  int b = (c->numnp + 127) / 128;
-  return b > kMaxRedBlocks ? kMaxRedBlocks : (b < 1 ? 1 : b);
+  const MarchPlan m = march_launch(g, (const void *)k_cg_spmv, 128, c->sm_count, blocks);
+  if(blocks > kMaxRedBlocks)
+    blocks = kMaxRedBlocks;
+  return m;
 }
 
 // One CG iteration (enqueued on c->stream).
@@ -337,9 +347,11 @@ static void enqueue_iteration(icarat_ctx *c, int method, int smooth,
   }
   else
   {
+    int blocks;
+    const MarchPlan m = spmv_plan(c, g, blocks);
     note_launch();
-    k_cg_spmv<<<spmv_blocks(c), 128, 0, c->stream>>>(g, c->ke0, c->d_E, c->d_fix, c->d_p,
-                                                     c->d_Ap, c->d_partials, c->d_cg);
+    k_cg_spmv<<<blocks, 128, 0, c->stream>>>(g, m, c->ke0, c->d_E, c->d_fix, c->d_p,
+                                             c->d_Ap, c->d_partials, c->d_cg);
   }
   if(method == ICARAT_SOLVER_JACOBI_PCG)
   {

@@ -6,6 +6,10 @@
 // write the same output and no atomics or colouring are needed.  Ke0 is a
 // by-value kernel parameter (constant bank).
 #pragma once
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "internal.cuh"
 
 namespace icarat_b200
@@ -164,6 +168,180 @@ __device__ __forceinline__ void node_Ku(const GridDev &g, const KP &ke,
     for(int sx = 0; sx < 2; sx++)
       Ev[sy * 2 + sx] = load_E(E, g, i - 1 + sx, j - 1 + sy, k);
   layer_contrib<1>(ke, ul, Ev, acc);
+}
+
+// Grid transfers of the geometric multigrid for one node (CG = true: loads
+// through L2 only, for vectors rewritten inside a persistent launch).
+// Restriction R = P^T: the 27 fine nodes around coarse node n with weights
+// 1/2 per offset axis; s = (R r)_n before masking.
+template <typename T, bool CG>
+__device__ __forceinline__ void restrict_node(const GridDev &f, const GridDev &c,
+                                              const T *__restrict__ rf, int n, T (&s)[3])
+{
+  const int I = n % c.NX, J = (n / c.NX) % c.NY, K = n / (c.NX * c.NY);
+  s[0] = s[1] = s[2] = T(0);
+#pragma unroll
+  for(int dz = -1; dz <= 1; dz++)
+#pragma unroll
+    for(int dy = -1; dy <= 1; dy++)
+#pragma unroll
+      for(int dx = -1; dx <= 1; dx++)
+      {
+        const int i = 2 * I + dx, j = 2 * J + dy, k = 2 * K + dz;
+        if(i < 0 || i >= f.NX || j < 0 || j >= f.NY || k < 0 || k >= f.NZ)
+          continue;
+        const T w = T((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
+        const long m = i + (long)j * f.NX + (long)k * f.NX * f.NY;
+#pragma unroll
+        for(int q = 0; q < 3; q++)
+          s[q] += w * (CG ? __ldcg(rf + (long)q * f.numnp + m) : rf[(long)q * f.numnp + m]);
+      }
+}
+
+// Trilinear prolongation: s = (P xc) at fine node n (odd coordinates take
+// both coarse neighbours with 1/2, even ones the coincident coarse node).
+template <typename T, bool CG>
+__device__ __forceinline__ void prolong_node(const GridDev &f, const GridDev &c,
+                                             const T *__restrict__ xc, int n, T (&s)[3])
+{
+  const int i = n % f.NX, j = (n / f.NX) % f.NY, k = n / (f.NX * f.NY);
+  const int I0 = i >> 1, J0 = j >> 1, K0 = k >> 1;
+  const int I1 = I0 + (i & 1), J1 = J0 + (j & 1), K1 = K0 + (k & 1);
+  const T wx = (i & 1) ? T(0.5) : T(1), wy = (j & 1) ? T(0.5) : T(1),
+          wz = (k & 1) ? T(0.5) : T(1);
+  s[0] = s[1] = s[2] = T(0);
+#pragma unroll
+  for(int cz = 0; cz < 2; cz++)
+#pragma unroll
+    for(int cy = 0; cy < 2; cy++)
+#pragma unroll
+      for(int cx = 0; cx < 2; cx++)
+      {
+        if((cx && !(i & 1)) || (cy && !(j & 1)) || (cz && !(k & 1)))
+          continue;
+        const int I = cx ? I1 : I0, J = cy ? J1 : J0, K = cz ? K1 : K0;
+        const long m = I + (long)J * c.NX + (long)K * c.NX * c.NY;
+        const T w = wx * wy * wz;
+#pragma unroll
+        for(int q = 0; q < 3; q++)
+          s[q] += w * (CG ? __ldcg(xc + (long)q * c.numnp + m) : xc[(long)q * c.numnp + m]);
+      }
+}
+
+// Column march.  The thread of node column (i, j) evaluates K u at the nodes
+// (i, j, k), k0 <= k < k1, sweeping the element layers e = k0 - 1 .. k1 - 1
+// once: element layer e closes node e (its elements above, SZ = 1) and opens
+// node e + 1 (its elements below, SZ = 0), so every node layer's 27
+// displacements and every element layer's 4 moduli are loaded once per
+// column instead of once per node, and the x / y bounds tests are per column.
+// The sums run in the order of node_Ku (below, then above), so the results
+// are identical.  emit(k, acc, uc) receives each node's K u and its own
+// displacement.
+template <typename T, typename KP, bool CG = false, typename F>
+__device__ __forceinline__ void column_Ku(const GridDev &g, const KP &ke,
+                                          const T *__restrict__ E, const T *__restrict__ u,
+                                          int i, int j, int k0, int k1, F &&emit)
+{
+  T ul[2][9][3];
+  T below[3] = {T(0), T(0), T(0)};
+  load_layer<T, CG>(u, g, i, j, k0 - 1, ul[0]);
+  for(int e = k0 - 1; e < k1; e++)
+  {
+    load_layer<T, CG>(u, g, i, j, e + 1, ul[1]);
+    T Ev[4];
+#pragma unroll
+    for(int sy = 0; sy < 2; sy++)
+#pragma unroll
+      for(int sx = 0; sx < 2; sx++)
+        Ev[sy * 2 + sx] = load_E(E, g, i - 1 + sx, j - 1 + sy, e);
+    if(e >= k0)
+    {
+      T acc[3] = {below[0], below[1], below[2]};
+      layer_contrib<1>(ke, ul, Ev, acc);
+      const T uc[3] = {ul[0][4][0], ul[0][4][1], ul[0][4][2]};
+      emit(e, acc, uc);
+    }
+    if(e + 1 < k1)
+    {
+      below[0] = below[1] = below[2] = T(0);
+      layer_contrib<0>(ke, ul, Ev, below);
+    }
+#pragma unroll
+    for(int s = 0; s < 9; s++)
+#pragma unroll
+      for(int d = 0; d < 3; d++)
+        ul[0][s][d] = ul[1][s][d];
+  }
+}
+
+// Work items of a column march: ncol columns (NX NY rounded up to whole
+// warps, so a warp never straddles two z chunks) times ceil(NZ / kc) chunks.
+struct MarchPlan
+{
+  int kc, ncol;
+  long items;
+};
+
+// node layers per chunk: the largest count that still gives every resident
+// thread slot (slots) about two items, at least 4
+inline MarchPlan march_plan(const GridDev &g, long slots)
+{
+  MarchPlan m;
+  m.ncol = ((g.NX * g.NY + 31) / 32) * 32;
+  int kc = g.NZ;
+  while(kc > 4 && (long)m.ncol * ((g.NZ + kc - 1) / kc) < 2 * slots)
+    kc = (kc + 1) / 2;
+  m.kc = kc < 1 ? 1 : kc;
+  m.items = (long)m.ncol * ((g.NZ + m.kc - 1) / m.kc);
+  return m;
+}
+
+// resident threads of `kernel` at `threads` per block on the whole GPU
+// (occupancy cached per kernel)
+inline long resident_threads(const void *kernel, int threads, int sms)
+{
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_pair(kernel, threads);
+  auto it = cache.find(key);
+  int occ;
+  if(it == cache.end())
+  {
+    occ = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, 0) != cudaSuccess ||
+       occ < 1)
+      occ = 1;
+    cache[key] = occ;
+  }
+  else
+    occ = it->second;
+  return (long)occ * threads * sms;
+}
+
+// plan and block count of a column-march launch of `kernel`
+inline MarchPlan march_launch(const GridDev &g, const void *kernel, int threads, int sms,
+                              int &blocks)
+{
+  const MarchPlan m = march_plan(g, resident_threads(kernel, threads, sms));
+  const long b = (m.items + threads - 1) / threads;
+  blocks = (int)(b < 1 ? 1 : b);
+  return m;
+}
+
+// the column and z range of item t; false for the padding columns
+__device__ __forceinline__ bool march_item(const GridDev &g, const MarchPlan &m, long t,
+                                           int &i, int &j, int &k0, int &k1)
+{
+  const int col = (int)(t % m.ncol);
+  const int chunk = (int)(t / m.ncol);
+  if(col >= g.NX * g.NY)
+    return false;
+  i = col % g.NX;
+  j = col / g.NX;
+  k0 = chunk * m.kc;
+  k1 = k0 + m.kc < g.NZ ? k0 + m.kc : g.NZ;
+  return true;
 }
 
 } // namespace icarat_b200

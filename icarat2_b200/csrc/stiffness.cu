@@ -11,25 +11,31 @@ namespace icarat_b200
 
 // y = K u (constrained rows zeroed); optional per-block partial of u . y.
 __global__ void __launch_bounds__(128)
-    k_apply_K_f64(GridDev g, KeParam ke, const double *__restrict__ E,
+    k_apply_K_f64(GridDev g, MarchPlan m, KeParam ke, const double *__restrict__ E,
                   const uint8_t *__restrict__ fix, const double *__restrict__ u,
                   double *__restrict__ y, double *__restrict__ partials)
 {
   __shared__ double sh[32];
   double dot = 0.0;
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
-      n += gridDim.x * blockDim.x)
+  for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
+      t += (long)gridDim.x * blockDim.x)
   {
-    double acc[3], uc[3];
-    node_Ku(g, ke, E, u, n, acc, uc);
-    const unsigned f = fix[n];
-    const double y0 = (f & 1u) ? 0.0 : acc[0];
-    const double y1 = (f & 2u) ? 0.0 : acc[1];
-    const double y2 = (f & 4u) ? 0.0 : acc[2];
-    y[n] = y0;
-    y[(long)g.numnp + n] = y1;
-    y[2L * g.numnp + n] = y2;
-    dot += uc[0] * y0 + uc[1] * y1 + uc[2] * y2;
+    int i, j, k0, k1;
+    if(!march_item(g, m, t, i, j, k0, k1))
+      continue;
+    column_Ku(g, ke, E, u, i, j, k0, k1,
+              [&](int k, const double(&acc)[3], const double(&uc)[3])
+              {
+                const int n = i + j * g.NX + k * g.NX * g.NY;
+                const unsigned f = fix[n];
+                const double y0 = (f & 1u) ? 0.0 : acc[0];
+                const double y1 = (f & 2u) ? 0.0 : acc[1];
+                const double y2 = (f & 4u) ? 0.0 : acc[2];
+                y[n] = y0;
+                y[(long)g.numnp + n] = y1;
+                y[2L * g.numnp + n] = y2;
+                dot += uc[0] * y0 + uc[1] * y1 + uc[2] * y2;
+              });
   }
   if(partials)
   {
@@ -177,38 +183,46 @@ void launch_apply_K(icarat_ctx *c, const GridDev &g, const double *E,
     launch_ku_dmma(c, TC_APPLY, a, c->stream);
     return;
   }
-  int blocks = node_blocks(g, 128);
+  int blocks;
+  const MarchPlan m = march_launch(g, (const void *)k_apply_K_f64, 128, c->sm_count, blocks);
   if(dot_partials && blocks > kMaxRedBlocks)
     blocks = kMaxRedBlocks;
   note_launch();
-  k_apply_K_f64<<<blocks, 128, 0, c->stream>>>(g, c->ke0, E, fix, u, y,
-                                               dot_partials);
+  k_apply_K_f64<<<blocks, 128, 0, c->stream>>>(g, m, c->ke0, E, fix, u, y, dot_partials);
   ICK(cudaGetLastError());
 }
 
 // y = K u in FP32 (the FP32 copies of Ke0 and of the moduli)
 __global__ void __launch_bounds__(128)
-    k_apply_K_f32(GridDev g, KeParamF ke, const float *__restrict__ E,
+    k_apply_K_f32(GridDev g, MarchPlan m, KeParamF ke, const float *__restrict__ E,
                   const uint8_t *__restrict__ fix, const float *__restrict__ u,
                   float *__restrict__ y)
 {
-  for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.numnp;
-      n += gridDim.x * blockDim.x)
+  for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
+      t += (long)gridDim.x * blockDim.x)
   {
-    float acc[3], uc[3];
-    node_Ku(g, ke, E, u, n, acc, uc);
-    const unsigned f = fix[n];
+    int i, j, k0, k1;
+    if(!march_item(g, m, t, i, j, k0, k1))
+      continue;
+    column_Ku(g, ke, E, u, i, j, k0, k1,
+              [&](int k, const float(&acc)[3], const float(&)[3])
+              {
+                const int n = i + j * g.NX + k * g.NX * g.NY;
+                const unsigned f = fix[n];
 #pragma unroll
-    for(int c = 0; c < 3; c++)
-      y[(long)c * g.numnp + n] = ((f >> c) & 1u) ? 0.0f : acc[c];
+                for(int c = 0; c < 3; c++)
+                  y[(long)c * g.numnp + n] = ((f >> c) & 1u) ? 0.0f : acc[c];
+              });
   }
 }
 
 void launch_apply_K_f32(icarat_ctx *c, const GridDev &g, const float *E,
                         const uint8_t *fix, const float *u, float *y)
 {
+  int blocks;
+  const MarchPlan m = march_launch(g, (const void *)k_apply_K_f32, 128, c->sm_count, blocks);
   note_launch();
-  k_apply_K_f32<<<node_blocks(g, 128), 128, 0, c->stream>>>(g, c->ke0f, E, fix, u, y);
+  k_apply_K_f32<<<blocks, 128, 0, c->stream>>>(g, m, c->ke0f, E, fix, u, y);
   ICK(cudaGetLastError());
 }
 

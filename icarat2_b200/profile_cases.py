@@ -24,6 +24,11 @@ set-up.
         one design iteration of the MMA loop (densities U[0.1, 0.5], seed 0,
         filter radius 3, move 0.2) after `warm` warm-up iterations; methods
         mg, mixed (warm-started), jacobi
+    python -m icarat2_b200.profile_cases ocloop 128x64x64 1.5 5
+        one design iteration of the OC loop of opt_macro_oc.cpp (uniform
+        start 0.3, radius filter R, move 0.15, 4-level MG-PCG to 1e-8 with
+        the coarse factor reused and warm starts) after `warm` warm-up
+        iterations: filter, sensitivity and the OC bisection kernel
     python -m icarat2_b200.profile_cases helm 256x128x128 2.0
         one Helmholtz PDE filter call (design U[0, 1], seed 0, CG to 1e-10)
         after one warm-up call
@@ -114,6 +119,23 @@ def headline(warm):
                                                          info.status))
 
 
+def ocloop(grid, radius, warm):
+    nx, ny, nz = _grid(grid)
+    G = gpu.Context(nx, ny, nz)
+    o = gpu.solve_opts(gpu.MG_PCG, rtol=1e-8, mg_levels=4, coarse_lag=1, warm_start=1)
+    G.loop_init(0.3, method="oc", filter_radius=float(radius), move=0.15, solve=o)
+    for _ in range(int(warm)):
+        G.loop_step()
+    G.synchronize()
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    info = G.loop_step()
+    G.synchronize()
+    rt.cudaProfilerStop()
+    print("cg iterations %d compliance %.6g oc steps %d status %d" % (
+        info.cg_iterations, info.compliance, info.update_steps, info.status))
+
+
 def net(grid):
     nx, ny, nz = _grid(grid)
     G = gpu.Context(nx, ny, nz)
@@ -151,6 +173,8 @@ def main(argv):
         solve(*argv[1:5])
     elif len(argv) >= 6 and argv[0] == "loop":
         loop(*argv[1:6])
+    elif len(argv) >= 4 and argv[0] == "ocloop":
+        ocloop(*argv[1:4])
     elif len(argv) >= 2 and argv[0] == "headline":
         headline(argv[1])
     elif len(argv) >= 3 and argv[0] == "helm":

@@ -154,9 +154,10 @@ typedef struct
    appended (Helmholtz filter); callers built against 10000 headers pass the
    shorter structs and must be rebuilt.  A caller checks
    icarat_version() == ICARAT_ABI_VERSION before passing option structs. */
-/* 10200: icarat_loop_is_convergence, icarat_ctx_create_selection and
-   icarat_selection_ids added (new functions; the 10100 structs are
-   unchanged). */
+/* 10200: icarat_loop_is_convergence, icarat_ctx_create_selection,
+   icarat_selection_ids and icarat_batch_autotune_mg added, and the batch
+   method ICARAT_SOLVER_MG_PCG (new functions and values; the 10100 structs
+   are unchanged). */
 #define ICARAT_ABI_VERSION 10200
 int icarat_version(void);
 const char *icarat_status_string(int status);
@@ -418,16 +419,25 @@ typedef struct
   int blocks_per_sm; /* persistent CTAs per SM (0 = autotuned, else the
                         occupancy limit) */
   int method;        /* 0 = the persistent Jacobi launch above;
+                        ICARAT_SOLVER_MG_PCG = one persistent launch of
+                        multigrid-PCG over all designs: every design's own
+                        geometric multigrid hierarchy (FP32 Chebyshev-smoothed
+                        V-cycle, FP64 dense coarsest solve) applied to all
+                        designs phase by phase inside the launch, FP64
+                        refresh and stopping test, under a CUDA graph, shape
+                        from icarat_batch_autotune_mg;
                         ICARAT_SOLVER_MIXED_IR = every design's own
                         mixed-precision multigrid-PCG (FP32 operator and
                         V-cycle, FP64 refresh and stopping test), the designs
                         interleaved on their own streams as CUDA-graph
                         replays of `chunk` iterations */
-  int mg_levels;     /* MIXED_IR: levels (0 = 4); a design whose divisions
-                        do not halve that often gets fewer */
+  int mg_levels;     /* MG_PCG, MIXED_IR: levels (0 = 4); MIXED_IR: a design
+                        whose divisions do not halve that often gets fewer;
+                        MG_PCG: the smallest count every design supports
+                        (at most 8) */
   int chunk;         /* MIXED_IR: iterations per replay (0 = 4) */
-  int warm_start;    /* MIXED_IR: start from each design's last solution
-                        (designs not solved yet start from 0) */
+  int warm_start;    /* MG_PCG, MIXED_IR: start from each design's last
+                        solution (designs not solved yet start from 0) */
 } icarat_batch_opts;
 
 int icarat_batch_create(const icarat_grid *grids, const icarat_bc *bcs, int count,
@@ -439,6 +449,11 @@ int icarat_batch_ctx(icarat_batch *batch, int i, icarat_ctx **ctx);
    keep the fastest for later solves; any output pointer may be NULL */
 int icarat_batch_autotune(icarat_batch *batch, int *tile, int *blocks_per_sm,
                           double *ms_per_iteration);
+/* the same for the persistent multigrid launch (method ICARAT_SOLVER_MG_PCG)
+   with mg_levels levels (0 = 4): the fastest (tile, CTAs per SM) of that
+   kernel on the current designs, kept for later MG_PCG solves */
+int icarat_batch_autotune_mg(icarat_batch *batch, int mg_levels, int *tile,
+                             int *blocks_per_sm, double *ms_per_iteration);
 /* K u = f for every design (f from its boundary conditions, u kept in its
    context as after icarat_solve); infos: count entries (may be NULL) */
 int icarat_batch_solve(icarat_batch *batch, const icarat_batch_opts *opts,

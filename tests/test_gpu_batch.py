@@ -235,7 +235,7 @@ def test_batch_concurrent_design_loop_tracks_individual_loops(gpu):
 def test_batch_rejects_unknown_method(gpu):
     B = gpu.Batch(problems(gpu, [(8, 4, 4)], 17))
     B[0].set_design(np.full(B[0].nelx, 0.5))
-    for o in (B.opts(method=gpu.MG_PCG), B.opts(method=gpu.MIXED_IR, mg_levels=1),
+    for o in (B.opts(method=7), B.opts(method=gpu.MIXED_IR, mg_levels=1),
               B.opts(method=gpu.MIXED_IR, chunk=-1)):
         with pytest.raises(gpu.IcaratError) as e:
             B.solve(o)
@@ -258,6 +258,77 @@ def test_batch_design_loop_with_helmholtz_filter(gpu):
         solo.append(G)
     o = B.opts(rtol=1e-10, method=gpu.MIXED_IR, warm_start=True)
     for _ in range(3):
+        infos = B.loop_step(o)
+        for i, G in enumerate(solo):
+            ref = G.loop_step()
+            assert infos[i].status == gpu.OK
+            assert abs(infos[i].compliance - ref.compliance) <= 1e-6 * ref.compliance
+    for i, G in enumerate(solo):
+        assert rel(B[i].loop_get("x"), G.loop_get("x")) <= 1e-6
+
+
+# ---- one persistent multigrid-PCG launch over all designs (method MG_PCG) ----
+
+MG_SIZES = [(16, 8, 8), (24, 12, 12), (32, 16, 16), (8, 8, 8), (16, 8, 8), (40, 16, 8)]
+
+
+def test_batch_persistent_mg_matches_individual_solves(gpu):
+    """uneven grids, one launch: every design meets rtol in FP64 and matches
+    its own FP64 MG-PCG solve to 1e-6; far fewer iterations than the
+    persistent Jacobi launch"""
+    prs = problems(gpu, MG_SIZES, 21)
+    B = gpu.Batch(prs)
+    rng = np.random.default_rng(22)
+    rhos = [rng.uniform(0.05, 1.0, B[i].nelx) for i in range(len(B))]
+    for i, r in enumerate(rhos):
+        B[i].set_design(r)
+    infos = B.solve(B.opts(rtol=1e-9, method=gpu.MG_PCG, mg_levels=4))
+    jac = B.solve(B.opts(rtol=1e-9))
+    for i, pr in enumerate(prs):
+        assert infos[i].status == gpu.OK and infos[i].rel_residual < 1e-9, (i, infos[i].status)
+        assert infos[i].iterations * 3 < jac[i].iterations
+    infos = B.solve(B.opts(rtol=1e-9, method=gpu.MG_PCG, mg_levels=4))
+    for i, pr in enumerate(prs):
+        u = B.solution(i)
+        assert rel(u, reference(gpu, pr, rhos[i], 2)) <= 1e-6
+        f = B[i].fext()
+        assert np.linalg.norm(f - B[i].apply_K(u)) < 1.001e-9 * np.linalg.norm(f)
+
+
+def test_batch_persistent_mg_warm_start_cap_and_autotune(gpu):
+    prs = problems(gpu, [(16, 8, 8), (32, 16, 16), (8, 4, 4)], 23)
+    B = gpu.Batch(prs)
+    rng = np.random.default_rng(24)
+    rhos = [rng.uniform(0.1, 0.9, B[i].nelx) for i in range(len(B))]
+    for i, r in enumerate(rhos):
+        B[i].set_design(r)
+    tile, bpsm, ms = B.autotune_mg(3)
+    assert tile in (128, 256, 512, 1024) and bpsm >= 1 and ms > 0
+    cold = B.solve(B.opts(rtol=1e-10, method=gpu.MG_PCG, mg_levels=3))
+    for i, r in enumerate(rhos):
+        B[i].set_design(np.clip(r * 1.02, 0.0, 1.0))
+    warm = B.solve(B.opts(rtol=1e-10, method=gpu.MG_PCG, mg_levels=3, warm_start=True))
+    for i, pr in enumerate(prs):
+        assert cold[i].status == gpu.OK and warm[i].status == gpu.OK
+        assert warm[i].iterations <= cold[i].iterations
+        ref = reference(gpu, pr, np.clip(rhos[i] * 1.02, 0.0, 1.0), 2)
+        assert rel(B.solution(i), ref) <= 1e-6
+    capped = B.solve(B.opts(rtol=1e-14, maxit=2, method=gpu.MG_PCG, mg_levels=3))
+    assert all(c.status == gpu.WARN_MAXITER and c.iterations == 2 for c in capped)
+
+
+def test_batch_persistent_mg_design_loop_tracks_individual_loops(gpu):
+    prs = problems(gpu, [(16, 8, 8), (24, 12, 12)], 25)
+    B = gpu.Batch(prs)
+    solo = []
+    for i, (nx, ny, nz, d, lo) in enumerate(prs):
+        B[i].loop_init(0.3, method="mma", filter_radius=1.5, move=0.2)
+        G = gpu.Context(nx, ny, nz, dirichlet=d, loads=lo)
+        G.loop_init(0.3, method="mma", filter_radius=1.5, move=0.2,
+                    solve=gpu.solve_opts(gpu.MG_PCG, rtol=1e-12, mg_levels=2))
+        solo.append(G)
+    o = B.opts(rtol=1e-10, method=gpu.MG_PCG, mg_levels=3, warm_start=True)
+    for _ in range(4):
         infos = B.loop_step(o)
         for i, G in enumerate(solo):
             ref = G.loop_step()
