@@ -393,9 +393,9 @@ def _bc_struct(dirichlet, loads):
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
                chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0, fp64_tc=0,
                coarse_lag=0):
-    """fp64_tc (JACOBI_PCG, MG_PCG): FP64 products on the FP64 tensor cores
-    by grid size (0), on every level of 32k nodes and more (1), or the node
-    stencil only (-1).  coarse_lag (MG_PCG, MIXED_IR): keep the previous
+    """fp64_tc (JACOBI_PCG, MG_PCG): FP64 products by the node stencil (0,
+    the default, and -1; the faster operator at every measured size) or on
+    the FP64 tensor cores on every level of 32k nodes and more (1).  coarse_lag (MG_PCG, MIXED_IR): keep the previous
     design's coarsest factor while this design's is computed on a second
     stream."""
     return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,

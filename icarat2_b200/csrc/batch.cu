@@ -657,7 +657,7 @@ static int batch_solve_concurrent(icarat_batch *B, const icarat_batch_opts *o, d
 }
 
 // ---------------------------------------------------------------- multigrid
-constexpr int kBmCoarseRows = 32; // coarse dense rows per work item
+constexpr int kBmCoarseRows = 8; // coarse dense rows per work item
 constexpr int kBmDeg = 2;         // Chebyshev steps per level and direction
 
 // Item tables of the persistent multigrid launch: node tiles of every level
@@ -690,7 +690,7 @@ static void batch_mg_tables(icarat_batch *B, int L, int tile)
     M.citems = std::max(1, (M.nc + kBmCoarseRows - 1) / kBmCoarseRows);
     for(int i = 0; i < M.citems; i++)
       citems.push_back((int)d);
-    ylen += std::max(1, M.nc);
+    ylen += 2L * std::max(1, M.nc);
   }
   if(B->mg_levels != L || B->mg_tile != tile)
   {
@@ -749,8 +749,10 @@ static void batch_mg_tables(icarat_batch *B, int L, int tile)
     M.W = c->coarse.W[c->coarse.cur];
     M.WT = c->coarse.work[c->coarse.cur];
     M.map = c->coarse.map;
-    M.y = B->d_y + yoff;
-    yoff += std::max(1, M.nc);
+    M.cmap = c->coarse.map + M.nc;
+    M.v = B->d_y + yoff;
+    M.y = M.v + std::max(1, M.nc);
+    yoff += 2L * std::max(1, M.nc);
     const double lmax = c->lam_max_dk, lmin = 0.1 * lmax;
     const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
     const double sigma = theta / delta;

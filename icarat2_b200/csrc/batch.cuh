@@ -133,8 +133,10 @@ struct BmDesign
 {
   BmLevel lv[kBmMaxLevels];
   const double *W, *WT;
-  const int *map; // coarse unknown -> index of the coarsest level's node vectors
-  double *y;      // W b
+  const int *map;  // coarse unknown -> index of the coarsest level's node vectors
+  const int *cmap; // node-major index 3 n + q of the coarsest level -> unknown (-1: fixed)
+  double *v;       // the coarsest right-hand side gathered to the unknowns
+  double *y;       // W v
   int nc;         // coarse unknowns
   int citem0, citems;
   float inv_theta;

@@ -204,7 +204,14 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
           const long id = (long)q * C.g.numnp + n;
           const float bq = ((fx >> q) & 1u) ? 0.0f : sr[q];
           C.b[id] = bq;
-          if(smooth)
+          if(!smooth)
+          {
+            // coarsest level: the dense solve's right-hand side, gathered
+            const int u = __ldg(B.cmap + 3L * n + q);
+            if(u >= 0)
+              B.v[u] = (double)bq;
+          }
+          else
           {
             const float di = B.inv_theta * __ldg(C.invd + id) * bq;
             C.x[id] = di;
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
     cur[lc] = 0;
   };
 
-  // coarsest level: y = W b (and the level's iterate cleared), then x = W^T y
+  // coarsest level: y = W v (and the level's iterate cleared), then x = W^T y
   auto coarse_lower = [&](int mode)
   {
     const Span sp = span_of(m.c_nitems);
@@ -232,10 +239,18 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
       const int r0 = q * m.ctile, r1 = min(r0 + m.ctile, B.nc);
       for(int r = r0 + warp; r < r1; r += nw)
       {
+        // four independent partial sums: four loads of the row and of v in
+        // flight per lane
         const double *row = B.W + (long)r * B.nc;
-        double sum = 0.0;
-        for(int j = lane; j <= r; j += 32)
-          sum = fma(__ldg(row + j), (double)__ldcg(C.b + __ldg(B.map + j)), sum);
+        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+        int j = lane;
+        for(; j + 96 <= r; j += 128)
+#pragma unroll
+          for(int u = 0; u < 4; u++)
+            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(B.v + j + 32 * u), s4[u]);
+        for(; j <= r; j += 32)
+          s4[0] = fma(__ldg(row + j), __ldcg(B.v + j), s4[0]);
+        double sum = (s4[0] + s4[1]) + (s4[2] + s4[3]);
         for(int o = 16; o > 0; o >>= 1)
           sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if(lane == 0)
@@ -267,9 +282,15 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
       for(int r = r0 + warp; r < r1; r += nw)
       {
         const double *row = B.WT + (long)r * B.nc;
-        double sum = 0.0;
-        for(int j = r + lane; j < B.nc; j += 32)
-          sum = fma(__ldg(row + j), __ldcg(B.y + j), sum);
+        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+        int j = r + lane;
+        for(; j + 96 < B.nc; j += 128)
+#pragma unroll
+          for(int u = 0; u < 4; u++)
+            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(B.y + j + 32 * u), s4[u]);
+        for(; j < B.nc; j += 32)
+          s4[0] = fma(__ldg(row + j), __ldcg(B.y + j), s4[0]);
+        double sum = (s4[0] + s4[1]) + (s4[2] + s4[3]);
         for(int o = 16; o > 0; o >>= 1)
           sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if(lane == 0)

@@ -149,23 +149,18 @@ static int node_blocks(const GridDev &g, int threads)
   return b < 1 ? 1 : b;
 }
 
-// Below kDmmaMinNodes the element tiles would leave most SMs idle; below
-// kDmmaAutoNodes the node stencil is the faster of the two on a B200
-// (measured: 60 us against 62 us at 129 x 65 x 65 nodes, 494 us against
-// 331 us at 257 x 129 x 129).
+// Below kDmmaMinNodes the element tiles would leave most SMs idle.  The
+// column-march node stencil is the faster FP64 operator at every grid size
+// measured on a B200 (35 us against 62 us at 129 x 65 x 65 nodes, 273 us
+// against 331 us at 257 x 129 x 129), so the default (fp64_tc 0) is the
+// stencil and the FP64 tensor cores run only when asked for.
 constexpr int kDmmaMinNodes = 1 << 15;
-constexpr int kDmmaAutoNodes = 1 << 21;
 
 bool use_dmma(const icarat_ctx *c, const GridDev &g)
 {
-  if(c->fp64_tc < 0 || !dmma_fits(g))
+  if(c->fp64_tc <= 0 || !dmma_fits(g))
     return false;
-  switch(c->fp64_tc)
-  {
-  case 0: return g.numnp >= kDmmaAutoNodes;
-  case 1: return g.numnp >= kDmmaMinNodes;
-  default: return true;
-  }
+  return c->fp64_tc == 1 ? g.numnp >= kDmmaMinNodes : true;
 }
 
 void launch_apply_K(icarat_ctx *c, const GridDev &g, const double *E,

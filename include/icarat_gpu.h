@@ -112,10 +112,10 @@ typedef struct
                      the loop): r0 = b - K x0, same stop test ||r|| < rtol ||b|| */
   int fp64_tc;    /* JACOBI_PCG, MG_PCG: FP64 products K u element by element
                      on the FP64 tensor cores (ICARAT_OP_TC_FP64) or by the
-                     node stencil on the CUDA cores: 0 (default) = by grid
-                     size (tensor cores on levels of 2M nodes and more),
-                     1 = tensor cores on every level of 32k nodes and more,
-                     -1 = node stencil only.  Also the operator of later
+                     node stencil on the CUDA cores: 0 (default) and -1 =
+                     the node stencil (the faster of the two at every
+                     measured size), 1 = tensor cores on every level of 32k
+                     nodes and more.  Also the operator of later
                      icarat_apply_K calls on the context. */
   int coarse_lag; /* MG_PCG, MIXED_IR: 1 = the V-cycle keeps the coarsest-level
                      factor of the previous design while this design's factor

@@ -8,7 +8,8 @@ on an L-bracket (the shape of sample/algorithm/opt-macro-gcmma/lbracket.toml):
     <= 1e-8, compliance <= 1e-10 relative;
   - radius filter, both directions: bit-exact (neighbours among the kept
     elements only, in ascending id);
-  - sensitivities (same displacements): <= 1e-12 relative;
+  - sensitivities (same displacements): <= 1e-11 relative (numpy sums
+    u_e^T Ke0 u_e in another order than the kernel);
   - OC and MMA design loops over 5 iterations: compliance <= 1e-10,
     design <= 1e-10.
 """
@@ -68,7 +69,7 @@ def test_stiffness_and_solves(pair, gpu):
     assert np.allclose(nv, Q.node_values(val), rtol=1e-8, atol=1e-14 * np.abs(nv).max())
     dfds, dgds = G.sensitivity(0.5)
     rd, rg = Q.sensitivity(rho, nv, 0.5)
-    assert rel(dfds, rd) <= 1e-12
+    assert rel(dfds, rd) <= 1e-11
     assert np.array_equal(dgds, rg)
 
 
