@@ -203,6 +203,8 @@ SIGNATURES = {
     "icarat_loop_step": (_i, [_vp, _P(StepInfo)]),
     "icarat_loop_get": (_i, [_vp, _i, _dp]),
     "icarat_loop_is_convergence": (_i, [_vp, _d, _d, _P(_i)]),
+    "icarat_loop_save": (_i, [_vp, C.c_char_p]),
+    "icarat_loop_load": (_i, [_vp, C.c_char_p]),
     "icarat_ctx_create_selection": (_i, [_P(Grid), _P(Material), _P(BC), _i, _dp, _i,
                                          _P(_vp)]),
     "icarat_selection_ids": (_i, [_vp, _vp, _vp]),
@@ -720,6 +722,14 @@ class Context:
         _check(self.lib.icarat_loop_is_convergence(self.h, epsilon, minstep, C.byref(conv)),
                "loop_is_convergence")
         return conv.value
+
+    def loop_save(self, path):
+        """checkpoint of the device loop (icarat_loop_save)"""
+        _check(self.lib.icarat_loop_save(self.h, os.fsencode(path)), "loop_save")
+
+    def loop_load(self, path):
+        """resume a device loop from a checkpoint (icarat_loop_load)"""
+        _check(self.lib.icarat_loop_load(self.h, os.fsencode(path)), "loop_load")
 
     def loop_get(self, which):
         idx = {"x": 0, "xfil": 1, "xthr": 2, "dfds": 3, "dgds": 4}[which]

@@ -31,6 +31,8 @@ void set_capturing(bool on) { g_capturing = on; }
 void build_rhs(icarat_ctx *c);
 int loop_init(icarat_ctx *c, const icarat_loop_opts *o, const double *x0);
 int loop_is_convergence(icarat_ctx *c, double epsilon, double minstep, int *convergence);
+int loop_save(icarat_ctx *c, const char *path);
+int loop_load(icarat_ctx *c, const char *path);
 int loop_step(icarat_ctx *c, icarat_step_info *info);
 int loop_get(icarat_ctx *c, int which, double *out);
 int set_load_cases(icarat_ctx *c, int ncases, const double *fext);
@@ -801,6 +803,24 @@ int icarat_loop_is_convergence(icarat_ctx *c, double epsilon, double minstep,
   check_ctx(c);
   IREQUIRE(convergence, ICARAT_ERR_ARG, "null argument");
   return loop_is_convergence(c, epsilon, minstep, convergence);
+  ICARAT_API_END
+}
+
+int icarat_loop_save(icarat_ctx *c, const char *path)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(path, ICARAT_ERR_ARG, "null path");
+  return loop_save(c, path);
+  ICARAT_API_END
+}
+
+int icarat_loop_load(icarat_ctx *c, const char *path)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(path, ICARAT_ERR_ARG, "null path");
+  return loop_load(c, path);
   ICARAT_API_END
 }
 

@@ -5,6 +5,9 @@
 // opt_macro_oc.cpp:73-74 / opt_mma_Helmholtz.cpp:70-72 and an optional
 // Heaviside threshold.
 #include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -17,6 +20,8 @@ void mma_create(int device, int n, int m, double a, double c, double d,
                 icarat_mma **out, cudaStream_t stream);
 void mma_set_move(icarat_mma *h, double move);
 int mma_last_newton(const icarat_mma *h);
+void mma_state_io(icarat_mma *h, bool save, int *iter, double *low, double *upp,
+                  double *xold1, double *xold2);
 
 __global__ void k_fill(int n, double v, double *__restrict__ out)
 {
@@ -505,6 +510,131 @@ int loop_is_convergence(icarat_ctx *c, double epsilon, double minstep, int *conv
     L.object_old = L.object_f;
     *convergence = 1;
   }
+  return ICARAT_OK;
+}
+
+// ---- loop snapshot (checkpoint / resume) ---------------------------------
+// Binary file, native byte order: magic, layout version, grid and sizes, the
+// loop options, the step counter, V0, the convergence test's objectives, the
+// design x (box element layout), the MMA state (asymptotes, two previous
+// designs, iteration count) and the displacement a warm start begins from.
+// Load cases and design domains are the caller's configuration: set them
+// again after icarat_loop_load, as after icarat_loop_init.
+namespace
+{
+const char kSnapMagic[8] = {'I', 'C', 'R', 'L', 'O', 'O', 'P', '1'};
+struct SnapHead
+{
+  char magic[8];
+  int version, nx, ny, nz, nelx, neq, numeq, sel_nelx;
+  int optstep, mma_iter, have_u, pad;
+  double lx, ly, lz, V0, object_f, object_old;
+  icarat_loop_opts opts;
+};
+
+struct File
+{
+  FILE *f;
+  explicit File(FILE *p) : f(p) {}
+  ~File()
+  {
+    if(f)
+      fclose(f);
+  }
+};
+} // namespace
+
+int loop_save(icarat_ctx *c, const char *path)
+{
+  LoopState &L = c->loop;
+  IREQUIRE(L.init, ICARAT_ERR_STATE, "icarat_loop_init first");
+  SnapHead h{};
+  std::memcpy(h.magic, kSnapMagic, 8);
+  h.version = 1;
+  h.nx = c->nx;
+  h.ny = c->ny;
+  h.nz = c->nz;
+  h.nelx = c->nelx;
+  h.neq = c->neq;
+  h.numeq = c->numeq;
+  h.sel_nelx = abi_nelx(c);
+  h.optstep = L.optstep;
+  h.mma_iter = -1;
+  h.have_u = c->have_u ? 1 : 0;
+  h.lx = c->lx;
+  h.ly = c->ly;
+  h.lz = c->lz;
+  h.V0 = L.V0;
+  h.object_f = L.object_f;
+  h.object_old = L.object_old;
+  h.opts = L.opts;
+  const size_t n = c->nelx;
+  std::vector<double> x(n), u(h.have_u ? (size_t)c->neq : 0);
+  ICK(cudaMemcpyAsync(x.data(), L.x, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  if(h.have_u)
+    ICK(cudaMemcpyAsync(u.data(), c->d_u, sizeof(double) * c->neq, cudaMemcpyDeviceToHost,
+                        c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
+  std::vector<double> mma;
+  if(L.mma)
+  {
+    const size_t m = abi_nelx(c);
+    mma.resize(4 * m);
+    mma_state_io(L.mma, true, &h.mma_iter, mma.data(), mma.data() + m, mma.data() + 2 * m,
+                 mma.data() + 3 * m);
+  }
+  File f(std::fopen(path, "wb"));
+  IREQUIRE(f.f != nullptr, ICARAT_ERR_ARG, std::string("cannot write ") + path);
+  bool ok = std::fwrite(&h, sizeof(h), 1, f.f) == 1 &&
+            std::fwrite(x.data(), sizeof(double), n, f.f) == n &&
+            std::fwrite(mma.data(), sizeof(double), mma.size(), f.f) == mma.size() &&
+            std::fwrite(u.data(), sizeof(double), u.size(), f.f) == u.size();
+  IREQUIRE(ok, ICARAT_ERR_ARG, std::string("write failed: ") + path);
+  return ICARAT_OK;
+}
+
+int loop_load(icarat_ctx *c, const char *path)
+{
+  File f(std::fopen(path, "rb"));
+  IREQUIRE(f.f != nullptr, ICARAT_ERR_ARG, std::string("cannot read ") + path);
+  SnapHead h{};
+  IREQUIRE(std::fread(&h, sizeof(h), 1, f.f) == 1 && std::memcmp(h.magic, kSnapMagic, 8) == 0 &&
+               h.version == 1,
+           ICARAT_ERR_ARG, std::string("not a loop snapshot: ") + path);
+  IREQUIRE(h.nx == c->nx && h.ny == c->ny && h.nz == c->nz && h.nelx == c->nelx &&
+               h.neq == c->neq && h.numeq == c->numeq && h.sel_nelx == abi_nelx(c) &&
+               h.lx == c->lx && h.ly == c->ly && h.lz == c->lz,
+           ICARAT_ERR_ARG, "the snapshot belongs to another mesh or boundary conditions");
+  const size_t n = c->nelx, m = abi_nelx(c);
+  std::vector<double> x(n), mma(h.mma_iter >= 0 ? 4 * m : 0), u(h.have_u ? (size_t)h.neq : 0);
+  bool ok = std::fread(x.data(), sizeof(double), n, f.f) == n &&
+            std::fread(mma.data(), sizeof(double), mma.size(), f.f) == mma.size() &&
+            std::fread(u.data(), sizeof(double), u.size(), f.f) == u.size();
+  IREQUIRE(ok, ICARAT_ERR_ARG, std::string("truncated snapshot: ") + path);
+  IREQUIRE((h.opts.method == 1) == (h.mma_iter >= 0), ICARAT_ERR_ARG, "inconsistent snapshot");
+  // a fresh loop with the saved options, then the saved state on top; x0 of
+  // loop_init is in the ABI's numbering, the saved x in box layout
+  std::vector<double> x0(m);
+  if(c->sel)
+    for(size_t q = 0; q < m; q++)
+      x0[q] = x[c->sel_elem_h[q]];
+  else
+    x0 = x;
+  loop_init(c, &h.opts, x0.data());
+  LoopState &L = c->loop;
+  ICK(cudaMemcpyAsync(L.x, x.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  if(h.have_u)
+    ICK(cudaMemcpyAsync(c->d_u, u.data(), sizeof(double) * h.neq, cudaMemcpyHostToDevice,
+                        c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
+  c->have_u = h.have_u != 0;
+  L.optstep = h.optstep;
+  L.V0 = h.V0;
+  L.object_f = h.object_f;
+  L.object_old = h.object_old;
+  if(L.mma)
+    mma_state_io(L.mma, false, &h.mma_iter, mma.data(), mma.data() + m, mma.data() + 2 * m,
+                 mma.data() + 3 * m);
   return ICARAT_OK;
 }
 

@@ -607,6 +607,25 @@ int mma_update_host(icarat_mma *h, double *x, const double *dfdx, const double *
 void mma_set_move(icarat_mma *h, double move) { h->move = move; }
 int mma_last_newton(const icarat_mma *h) { return h->last_newton; }
 
+// The state an MMA update carries to the next (asymptotes, the two previous
+// designs, the iteration count that selects the asymptote rule), copied to
+// (save) or from (load) host arrays of n entries.
+void mma_state_io(icarat_mma *h, bool save, int *iter, double *low, double *upp,
+                  double *xold1, double *xold2)
+{
+  const size_t bytes = sizeof(double) * h->n;
+  double *dev[4] = {h->low, h->upp, h->xold1, h->xold2};
+  double *host[4] = {low, upp, xold1, xold2};
+  for(int q = 0; q < 4; q++)
+    ICK(cudaMemcpyAsync(save ? host[q] : dev[q], save ? dev[q] : host[q], bytes,
+                        save ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice, h->stream));
+  ICK(cudaStreamSynchronize(h->stream));
+  if(save)
+    *iter = h->iter;
+  else
+    h->iter = *iter;
+}
+
 } // namespace icarat_b200
 
 using namespace icarat_b200;

@@ -154,8 +154,9 @@ typedef struct
    appended (Helmholtz filter); callers built against 10000 headers pass the
    shorter structs and must be rebuilt.  A caller checks
    icarat_version() == ICARAT_ABI_VERSION before passing option structs. */
-/* 10200: icarat_loop_is_convergence, icarat_ctx_create_selection,
-   icarat_selection_ids and icarat_batch_autotune_mg added, and the batch
+/* 10200: icarat_loop_is_convergence, icarat_loop_save / _load,
+   icarat_ctx_create_selection, icarat_selection_ids and
+   icarat_batch_autotune_mg added, and the batch
    method ICARAT_SOLVER_MG_PCG (new functions and values; the 10100 structs
    are unchanged). */
 #define ICARAT_ABI_VERSION 10200
@@ -535,6 +536,18 @@ int icarat_loop_get(icarat_ctx *ctx, int which, double *out);
  * after the step in which it returned 0. */
 int icarat_loop_is_convergence(icarat_ctx *ctx, double epsilon, double minstep,
                                int *convergence);
+/* Checkpoint / resume of the device loop (the reference writes VTK files per
+ * step, opt_macro_oc.cpp:214-237, but cannot resume): a binary snapshot of
+ * the loop options, step count, V0, the convergence test's objectives, the
+ * design, the MMA state (asymptotes, two previous designs, iteration count)
+ * and the displacement a warm start begins from.  icarat_loop_load re-creates
+ * the loop from it on a context of the same mesh and boundary conditions
+ * (ICARAT_ERR_ARG otherwise); load cases and design domains are set again
+ * afterwards, as after icarat_loop_init.  Later steps then repeat those of
+ * the uninterrupted run (with coarse_lag the first resumed solve factors its
+ * own coarse level, so its iteration count may differ). */
+int icarat_loop_save(icarat_ctx *ctx, const char *path);
+int icarat_loop_load(icarat_ctx *ctx, const char *path);
 /* Load cases (the vector<Force> of opt_multi_load.cpp:68-80): fext holds
  * ncases load vectors of numeq entries (the layout of icarat_fext), case
  * after case.  With ncases >= 1 icarat_loop_step solves every case on the
