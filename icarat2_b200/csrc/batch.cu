@@ -405,6 +405,9 @@ struct icarat_batch
   int lv_nitems[kBmMaxLevels] = {};
   int *d_citems = nullptr;
   int c_nitems = 0;
+  int *d_lv_col[kBmMaxLevels] = {};
+  int lv_col_items[kBmMaxLevels] = {};
+  double *d_partc = nullptr;
   double *d_y = nullptr;
   int mg_levels = 0, mg_tile = 0;         // tables built for these
   int occ_mg = 0;                         // co-resident CTAs per SM
@@ -659,6 +662,7 @@ static int batch_solve_concurrent(icarat_batch *B, const icarat_batch_opts *o, d
 // ---------------------------------------------------------------- multigrid
 constexpr int kBmCoarseRows = 8; // coarse dense rows per work item
 constexpr int kBmDeg = 2;         // Chebyshev steps per level and direction
+constexpr int kBmLayers = 8;      // node layers per column item of the stencil phases
 
 // Item tables of the persistent multigrid launch: node tiles of every level
 // of every design, and row blocks of every design's coarsest dense solve.
@@ -668,7 +672,7 @@ static void batch_mg_tables(icarat_batch *B, int L, int tile)
   batch_items(B, tile);
   const size_t n = B->ctx.size();
   B->h_bm.assign(n, BmDesign{});
-  std::vector<std::vector<int>> lv(L);
+  std::vector<std::vector<int>> lv(L), lvc(L);
   std::vector<int> citems;
   long ylen = 0;
   for(size_t d = 0; d < n; d++)
@@ -684,6 +688,14 @@ static void batch_mg_tables(icarat_batch *B, int L, int tile)
       V.nitems = (g.numnp + tile - 1) / tile;
       for(int i = 0; i < V.nitems; i++)
         lv[l].push_back((int)d);
+      // stencil phases: blocks of kBatchThreads node columns x kBmLayers
+      // node layers
+      V.ncb = (g.NX * g.NY + kBatchThreads - 1) / kBatchThreads;
+      V.kc = std::min(g.NZ, kBmLayers);
+      V.mitem0 = (int)lvc[l].size();
+      V.mitems = V.ncb * ((g.NZ + V.kc - 1) / V.kc);
+      for(int i = 0; i < V.mitems; i++)
+        lvc[l].push_back((int)d);
     }
     M.nc = c->coarse.n;
     M.citem0 = (int)citems.size();
@@ -700,9 +712,21 @@ static void batch_mg_tables(icarat_batch *B, int L, int tile)
         dfree(B->d_lv_items[l]);
       B->d_lv_items[l] = nullptr;
       B->lv_nitems[l] = 0;
+      dfree(B->d_lv_col[l]);
+      B->d_lv_col[l] = nullptr;
+      B->lv_col_items[l] = 0;
     }
     dfree(B->d_citems);
     dfree(B->d_y);
+    dfree(B->d_partc);
+    for(int l = 0; l < L; l++)
+    {
+      ICK(cudaMalloc(&B->d_lv_col[l], sizeof(int) * lvc[l].size()));
+      ICK(cudaMemcpy(B->d_lv_col[l], lvc[l].data(), sizeof(int) * lvc[l].size(),
+                     cudaMemcpyHostToDevice));
+      B->lv_col_items[l] = (int)lvc[l].size();
+    }
+    B->d_partc = dalloc(4 * lvc[0].size());
     B->d_lv_items[0] = B->d_item_design;
     B->lv_nitems[0] = B->nitems;
     for(int l = 1; l < L; l++)
@@ -816,6 +840,12 @@ static void batch_mg_launch(icarat_batch *B, int tile, int bpsm, double rtol, in
   }
   m.c_item_design = B->d_citems;
   m.c_nitems = B->c_nitems;
+  for(int l = 0; l < kBmMaxLevels; l++)
+  {
+    m.lv_col_design[l] = B->d_lv_col[l];
+    m.lv_col_items[l] = B->lv_col_items[l];
+  }
+  m.partc = B->d_partc;
   const int sms = B->ctx[0]->sm_count;
   const int blocks = sms * std::max(1, std::min(bpsm, B->occ_mg));
   void *args[] = {&a, &m};
@@ -1025,6 +1055,9 @@ int icarat_batch_destroy(icarat_batch *B)
     cudaGraphExecDestroy(B->mg_graph);
   for(int l = 1; l < kBmMaxLevels; l++)
     dfree(B->d_lv_items[l]);
+  for(int l = 0; l < kBmMaxLevels; l++)
+    dfree(B->d_lv_col[l]);
+  dfree(B->d_partc);
   dfree(B->d_citems);
   dfree(B->d_y);
   dfree(B->d_bm);

@@ -124,6 +124,9 @@ struct BmLevel
   const uint8_t *fix;
   float *x, *t, *r, *b; // iterate, its alternate, residual / Chebyshev d, right-hand side
   int item0, nitems;     // node tiles of this level in the level's item table
+  // column items of the stencil phases: blocks of kBatchThreads node
+  // columns (i, j) times chunks of kc node layers, in the level's column table
+  int mitem0, mitems, ncb, kc;
 };
 
 // the multigrid hierarchy of one design: levels, the coarsest level's dense
@@ -152,7 +155,28 @@ struct BmArgs
   int lv_nitems[kBmMaxLevels];
   const int *c_item_design; // coarse row items -> design
   int c_nitems;
+  const int *lv_col_design[kBmMaxLevels]; // per level: column item -> design
+  int lv_col_items[kBmMaxLevels];
+  double *partc; // 4 per finest-level column item: p.Ap, z.r, z.Ap
 };
+
+// sum of partial k over items [i0, i0 + n) of `part` (4 per item), in item
+// order; every thread of the block gets the result
+__device__ __forceinline__ double range_sum(const double *part, int i0, int n, int k,
+                                            double *sh, double *bc)
+{
+  double v = 0.0;
+  for(int i = threadIdx.x; i < n; i += blockDim.x)
+    v += __ldcg(part + 4L * (i0 + i) + k);
+  double arr[1] = {v};
+  block_sum<1>(arr, sh);
+  if(threadIdx.x == 0)
+    *bc = arr[0];
+  __syncthreads();
+  const double r = *bc;
+  __syncthreads();
+  return r;
+}
 
 __global__ void k_batch_mg(BatchArgs a, BmArgs m);
 

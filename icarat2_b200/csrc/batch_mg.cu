@@ -57,9 +57,24 @@ __device__ __forceinline__ bool takes_part(const BatchArgs &a, int d, int mode)
     return false;
   return mode == 0 || *(volatile const int *)&S.refresh;
 }
+// node column and z range of this thread in column item `item` of level Lv;
+// false for the columns past the level's last
+__device__ __forceinline__ bool col_item(const BmLevel &Lv, int item, int &i, int &j, int &k0,
+                                         int &k1)
+{
+  const int q = item - Lv.mitem0;
+  const int col = (q % Lv.ncb) * kBatchThreads + (int)threadIdx.x;
+  k0 = (q / Lv.ncb) * Lv.kc;
+  k1 = min(k0 + Lv.kc, Lv.g.NZ);
+  if(col >= Lv.g.NX * Lv.g.NY)
+    return false;
+  i = col % Lv.g.NX;
+  j = col / Lv.g.NX;
+  return true;
+}
 } // namespace
 
-__global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmArgs m)
+__global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmArgs m)
 {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[4 * 32];
@@ -93,11 +108,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
   // are written
   auto cheb = [&](int l, int mode, bool post, int k, bool fin)
   {
-    const Span sp = span_of(m.lv_nitems[l]);
+    const Span sp = span_of(m.lv_col_items[l]);
     const int c = cur[l];
     for(int item = sp.i0; item < sp.i1; item++)
     {
-      const int d = m.lv_item_design[l][item];
+      const int d = m.lv_col_design[l][item];
       if(!takes_part(a, d, mode))
         continue;
       const BmDesign &B = m.bm[d];
@@ -108,39 +123,41 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
       const float *x = c ? Lv.t : Lv.x;
       float *xo = fin ? a.z + D.off : (c ? Lv.x : Lv.t);
       const float *b = l == 0 ? a.r + D.off : Lv.b;
-      const int n0 = (item - Lv.item0) * a.tile, n1 = min(n0 + a.tile, Lv.g.numnp);
       double rz = 0.0, zap = 0.0;
-      for(int n = n0 + t; n < n1; n += blockDim.x)
-      {
-        float acc[3], uc[3];
-        node_Ku<float, KeParamF, true>(Lv.g, a.kef, Lv.E32, x, n, acc, uc);
-        const unsigned f = Lv.fix[n];
+      int i, j, k0, k1;
+      if(col_item(Lv, item, i, j, k0, k1))
+        column_Ku<float, KeParamF, true>(
+            Lv.g, a.kef, Lv.E32, x, i, j, k0, k1,
+            [&](int kk, const float(&acc)[3], const float(&uc)[3])
+            {
+              const int n = i + j * Lv.g.NX + kk * Lv.g.NX * Lv.g.NY;
+              const unsigned f = Lv.fix[n];
 #pragma unroll
-        for(int q = 0; q < 3; q++)
-        {
-          const long id = (long)q * Lv.g.numnp + n;
-          float dn = 0.0f;
-          if(!((f >> q) & 1u))
-            dn = (c1 != 0.0f ? c1 * __ldcg(Lv.r + id) : 0.0f) +
-                 c2 * __ldg(Lv.invd + id) * (__ldcg(b + id) - acc[q]);
-          Lv.r[id] = dn;
-          const float xn = uc[q] + dn;
-          xo[id] = xn;
-          if(fin)
-          {
-            rz += (double)xn * (double)__ldcg(b + id);
-            zap += (double)xn * (double)__ldcg(a.Ap + D.off + id);
-          }
-        }
-      }
+              for(int q = 0; q < 3; q++)
+              {
+                const long id = (long)q * Lv.g.numnp + n;
+                float dn = 0.0f;
+                if(!((f >> q) & 1u))
+                  dn = (c1 != 0.0f ? c1 * __ldcg(Lv.r + id) : 0.0f) +
+                       c2 * __ldg(Lv.invd + id) * (__ldcg(b + id) - acc[q]);
+                Lv.r[id] = dn;
+                const float xn = uc[q] + dn;
+                xo[id] = xn;
+                if(fin)
+                {
+                  rz += (double)xn * (double)__ldcg(b + id);
+                  zap += (double)xn * (double)__ldcg(a.Ap + D.off + id);
+                }
+              }
+            });
       if(fin)
       {
         double v[2] = {rz, zap};
         block_sum<2>(v, sh);
         if(t == 0)
         {
-          a.part[4L * item + 1] = v[0];
-          a.part[4L * item + 2] = v[1];
+          m.partc[4L * item + 1] = v[0];
+          m.partc[4L * item + 2] = v[1];
         }
         __syncthreads();
       }
@@ -151,30 +168,32 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
   // r_l = b_l - K x_l
   auto residual = [&](int l, int mode)
   {
-    const Span sp = span_of(m.lv_nitems[l]);
+    const Span sp = span_of(m.lv_col_items[l]);
     const int c = cur[l];
     for(int item = sp.i0; item < sp.i1; item++)
     {
-      const int d = m.lv_item_design[l][item];
+      const int d = m.lv_col_design[l][item];
       if(!takes_part(a, d, mode))
         continue;
       const BmDesign &B = m.bm[d];
       const BmLevel &Lv = B.lv[l];
       const float *x = c ? Lv.t : Lv.x;
       const float *b = l == 0 ? a.r + a.des[d].off : Lv.b;
-      const int n0 = (item - Lv.item0) * a.tile, n1 = min(n0 + a.tile, Lv.g.numnp);
-      for(int n = n0 + t; n < n1; n += blockDim.x)
-      {
-        float acc[3], uc[3];
-        node_Ku<float, KeParamF, true>(Lv.g, a.kef, Lv.E32, x, n, acc, uc);
-        const unsigned f = Lv.fix[n];
+      int i, j, k0, k1;
+      if(col_item(Lv, item, i, j, k0, k1))
+        column_Ku<float, KeParamF, true>(
+            Lv.g, a.kef, Lv.E32, x, i, j, k0, k1,
+            [&](int kk, const float(&acc)[3], const float(&)[3])
+            {
+              const int n = i + j * Lv.g.NX + kk * Lv.g.NX * Lv.g.NY;
+              const unsigned f = Lv.fix[n];
 #pragma unroll
-        for(int q = 0; q < 3; q++)
-        {
-          const long id = (long)q * Lv.g.numnp + n;
-          Lv.r[id] = ((f >> q) & 1u) ? 0.0f : __ldcg(b + id) - acc[q];
-        }
-      }
+              for(int q = 0; q < 3; q++)
+              {
+                const long id = (long)q * Lv.g.numnp + n;
+                Lv.r[id] = ((f >> q) & 1u) ? 0.0f : __ldcg(b + id) - acc[q];
+              }
+            });
     }
   };
 
@@ -436,7 +455,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
     if(!takes_part(a, d, 0))
       continue;
     const BatchDesign &D = a.des[d];
-    const double rz = design_sum(a, D, 1, sh, bc);
+    const BmLevel &L0 = m.bm[d].lv[0];
+    const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
     const int n0 = (item - D.item0) * a.tile;
     for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
 #pragma unroll
@@ -454,33 +474,39 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
   {
     if(*(volatile int *)&a.ctl[0] <= 0)
       break;
-    // ---- P1: Ap = K p, partial p . Ap
-    for(int item = s0.i0; item < s0.i1; item++)
+    // ---- P1: Ap = K p, partial p . Ap (finest-level column items)
     {
-      const int d = a.item_design[item];
-      if(!takes_part(a, d, 0))
-        continue;
-      const BatchDesign &D = a.des[d];
-      const int n0 = (item - D.item0) * a.tile;
-      double pap = 0.0;
-      for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+      const Span sp = span_of(m.lv_col_items[0]);
+      for(int item = sp.i0; item < sp.i1; item++)
       {
-        float acc[3], uc[3];
-        node_Ku<float, KeParamF, true>(D.g, a.kef, D.E32, a.p + D.off, n, acc, uc);
-        const unsigned f = D.fix[n];
+        const int d = m.lv_col_design[0][item];
+        if(!takes_part(a, d, 0))
+          continue;
+        const BatchDesign &D = a.des[d];
+        const BmLevel &Lv = m.bm[d].lv[0];
+        double pap = 0.0;
+        int i, j, k0, k1;
+        if(col_item(Lv, item, i, j, k0, k1))
+          column_Ku<float, KeParamF, true>(
+              D.g, a.kef, D.E32, a.p + D.off, i, j, k0, k1,
+              [&](int kk, const float(&acc)[3], const float(&uc)[3])
+              {
+                const int n = i + j * D.g.NX + kk * D.g.NX * D.g.NY;
+                const unsigned f = D.fix[n];
 #pragma unroll
-        for(int c = 0; c < 3; c++)
-        {
-          const float y = ((f >> c) & 1u) ? 0.0f : acc[c];
-          a.Ap[D.off + (long)c * D.g.numnp + n] = y;
-          pap += (double)uc[c] * (double)y;
-        }
+                for(int c = 0; c < 3; c++)
+                {
+                  const float y = ((f >> c) & 1u) ? 0.0f : acc[c];
+                  a.Ap[D.off + (long)c * D.g.numnp + n] = y;
+                  pap += (double)uc[c] * (double)y;
+                }
+              });
+        double v[1] = {pap};
+        block_sum<1>(v, sh);
+        if(t == 0)
+          m.partc[4L * item] = v[0];
+        __syncthreads();
       }
-      double v[1] = {pap};
-      block_sum<1>(v, sh);
-      if(t == 0)
-        a.part[4L * item] = v[0];
-      __syncthreads();
     }
     grid.sync();
     // ---- P2: x32, r updates, partial r . r, first smoothing step
@@ -496,7 +522,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
         const BmDesign &B = m.bm[d];
         if(d != cached)
         {
-          const double pap = design_sum(a, D, 0, sh, bc);
+          const double pap =
+              range_sum(m.partc, B.lv[0].mitem0, B.lv[0].mitems, 0, sh, bc);
           alpha = a.s[d].rz / pap;
           cached = d;
         }
@@ -541,13 +568,14 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
         const BatchDesign &D = a.des[d];
         if(d != cached)
         {
-          const double pap = design_sum(a, D, 0, sh, bc);
-          const double zap = design_sum(a, D, 2, sh, bc);
+          const BmLevel &L0 = m.bm[d].lv[0];
+          const double pap = range_sum(m.partc, L0.mitem0, L0.mitems, 0, sh, bc);
+          const double zap = range_sum(m.partc, L0.mitem0, L0.mitems, 2, sh, bc);
           beta = -zap / pap;
           cached = d;
           if(item == D.item0)
           {
-            const double rz = design_sum(a, D, 1, sh, bc);
+            const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
             const double rr = design_sum(a, D, 3, sh, bc);
             if(t == 0)
             {
@@ -648,7 +676,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2) k_batch_mg(BatchArgs a, BmAr
       if(item != D.item0)
         continue;
       const double rr = design_sum(a, D, 0, sh, bc);
-      const double rz = design_sum(a, D, 1, sh, bc);
+      const BmLevel &L0 = m.bm[d].lv[0];
+      const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
       if(t == 0)
       {
         BScal &S = a.s[d];
