@@ -90,6 +90,12 @@ def parse():
                    help="measure the 3-case multi-load loop (0 skips it)")
     p.add_argument("--cpu-helm", action="store_true",
                    help="(internal) time the oracle's Helmholtz filter and exit")
+    p.add_argument("--cpu-config1", action="store_true",
+                   help="(internal) time the oracle's 50-iteration OC run of the "
+                        "32x16x16 cantilever and exit")
+    p.add_argument("--config1", type=int, default=1,
+                   help="time the 32x16x16 OC run (50 iterations, rtol 1e-10) on the GPU "
+                        "and on the CPU restatement (0 skips it)")
     return p.parse_args()
 
 
@@ -227,6 +233,71 @@ def cpu_helm(a):
     t = time.perf_counter() - t0
     print(json.dumps({"t": t, "iters": its, "threads": 1, "grid": a.helm_sample}), flush=True)
     return 0
+
+
+CONFIG1 = dict(grid=(32, 16, 16), radius=1.5, move=0.15, x0=0.3, rtol=1e-10, steps=50)
+
+
+def cpu_config1(a):
+    """The 32x16x16 OC run of opt_macro_oc.cpp (50 iterations, Jacobi-PCG to
+    1e-10 as Eigen_CG) on the CPU restatement, physical cores; setup excluded."""
+    from oracle import oracle as O
+    cores, model = host_cpu()
+    O.lib.or_set_threads(cores)
+    c = CONFIG1
+    P = O.Problem(*c["grid"])
+    L = O.Loop(P, O.Filter(P, c["radius"]), method="oc", x0=c["x0"], move=c["move"],
+               cg_tol=c["rtol"])
+    t0 = time.perf_counter()
+    comp = []
+    for _ in range(c["steps"]):
+        L.step()
+        comp.append(L.scalars()["compliance"])
+    t = time.perf_counter() - t0
+    print(json.dumps({"t": t, "threads": cores, "model": model, "compliance": comp,
+                      "x": L.get("x").tolist()}), flush=True)
+    return 0
+
+
+def config1_section(a, G, torch, dev):
+    """The reference's own configuration on the GPU: the 32x16x16 OC run of
+    opt_macro_oc.cpp (R = 1.5, move 0.15, start 0.3, rtol 1e-10, 50
+    iterations) with Jacobi-PCG (the reference's solver) and with MG-PCG,
+    CUDA events around all 50 iterations, against the CPU restatement's run of
+    the same 50 iterations; the trajectories' largest differences from the
+    CPU run are reported beside the rates."""
+    c = CONFIG1
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--cpu-config1"],
+                       capture_output=True, text=True)
+    cpu = json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else None
+    out = {"workload": "opt_macro_oc.cpp run: 32x16x16, OC move 0.15, R = 1.5, start 0.3, "
+                       "rtol 1e-10, 50 iterations", "steps": c["steps"]}
+    for name, meth in (("gpu_jacobi_pcg", G.JACOBI_PCG), ("gpu_mg_pcg", G.MG_PCG)):
+        C = G.Context(*c["grid"], device=dev.index)
+        C.loop_init(c["x0"], method="oc", filter_radius=c["radius"], move=c["move"],
+                    solve=G.solve_opts(meth, c["rtol"], 10000, 4, a.smooth))
+        s = torch.cuda.ExternalStream(C.stream_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        comp = [C.loop_step().compliance for _ in range(c["steps"])]
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        row = {"value": 1000.0 * c["steps"] / ms, "unit": "design-iter/s",
+               "ms_per_step": ms / c["steps"], "compliance_last": comp[-1]}
+        if cpu:
+            row["max_rel_compliance_diff_vs_cpu"] = max(
+                abs(x - y) / y for x, y in zip(comp, cpu["compliance"]))
+            row["max_abs_design_diff_vs_cpu"] = float(
+                np.abs(C.loop_get("x") - np.array(cpu["x"])).max())
+        out[name] = row
+        C.close()
+    if cpu:
+        out["cpu_port"] = {"value": c["steps"] / cpu["t"], "unit": "design-iter/s",
+                           "s_total": cpu["t"], "cores": cpu["threads"], "model": cpu["model"],
+                           "kind": "port"}
+    return out
 
 
 def cpu_sample(a):
@@ -1013,6 +1084,7 @@ def gpu_arm(a):
     if a.multi_load:
         multi = multi_load_section(a, G, torch, dev, flush, world, dist)
     vox = voxel_section(a, G, dev) if a.multi_load else None
+    conf1 = config1_section(a, G, torch, dev) if (a.config1 and world == 1) else None
 
     if rank == 0:
         cg = [i.cg_iterations for i in infos]
@@ -1046,6 +1118,7 @@ def gpu_arm(a):
             "helmholtz_filter": helm,
             "multi_load": multi,
             "voxelize": vox,
+            "config1_oc_32x16x16": conf1,
             "compliance_last": infos[-1].compliance,
             "clocks": clk,
         }
@@ -1070,6 +1143,8 @@ def main():
         return cpu_sample(a)
     if a.cpu_helm:
         return cpu_helm(a)
+    if a.cpu_config1:
+        return cpu_config1(a)
     if a.impl == "reference":
         return reference_arm(a)
     return gpu_arm(a)
