@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_pcg(BatchArgs a)
       BScal &S = a.s[d];
       S.bb = bb;
       S.rz = rz;
-      S.rr_ref = S.rr_true = bb;
+      S.rr_ref = S.rr_true = S.rr_nat = bb;
       S.tol2 = a.tol * a.tol * bb;
       S.delta2 = a.delta * a.delta;
       S.iter = 0;

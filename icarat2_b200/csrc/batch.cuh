@@ -25,6 +25,7 @@ struct BatchDesign
 struct BScal
 {
   double rz, bb, rr_ref, rr_true, tol2, delta2;
+  double rr_nat; // FP64 r . r at the last refresh the design asked for itself
   int iter, maxit, done, status, refresh, final_, nrefresh, nstall;
 };
 

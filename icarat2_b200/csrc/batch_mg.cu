@@ -10,22 +10,28 @@
 // its item table (a contiguous run per CTA) and ends at a grid-wide barrier,
 // so designs of different sizes share the GPU in proportion to their work:
 //
-//   P1  Ap = K p (FP32 node stencil), partial p . Ap
+//   P1  Ap = K p (FP32 column-march stencil), partial p . Ap
 //   P2  alpha; x32 += alpha p, r -= alpha Ap, partial r . r; and the first
 //       Chebyshev step of the finest level from zero, x = d = D^-1 r / theta
+//   F   the FP64 refresh decision of each design (r . r fell by the factor
+//       `refresh` below the last FP64 residual, below the target, or the
+//       iteration cap); x += x32, x32 = 0 for the designs that refresh
+//   R   (only when some design refreshes) r = b - K x in FP64 for those
+//       designs, and their first Chebyshev step redone from that r
 //   V   z = M r: one V-cycle over all designs (per level down: deg-1
 //       Chebyshev steps, residual, restriction fused with the next level's
 //       first Chebyshev step; coarsest: y = W b, x = W^T y; per level up:
 //       prolongation, deg Chebyshev steps; the finest level's last step
 //       writes z with the partials z . r and z . Ap)
-//   P3  beta = -z.Ap / p.Ap (flexible CG), p = z + beta p; the design's
-//       first item decides an FP64 refresh
-//   R   (designs that refresh) x += x32; r = b - K x in FP64; z = M r;
-//       p = z (restart); stop test on the FP64 residual
-// Vectors and the V-cycle are FP32 (as the mixed-precision solver's);
-// the solution, right-hand side, dot products and scalars are FP64; the
-// coarse dense solve is FP64.  Every grid barrier is reached by every CTA
-// the same number of times; the loop is capped at maxit + 2 iterations.
+//   P3  beta = -z.Ap / p.Ap (flexible CG), p = z + beta p; after a refresh
+//       the design's first item takes the stop test on the FP64 residual
+// The refresh replaces the FP32 recurrence residual by the FP64 one before
+// the V-cycle, as the single-design mixed-precision solver does: the search
+// direction survives it and no extra V-cycle is spent.  Vectors and the
+// V-cycle are FP32 (as the mixed-precision solver's); the solution,
+// right-hand side, dot products and scalars are FP64; the coarse dense solve
+// is FP64.  Every grid barrier is reached by every CTA the same number of
+// times; the loop is capped at maxit + 2 iterations.
 #include "batch.cuh"
 
 namespace cg = cooperative_groups;
@@ -57,28 +63,99 @@ __device__ __forceinline__ bool takes_part(const BatchArgs &a, int d, int mode)
     return false;
   return mode == 0 || *(volatile const int *)&S.refresh;
 }
-// node column and z range of this thread in column item `item` of level Lv;
-// false for the columns past the level's last
-__device__ __forceinline__ bool col_item(const BmLevel &Lv, int item, int &i, int &j, int &k0,
-                                         int &k1)
+// takes_part, read by thread 0 and shared with the block: for a phase in
+// which another CTA may set the design's done flag (P3), so that every
+// thread of the block takes the same branch around the block reductions
+__device__ __forceinline__ bool takes_part_block(const BatchArgs &a, int d, int mode, int *flag)
 {
-  const int q = item - Lv.mitem0;
-  const int col = (q % Lv.ncb) * kBatchThreads + (int)threadIdx.x;
-  k0 = (q / Lv.ncb) * Lv.kc;
-  k1 = min(k0 + Lv.kc, Lv.g.NZ);
-  if(col >= Lv.g.NX * Lv.g.NY)
+  if(threadIdx.x == 0)
+    *flag = takes_part(a, d, mode) ? 1 : 0;
+  __syncthreads();
+  const bool r = *flag != 0;
+  __syncthreads();
+  return r;
+}
+
+// node column and z range of this thread in column item q of a level (q
+// counted from the level's first column item; ncb column blocks, chunks of
+// kc node layers); false for the columns past the level's last
+__device__ __forceinline__ bool col_item(const GridDev &g, int q, int ncb, int kc, int &i, int &j,
+                                         int &k0, int &k1)
+{
+  const int col = (q % ncb) * kBatchThreads + (int)threadIdx.x;
+  k0 = (q / ncb) * kc;
+  k1 = min(k0 + kc, g.NZ);
+  if(col >= g.NX * g.NY)
     return false;
-  i = col % Lv.g.NX;
-  j = col / Lv.g.NX;
+  i = col % g.NX;
+  j = col / g.NX;
   return true;
+}
+
+// the finest level's first Chebyshev step from zero, x = d = D^-1 r / theta,
+// with the design's fields held in registers across a phase's nodes
+struct Step0
+{
+  float inv_theta;
+  const float *invd;
+  float *x, *d;
+  __device__ __forceinline__ void operator()(long id, float ri) const
+  {
+    const float di = inv_theta * __ldg(invd + id) * ri;
+    x[id] = di;
+    d[id] = di;
+  }
+};
+
+__device__ __forceinline__ Step0 step0_of(const BmDesign &B)
+{
+  return Step0{B.inv_theta, B.lv[0].invd, B.lv[0].x, B.lv[0].r};
+}
+
+// nodes a thread has in flight in the elementwise phases: all loads of kU
+// nodes are issued before the first store, so a thread waits for memory
+// once per kU nodes rather than once per component
+constexpr int kU = 4;
+
+// y = c x + y (c = 0: y = x) over the nodes [n0, n1) of one design's three
+// component blocks (stride numnp)
+__device__ __forceinline__ void xpby_nodes(float *y, const float *x, float c, int numnp, int n0,
+                                           int n1)
+{
+  for(int nb = n0 + (int)threadIdx.x; nb < n1; nb += kU * (int)blockDim.x)
+  {
+    float xv[kU][3], yv[kU][3];
+#pragma unroll
+    for(int u = 0; u < kU; u++)
+    {
+      const int n = nb + u * (int)blockDim.x;
+#pragma unroll
+      for(int q = 0; q < 3; q++)
+      {
+        const long id = (long)q * numnp + n;
+        xv[u][q] = n < n1 ? __ldcg(x + id) : 0.0f;
+        yv[u][q] = (n < n1 && c != 0.0f) ? __ldcg(y + id) : 0.0f;
+      }
+    }
+#pragma unroll
+    for(int u = 0; u < kU; u++)
+    {
+      const int n = nb + u * (int)blockDim.x;
+      if(n < n1)
+#pragma unroll
+        for(int q = 0; q < 3; q++)
+          y[(long)q * numnp + n] = fmaf(c, yv[u][q], xv[u][q]);
+    }
+  }
 }
 } // namespace
 
-__global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmArgs m)
+__global__ void __launch_bounds__(kBatchThreads, 4) k_batch_mg(BatchArgs a, BmArgs m)
 {
   cg::grid_group grid = cg::this_grid();
   __shared__ double sh[4 * 32];
   __shared__ double bc[4];
+  __shared__ int part_flag;
   const int t = threadIdx.x;
   const int L = m.levels;
   const Span s0 = span_of(a.nitems);
@@ -93,15 +170,6 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
     a.ctl[1] = a.ctl[2] = 0;
   }
 
-  // first Chebyshev step of the finest level from zero, fused into the
-  // phases that produce r (node o of design D, component offset id)
-  auto first_step0 = [&](const BmDesign &B, long id, float ri)
-  {
-    const float di = B.inv_theta * __ldg(B.lv[0].invd + id) * ri;
-    B.lv[0].x[id] = di;
-    B.lv[0].r[id] = di;
-  };
-
   // one Chebyshev step on level l of the designs in `mode`:
   // d = c1 d + c2 D^-1 (b - K x), xo = x + d; on the finest level's last
   // step (fin) xo is z and the partials z . r (slot 1) and z . Ap (slot 2)
@@ -110,46 +178,72 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
   {
     const Span sp = span_of(m.lv_col_items[l]);
     const int c = cur[l];
+    // the design's fields in registers, reloaded when the item's design
+    // changes: the stores below would otherwise make every use reload them
+    int cd = -1, mitem0 = 0, ncb = 0, kc = 0;
+    bool part = false;
+    GridDev g{};
+    float c1 = 0.0f, c2 = 0.0f;
+    const float *x = nullptr, *b = nullptr, *ap = nullptr, *invd = nullptr, *E = nullptr;
+    float *xo = nullptr, *dv = nullptr;
+    const uint8_t *fix = nullptr;
     for(int item = sp.i0; item < sp.i1; item++)
     {
       const int d = m.lv_col_design[l][item];
-      if(!takes_part(a, d, mode))
+      if(d != cd)
+      {
+        cd = d;
+        part = takes_part(a, d, mode);
+        const BmDesign &B = m.bm[d];
+        const BmLevel &Lv = B.lv[l];
+        const long off = a.des[d].off;
+        g = Lv.g;
+        c1 = post ? B.post_c1[k] : B.pre_c1[k];
+        c2 = post ? B.post_c2[k] : B.pre_c2[k];
+        x = c ? Lv.t : Lv.x;
+        xo = fin ? a.z + off : (c ? Lv.x : Lv.t);
+        b = l == 0 ? a.r + off : Lv.b;
+        ap = a.Ap + off;
+        dv = Lv.r;
+        invd = Lv.invd;
+        fix = Lv.fix;
+        E = Lv.E32;
+        mitem0 = Lv.mitem0;
+        ncb = Lv.ncb;
+        kc = Lv.kc;
+      }
+      if(!part)
         continue;
-      const BmDesign &B = m.bm[d];
-      const BmLevel &Lv = B.lv[l];
-      const BatchDesign &D = a.des[d];
-      const float c1 = post ? B.post_c1[k] : B.pre_c1[k];
-      const float c2 = post ? B.post_c2[k] : B.pre_c2[k];
-      const float *x = c ? Lv.t : Lv.x;
-      float *xo = fin ? a.z + D.off : (c ? Lv.x : Lv.t);
-      const float *b = l == 0 ? a.r + D.off : Lv.b;
       double rz = 0.0, zap = 0.0;
       int i, j, k0, k1;
-      if(col_item(Lv, item, i, j, k0, k1))
+      if(col_item(g, item - mitem0, ncb, kc, i, j, k0, k1))
+      {
+        const int n_ij = i + j * g.NX, nxy = g.NX * g.NY;
         column_Ku<float, KeParamF, true>(
-            Lv.g, a.kef, Lv.E32, x, i, j, k0, k1,
+            g, a.kef, E, x, i, j, k0, k1,
             [&](int kk, const float(&acc)[3], const float(&uc)[3])
             {
-              const int n = i + j * Lv.g.NX + kk * Lv.g.NX * Lv.g.NY;
-              const unsigned f = Lv.fix[n];
+              const int n = n_ij + kk * nxy;
+              const unsigned f = fix[n];
 #pragma unroll
               for(int q = 0; q < 3; q++)
               {
-                const long id = (long)q * Lv.g.numnp + n;
+                const long id = (long)q * g.numnp + n;
                 float dn = 0.0f;
                 if(!((f >> q) & 1u))
-                  dn = (c1 != 0.0f ? c1 * __ldcg(Lv.r + id) : 0.0f) +
-                       c2 * __ldg(Lv.invd + id) * (__ldcg(b + id) - acc[q]);
-                Lv.r[id] = dn;
+                  dn = (c1 != 0.0f ? c1 * __ldcg(dv + id) : 0.0f) +
+                       c2 * __ldg(invd + id) * (__ldcg(b + id) - acc[q]);
+                dv[id] = dn;
                 const float xn = uc[q] + dn;
                 xo[id] = xn;
                 if(fin)
                 {
                   rz += (double)xn * (double)__ldcg(b + id);
-                  zap += (double)xn * (double)__ldcg(a.Ap + D.off + id);
+                  zap += (double)xn * (double)__ldcg(ap + id);
                 }
               }
             });
+      }
       if(fin)
       {
         double v[2] = {rz, zap};
@@ -170,30 +264,50 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
   {
     const Span sp = span_of(m.lv_col_items[l]);
     const int c = cur[l];
+    int cd = -1, mitem0 = 0, ncb = 0, kc = 0;
+    bool part = false;
+    GridDev g{};
+    const float *x = nullptr, *b = nullptr, *E = nullptr;
+    float *r = nullptr;
+    const uint8_t *fix = nullptr;
     for(int item = sp.i0; item < sp.i1; item++)
     {
       const int d = m.lv_col_design[l][item];
-      if(!takes_part(a, d, mode))
+      if(d != cd)
+      {
+        cd = d;
+        part = takes_part(a, d, mode);
+        const BmLevel &Lv = m.bm[d].lv[l];
+        g = Lv.g;
+        x = c ? Lv.t : Lv.x;
+        b = l == 0 ? a.r + a.des[d].off : Lv.b;
+        r = Lv.r;
+        fix = Lv.fix;
+        E = Lv.E32;
+        mitem0 = Lv.mitem0;
+        ncb = Lv.ncb;
+        kc = Lv.kc;
+      }
+      if(!part)
         continue;
-      const BmDesign &B = m.bm[d];
-      const BmLevel &Lv = B.lv[l];
-      const float *x = c ? Lv.t : Lv.x;
-      const float *b = l == 0 ? a.r + a.des[d].off : Lv.b;
       int i, j, k0, k1;
-      if(col_item(Lv, item, i, j, k0, k1))
+      if(col_item(g, item - mitem0, ncb, kc, i, j, k0, k1))
+      {
+        const int n_ij = i + j * g.NX, nxy = g.NX * g.NY;
         column_Ku<float, KeParamF, true>(
-            Lv.g, a.kef, Lv.E32, x, i, j, k0, k1,
+            g, a.kef, E, x, i, j, k0, k1,
             [&](int kk, const float(&acc)[3], const float(&)[3])
             {
-              const int n = i + j * Lv.g.NX + kk * Lv.g.NX * Lv.g.NY;
-              const unsigned f = Lv.fix[n];
+              const int n = n_ij + kk * nxy;
+              const unsigned f = fix[n];
 #pragma unroll
               for(int q = 0; q < 3; q++)
               {
-                const long id = (long)q * Lv.g.numnp + n;
-                Lv.r[id] = ((f >> q) & 1u) ? 0.0f : __ldcg(b + id) - acc[q];
+                const long id = (long)q * g.numnp + n;
+                r[id] = ((f >> q) & 1u) ? 0.0f : __ldcg(b + id) - acc[q];
               }
             });
+      }
     }
   };
 
@@ -211,30 +325,39 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
         continue;
       const BmDesign &B = m.bm[d];
       const BmLevel &F = B.lv[l], &C = B.lv[lc];
-      const int n0 = (item - C.item0) * a.tile, n1 = min(n0 + a.tile, C.g.numnp);
+      const GridDev gf = F.g, gc = C.g;
+      const float *rf = F.r;
+      const uint8_t *fix = C.fix;
+      float *bc_ = C.b;
+      const int *cmap = B.cmap;
+      double *v = B.v;
+      const float inv_theta = B.inv_theta;
+      const float *invd = C.invd;
+      float *xc = C.x, *dc = C.r;
+      const int n0 = (item - C.item0) * a.tile, n1 = min(n0 + a.tile, gc.numnp);
       for(int n = n0 + t; n < n1; n += blockDim.x)
       {
         float sr[3];
-        restrict_node<float, true>(F.g, C.g, F.r, n, sr);
-        const unsigned fx = C.fix[n];
+        restrict_node<float, true>(gf, gc, rf, n, sr);
+        const unsigned fx = fix[n];
 #pragma unroll
         for(int q = 0; q < 3; q++)
         {
-          const long id = (long)q * C.g.numnp + n;
+          const long id = (long)q * gc.numnp + n;
           const float bq = ((fx >> q) & 1u) ? 0.0f : sr[q];
-          C.b[id] = bq;
+          bc_[id] = bq;
           if(!smooth)
           {
             // coarsest level: the dense solve's right-hand side, gathered
-            const int u = __ldg(B.cmap + 3L * n + q);
+            const int u = __ldg(cmap + 3L * n + q);
             if(u >= 0)
-              B.v[u] = (double)bq;
+              v[u] = (double)bq;
           }
           else
           {
-            const float di = B.inv_theta * __ldg(C.invd + id) * bq;
-            C.x[id] = di;
-            C.r[id] = di;
+            const float di = inv_theta * __ldg(invd + id) * bq;
+            xc[id] = di;
+            dc[id] = di;
           }
         }
       }
@@ -253,35 +376,38 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
       if(!takes_part(a, d, mode))
         continue;
       const BmDesign &B = m.bm[d];
-      const BmLevel &C = B.lv[L - 1];
+      const int nc = B.nc, citems = B.citems;
+      const double *W = B.W, *v = B.v;
+      double *y = B.y;
+      float *xc = B.lv[L - 1].x;
+      const long nv = 3L * B.lv[L - 1].g.numnp;
       const int q = item - B.citem0;
-      const int r0 = q * m.ctile, r1 = min(r0 + m.ctile, B.nc);
+      const int r0 = q * m.ctile, r1 = min(r0 + m.ctile, nc);
       for(int r = r0 + warp; r < r1; r += nw)
       {
         // four independent partial sums: four loads of the row and of v in
         // flight per lane
-        const double *row = B.W + (long)r * B.nc;
+        const double *row = W + (long)r * nc;
         double s4[4] = {0.0, 0.0, 0.0, 0.0};
         int j = lane;
         for(; j + 96 <= r; j += 128)
 #pragma unroll
           for(int u = 0; u < 4; u++)
-            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(B.v + j + 32 * u), s4[u]);
+            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(v + j + 32 * u), s4[u]);
         for(; j <= r; j += 32)
-          s4[0] = fma(__ldg(row + j), __ldcg(B.v + j), s4[0]);
+          s4[0] = fma(__ldg(row + j), __ldcg(v + j), s4[0]);
         double sum = (s4[0] + s4[1]) + (s4[2] + s4[3]);
         for(int o = 16; o > 0; o >>= 1)
           sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if(lane == 0)
-          B.y[r] = sum;
+          y[r] = sum;
       }
       // this item's share of the coarsest iterate, cleared (constrained
       // entries stay 0; the free ones are written below)
-      const long nv = 3L * C.g.numnp;
-      const long per = (nv + B.citems - 1) / B.citems;
+      const long per = (nv + citems - 1) / citems;
       const long e0 = (long)q * per, e1 = min(e0 + per, nv);
       for(long e = e0 + t; e < e1; e += blockDim.x)
-        C.x[e] = 0.0f;
+        xc[e] = 0.0f;
     }
     cur[L - 1] = 0;
   };
@@ -295,25 +421,28 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
       if(!takes_part(a, d, mode))
         continue;
       const BmDesign &B = m.bm[d];
-      const BmLevel &C = B.lv[L - 1];
+      const int nc = B.nc;
+      const double *WT = B.WT, *y = B.y;
+      const int *map = B.map;
+      float *xc = B.lv[L - 1].x;
       const int q = item - B.citem0;
-      const int r0 = q * m.ctile, r1 = min(r0 + m.ctile, B.nc);
+      const int r0 = q * m.ctile, r1 = min(r0 + m.ctile, nc);
       for(int r = r0 + warp; r < r1; r += nw)
       {
-        const double *row = B.WT + (long)r * B.nc;
+        const double *row = WT + (long)r * nc;
         double s4[4] = {0.0, 0.0, 0.0, 0.0};
         int j = r + lane;
-        for(; j + 96 < B.nc; j += 128)
+        for(; j + 96 < nc; j += 128)
 #pragma unroll
           for(int u = 0; u < 4; u++)
-            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(B.y + j + 32 * u), s4[u]);
-        for(; j < B.nc; j += 32)
-          s4[0] = fma(__ldg(row + j), __ldcg(B.y + j), s4[0]);
+            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(y + j + 32 * u), s4[u]);
+        for(; j < nc; j += 32)
+          s4[0] = fma(__ldg(row + j), __ldcg(y + j), s4[0]);
         double sum = (s4[0] + s4[1]) + (s4[2] + s4[3]);
         for(int o = 16; o > 0; o >>= 1)
           sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if(lane == 0)
-          C.x[__ldg(B.map + r)] = (float)sum;
+          xc[__ldg(map + r)] = (float)sum;
       }
     }
   };
@@ -330,19 +459,21 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
         continue;
       const BmDesign &B = m.bm[d];
       const BmLevel &F = B.lv[l], &C = B.lv[l + 1];
+      const GridDev gf = F.g, gc = C.g;
       float *x = c ? F.t : F.x;
       const float *xc = cc ? C.t : C.x;
-      const int n0 = (item - F.item0) * a.tile, n1 = min(n0 + a.tile, F.g.numnp);
+      const uint8_t *fix = F.fix;
+      const int n0 = (item - F.item0) * a.tile, n1 = min(n0 + a.tile, gf.numnp);
       for(int n = n0 + t; n < n1; n += blockDim.x)
       {
         float s[3];
-        prolong_node<float, true>(F.g, C.g, xc, n, s);
-        const unsigned fx = F.fix[n];
+        prolong_node<float, true>(gf, gc, xc, n, s);
+        const unsigned fx = fix[n];
 #pragma unroll
         for(int q = 0; q < 3; q++)
           if(!((fx >> q) & 1u))
           {
-            const long id = (long)q * F.g.numnp + n;
+            const long id = (long)q * gf.numnp + n;
             x[id] = __ldcg(x + id) + s[q];
           }
       }
@@ -391,6 +522,8 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
     const BmDesign &B = m.bm[d];
     const int n0 = (item - D.item0) * a.tile;
     double bb = 0.0;
+    // the FP64 node stencil leaves no registers to hold the design's fields:
+    // they are read from the tables (this phase runs once per solve)
     for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
     {
       const unsigned f = D.fix[n];
@@ -405,7 +538,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
         const float ri = ((f >> c) & 1u) ? 0.0f : (float)(bi - acc[c]);
         a.x32[o] = 0.0f;
         a.r[o] = ri;
-        first_step0(B, id, ri);
+        step0_of(B)(id, ri);
         bb += bi * bi;
       }
     }
@@ -427,7 +560,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
     {
       BScal &S = a.s[d];
       S.bb = bb;
-      S.rr_ref = S.rr_true = bb;
+      S.rr_ref = S.rr_true = S.rr_nat = bb;
       S.tol2 = a.tol * a.tol * bb;
       S.delta2 = a.delta * a.delta;
       S.iter = 0;
@@ -449,24 +582,34 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
   grid.sync();
   // ---- z = M r, p = z, z . r
   vcycle(0);
-  for(int item = s0.i0; item < s0.i1; item++)
   {
-    const int d = a.item_design[item];
-    if(!takes_part(a, d, 0))
-      continue;
-    const BatchDesign &D = a.des[d];
-    const BmLevel &L0 = m.bm[d].lv[0];
-    const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
-    const int n0 = (item - D.item0) * a.tile;
-    for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
-#pragma unroll
-      for(int c = 0; c < 3; c++)
+    int cd = -1, numnp = 0, item0 = 0;
+    long off = 0;
+    bool part = false;
+    for(int item = s0.i0; item < s0.i1; item++)
+    {
+      const int d = a.item_design[item];
+      if(d != cd)
       {
-        const long o = D.off + (long)c * D.g.numnp + n;
-        a.p[o] = __ldcg(a.z + o);
+        cd = d;
+        part = takes_part(a, d, 0);
+        const BatchDesign &D = a.des[d];
+        numnp = D.g.numnp;
+        off = D.off;
+        item0 = D.item0;
       }
-    if(item == D.item0 && t == 0)
-      a.s[d].rz = rz;
+      if(!part)
+        continue;
+      if(item == item0)
+      {
+        const BmLevel &L0 = m.bm[d].lv[0];
+        const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
+        if(t == 0)
+          a.s[d].rz = rz;
+      }
+      const int n0 = (item - item0) * a.tile, n1 = min(n0 + a.tile, numnp);
+      xpby_nodes(a.p + off, a.z + off, 0.0f, numnp, n0, n1);
+    }
   }
   grid.sync();
 
@@ -477,30 +620,52 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
     // ---- P1: Ap = K p, partial p . Ap (finest-level column items)
     {
       const Span sp = span_of(m.lv_col_items[0]);
+      int cd = -1, mitem0 = 0, ncb = 0, kc = 0;
+      bool part = false;
+      GridDev g{};
+      const float *E = nullptr, *p = nullptr;
+      float *ap = nullptr;
+      const uint8_t *fix = nullptr;
       for(int item = sp.i0; item < sp.i1; item++)
       {
         const int d = m.lv_col_design[0][item];
-        if(!takes_part(a, d, 0))
+        if(d != cd)
+        {
+          cd = d;
+          part = takes_part(a, d, 0);
+          const BatchDesign &D = a.des[d];
+          const BmLevel &Lv = m.bm[d].lv[0];
+          g = D.g;
+          E = D.E32;
+          p = a.p + D.off;
+          ap = a.Ap + D.off;
+          fix = D.fix;
+          mitem0 = Lv.mitem0;
+          ncb = Lv.ncb;
+          kc = Lv.kc;
+        }
+        if(!part)
           continue;
-        const BatchDesign &D = a.des[d];
-        const BmLevel &Lv = m.bm[d].lv[0];
         double pap = 0.0;
         int i, j, k0, k1;
-        if(col_item(Lv, item, i, j, k0, k1))
+        if(col_item(g, item - mitem0, ncb, kc, i, j, k0, k1))
+        {
+          const int n_ij = i + j * g.NX, nxy = g.NX * g.NY;
           column_Ku<float, KeParamF, true>(
-              D.g, a.kef, D.E32, a.p + D.off, i, j, k0, k1,
+              g, a.kef, E, p, i, j, k0, k1,
               [&](int kk, const float(&acc)[3], const float(&uc)[3])
               {
-                const int n = i + j * D.g.NX + kk * D.g.NX * D.g.NY;
-                const unsigned f = D.fix[n];
+                const int n = n_ij + kk * nxy;
+                const unsigned f = fix[n];
 #pragma unroll
                 for(int c = 0; c < 3; c++)
                 {
                   const float y = ((f >> c) & 1u) ? 0.0f : acc[c];
-                  a.Ap[D.off + (long)c * D.g.numnp + n] = y;
+                  ap[(long)c * g.numnp + n] = y;
                   pap += (double)uc[c] * (double)y;
                 }
               });
+        }
         double v[1] = {pap};
         block_sum<1>(v, sh);
         if(t == 0)
@@ -509,10 +674,185 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
       }
     }
     grid.sync();
-    // ---- P2: x32, r updates, partial r . r, first smoothing step
+    // ---- P2: alpha; x32 += alpha p, r -= alpha Ap, partial r . r (slot 3);
+    // the first smoothing step of the V-cycle below
     {
-      int cached = -1;
-      double alpha = 0.0;
+      int cd = -1, numnp = 0, item0 = 0;
+      long off = 0;
+      bool part = false;
+      float al = 0.0f;
+      Step0 st{};
+      for(int item = s0.i0; item < s0.i1; item++)
+      {
+        const int d = a.item_design[item];
+        if(d != cd)
+        {
+          cd = d;
+          part = takes_part(a, d, 0);
+          if(part)
+          {
+            const BatchDesign &D = a.des[d];
+            const BmDesign &B = m.bm[d];
+            const double pap =
+                range_sum(m.partc, B.lv[0].mitem0, B.lv[0].mitems, 0, sh, bc);
+            al = (float)(a.s[d].rz / pap);
+            numnp = D.g.numnp;
+            off = D.off;
+            item0 = D.item0;
+            st = step0_of(B);
+          }
+        }
+        if(!part)
+          continue;
+        const int n0 = (item - item0) * a.tile, n1 = min(n0 + a.tile, numnp);
+        float *x32 = a.x32 + off, *r = a.r + off;
+        const float *p = a.p + off, *ap = a.Ap + off;
+        double rr = 0.0;
+        for(int nb = n0 + t; nb < n1; nb += kU * (int)blockDim.x)
+        {
+          float pv[kU][3], av[kU][3], xv[kU][3], rv[kU][3], iv[kU][3];
+#pragma unroll
+          for(int u = 0; u < kU; u++)
+          {
+            const int n = nb + u * (int)blockDim.x;
+            const bool in = n < n1;
+#pragma unroll
+            for(int c = 0; c < 3; c++)
+            {
+              const long id = (long)c * numnp + n;
+              pv[u][c] = in ? __ldcg(p + id) : 0.0f;
+              av[u][c] = in ? __ldcg(ap + id) : 0.0f;
+              xv[u][c] = in ? __ldcg(x32 + id) : 0.0f;
+              rv[u][c] = in ? __ldcg(r + id) : 0.0f;
+              iv[u][c] = in ? __ldg(st.invd + id) : 0.0f;
+            }
+          }
+#pragma unroll
+          for(int u = 0; u < kU; u++)
+          {
+            const int n = nb + u * (int)blockDim.x;
+            if(n >= n1)
+              continue;
+#pragma unroll
+            for(int c = 0; c < 3; c++)
+            {
+              const long id = (long)c * numnp + n;
+              x32[id] = fmaf(al, pv[u][c], xv[u][c]);
+              const float ri = fmaf(-al, av[u][c], rv[u][c]);
+              r[id] = ri;
+              const float di = st.inv_theta * iv[u][c] * ri;
+              st.x[id] = di;
+              st.d[id] = di;
+              rr += (double)ri * (double)ri;
+            }
+          }
+        }
+        double v[1] = {rr};
+        block_sum<1>(v, sh);
+        if(t == 0)
+        {
+          a.part[4L * item + 3] = v[0];
+          if(item == item0)
+            a.s[d].iter += 1;
+        }
+        __syncthreads();
+      }
+    }
+    grid.sync();
+    // ---- F: each design's own FP64 refresh request (r . r fell by the
+    // factor `refresh` below the last FP64 residual, below the target, the
+    // iteration cap, or not a number)
+    {
+      int cd = -1;
+      for(int item = s0.i0; item < s0.i1; item++)
+      {
+        const int d = a.item_design[item];
+        if(d == cd)
+          continue;
+        cd = d;
+        const BatchDesign &D = a.des[d];
+        if(item != D.item0 || !takes_part(a, d, 0))
+          continue;
+        const double rr = design_sum(a, D, 3, sh, bc);
+        if(t == 0)
+        {
+          BScal &S = a.s[d];
+          const bool fin = !(rr == rr) || S.iter >= S.maxit;
+          const bool fresh = fin || rr < S.tol2 || rr < S.delta2 * S.rr_ref;
+          S.final_ = fin ? 1 : 0;
+          S.refresh = fresh ? 1 : 0;
+          if(fresh)
+            atomicAdd(&a.ctl[1 + (it & 1)], 1);
+        }
+      }
+      if(blockIdx.x == 0 && t == 0)
+        a.ctl[1 + ((it + 1) & 1)] = 0; // the counter of the next iteration
+    }
+    grid.sync();
+    // A refresh of some designs takes as long as one of all (each design's
+    // node tiles are spread over many CTAs), so once one design asks, every
+    // design refreshes: x += x32, x32 = 0, then r = b - K x in FP64
+    if(*(volatile int *)&a.ctl[1 + (it & 1)] != 0)
+    {
+      // ---- R1: x += x32, x32 = 0; the designs that did not ask are marked
+      // (refresh = 2) so that the stop test below knows the refresh was forced
+      int cd = -1, numnp = 0, item0 = 0;
+      long off = 0;
+      bool part = false;
+      double *x64 = nullptr;
+      for(int item = s0.i0; item < s0.i1; item++)
+      {
+        const int d = a.item_design[item];
+        if(d != cd)
+        {
+          cd = d;
+          part = takes_part(a, d, 0);
+          const BatchDesign &D = a.des[d];
+          numnp = D.g.numnp;
+          off = D.off;
+          item0 = D.item0;
+          x64 = D.x64;
+        }
+        if(!part)
+          continue;
+        if(item == item0 && t == 0 && a.s[d].refresh == 0)
+          a.s[d].refresh = 2;
+        const int n0 = (item - item0) * a.tile, n1 = min(n0 + a.tile, numnp);
+        float *x32 = a.x32 + off;
+        for(int nb = n0 + t; nb < n1; nb += kU * (int)blockDim.x)
+        {
+          float xv[kU][3];
+          double yv[kU][3];
+#pragma unroll
+          for(int u = 0; u < kU; u++)
+          {
+            const int n = nb + u * (int)blockDim.x;
+#pragma unroll
+            for(int c = 0; c < 3; c++)
+            {
+              const long id = (long)c * numnp + n;
+              xv[u][c] = n < n1 ? __ldcg(x32 + id) : 0.0f;
+              yv[u][c] = n < n1 ? __ldcg(x64 + id) : 0.0;
+            }
+          }
+#pragma unroll
+          for(int u = 0; u < kU; u++)
+          {
+            const int n = nb + u * (int)blockDim.x;
+            if(n < n1)
+#pragma unroll
+              for(int c = 0; c < 3; c++)
+              {
+                const long id = (long)c * numnp + n;
+                x64[id] = yv[u][c] + (double)xv[u][c];
+                x32[id] = 0.0f;
+              }
+          }
+        }
+      }
+      grid.sync();
+      // ---- R2: r = b - K x in FP64, partial r . r (slot 0), the first
+      // smoothing step redone from this r
       for(int item = s0.i0; item < s0.i1; item++)
       {
         const int d = a.item_design[item];
@@ -520,195 +860,119 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_mg(BatchArgs a, BmAr
           continue;
         const BatchDesign &D = a.des[d];
         const BmDesign &B = m.bm[d];
-        if(d != cached)
-        {
-          const double pap =
-              range_sum(m.partc, B.lv[0].mitem0, B.lv[0].mitems, 0, sh, bc);
-          alpha = a.s[d].rz / pap;
-          cached = d;
-        }
-        const float al = (float)alpha;
         const int n0 = (item - D.item0) * a.tile;
         double rr = 0.0;
+        // the FP64 node stencil leaves no registers to hold the design's
+        // fields: they are read from the tables
         for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
+        {
+          double acc[3];
+          node_Ku_lean(D.g, a.ke, D.E64, D.x64, n, acc);
+          const unsigned f = D.fix[n];
 #pragma unroll
           for(int c = 0; c < 3; c++)
           {
             const long id = (long)c * D.g.numnp + n, o = D.off + id;
-            const float pi = __ldcg(a.p + o), api = __ldcg(a.Ap + o);
-            a.x32[o] = fmaf(al, pi, __ldcg(a.x32 + o));
-            const float ri = fmaf(-al, api, __ldcg(a.r + o));
-            a.r[o] = ri;
-            first_step0(B, id, ri);
-            rr += (double)ri * (double)ri;
+            const double ri = ((f >> c) & 1u) ? 0.0 : D.b[id] - acc[c];
+            const float r32 = (float)ri;
+            a.r[o] = r32;
+            step0_of(B)(id, r32);
+            rr += ri * ri;
           }
+        }
         double v[1] = {rr};
         block_sum<1>(v, sh);
         if(t == 0)
-        {
-          a.part[4L * item + 3] = v[0];
-          if(item == D.item0)
-            a.s[d].iter += 1;
-        }
+          a.part[4L * item + 0] = v[0];
         __syncthreads();
       }
+      grid.sync();
     }
-    grid.sync();
     // ---- V: z = M r, partials z . r, z . Ap
     vcycle(0);
-    // ---- P3: p = z + beta p; refresh decision
+    // ---- P3: beta = -z.Ap / p.Ap, p = z + beta p; the design's first item
+    // stores z . r and, after a refresh, takes the stop test on the FP64
+    // residual
     {
-      int cached = -1;
+      int cd = -1, numnp = 0, item0 = 0;
+      long off = 0;
+      bool part = false;
       double beta = 0.0;
       for(int item = s0.i0; item < s0.i1; item++)
       {
         const int d = a.item_design[item];
-        if(!takes_part(a, d, 0))
+        if(d != cd)
+        {
+          cd = d;
+          part = takes_part_block(a, d, 0, &part_flag);
+          if(part)
+          {
+            const BatchDesign &D = a.des[d];
+            const BmLevel &L0 = m.bm[d].lv[0];
+            const double pap = range_sum(m.partc, L0.mitem0, L0.mitems, 0, sh, bc);
+            const double zap = range_sum(m.partc, L0.mitem0, L0.mitems, 2, sh, bc);
+            beta = -zap / pap;
+            numnp = D.g.numnp;
+            off = D.off;
+            item0 = D.item0;
+          }
+        }
+        if(!part)
           continue;
-        const BatchDesign &D = a.des[d];
-        if(d != cached)
+        if(item == item0)
         {
+          const BatchDesign &D = a.des[d];
           const BmLevel &L0 = m.bm[d].lv[0];
-          const double pap = range_sum(m.partc, L0.mitem0, L0.mitems, 0, sh, bc);
-          const double zap = range_sum(m.partc, L0.mitem0, L0.mitems, 2, sh, bc);
-          beta = -zap / pap;
-          cached = d;
-          if(item == D.item0)
+          const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
+          const bool fresh = *(volatile const int *)&a.s[d].refresh != 0;
+          const double rr = fresh ? design_sum(a, D, 0, sh, bc) : 0.0;
+          if(t == 0)
           {
-            const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
-            const double rr = design_sum(a, D, 3, sh, bc);
-            if(t == 0)
+            BScal &S = a.s[d];
+            S.rz = rz;
+            if(fresh)
             {
-              BScal &S = a.s[d];
-              S.rz = rz;
-              const bool nan = !(rr == rr) || !(beta == beta);
-              S.final_ = (nan || S.iter >= S.maxit) ? 1 : 0;
-              S.refresh = (S.final_ || rr < S.tol2 || rr < S.delta2 * S.rr_ref) ? 1 : 0;
-              if(S.refresh)
-                atomicAdd(&a.ctl[1 + (it & 1)], 1);
+              // stagnation is measured between the refreshes the design
+              // asked for: a forced one may follow the last by one iteration
+              if(S.refresh == 1)
+              {
+                S.nstall = rr > 0.81 * S.rr_nat ? S.nstall + 1 : 0;
+                S.rr_nat = rr;
+              }
+              S.rr_true = S.rr_ref = rr;
+              S.nrefresh += 1;
+              if(!(rr == rr))
+              {
+                S.done = 1;
+                S.status = ICARAT_ERR_NAN;
+              }
+              else if(rr < S.tol2)
+              {
+                S.done = 1;
+                S.status = ICARAT_OK;
+              }
+              else if(S.final_)
+              {
+                S.done = 1;
+                S.status = ICARAT_WARN_MAXITER;
+              }
+              else if(S.nstall >= 3)
+              {
+                S.done = 1;
+                S.status = ICARAT_WARN_STAGNATION;
+              }
             }
+            if(!S.done && !(beta == beta && rz == rz))
+            {
+              S.done = 1;
+              S.status = ICARAT_ERR_NAN;
+            }
+            if(S.done)
+              atomicSub(&a.ctl[0], 1);
           }
         }
-        const float be = (float)beta;
-        const int n0 = (item - D.item0) * a.tile;
-        for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
-#pragma unroll
-          for(int c = 0; c < 3; c++)
-          {
-            const long o = D.off + (long)c * D.g.numnp + n;
-            a.p[o] = fmaf(be, __ldcg(a.p + o), __ldcg(a.z + o));
-          }
-      }
-      if(blockIdx.x == 0 && t == 0)
-        a.ctl[1 + ((it + 1) & 1)] = 0; // the counter of the next iteration
-    }
-    grid.sync();
-    if(*(volatile int *)&a.ctl[1 + (it & 1)] == 0)
-      continue;
-    // ---- R1: x += x32, x32 = 0 for the designs that refresh
-    for(int item = s0.i0; item < s0.i1; item++)
-    {
-      const int d = a.item_design[item];
-      if(!takes_part(a, d, 1))
-        continue;
-      const BatchDesign &D = a.des[d];
-      const int n0 = (item - D.item0) * a.tile;
-      for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
-#pragma unroll
-        for(int c = 0; c < 3; c++)
-        {
-          const long id = (long)c * D.g.numnp + n;
-          D.x64[id] += (double)__ldcg(a.x32 + D.off + id);
-          a.x32[D.off + id] = 0.0f;
-        }
-    }
-    grid.sync();
-    // ---- R2: r = b - K x in FP64; partial r . r (slot 0); first smoothing step
-    for(int item = s0.i0; item < s0.i1; item++)
-    {
-      const int d = a.item_design[item];
-      if(!takes_part(a, d, 1))
-        continue;
-      const BatchDesign &D = a.des[d];
-      const BmDesign &B = m.bm[d];
-      const int n0 = (item - D.item0) * a.tile;
-      double rr = 0.0;
-      for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
-      {
-        double acc[3];
-        node_Ku_lean(D.g, a.ke, D.E64, D.x64, n, acc);
-        const unsigned f = D.fix[n];
-#pragma unroll
-        for(int c = 0; c < 3; c++)
-        {
-          const long id = (long)c * D.g.numnp + n, o = D.off + id;
-          const double ri = ((f >> c) & 1u) ? 0.0 : D.b[id] - acc[c];
-          const float r32 = (float)ri;
-          a.r[o] = r32;
-          first_step0(B, id, r32);
-          rr += ri * ri;
-        }
-      }
-      double v[1] = {rr};
-      block_sum<1>(v, sh);
-      if(t == 0)
-        a.part[4L * item + 0] = v[0];
-      __syncthreads();
-    }
-    grid.sync();
-    // ---- z = M r for the refreshing designs
-    vcycle(1);
-    // ---- R3: p = z (restart), stop test on the FP64 residual
-    for(int item = s0.i0; item < s0.i1; item++)
-    {
-      const int d = a.item_design[item];
-      if(!takes_part(a, d, 1))
-        continue;
-      const BatchDesign &D = a.des[d];
-      const int n0 = (item - D.item0) * a.tile;
-      for(int n = n0 + t; n < min(n0 + a.tile, D.g.numnp); n += blockDim.x)
-#pragma unroll
-        for(int c = 0; c < 3; c++)
-        {
-          const long o = D.off + (long)c * D.g.numnp + n;
-          a.p[o] = __ldcg(a.z + o);
-        }
-      if(item != D.item0)
-        continue;
-      const double rr = design_sum(a, D, 0, sh, bc);
-      const BmLevel &L0 = m.bm[d].lv[0];
-      const double rz = range_sum(m.partc, L0.mitem0, L0.mitems, 1, sh, bc);
-      if(t == 0)
-      {
-        BScal &S = a.s[d];
-        S.nstall = rr > 0.81 * S.rr_true ? S.nstall + 1 : 0;
-        S.rr_true = S.rr_ref = rr;
-        S.rz = rz;
-        S.nrefresh += 1;
-        // S.refresh stays set until the next P3 decides anew: the other
-        // items of this design test it in this same phase
-        if(!(rr == rr))
-        {
-          S.done = 1;
-          S.status = ICARAT_ERR_NAN;
-        }
-        else if(rr < S.tol2)
-        {
-          S.done = 1;
-          S.status = ICARAT_OK;
-        }
-        else if(S.final_)
-        {
-          S.done = 1;
-          S.status = ICARAT_WARN_MAXITER;
-        }
-        else if(S.nstall >= 3)
-        {
-          S.done = 1;
-          S.status = ICARAT_WARN_STAGNATION;
-        }
-        if(S.done)
-          atomicSub(&a.ctl[0], 1);
+        const int n0 = (item - item0) * a.tile, n1 = min(n0 + a.tile, numnp);
+        xpby_nodes(a.p + off, a.z + off, (float)beta, numnp, n0, n1);
       }
     }
     grid.sync();
