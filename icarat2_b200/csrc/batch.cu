@@ -688,10 +688,14 @@ static void batch_mg_tables(icarat_batch *B, int L, int tile)
       V.nitems = (g.numnp + tile - 1) / tile;
       for(int i = 0; i < V.nitems; i++)
         lv[l].push_back((int)d);
-      // stencil phases: blocks of kBatchThreads node columns x kBmLayers
-      // node layers
+      // stencil phases: blocks of kBatchThreads node columns x chunks of
+      // about kBmLayers node layers (balanced: chunk lengths differ by at
+      // most one, so that no item is a short remainder)
       V.ncb = (g.NX * g.NY + kBatchThreads - 1) / kBatchThreads;
-      V.kc = std::min(g.NZ, kBmLayers);
+      {
+        const int nch = (g.NZ + kBmLayers - 1) / kBmLayers;
+        V.kc = (g.NZ + nch - 1) / nch;
+      }
       V.mitem0 = (int)lvc[l].size();
       V.mitems = V.ncb * ((g.NZ + V.kc - 1) / V.kc);
       for(int i = 0; i < V.mitems; i++)

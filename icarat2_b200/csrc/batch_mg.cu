@@ -383,24 +383,46 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_mg(BatchArgs a, BmAr
       const long nv = 3L * B.lv[L - 1].g.numnp;
       const int q = item - B.citem0;
       const int r0 = q * m.ctile, r1 = min(r0 + m.ctile, nc);
-      for(int r = r0 + warp; r < r1; r += nw)
+      // rows ra and rb = ra + nw of the item together: eight loads of W and
+      // of v in flight per lane (four independent partial sums per row)
+      for(int ra = r0 + warp; ra < r1; ra += 2 * nw)
       {
-        // four independent partial sums: four loads of the row and of v in
-        // flight per lane
-        const double *row = W + (long)r * nc;
-        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+        const int rb = ra + nw < r1 ? ra + nw : -1;
+        const double *rowa = W + (long)ra * nc, *rowb = W + (long)(rb < 0 ? ra : rb) * nc;
+        const int lenb = rb < 0 ? 0 : rb + 1;
+        double sa[4] = {0.0, 0.0, 0.0, 0.0}, sb[4] = {0.0, 0.0, 0.0, 0.0};
         int j = lane;
-        for(; j + 96 <= r; j += 128)
+        for(; j + 96 <= ra; j += 128)
 #pragma unroll
           for(int u = 0; u < 4; u++)
-            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(v + j + 32 * u), s4[u]);
-        for(; j <= r; j += 32)
-          s4[0] = fma(__ldg(row + j), __ldcg(v + j), s4[0]);
-        double sum = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+          {
+            const double vj = __ldcg(v + j + 32 * u);
+            sa[u] = fma(__ldg(rowa + j + 32 * u), vj, sa[u]);
+            sb[u] = fma(__ldg(rowb + j + 32 * u), vj, sb[u]);
+          }
+        // the rest of row ra (its last entry is column ra)
+        for(int jj = j; jj <= ra; jj += 32)
+          sa[0] = fma(__ldg(rowa + jj), __ldcg(v + jj), sa[0]);
+        // the rest of row rb (rb > ra: longer)
+        for(; j + 96 < lenb; j += 128)
+#pragma unroll
+          for(int u = 0; u < 4; u++)
+            sb[u] = fma(__ldg(rowb + j + 32 * u), __ldcg(v + j + 32 * u), sb[u]);
+        for(; j < lenb; j += 32)
+          sb[0] = fma(__ldg(rowb + j), __ldcg(v + j), sb[0]);
+        double suma = (sa[0] + sa[1]) + (sa[2] + sa[3]);
+        double sumb = (sb[0] + sb[1]) + (sb[2] + sb[3]);
         for(int o = 16; o > 0; o >>= 1)
-          sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        {
+          suma += __shfl_xor_sync(0xffffffffu, suma, o);
+          sumb += __shfl_xor_sync(0xffffffffu, sumb, o);
+        }
         if(lane == 0)
-          y[r] = sum;
+        {
+          y[ra] = suma;
+          if(rb >= 0)
+            y[rb] = sumb;
+        }
       }
       // this item's share of the coarsest iterate, cleared (constrained
       // entries stay 0; the free ones are written below)
@@ -427,22 +449,42 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_mg(BatchArgs a, BmAr
       float *xc = B.lv[L - 1].x;
       const int q = item - B.citem0;
       const int r0 = q * m.ctile, r1 = min(r0 + m.ctile, nc);
-      for(int r = r0 + warp; r < r1; r += nw)
+      // rows ra and rb = ra + nw together, as in the lower solve (row r of
+      // W^T holds columns r .. nc - 1)
+      for(int ra = r0 + warp; ra < r1; ra += 2 * nw)
       {
-        const double *row = WT + (long)r * nc;
-        double s4[4] = {0.0, 0.0, 0.0, 0.0};
-        int j = r + lane;
-        for(; j + 96 < nc; j += 128)
+        const int rb = ra + nw < r1 ? ra + nw : nc; // nc: no second row
+        const double *rowa = WT + (long)ra * nc, *rowb = WT + (long)(rb < nc ? rb : ra) * nc;
+        double sa[4] = {0.0, 0.0, 0.0, 0.0}, sb[4] = {0.0, 0.0, 0.0, 0.0};
+        int ja = ra + lane, jb = rb + lane;
+        for(; jb + 96 < nc; ja += 128, jb += 128)
 #pragma unroll
           for(int u = 0; u < 4; u++)
-            s4[u] = fma(__ldg(row + j + 32 * u), __ldcg(y + j + 32 * u), s4[u]);
-        for(; j < nc; j += 32)
-          s4[0] = fma(__ldg(row + j), __ldcg(y + j), s4[0]);
-        double sum = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+          {
+            sa[u] = fma(__ldg(rowa + ja + 32 * u), __ldcg(y + ja + 32 * u), sa[u]);
+            sb[u] = fma(__ldg(rowb + jb + 32 * u), __ldcg(y + jb + 32 * u), sb[u]);
+          }
+        for(; ja + 96 < nc; ja += 128)
+#pragma unroll
+          for(int u = 0; u < 4; u++)
+            sa[u] = fma(__ldg(rowa + ja + 32 * u), __ldcg(y + ja + 32 * u), sa[u]);
+        for(; ja < nc; ja += 32)
+          sa[0] = fma(__ldg(rowa + ja), __ldcg(y + ja), sa[0]);
+        for(; jb < nc; jb += 32)
+          sb[0] = fma(__ldg(rowb + jb), __ldcg(y + jb), sb[0]);
+        double suma = (sa[0] + sa[1]) + (sa[2] + sa[3]);
+        double sumb = (sb[0] + sb[1]) + (sb[2] + sb[3]);
         for(int o = 16; o > 0; o >>= 1)
-          sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        {
+          suma += __shfl_xor_sync(0xffffffffu, suma, o);
+          sumb += __shfl_xor_sync(0xffffffffu, sumb, o);
+        }
         if(lane == 0)
-          xc[__ldg(map + r)] = (float)sum;
+        {
+          xc[__ldg(map + ra)] = (float)suma;
+          if(rb < nc)
+            xc[__ldg(map + rb)] = (float)sumb;
+        }
       }
     }
   };
