@@ -88,6 +88,9 @@ def parse():
                    help="grid of the oracle's timed Helmholtz call")
     p.add_argument("--multi-load", type=int, default=1,
                    help="measure the 3-case multi-load loop (0 skips it)")
+    p.add_argument("--multi-steps", type=int, default=20,
+                   help="timed design iterations of each multi-load run (the "
+                        "iteration growth along the trajectory is the point)")
     p.add_argument("--cpu-helm", action="store_true",
                    help="(internal) time the oracle's Helmholtz filter and exit")
     p.add_argument("--cpu-config1", action="store_true",
@@ -605,10 +608,11 @@ def helmholtz_section(a, G, torch, dev, flush, world, dist):
     return out
 
 
-def multi_load_section(a, G, torch, dev, flush, world, dist):
+def multi_load_section(a, G, torch, dev, flush, world, dist, coarse_op=0):
     """The opt_multi_load loop on the headline grid: 3 point-load cases (tip
     down, tip sideways at the top edge, tip up at the far edge), Helmholtz
-    filter R = 2, threshold, MMA move 0.2, the headline solver per case."""
+    filter R = 2, threshold, MMA move 0.2, the headline solver per case
+    (coarse_op: its coarse multigrid operators), a.multi_steps timed steps."""
     from icarat2_b200.replicas import job_rate
 
     nx, ny, nz = grid_of(a)
@@ -624,7 +628,8 @@ def multi_load_section(a, G, torch, dev, flush, world, dist):
     c = G.Context(nx, ny, nz, dirichlet=dirich, loads=cases[0], device=dev.index)
     c.loop_init(0.3, method="mma", filter_radius=2.0, move=0.2, use_threshold=True,
                 solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, a.levels, a.smooth,
-                                   coarse_lag=a.coarse_lag, warm_start=a.warm_start),
+                                   coarse_lag=a.coarse_lag, warm_start=a.warm_start,
+                                   coarse_op=coarse_op),
                 filter="helmholtz")
     c.set_load_cases(np.array(F))
     st = torch.cuda.ExternalStream(c.stream_ptr(), device=dev)
@@ -632,7 +637,7 @@ def multi_load_section(a, G, torch, dev, flush, world, dist):
         c.loop_step()
     torch.cuda.synchronize()
     ms, its = 0.0, []
-    for _ in range(a.steps):
+    for _ in range(a.multi_steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         its.append(c.loop_step().cg_iterations)
@@ -642,10 +647,12 @@ def multi_load_section(a, G, torch, dev, flush, world, dist):
         with torch.cuda.stream(st):
             flush.zero_()
         torch.cuda.synchronize()
-    v, total = job_rate(ms, a.steps, world, dist, dev)
+    v, total = job_rate(ms, a.multi_steps, world, dist, dev)
     c.close()
     return {"grid": a.grid, "load_cases": len(cases), "value": v, "unit": "design-iter/s",
-            "ms_per_step": total / a.steps, "cg_iterations_per_step": its,
+            "ms_per_step": total / a.multi_steps, "steps": a.multi_steps,
+            "cg_iterations_per_step": its,
+            "coarse_operators": "Galerkin" if coarse_op else "rediscretised",
             "workload": "opt_multi_load loop: 3 load cases, Helmholtz filter R = 2, "
                         "threshold, MMA move 0.2, MG-PCG %g per case" % a.rtol}
 
@@ -1080,9 +1087,11 @@ def gpu_arm(a):
     helm = None
     if a.helm_grid:
         helm = helmholtz_section(a, G, torch, dev, flush, world, dist)
-    multi = None
+    multi = multi_gal = None
     if a.multi_load:
         multi = multi_load_section(a, G, torch, dev, flush, world, dist)
+        multi_gal = multi_load_section(a, G, torch, dev, flush, world, dist,
+                                       coarse_op=G.COARSE_GALERKIN)
     vox = voxel_section(a, G, dev) if a.multi_load else None
     conf1 = config1_section(a, G, torch, dev) if (a.config1 and world == 1) else None
 
@@ -1117,6 +1126,7 @@ def gpu_arm(a):
             "learned": learned,
             "helmholtz_filter": helm,
             "multi_load": multi,
+            "multi_load_galerkin": multi_gal,
             "voxelize": vox,
             "config1_oc_32x16x16": conf1,
             "compliance_last": infos[-1].compliance,

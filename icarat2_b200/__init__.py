@@ -38,6 +38,8 @@ MG_PCG = 1
 MIXED_IR = 2
 LEARNED_FPCG = 3
 
+COARSE_REDISCRETISED = 0  # ICARAT_COARSE_*: coarse multigrid operators
+COARSE_GALERKIN = 1
 OP_FP64 = 0
 OP_FP32 = 1
 OP_TC_BF16X3 = 2
@@ -79,7 +81,8 @@ class SolveOpts(C.Structure):
     _fields_ = [("method", C.c_int), ("rtol", C.c_double), ("maxit", C.c_int),
                 ("mg_levels", C.c_int), ("mg_smooth", C.c_int), ("chunk", C.c_int),
                 ("refresh", C.c_double), ("fine_op", C.c_int), ("krylov_op", C.c_int),
-                ("warm_start", C.c_int), ("fp64_tc", C.c_int), ("coarse_lag", C.c_int)]
+                ("warm_start", C.c_int), ("fp64_tc", C.c_int), ("coarse_lag", C.c_int),
+                ("coarse_op", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -119,7 +122,7 @@ _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _vp = C.c_void_p
 # ICARAT_ABI_VERSION of include/icarat_gpu.h that the structs below mirror
-ABI_VERSION = 10200
+ABI_VERSION = 10300
 
 _i = C.c_int
 _d = C.c_double
@@ -199,6 +202,7 @@ SIGNATURES = {
     "icarat_batch_loop_step": (_i, [_vp, _P(BatchOpts), _vp]),
     "icarat_time_operator_op": (_i, [_vp, _i, _i, _P(_d)]),
     "icarat_mg_coarse_check": (_i, [_vp, _i, _P(_d), _P(_i)]),
+    "icarat_mg_level_apply": (_i, [_vp, _P(SolveOpts), _i, _dp, _dp]),
     "icarat_loop_init": (_i, [_vp, _P(LoopOpts), _dp]),
     "icarat_loop_step": (_i, [_vp, _P(StepInfo)]),
     "icarat_loop_get": (_i, [_vp, _i, _dp]),
@@ -394,14 +398,17 @@ def _bc_struct(dirichlet, loads):
 
 def solve_opts(method=JACOBI_PCG, rtol=1e-10, maxit=10000, mg_levels=4, mg_smooth=2,
                chunk=0, refresh=0.0, fine_op=0, krylov_op=0, warm_start=0, fp64_tc=0,
-               coarse_lag=0):
+               coarse_lag=0, coarse_op=COARSE_REDISCRETISED):
     """fp64_tc (JACOBI_PCG, MG_PCG): FP64 products by the node stencil (0,
     the default, and -1; the faster operator at every measured size) or on
-    the FP64 tensor cores on every level of 32k nodes and more (1).  coarse_lag (MG_PCG, MIXED_IR): keep the previous
-    design's coarsest factor while this design's is computed on a second
-    stream."""
+    the FP64 tensor cores on every level of 32k nodes and more (1).
+    coarse_lag (MG_PCG, MIXED_IR): keep the previous design's coarsest factor
+    while this design's is computed on a second stream.  coarse_op (MG_PCG,
+    MIXED_IR): COARSE_REDISCRETISED (default) or COARSE_GALERKIN coarse
+    operators."""
     return SolveOpts(method, rtol, maxit, mg_levels, mg_smooth, chunk, refresh, fine_op,
-                     krylov_op, warm_start, int(fp64_tc), int(bool(coarse_lag)))
+                     krylov_op, warm_start, int(fp64_tc), int(bool(coarse_lag)),
+                     int(coarse_op))
 
 
 class Context:
@@ -644,6 +651,20 @@ class Context:
                      xmax, filter_radius, solve if solve is not None else solve_opts(),
                      1 if filter == "helmholtz" else 0)
         _check(self.lib.icarat_loop_init(self.h, C.byref(o), _f64(x0)), "loop_init")
+
+    def mg_level_apply(self, level, x, opts=None):
+        """y = A_level x for the V-cycle of opts (mg_levels, coarse_op) on the
+        current design; x and y component-major over the level's nodes."""
+        o = opts if opts is not None else solve_opts(MG_PCG)
+        xx = np.ascontiguousarray(x, dtype=np.float64)
+        s = 2 ** int(level)
+        n = 3 * (self.nx // s + 1) * (self.ny // s + 1) * (self.nz // s + 1)
+        if xx.size != n:
+            raise ValueError("x must hold %d entries on level %d" % (n, level))
+        y = np.zeros_like(xx)
+        _check(self.lib.icarat_mg_level_apply(self.h, C.byref(o), int(level), xx, y),
+               "icarat_mg_level_apply")
+        return y
 
     def coarse_check(self, mg_levels=4):
         """(||b - K_c x|| / ||b||, unknowns) of the multigrid's coarsest dense

@@ -908,6 +908,7 @@ static int batch_mg_prepare(icarat_batch *B, int want, int tile, bool warm)
   for(size_t d = 0; d < B->ctx.size(); d++)
   {
     icarat_ctx *c = B->ctx[d];
+    c->mg_galerkin_req = 0; // the batch kernel runs the rediscretised hierarchy
     mg_setup(c, L, false);
     ICK(cudaEventRecord(B->ev[d], c->stream));
     ICK(cudaStreamWaitEvent(B->stream, B->ev[d], 0));

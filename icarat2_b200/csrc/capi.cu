@@ -104,6 +104,18 @@ int icarat_mg_coarse_check(icarat_ctx *c, int mg_levels, double *rel_residual,
   ICARAT_API_END
 }
 
+int icarat_mg_level_apply(icarat_ctx *c, const icarat_solve_opts *opts, int level,
+                          const double *x, double *y)
+{
+  ICARAT_API_BEGIN
+  check_ctx(c);
+  IREQUIRE(opts && x && y, ICARAT_ERR_ARG, "bad argument");
+  IREQUIRE(c->design_set, ICARAT_ERR_STATE, "set the design first");
+  mg_level_apply(c, opts, level, x, y);
+  return ICARAT_OK;
+  ICARAT_API_END
+}
+
 int icarat_time_operator(icarat_ctx *c, int reps, double *ms_per_launch)
 {
   ICARAT_API_BEGIN

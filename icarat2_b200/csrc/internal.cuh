@@ -182,6 +182,10 @@ inline int device_slot()
 constexpr int kRedThreads = 256;
 constexpr int kMaxRedBlocks = 2048;
 
+// Chebyshev coefficients per Galerkin level (1 / theta, then (c1, c2) of
+// steps 1 .. (kGalCoef - 1) / 2)
+constexpr int kGalCoef = 16;
+
 struct MgLevel
 {
   GridDev g;
@@ -192,6 +196,11 @@ struct MgLevel
   // FP32 copies of E and invd and FP32 work vectors (mixed-precision solver)
   float *E32 = nullptr, *invd32 = nullptr;
   float *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *t32 = nullptr;
+  // Galerkin coarse operator (levels >= 1 of a Galerkin hierarchy): cell
+  // matrices (nelx x 576), node stencil (243 x numnp, coefficient-major) and
+  // its FP32 copy
+  double *Kc = nullptr, *S = nullptr;
+  float *S32 = nullptr;
 };
 
 struct CoarseSolver
@@ -351,6 +360,11 @@ struct icarat_ctx
   // multigrid
   std::vector<icarat_b200::MgLevel> mg;
   int mg_built_levels = 0;
+  // Galerkin coarse operators: requested by the current solve's options,
+  // and built into the hierarchy (which is rebuilt when they differ)
+  int mg_galerkin_req = 0, mg_galerkin = 0;
+  double *gal_lmax = nullptr; // per level: Chebyshev bound of D^-1 A
+  double *gal_coef = nullptr; // per level: kGalCoef Chebyshev coefficients
   icarat_b200::CoarseSolver coarse;
   // filter
   icarat_b200::FilterState filt;
@@ -460,6 +474,8 @@ void widen_f64(icarat_ctx *c, long n, const float *in, double *out);
 // this design's factor is computed on a side stream (first call after a
 // hierarchy change: synchronous)
 void mg_setup(icarat_ctx *c, int levels, bool lag = false);
+void mg_level_apply(icarat_ctx *c, const icarat_solve_opts *o, int level, const double *x,
+                    double *y);
 // the context's stream waits for a lagged factorization in flight (so that a
 // solve's work, side stream included, ends with the solve)
 void mg_join(icarat_ctx *c);

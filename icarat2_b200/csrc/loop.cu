@@ -550,7 +550,7 @@ int loop_save(icarat_ctx *c, const char *path)
   IREQUIRE(L.init, ICARAT_ERR_STATE, "icarat_loop_init first");
   SnapHead h{};
   std::memcpy(h.magic, kSnapMagic, 8);
-  h.version = 1;
+  h.version = 2;
   h.nx = c->nx;
   h.ny = c->ny;
   h.nz = c->nz;
@@ -599,7 +599,7 @@ int loop_load(icarat_ctx *c, const char *path)
   IREQUIRE(f.f != nullptr, ICARAT_ERR_ARG, std::string("cannot read ") + path);
   SnapHead h{};
   IREQUIRE(std::fread(&h, sizeof(h), 1, f.f) == 1 && std::memcmp(h.magic, kSnapMagic, 8) == 0 &&
-               h.version == 1,
+               h.version == 2,
            ICARAT_ERR_ARG, std::string("not a loop snapshot: ") + path);
   IREQUIRE(h.nx == c->nx && h.ny == c->ny && h.nz == c->nz && h.nelx == c->nelx &&
                h.neq == c->neq && h.numeq == c->numeq && h.sel_nelx == abi_nelx(c) &&

@@ -559,6 +559,9 @@ void mixed_begin(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, d
   const bool learned = o->method == ICARAT_SOLVER_LEARNED_FPCG;
   IREQUIRE(!learned || c->net, ICARAT_ERR_STATE,
            "attach a net with icarat_ctx_set_net before the learned solver");
+  IREQUIRE(o->coarse_op == ICARAT_COARSE_REDISCRETISED || o->coarse_op == ICARAT_COARSE_GALERKIN,
+           ICARAT_ERR_ARG, "coarse_op must be ICARAT_COARSE_REDISCRETISED or _GALERKIN");
+  c->mg_galerkin_req = o->coarse_op == ICARAT_COARSE_GALERKIN ? 1 : 0;
   mg_setup(c, levels, o->coarse_lag != 0);
   mixed_alloc(c);
   const int n = c->neq;

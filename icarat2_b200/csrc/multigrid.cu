@@ -35,6 +35,34 @@ void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, 
 void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
                      const double *v, double *t, const int *rowmap, double *x);
 
+// Galerkin coarse operators (galerkin.cu)
+__global__ void k_gal_cells(GridDev f, GridDev c, KeParam ke, const double *__restrict__ E,
+                            const double *__restrict__ Kf, const uint8_t *__restrict__ fix_f,
+                            const uint8_t *__restrict__ fix_c, double *__restrict__ Kc,
+                            double *__restrict__ lmax);
+__global__ void k_gal_stencil(GridDev g, const double *__restrict__ Kc,
+                              const uint8_t *__restrict__ fix, double *__restrict__ S,
+                              double *__restrict__ invd);
+__global__ void k_gal_coefs(int levels, const double *__restrict__ lmax,
+                            double *__restrict__ coef);
+template <typename T>
+__global__ void k_st_first(int n, const T *__restrict__ b, const T *__restrict__ invd,
+                           const double *__restrict__ coef, T *__restrict__ x,
+                           T *__restrict__ d);
+template <typename T>
+__global__ void k_st_cheb(GridDev g, const T *__restrict__ S, const uint8_t *__restrict__ fix,
+                          const T *__restrict__ invd, const T *__restrict__ b,
+                          const T *__restrict__ x, T *__restrict__ d, T *__restrict__ xo,
+                          const double *__restrict__ coef, int k);
+template <typename T>
+__global__ void k_st_residual(GridDev g, const T *__restrict__ S,
+                              const uint8_t *__restrict__ fix, const T *__restrict__ b,
+                              const T *__restrict__ x, T *__restrict__ r);
+__global__ void k_coarse_assemble_st(GridDev g, const double *__restrict__ S,
+                                     const int *__restrict__ rowmap,
+                                     const int *__restrict__ colmap, int nfree,
+                                     double *__restrict__ A);
+
 // ---------------------------------------------------------------- level data
 __global__ void k_coarsen_E(GridDev f, GridDev c, const double *__restrict__ Ef,
                             double *__restrict__ Ec)
@@ -250,6 +278,7 @@ template <> struct LevelBuf<double>
   static double *b(MgLevel &L) { return L.b; }
   static double *r(MgLevel &L) { return L.r; }
   static double *t(MgLevel &L) { return L.t; }
+  static double *S(MgLevel &L) { return L.S; }
   static const KeParam &ke(icarat_ctx *c) { return c->ke0; }
 };
 template <> struct LevelBuf<float>
@@ -260,6 +289,7 @@ template <> struct LevelBuf<float>
   static float *b(MgLevel &L) { return L.b32; }
   static float *r(MgLevel &L) { return L.r32; }
   static float *t(MgLevel &L) { return L.t32; }
+  static float *S(MgLevel &L) { return L.S32; }
   static const KeParamF &ke(icarat_ctx *c) { return c->ke0f; }
 };
 
@@ -276,10 +306,15 @@ void mg_free(icarat_ctx *c)
       dfree(L.E32);
     }
     for(void *p : {(void *)L.x, (void *)L.b, (void *)L.r, (void *)L.t, (void *)L.invd32,
-                   (void *)L.x32, (void *)L.b32, (void *)L.r32, (void *)L.t32})
+                   (void *)L.x32, (void *)L.b32, (void *)L.r32, (void *)L.t32, (void *)L.Kc,
+                   (void *)L.S, (void *)L.S32})
       dfree(p);
   }
   c->mg.clear();
+  dfree(c->gal_lmax);
+  c->gal_lmax = nullptr;
+  c->gal_coef = nullptr; // part of the gal_lmax allocation
+  c->mg_galerkin = 0;
   CoarseSolver &C = c->coarse;
   if(C.side)
     cudaStreamSynchronize(C.side); // a lagged factorization may still run
@@ -349,6 +384,12 @@ static void allocate_levels(icarat_ctx *c, int levels)
       ICK(cudaMalloc(&L.fix, L.g.numnp));
       L.invd = dalloc(nv);
     }
+    if(l > 0 && c->mg_galerkin_req)
+    {
+      L.Kc = dalloc(576 * (size_t)L.g.nelx);
+      L.S = dalloc(243 * (size_t)L.g.numnp);
+      L.S32 = falloc(243 * (size_t)L.g.numnp);
+    }
     L.x = dalloc(nv);
     L.b = dalloc(nv);
     L.r = dalloc(nv);
@@ -360,6 +401,13 @@ static void allocate_levels(icarat_ctx *c, int levels)
     L.t32 = falloc(nv);
     c->mg.push_back(L);
   }
+  if(c->mg_galerkin_req)
+  {
+    // per level: the Chebyshev bound, then kGalCoef coefficients
+    c->gal_lmax = dalloc((size_t)levels * (1 + kGalCoef));
+    c->gal_coef = c->gal_lmax + levels;
+  }
+  c->mg_galerkin = c->mg_galerkin_req;
   // coarse constraint pattern on the host (fixed for the context)
   std::vector<uint8_t> fix = c->fix_h;
   GridDev gf = c->mg[0].g;
@@ -442,6 +490,8 @@ static void allocate_levels(icarat_ctx *c, int levels)
 // Jacobi diagonals (and their FP32 copies).
 static void enqueue_levels(icarat_ctx *c, int levels, cudaStream_t st)
 {
+  if(c->mg_galerkin)
+    ICK(cudaMemsetAsync(c->gal_lmax, 0, sizeof(double) * levels, st));
   for(int l = 0; l < levels; l++)
   {
     MgLevel &L = c->mg[l];
@@ -451,7 +501,20 @@ static void enqueue_levels(icarat_ctx *c, int levels, cudaStream_t st)
       note_launch();
       k_coarsen_E<<<blocks_for(L.g.nelx, 256), 256, 0, st>>>(F.g, L.g, F.E, L.E);
     }
-    launch_diag(c, L.g, L.E, L.fix, L.invd, st);
+    if(l > 0 && c->mg_galerkin)
+    {
+      // Galerkin: cell matrices from the level above, the node stencil, the
+      // Jacobi diagonal from it, the FP32 copies
+      const MgLevel &F = c->mg[l - 1];
+      note_launch(3);
+      k_gal_cells<<<L.g.nelx, 128, 0, st>>>(F.g, L.g, c->ke0, F.E, l > 1 ? F.Kc : nullptr,
+                                            F.fix, L.fix, L.Kc, c->gal_lmax + l);
+      k_gal_stencil<<<blocks_for(27L * L.g.numnp, 256), 256, 0, st>>>(L.g, L.Kc, L.fix, L.S,
+                                                                      L.invd);
+      k_cast<<<blocks_for(243L * L.g.numnp, 256), 256, 0, st>>>(243L * L.g.numnp, L.S, L.S32);
+    }
+    else
+      launch_diag(c, L.g, L.E, L.fix, L.invd, st);
     if(l > 0) // the finest FP32 moduli come with the design
     {
       note_launch();
@@ -460,6 +523,11 @@ static void enqueue_levels(icarat_ctx *c, int levels, cudaStream_t st)
     note_launch();
     k_cast<<<blocks_for(3L * L.g.numnp, 256), 256, 0, st>>>(3L * L.g.numnp, L.invd,
                                                            L.invd32);
+  }
+  if(c->mg_galerkin)
+  {
+    note_launch();
+    k_gal_coefs<<<1, 32, 0, st>>>(levels, c->gal_lmax, c->gal_coef);
   }
 }
 
@@ -473,8 +541,13 @@ static void enqueue_factor(icarat_ctx *c, int b, cudaStream_t st)
     return;
   ICK(cudaMemsetAsync(c->coarse.A[b], 0, sizeof(double) * (size_t)n * n, st));
   note_launch();
-  k_coarse_assemble<<<blocks_for(n, 64), 64, 0, st>>>(C.g, c->ke0, C.E, c->coarse.map,
-                                                     c->coarse.map + n, n, c->coarse.A[b]);
+  if(c->mg_galerkin)
+    k_coarse_assemble_st<<<blocks_for(n, 64), 64, 0, st>>>(C.g, C.S, c->coarse.map,
+                                                           c->coarse.map + n, n,
+                                                           c->coarse.A[b]);
+  else
+    k_coarse_assemble<<<blocks_for(n, 64), 64, 0, st>>>(C.g, c->ke0, C.E, c->coarse.map,
+                                                       c->coarse.map + n, n, c->coarse.A[b]);
   ICK(cudaGetLastError());
   dense_spd_inverse_factor(st, c->coarse.A[b], c->coarse.W[b], c->coarse.work[b], n,
                            c->coarse.bw);
@@ -503,7 +576,22 @@ double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
   ICK(cudaMemsetAsync(C.x, 0, sizeof(double) * nv, c->stream));
   dense_spd_solve(c->stream, c->coarse.W[c->coarse.cur], c->coarse.work[c->coarse.cur], n,
                   c->coarse.vin, c->coarse.vout, c->coarse.map, C.x);
-  launch_apply_K(c, C.g, C.E, C.fix, C.x, C.t, nullptr);
+  if(c->mg_galerkin)
+  {
+    // A x with the stencil: the residual of b = 0 is -A x
+    ICK(cudaMemsetAsync(C.b, 0, sizeof(double) * nv, c->stream));
+    note_launch();
+    k_st_residual<double><<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(C.g, C.S, C.fix,
+                                                                             C.b, C.x, C.t);
+    ICK(cudaStreamSynchronize(c->stream));
+    std::vector<double> tmp(nv);
+    ICK(cudaMemcpy(tmp.data(), C.t, sizeof(double) * nv, cudaMemcpyDeviceToHost));
+    for(double &v : tmp)
+      v = -v;
+    ICK(cudaMemcpy(C.t, tmp.data(), sizeof(double) * nv, cudaMemcpyHostToDevice));
+  }
+  else
+    launch_apply_K(c, C.g, C.E, C.fix, C.x, C.t, nullptr);
   ICK(cudaMemcpyAsync(y.data(), C.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
   ICK(cudaStreamSynchronize(c->stream));
   double rr = 0.0, bb = 0.0;
@@ -514,6 +602,38 @@ double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
     bb += b[i] * b[i];
   }
   return std::sqrt(rr / bb);
+}
+
+// y = A_level x on the host (component-major vectors of the level's 3 numnp
+// entries): the operator the V-cycle applies on that level for the options'
+// levels and coarse operators (constrained rows 0).
+void mg_level_apply(icarat_ctx *c, const icarat_solve_opts *o, int level, const double *x,
+                    double *y)
+{
+  const int levels = o->mg_levels > 0 ? o->mg_levels : 4;
+  IREQUIRE(o->coarse_op == ICARAT_COARSE_REDISCRETISED || o->coarse_op == ICARAT_COARSE_GALERKIN,
+           ICARAT_ERR_ARG, "coarse_op must be ICARAT_COARSE_REDISCRETISED or _GALERKIN");
+  IREQUIRE(level >= 0 && level < levels, ICARAT_ERR_ARG, "level out of range");
+  c->mg_galerkin_req = o->coarse_op == ICARAT_COARSE_GALERKIN ? 1 : 0;
+  mg_setup(c, levels);
+  MgLevel &L = c->mg[level];
+  const size_t nv = 3 * (size_t)L.g.numnp;
+  ICK(cudaMemcpyAsync(L.x, x, sizeof(double) * nv, cudaMemcpyHostToDevice, c->stream));
+  if(level > 0 && c->mg_galerkin)
+  {
+    ICK(cudaMemsetAsync(L.b, 0, sizeof(double) * nv, c->stream));
+    note_launch();
+    k_st_residual<double><<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, L.S, L.fix,
+                                                                             L.b, L.x, L.t);
+    ICK(cudaMemcpyAsync(y, L.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
+    ICK(cudaStreamSynchronize(c->stream));
+    for(size_t i = 0; i < nv; i++)
+      y[i] = -y[i];
+    return;
+  }
+  launch_apply_K(c, L.g, L.E, L.fix, L.x, L.t, nullptr);
+  ICK(cudaMemcpyAsync(y, L.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
+  ICK(cudaStreamSynchronize(c->stream));
 }
 
 // Captures what f enqueues on stream st into an instantiated graph.
@@ -566,7 +686,7 @@ static cudaGraphExec_t capture(cudaStream_t st, int &kernels, F f)
 void mg_setup(icarat_ctx *c, int levels, bool lag)
 {
   IREQUIRE(levels >= 2 && levels <= 12, ICARAT_ERR_ARG, "mg_levels must be in [2, 12]");
-  if((int)c->mg.size() != levels)
+  if((int)c->mg.size() != levels || c->mg_galerkin != c->mg_galerkin_req)
     allocate_levels(c, levels);
   else if(c->mg_version == c->design_version)
   {
@@ -700,6 +820,13 @@ template <typename T>
 static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x, T *r)
 {
   using B = LevelBuf<T>;
+  if(lvl > 0 && c->mg_galerkin)
+  {
+    note_launch();
+    k_st_residual<T><<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, B::S(L), L.fix, b,
+                                                                        x, r);
+    return;
+  }
   if(tc_level<T>(c, lvl))
   {
     TcArgs a;
@@ -739,6 +866,39 @@ template <typename T>
 static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool from_zero)
 {
   using B = LevelBuf<T>;
+  if(lvl > 0 && c->mg_galerkin)
+  {
+    // the same Chebyshev sequence with the level's own bound: coefficients
+    // from the device (computed at set-up from the design's cell matrices)
+    IREQUIRE(deg <= (kGalCoef + 1) / 2, ICARAT_ERR_ARG,
+             "mg_smooth too large for the Galerkin coarse levels");
+    const double *coef = c->gal_coef + (size_t)lvl * kGalCoef;
+    const int nv = 3 * L.g.numnp;
+    T *x = B::x(L), *xo = B::t(L), *d = B::r(L);
+    const int nb = blocks_for(L.g.numnp, 128);
+    if(from_zero)
+    {
+      note_launch();
+      k_st_first<T><<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, B::invd(L), coef, x, d);
+    }
+    else
+    {
+      note_launch();
+      k_st_cheb<T><<<nb, 128, 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
+                                               coef, 0);
+      std::swap(x, xo);
+    }
+    for(int k = 1; k < deg; k++)
+    {
+      note_launch();
+      k_st_cheb<T><<<nb, 128, 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
+                                               coef, k);
+      std::swap(x, xo);
+    }
+    if(x != B::x(L))
+      ICK(cudaMemcpyAsync(B::x(L), x, sizeof(T) * nv, cudaMemcpyDeviceToDevice, c->stream));
+    return;
+  }
   const double lmax = c->lam_max_dk;
   const double lmin = 0.1 * lmax;
   const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);

@@ -399,6 +399,9 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   {
     levels = o->mg_levels > 0 ? o->mg_levels : 4;
     smooth = o->mg_smooth > 0 ? o->mg_smooth : 2;
+    IREQUIRE(o->coarse_op == ICARAT_COARSE_REDISCRETISED || o->coarse_op == ICARAT_COARSE_GALERKIN,
+             ICARAT_ERR_ARG, "coarse_op must be ICARAT_COARSE_REDISCRETISED or _GALERKIN");
+    c->mg_galerkin_req = o->coarse_op == ICARAT_COARSE_GALERKIN ? 1 : 0;
     mg_setup(c, levels, o->coarse_lag != 0);
   }
   else

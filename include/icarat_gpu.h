@@ -123,7 +123,22 @@ typedef struct
                      (factor reuse across design iterations; every solve still
                      meets rtol on the current operator).  The first solve on a
                      new hierarchy factors synchronously. */
+  int coarse_op;  /* MG_PCG, MIXED_IR: ICARAT_COARSE_* operators of the coarse
+                     multigrid levels (0 = rediscretised) */
 } icarat_solve_opts;
+
+enum
+{
+  /* coarse element moduli = 2 x mean of the 8 children, the fine Ke0 and
+     the matrix-free stencil on every level (the default) */
+  ICARAT_COARSE_REDISCRETISED = 0,
+  /* Galerkin products P^T A P of the masked fine operator, assembled per
+     coarse cell and applied as 27-point node stencils; their Chebyshev
+     bounds come from the cells.  Keeps the multigrid's convergence on
+     solid / void designs at the price of a set-up per design and a
+     memory-bound coarse-level stencil.  Not for the batch solver. */
+  ICARAT_COARSE_GALERKIN = 1
+};
 
 typedef struct
 {
@@ -159,7 +174,12 @@ typedef struct
    icarat_batch_autotune_mg added, and the batch
    method ICARAT_SOLVER_MG_PCG (new functions and values; the 10100 structs
    are unchanged). */
-#define ICARAT_ABI_VERSION 10200
+/* 10300: icarat_solve_opts.coarse_op appended (Galerkin coarse operators)
+   and icarat_mg_level_apply added;
+   the loop options embed it, so loop snapshots are layout version 2.
+   Callers built against older headers pass the shorter struct and must be
+   rebuilt. */
+#define ICARAT_ABI_VERSION 10300
 int icarat_version(void);
 const char *icarat_status_string(int status);
 /* message of the last failed call on this thread */
@@ -397,6 +417,12 @@ int icarat_time_operator(icarat_ctx *ctx, int reps, double *ms_per_launch);
    coarsest level's stencil; *n_coarse (may be NULL): number of unknowns */
 int icarat_mg_coarse_check(icarat_ctx *ctx, int mg_levels, double *rel_residual,
                            int *n_coarse);
+/* y = A_level x on the current design, host vectors of 3 numnp_level
+   entries, component-major (c numnp_level + n): the operator the V-cycle of
+   `opts` (mg_levels, coarse_op) applies on that level (level 0 = the fine
+   stiffness; constrained rows 0).  Builds the hierarchy as a solve would. */
+int icarat_mg_level_apply(icarat_ctx *ctx, const icarat_solve_opts *opts, int level,
+                          const double *x, double *y);
 
 /* ---- batched solver (no reference counterpart) ---------------------------
    Many independent designs, of equal or different grid sizes, solved
