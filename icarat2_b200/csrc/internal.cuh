@@ -197,8 +197,8 @@ struct MgLevel
   float *E32 = nullptr, *invd32 = nullptr;
   float *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *t32 = nullptr;
   // Galerkin coarse operator (levels >= 1 of a Galerkin hierarchy): cell
-  // matrices (nelx x 576), node stencil (243 x numnp, coefficient-major) and
-  // its FP32 copy
+  // matrices (nelx x 576), node stencil (the 14 blocks o >= 13, 126 x numnp,
+  // coefficient-major) and its FP32 copy
   double *Kc = nullptr, *S = nullptr;
   float *S32 = nullptr;
 };
@@ -365,6 +365,11 @@ struct icarat_ctx
   int mg_galerkin_req = 0, mg_galerkin = 0;
   double *gal_lmax = nullptr; // per level: Chebyshev bound of D^-1 A
   double *gal_coef = nullptr; // per level: kGalCoef Chebyshev coefficients
+  double *gal_G = nullptr;    // the 8 child matrices P_s^T Ke0 P_s
+  double gal_lam1 = 0.0;      // their Jacobi bound (level 1, unconstrained cells)
+  uint8_t *gal_flag1 = nullptr; // level-1 cells with a constrained child node
+  int *gal_cells1 = nullptr;    // ... as a list
+  int gal_ncells1 = 0;
   icarat_b200::CoarseSolver coarse;
   // filter
   icarat_b200::FilterState filt;

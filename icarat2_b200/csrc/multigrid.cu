@@ -36,15 +36,19 @@ void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
                      const double *v, double *t, const int *rowmap, double *x);
 
 // Galerkin coarse operators (galerkin.cu)
+__global__ void k_gal_cells_free(GridDev f, GridDev c, const double *__restrict__ E,
+                                 const double *__restrict__ G,
+                                 const uint8_t *__restrict__ flag, double *__restrict__ Kc);
 __global__ void k_gal_cells(GridDev f, GridDev c, KeParam ke, const double *__restrict__ E,
                             const double *__restrict__ Kf, const uint8_t *__restrict__ fix_f,
-                            const uint8_t *__restrict__ fix_c, double *__restrict__ Kc,
-                            double *__restrict__ lmax);
+                            const uint8_t *__restrict__ fix_c, const int *__restrict__ cells,
+                            int ncells, double *__restrict__ Kc, double *__restrict__ lmax);
 __global__ void k_gal_stencil(GridDev g, const double *__restrict__ Kc,
                               const uint8_t *__restrict__ fix, double *__restrict__ S,
                               double *__restrict__ invd);
-__global__ void k_gal_coefs(int levels, const double *__restrict__ lmax,
+__global__ void k_gal_coefs(int levels, const double *__restrict__ lmax, double lam1,
                             double *__restrict__ coef);
+double galerkin_child_matrices(const double *ke0, double *G);
 template <typename T>
 __global__ void k_st_first(int n, const T *__restrict__ b, const T *__restrict__ invd,
                            const double *__restrict__ coef, T *__restrict__ x,
@@ -58,6 +62,8 @@ template <typename T>
 __global__ void k_st_residual(GridDev g, const T *__restrict__ S,
                               const uint8_t *__restrict__ fix, const T *__restrict__ b,
                               const T *__restrict__ x, T *__restrict__ r);
+dim3 st_block();
+int st_blocks(int numnp);
 __global__ void k_coarse_assemble_st(GridDev g, const double *__restrict__ S,
                                      const int *__restrict__ rowmap,
                                      const int *__restrict__ colmap, int nfree,
@@ -313,6 +319,13 @@ void mg_free(icarat_ctx *c)
   c->mg.clear();
   dfree(c->gal_lmax);
   c->gal_lmax = nullptr;
+  dfree(c->gal_G);
+  c->gal_G = nullptr;
+  dfree(c->gal_flag1);
+  c->gal_flag1 = nullptr;
+  dfree(c->gal_cells1);
+  c->gal_cells1 = nullptr;
+  c->gal_ncells1 = 0;
   c->gal_coef = nullptr; // part of the gal_lmax allocation
   c->mg_galerkin = 0;
   CoarseSolver &C = c->coarse;
@@ -387,8 +400,8 @@ static void allocate_levels(icarat_ctx *c, int levels)
     if(l > 0 && c->mg_galerkin_req)
     {
       L.Kc = dalloc(576 * (size_t)L.g.nelx);
-      L.S = dalloc(243 * (size_t)L.g.numnp);
-      L.S32 = falloc(243 * (size_t)L.g.numnp);
+      L.S = dalloc(126 * (size_t)L.g.numnp);
+      L.S32 = falloc(126 * (size_t)L.g.numnp);
     }
     L.x = dalloc(nv);
     L.b = dalloc(nv);
@@ -406,6 +419,34 @@ static void allocate_levels(icarat_ctx *c, int levels)
     // per level: the Chebyshev bound, then kGalCoef coefficients
     c->gal_lmax = dalloc((size_t)levels * (1 + kGalCoef));
     c->gal_coef = c->gal_lmax + levels;
+    std::vector<double> G(8 * 576);
+    c->gal_lam1 = 1.001 * galerkin_child_matrices(c->ke0.k, G.data());
+    c->gal_G = dalloc(G.size());
+    ICK(cudaMemcpy(c->gal_G, G.data(), sizeof(double) * G.size(), cudaMemcpyHostToDevice));
+    // level-1 cells with a constrained child node (fixed for the context):
+    // they take the general cell kernel, the others the free form
+    const GridDev f0 = c->mg[0].g, g1 = c->mg[1].g;
+    std::vector<uint8_t> flag(g1.nelx, 0);
+    std::vector<int> cells;
+    for(int cell = 0; cell < g1.nelx; cell++)
+    {
+      const int CI = cell % g1.nx, CJ = (cell / g1.nx) % g1.ny, CK = cell / (g1.nx * g1.ny);
+      for(int t = 0; t < 27 && !flag[cell]; t++)
+      {
+        const int fx = t % 3, fy = (t / 3) % 3, fz = t / 9;
+        if(c->fix_h[(2 * CI + fx) + (2L * CJ + fy) * f0.NX + (2L * CK + fz) * f0.NX * f0.NY])
+          flag[cell] = 1;
+      }
+      if(flag[cell])
+        cells.push_back(cell);
+    }
+    ICK(cudaMalloc(&c->gal_flag1, g1.nelx));
+    ICK(cudaMemcpy(c->gal_flag1, flag.data(), g1.nelx, cudaMemcpyHostToDevice));
+    c->gal_ncells1 = (int)cells.size();
+    ICK(cudaMalloc(&c->gal_cells1, sizeof(int) * std::max<size_t>(1, cells.size())));
+    if(!cells.empty())
+      ICK(cudaMemcpy(c->gal_cells1, cells.data(), sizeof(int) * cells.size(),
+                     cudaMemcpyHostToDevice));
   }
   c->mg_galerkin = c->mg_galerkin_req;
   // coarse constraint pattern on the host (fixed for the context)
@@ -506,12 +547,29 @@ static void enqueue_levels(icarat_ctx *c, int levels, cudaStream_t st)
       // Galerkin: cell matrices from the level above, the node stencil, the
       // Jacobi diagonal from it, the FP32 copies
       const MgLevel &F = c->mg[l - 1];
-      note_launch(3);
-      k_gal_cells<<<L.g.nelx, 128, 0, st>>>(F.g, L.g, c->ke0, F.E, l > 1 ? F.Kc : nullptr,
-                                            F.fix, L.fix, L.Kc, c->gal_lmax + l);
-      k_gal_stencil<<<blocks_for(27L * L.g.numnp, 256), 256, 0, st>>>(L.g, L.Kc, L.fix, L.S,
+      if(l == 1)
+      {
+        note_launch();
+        k_gal_cells_free<<<blocks_for(576L * L.g.nelx, 256), 256, 0, st>>>(
+            F.g, L.g, F.E, c->gal_G, c->gal_flag1, L.Kc);
+        if(c->gal_ncells1 > 0)
+        {
+          note_launch();
+          k_gal_cells<<<c->gal_ncells1, 128, 0, st>>>(F.g, L.g, c->ke0, F.E, nullptr, F.fix,
+                                                      L.fix, c->gal_cells1, c->gal_ncells1, L.Kc,
+                                                      c->gal_lmax + l);
+        }
+      }
+      else
+      {
+        note_launch();
+        k_gal_cells<<<L.g.nelx, 128, 0, st>>>(F.g, L.g, c->ke0, F.E, F.Kc, F.fix, L.fix, nullptr,
+                                              L.g.nelx, L.Kc, c->gal_lmax + l);
+      }
+      note_launch(2);
+      k_gal_stencil<<<blocks_for(14L * L.g.numnp, 256), 256, 0, st>>>(L.g, L.Kc, L.fix, L.S,
                                                                       L.invd);
-      k_cast<<<blocks_for(243L * L.g.numnp, 256), 256, 0, st>>>(243L * L.g.numnp, L.S, L.S32);
+      k_cast<<<blocks_for(126L * L.g.numnp, 256), 256, 0, st>>>(126L * L.g.numnp, L.S, L.S32);
     }
     else
       launch_diag(c, L.g, L.E, L.fix, L.invd, st);
@@ -527,7 +585,7 @@ static void enqueue_levels(icarat_ctx *c, int levels, cudaStream_t st)
   if(c->mg_galerkin)
   {
     note_launch();
-    k_gal_coefs<<<1, 32, 0, st>>>(levels, c->gal_lmax, c->gal_coef);
+    k_gal_coefs<<<1, 32, 0, st>>>(levels, c->gal_lmax, c->gal_lam1, c->gal_coef);
   }
 }
 
@@ -581,7 +639,7 @@ double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
     // A x with the stencil: the residual of b = 0 is -A x
     ICK(cudaMemsetAsync(C.b, 0, sizeof(double) * nv, c->stream));
     note_launch();
-    k_st_residual<double><<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(C.g, C.S, C.fix,
+    k_st_residual<double><<<st_blocks(C.g.numnp), st_block(), 0, c->stream>>>(C.g, C.S, C.fix,
                                                                              C.b, C.x, C.t);
     ICK(cudaStreamSynchronize(c->stream));
     std::vector<double> tmp(nv);
@@ -623,7 +681,7 @@ void mg_level_apply(icarat_ctx *c, const icarat_solve_opts *o, int level, const 
   {
     ICK(cudaMemsetAsync(L.b, 0, sizeof(double) * nv, c->stream));
     note_launch();
-    k_st_residual<double><<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, L.S, L.fix,
+    k_st_residual<double><<<st_blocks(L.g.numnp), st_block(), 0, c->stream>>>(L.g, L.S, L.fix,
                                                                              L.b, L.x, L.t);
     ICK(cudaMemcpyAsync(y, L.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
     ICK(cudaStreamSynchronize(c->stream));
@@ -823,7 +881,7 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
   if(lvl > 0 && c->mg_galerkin)
   {
     note_launch();
-    k_st_residual<T><<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, B::S(L), L.fix, b,
+    k_st_residual<T><<<st_blocks(L.g.numnp), st_block(), 0, c->stream>>>(L.g, B::S(L), L.fix, b,
                                                                         x, r);
     return;
   }
@@ -875,7 +933,7 @@ static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool
     const double *coef = c->gal_coef + (size_t)lvl * kGalCoef;
     const int nv = 3 * L.g.numnp;
     T *x = B::x(L), *xo = B::t(L), *d = B::r(L);
-    const int nb = blocks_for(L.g.numnp, 128);
+    const int nb = st_blocks(L.g.numnp);
     if(from_zero)
     {
       note_launch();
@@ -884,14 +942,14 @@ static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool
     else
     {
       note_launch();
-      k_st_cheb<T><<<nb, 128, 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
+      k_st_cheb<T><<<nb, st_block(), 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
                                                coef, 0);
       std::swap(x, xo);
     }
     for(int k = 1; k < deg; k++)
     {
       note_launch();
-      k_st_cheb<T><<<nb, 128, 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
+      k_st_cheb<T><<<nb, st_block(), 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
                                                coef, k);
       std::swap(x, xo);
     }
