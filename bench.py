@@ -955,12 +955,12 @@ def gpu_arm(a):
     ms_steps = [e0.elapsed_time(e1) for e0, e1 in evs]
     value, total_ms = job_rate(sum(ms_steps), a.steps, world, dist, dev)
 
-    def alt_loop(levels, lag, warm=None):
+    def alt_loop(levels, lag, warm=None, coarse_op=0):
         warm = a.warm_start if warm is None else warm
         ca = make_ctx()
         ca.loop_init(0.3, method="mma", filter_radius=a.radius, move=0.2,
                      solve=G.solve_opts(G.MG_PCG, a.rtol, 10000, levels, a.smooth,
-                                        coarse_lag=lag, warm_start=warm))
+                                        coarse_lag=lag, warm_start=warm, coarse_op=coarse_op))
         sa = torch.cuda.ExternalStream(ca.stream_ptr(), device=dev)
         for _ in range(a.warmup):
             ca.loop_step()
@@ -978,7 +978,8 @@ def gpu_arm(a):
         torch.cuda.synchronize()
         v, alt_ms = job_rate(alt_ms, a.steps, world, dist, dev)
         ca.close()
-        return {"mg_levels": levels, "coarse_lag": lag, "warm_start": warm, "value": v,
+        return {"mg_levels": levels, "coarse_lag": lag, "warm_start": warm,
+                "coarse_operators": "Galerkin" if coarse_op else "rediscretised", "value": v,
                 "unit": "design-iter/s", "ms_per_step": alt_ms / a.steps,
                 "cg_iterations_per_step": its}
 
@@ -988,6 +989,8 @@ def gpu_arm(a):
     other_coarse = alt_loop(a.levels, 1 - a.coarse_lag) if a.alt_levels else None
     other_warm = alt_loop(a.levels, a.coarse_lag, 1 - a.warm_start) if a.alt_levels else None
     alt = alt_loop(a.alt_levels, a.coarse_lag) if a.alt_levels else None
+    alt_gal = alt_loop(a.levels, a.coarse_lag, coarse_op=G.COARSE_GALERKIN) \
+        if a.alt_levels else None
 
     # ---------------- dominant kernel: FP64 stencil K u on the final design
     ms_op = ctx.time_operator(30)
@@ -1121,6 +1124,7 @@ def gpu_arm(a):
             "alt_levels": alt,
             "alt_coarse_lag": other_coarse,
             "alt_warm_start": other_warm,
+            "alt_galerkin": alt_gal,
             "mixed_256x128x128": mixed,
             "batched_80_designs": batched,
             "learned": learned,
