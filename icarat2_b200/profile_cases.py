@@ -7,7 +7,8 @@ set-up.
         one K u = f solve of the cantilever (densities U[0.1, 0.5], seed 0),
         after a warm-up solve and a design change (so the per-design
         multigrid set-up is inside the captured region);
-        methods: jacobi, mg, mixed
+        methods: jacobi, mg, mixed; an optional 6th argument "galerkin"
+        selects Galerkin coarse operators
     python -m icarat2_b200.profile_cases operator 256x128x128 2 3
         `reps` launches of K u with operator 0 FP64, 1 FP32, 2 tensor cores
         BF16x3, 3 tensor cores BF16, 4 FP64 tensor cores (after one warm-up
@@ -29,6 +30,10 @@ set-up.
         start 0.3, radius filter R, move 0.15, 4-level MG-PCG to 1e-8 with
         the coarse factor reused and warm starts) after `warm` warm-up
         iterations: filter, sensitivity and the OC bisection kernel
+    python -m icarat2_b200.profile_cases batch 8 64x32x32 1e-6
+        one batched multigrid-PCG solve (the persistent launch, 4 levels) of
+        `n` cantilevers of the grid (densities U[0.1, 0.6], seed 3) after
+        two warm-up solves
     python -m icarat2_b200.profile_cases helm 256x128x128 2.0
         one Helmholtz PDE filter call (design U[0, 1], seed 0, CG to 1e-10)
         after one warm-up call
@@ -54,13 +59,14 @@ def _grid(s):
     return tuple(int(v) for v in s.split("x"))
 
 
-def solve(grid, method, levels, rtol):
+def solve(grid, method, levels, rtol, coarse="rediscretised"):
     nx, ny, nz = _grid(grid)
     G = gpu.Context(nx, ny, nz)
     rho = np.random.default_rng(0).uniform(0.1, 0.5, G.nelx)
     G.set_design(rho)
     m = {"jacobi": gpu.JACOBI_PCG, "mg": gpu.MG_PCG, "mixed": gpu.MIXED_IR}[method]
-    o = gpu.solve_opts(m, rtol=float(rtol), mg_levels=int(levels))
+    cop = gpu.COARSE_GALERKIN if coarse == "galerkin" else gpu.COARSE_REDISCRETISED
+    o = gpu.solve_opts(m, rtol=float(rtol), mg_levels=int(levels), coarse_op=cop)
     G.solve(o, want_val=False)
     G.set_design(rho * 1.01)
     G.synchronize()
@@ -168,9 +174,30 @@ def helm(grid, radius):
                                                            info.rel_residual, out.sum()))
 
 
+def batch(n, grid, rtol):
+    nx, ny, nz = _grid(grid)
+    bc = gpu.cantilever_bc(nx, ny, nz)
+    B = gpu.Batch([(nx, ny, nz) + tuple(bc)] * int(n))
+    rng = np.random.default_rng(3)
+    for i in range(int(n)):
+        B[i].set_design(rng.uniform(0.1, 0.6, B[i].nelx))
+    o = B.opts(rtol=float(rtol), method=gpu.MG_PCG, mg_levels=4)
+    for _ in range(2):
+        B.solve(o)
+    B[0].synchronize()
+    rt = _profiler()
+    rt.cudaProfilerStart()
+    inf = B.solve(o)
+    rt.cudaProfilerStop()
+    print("iterations %d status %s" % (max(x.iterations for x in inf),
+                                       sorted({x.status for x in inf})))
+
+
 def main(argv):
     if len(argv) >= 5 and argv[0] == "solve":
-        solve(*argv[1:5])
+        solve(*argv[1:6])
+    elif len(argv) >= 4 and argv[0] == "batch":
+        batch(*argv[1:4])
     elif len(argv) >= 6 and argv[0] == "loop":
         loop(*argv[1:6])
     elif len(argv) >= 4 and argv[0] == "ocloop":
