@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_pcg(BatchArgs a)
       S.delta2 = a.delta * a.delta;
       S.iter = 0;
       S.maxit = a.maxit;
-      S.refresh = S.final_ = S.nrefresh = S.nstall = 0;
+      S.refresh = S.final_ = S.nrefresh = S.nstall = S.last_refresh = 0;
       S.status = ICARAT_OK;
       S.done = 0;
       if(!(bb == bb))
@@ -248,7 +248,10 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_pcg(BatchArgs a)
               S.rz = rz;
               const bool nan = !(rr == rr) || !(beta == beta);
               S.final_ = (nan || S.iter >= S.maxit) ? 1 : 0;
-              S.refresh = (S.final_ || rr < S.tol2 || rr < S.delta2 * S.rr_ref) ? 1 : 0;
+              S.refresh = (S.final_ || rr < S.tol2 || rr < S.delta2 * S.rr_ref ||
+                           S.iter - S.last_refresh >= kRefreshEvery)
+                              ? 1
+                              : 0;
               if(S.refresh)
                 atomicAdd(&a.ctl[1 + (it & 1)], 1);
             }
@@ -344,6 +347,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) k_batch_pcg(BatchArgs a)
         S.rr_true = S.rr_ref = rr;
         S.rz = rz;
         S.nrefresh += 1;
+        S.last_refresh = S.iter;
         S.refresh = 0;
         if(!(rr == rr))
         {

@@ -27,6 +27,7 @@ struct BScal
   double rz, bb, rr_ref, rr_true, tol2, delta2;
   double rr_nat; // FP64 r . r at the last refresh the design asked for itself
   int iter, maxit, done, status, refresh, final_, nrefresh, nstall;
+  int last_refresh; // iteration of the last FP64 residual
 };
 
 struct BatchArgs

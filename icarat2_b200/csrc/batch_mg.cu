@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_mg(BatchArgs a, BmAr
       S.delta2 = a.delta * a.delta;
       S.iter = 0;
       S.maxit = a.maxit;
-      S.refresh = S.final_ = S.nrefresh = S.nstall = 0;
+      S.refresh = S.final_ = S.nrefresh = S.nstall = S.last_refresh = 0;
       S.status = ICARAT_OK;
       S.done = 0;
       if(!(bb == bb))
@@ -820,7 +820,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_mg(BatchArgs a, BmAr
         {
           BScal &S = a.s[d];
           const bool fin = !(rr == rr) || S.iter >= S.maxit;
-          const bool fresh = fin || rr < S.tol2 || rr < S.delta2 * S.rr_ref;
+          const bool fresh = fin || rr < S.tol2 || rr < S.delta2 * S.rr_ref ||
+                             S.iter - S.last_refresh >= kRefreshEvery;
           S.final_ = fin ? 1 : 0;
           S.refresh = fresh ? 1 : 0;
           if(fresh)
@@ -983,6 +984,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_mg(BatchArgs a, BmAr
               }
               S.rr_true = S.rr_ref = rr;
               S.nrefresh += 1;
+              S.last_refresh = S.iter;
               if(!(rr == rr))
               {
                 S.done = 1;

@@ -118,8 +118,15 @@ struct MxScalars
   int refresh;  // FP64 residual due after this iteration's update
   int final_;   // iteration cap reached: last refresh, then stop
   int nrefresh; // FP64 residuals evaluated
+  int last_refresh; // iteration of the last FP64 residual
   unsigned int counter;
 };
+
+// the FP64 residual of the mixed-precision solvers is recomputed at least
+// every kRefreshEvery iterations: on ill-conditioned systems (floating solid
+// islands in a 1e-9 void) the FP32 recurrence residual can stall while the
+// FP32 iterate drifts away from the FP64 solution
+constexpr int kRefreshEvery = 50;
 
 // Variants of the tensor-core element-by-element operator (tc_stencil.cu).
 enum TcOp

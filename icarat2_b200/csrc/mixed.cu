@@ -7,12 +7,16 @@
 // solution is refined in FP64: the iteration accumulates a correction x32;
 // once the FP32 recurrence residual has fallen by the factor `refresh` below
 // the last FP64 residual (or below the stopping threshold, or at the
-// iteration cap) the correction is added to the FP64 solution x, x32 is
+// iteration cap, or kRefreshEvery iterations after the last refresh) the
+// correction is added to the FP64 solution x, x32 is
 // cleared and the residual is recomputed as r = b - K x with the FP64
 // operator.  Convergence is decided on that FP64 residual only:
 // ||b - K x|| < rtol ||b||; three refreshes in a row that cut it by less than
-// 10 % end the solve with ICARAT_WARN_STAGNATION (the residual is then at the
-// accuracy FP64 evaluation allows for the design).  The search direction
+// 10 % end the FP32 iteration; then, and after a breakdown (a non-finite
+// scalar), FP64 MG-PCG on the same hierarchy finishes the solve, started
+// from the FP32 solution where that is finite (ill-conditioned systems such
+// as solid islands floating in a 1e-9 void), and its status is the
+// solve's.  The search direction
 // survives the refresh, so the refinement does not restart the Krylov space;
 // beta is the flexible
 // (Polak-Ribiere) form beta = -(z . K p) / (p . K p), which keeps
@@ -79,6 +83,7 @@ __global__ void __launch_bounds__(128)
       s->refresh = 0;
       s->final_ = 0;
       s->nrefresh = 0;
+      s->last_refresh = 0;
       s->nstall = 0;
       s->status = ICARAT_OK;
       s->done = (t[0] == 0.0 || t[1] < s->tol2) ? 1 : 0;
@@ -127,6 +132,7 @@ __global__ void k_mx_init(int n, const double *__restrict__ b, double *__restric
       s->refresh = 0;
       s->final_ = 0;
       s->nrefresh = 0;
+      s->last_refresh = 0;
       s->nstall = 0;
       s->status = ICARAT_OK;
       s->done = (t[0] == 0.0) ? 1 : 0;
@@ -225,7 +231,10 @@ __global__ void k_mx_update(int n, float *__restrict__ x32, float *__restrict__ 
       else
       {
         s->final_ = s->iter > s->maxit ? 1 : 0;
-        s->refresh = (r2 < s->delta2 * s->rr_ref || r2 < s->tol2 || s->final_) ? 1 : 0;
+        s->refresh = (r2 < s->delta2 * s->rr_ref || r2 < s->tol2 || s->final_ ||
+                      s->iter - s->last_refresh >= kRefreshEvery)
+                         ? 1
+                         : 0;
       }
       s->counter = 0;
     }
@@ -291,6 +300,7 @@ __global__ void __launch_bounds__(128)
       s->nstall = r2 > 0.81 * s->rr_true ? s->nstall + 1 : 0;
       s->rr_true = s->rr_ref = s->rr = r2;
       s->nrefresh += 1;
+      s->last_refresh = s->iter;
       s->refresh = 0;
       if(!(r2 == r2))
       {
@@ -758,7 +768,26 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   }
   mg_join(c);
   ICK(cudaStreamSynchronize(c->stream));
-  return mixed_finish(c, run, info);
+  const int st = mixed_finish(c, run, info);
+  // FP64 finish: an FP32 iteration that stalls above the tolerance (or
+  // breaks down) on an ill-conditioned system hands over to FP64 MG-PCG on
+  // the same hierarchy, started from its solution where that is finite
+  if(st == ICARAT_ERR_NAN || st == ICARAT_WARN_STAGNATION)
+  {
+    icarat_solve_opts f = *o;
+    f.method = ICARAT_SOLVER_MG_PCG;
+    f.chunk = 0;
+    f.fp64_tc = 0;
+    f.warm_start = st == ICARAT_WARN_STAGNATION ? 1 : 0;
+    icarat_solve_info fi{};
+    const int s2 = solve_full(c, &f, d_b, d_x, &fi);
+    info->iterations += fi.iterations;
+    info->rel_residual = fi.rel_residual;
+    info->refreshes += fi.refreshes;
+    info->status = s2;
+    return s2;
+  }
+  return st;
 }
 
 } // namespace icarat_b200

@@ -87,7 +87,10 @@ enum
   ICARAT_SOLVER_JACOBI_PCG = 0, /* "Eigen_CG" / "Scaling_CG" semantics */
   ICARAT_SOLVER_MG_PCG = 1,     /* geometric multigrid preconditioned CG */
   ICARAT_SOLVER_MIXED_IR = 2,   /* FP32 multigrid-PCG iterations refined by FP64
-                                   residuals (no reference counterpart) */
+                                   residuals (no reference counterpart); an
+                                   FP32 iteration that stalls above rtol or
+                                   breaks down is finished by FP64 MG-PCG
+                                   (iterations add up) */
   ICARAT_SOLVER_LEARNED_FPCG = 3 /* MIXED_IR with the context's learned net as
                                     initial guess and first preconditioner */
 };
