@@ -617,10 +617,12 @@ static int batch_solve_concurrent(icarat_batch *B, const icarat_batch_opts *o, d
   IREQUIRE(want >= 2 && want <= 12, ICARAT_ERR_ARG, "mg_levels must be in [2, 12]");
   IREQUIRE(o->chunk >= 0, ICARAT_ERR_ARG, "chunk must be non-negative");
   std::vector<MixedRun> run(n);
+  std::vector<icarat_solve_opts> opts(n);
   for(size_t d = 0; d < n; d++)
   {
     icarat_ctx *c = B->ctx[d];
-    icarat_solve_opts so{};
+    icarat_solve_opts &so = opts[d];
+    so = icarat_solve_opts{};
     so.method = ICARAT_SOLVER_MIXED_IR;
     so.rtol = rtol;
     so.maxit = maxit;
@@ -657,8 +659,11 @@ static int batch_solve_concurrent(icarat_batch *B, const icarat_batch_opts *o, d
   for(size_t d = 0; d < n; d++)
   {
     icarat_solve_info si{};
-    mixed_finish(B->ctx[d], run[d], &si);
-    note_result(B->ctx[d], si, infos ? &infos[d] : nullptr, worst);
+    icarat_ctx *c = B->ctx[d];
+    // a design whose FP32 iteration stalled or broke down is finished in
+    // FP64, as the single-design mixed solve does
+    mixed_fp64_finish(c, &opts[d], c->d_rhs, c->d_u, &si, mixed_finish(c, run[d], &si));
+    note_result(c, si, infos ? &infos[d] : nullptr, worst);
   }
   return worst;
 }
@@ -938,7 +943,7 @@ static int pick_mg_bpsm(icarat_batch *B, const icarat_batch_opts *o)
   return B->mg_tuned_bpsm > 0 ? B->mg_tuned_bpsm : B->occ_mg;
 }
 
-static int batch_collect(icarat_batch *B, icarat_solve_info *infos);
+static int batch_collect(icarat_batch *B, double rtol, int maxit, icarat_solve_info *infos);
 
 static int batch_solve_mg(icarat_batch *B, const icarat_batch_opts *o, double rtol, int maxit,
                           double refresh, icarat_solve_info *infos)
@@ -948,7 +953,7 @@ static int batch_solve_mg(icarat_batch *B, const icarat_batch_opts *o, double rt
   const bool warm = o && o->warm_start;
   const int L = batch_mg_prepare(B, o && o->mg_levels > 0 ? o->mg_levels : 4, tile, warm);
   batch_mg_run(B, tile, bpsm, rtol, maxit, refresh, L, warm ? 1 : 0);
-  return batch_collect(B, infos);
+  return batch_collect(B, rtol, maxit, infos);
 }
 
 static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
@@ -968,11 +973,11 @@ static int batch_solve_impl(icarat_batch *B, const icarat_batch_opts *o,
   const int tile = pick_tile(B, o), bpsm = pick_bpsm(B, o);
   IREQUIRE(tile >= 32 && tile <= (1 << 16), ICARAT_ERR_ARG, "tile must be in [32, 65536]");
   batch_run(B, tile, bpsm, rtol, maxit, refresh);
-  return batch_collect(B, infos);
+  return batch_collect(B, rtol, maxit, infos);
 }
 
 // per-design results of a persistent launch
-static int batch_collect(icarat_batch *B, icarat_solve_info *infos)
+static int batch_collect(icarat_batch *B, double rtol, int maxit, icarat_solve_info *infos)
 {
   const size_t n = B->ctx.size();
   ICK(cudaMemcpyAsync(B->h_s, B->d_s, sizeof(BScal) * n, cudaMemcpyDeviceToHost, B->stream));
@@ -989,6 +994,20 @@ static int batch_collect(icarat_batch *B, icarat_solve_info *infos)
     si.rel_residual = S.bb > 0 ? std::sqrt(S.rr_true / S.bb) : 0.0;
     si.status = S.done ? S.status : ICARAT_WARN_MAXITER;
     si.refreshes = S.nrefresh;
+    if(si.status == ICARAT_ERR_NAN || si.status == ICARAT_WARN_STAGNATION)
+    {
+      // the design's FP32 iteration stalled or broke down: FP64 MG-PCG
+      // finishes it from the solution the launch left in the context (as
+      // the single-design mixed solve does)
+      icarat_solve_opts f{};
+      f.method = ICARAT_SOLVER_MIXED_IR;
+      f.rtol = rtol;
+      f.maxit = maxit;
+      f.mg_levels = B->mg_levels > 0 ? B->mg_levels : design_levels(c, 4);
+      c->have_u = true;
+      ICK(cudaStreamSynchronize(c->stream));
+      mixed_fp64_finish(c, &f, c->d_rhs, c->d_u, &si, si.status);
+    }
     note_result(c, si, infos ? &infos[d] : nullptr, worst);
   }
   return worst;

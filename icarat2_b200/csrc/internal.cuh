@@ -435,6 +435,8 @@ double device_dot(icarat_ctx *c, const double *a, const double *b, int n);
 
 // pcg.cu
 void release_graphs(icarat_ctx *c);
+int mixed_fp64_finish(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, double *d_x,
+                      icarat_solve_info *info, int st);
 int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
                double *d_x, icarat_solve_info *info);
 

@@ -768,10 +768,16 @@ int mixed_solve(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   }
   mg_join(c);
   ICK(cudaStreamSynchronize(c->stream));
-  const int st = mixed_finish(c, run, info);
-  // FP64 finish: an FP32 iteration that stalls above the tolerance (or
-  // breaks down) on an ill-conditioned system hands over to FP64 MG-PCG on
-  // the same hierarchy, started from its solution where that is finite
+  return mixed_fp64_finish(c, o, d_b, d_x, info, mixed_finish(c, run, info));
+}
+
+// FP64 finish: an FP32 iteration that stalled above the tolerance (or broke
+// down) on an ill-conditioned system hands over to FP64 MG-PCG on the same
+// hierarchy, started from its solution where that is finite.  st: the
+// status of the FP32 iteration, info its result (updated).
+int mixed_fp64_finish(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, double *d_x,
+                      icarat_solve_info *info, int st)
+{
   if(st == ICARAT_ERR_NAN || st == ICARAT_WARN_STAGNATION)
   {
     icarat_solve_opts f = *o;

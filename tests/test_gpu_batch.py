@@ -336,3 +336,23 @@ def test_batch_persistent_mg_design_loop_tracks_individual_loops(gpu):
             assert abs(infos[i].compliance - ref.compliance) <= 1e-6 * ref.compliance
     for i, G in enumerate(solo):
         assert rel(B[i].loop_get("x"), G.loop_get("x")) <= 1e-6
+
+
+@pytest.mark.parametrize("method", ["MG_PCG", "MIXED_IR"])
+def test_batch_floating_islands_finish_in_fp64(gpu, method):
+    """A design of solid streaks floating in a 1e-9 void beside an ordinary
+    one: a design whose FP32 iteration stalls is finished by FP64 MG-PCG, so
+    every design of the batch meets rtol.  Checked again with the context's
+    FP64 K u, whose rounding, with island displacements of 1e6, is itself
+    about 1e-8 of ||f||: to 10 rtol."""
+    prs = problems(gpu, [(32, 16, 16), (32, 16, 16)], 41)
+    B = gpu.Batch(prs)
+    rng = np.random.default_rng(5)
+    x = np.convolve(rng.standard_normal(B[0].nelx), np.ones(9) / 9.0, mode="same")
+    B[0].set_design(np.where(x >= np.quantile(x, 0.65), 1.0, 1e-3))
+    B[1].set_design(rng.uniform(0.1, 0.6, B[1].nelx))
+    infos = B.solve(B.opts(rtol=1e-8, method=getattr(gpu, method), mg_levels=3))
+    for i in range(2):
+        assert infos[i].status == gpu.OK, (i, infos[i].status, infos[i].rel_residual)
+        u, f = B.solution(i), B[i].fext()
+        assert np.linalg.norm(f - B[i].apply_K(u)) < 1e-7 * np.linalg.norm(f)
