@@ -1114,7 +1114,9 @@ def gpu_arm(a):
                          "unit": "TFLOP/s", "frac": achieved / peak64,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                          "traffic": traffic_from_profiles(a.grid),
-                         "flops_per_launch": flops, "ms_per_launch": ms_op},
+                         "flops_per_launch": flops, "ms_per_launch": ms_op,
+                         "caches": "cold: each timed launch follows a 256 MiB write "
+                                   "that evicts L2"},
             "roofline_hbm": {"achieved": bytes_alg / (ms_op * 1e-3) / 1e9, "peak": hbm_peak,
                              "unit": "GB/s", "frac": bytes_alg / (ms_op * 1e-3) / 1e9 / hbm_peak,
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",

@@ -410,8 +410,9 @@ int icarat_solve_noalloc(icarat_ctx *ctx, const icarat_solve_opts *opts,
 /* number of kernels this library has launched in this process */
 int icarat_kernel_launches(unsigned long long *count);
 /* average device time of the FP64 stiffness stencil y = K u on the current
-   design, over `reps` back-to-back launches timed with CUDA events on the
-   context's stream */
+   design, over `reps` launches timed with CUDA events on the context's
+   stream, each after a 256 MiB write that evicts the L2 (cold caches; the
+   call allocates and frees that buffer) */
 int icarat_time_operator(icarat_ctx *ctx, int reps, double *ms_per_launch);
 /* check of the multigrid's coarsest dense solve on the current design:
    builds the hierarchy of `mg_levels` levels, solves K_c x = b for
