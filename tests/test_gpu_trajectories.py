@@ -69,7 +69,10 @@ def test_config1_oc_trajectory(gpu, config1, solver, x_tol):
         assert rel(G.loop_get("dfds"), r["dfds"]) <= 1e-10, k
         assert rel(G.loop_get("x"), r["x"]) <= x_tol, k
         if solver == "jacobi":
-            assert abs(info.cg_iterations - r["it"]) <= 1, k
+            # the oracle's OpenMP dot products sum in an order that depends on
+            # the host's thread count, so near rtol 1e-10 its iteration count
+            # can move by a few out of ~400 from one machine to the next
+            assert abs(info.cg_iterations - r["it"]) <= max(1, 0.01 * r["it"]), k
 
 
 def test_headline_settings_trajectory(oracle, gpu):
