@@ -412,11 +412,11 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
     out = {"grid": [nx, ny, nz], "mg_levels": levels, "filter_radius": 3.0,
            "update": "MMA move 0.2", "rho0": "U[0.1, 0.5] seed 0"}
 
-    def loop_rate(method, rtol, warm=0):
+    def loop_rate(method, rtol, warm=0, lag=0):
         c = G.Context(nx, ny, nz, device=dev.index)
         c.loop_init(rho0, method="mma", filter_radius=3.0, move=0.2,
                     solve=G.solve_opts(method, rtol, 10000, levels, a.smooth,
-                                       warm_start=warm))
+                                       warm_start=warm, coarse_lag=lag))
         s = torch.cuda.ExternalStream(c.stream_ptr(), device=dev)
         for _ in range(a.warmup):
             c.loop_step()
@@ -447,6 +447,15 @@ def mixed_section(a, G, torch, dev, flush, world, dist):
                                  "speedup_mixed_vs_fp64": m["value"] / p["value"],
                                  "speedup_mixed_warm_vs_fp64": w["value"] / p["value"],
                                  "speedup_mixed_warm_vs_fp64_warm": w["value"] / pw["value"]}
+        if rtol == 1e-6:
+            # both solvers with warm starts and the coarsest factor reused
+            # from the previous design (computed beside the solve)
+            wl = loop_rate(G.MIXED_IR, rtol, warm=1, lag=1)
+            pwl = loop_rate(G.MG_PCG, rtol, warm=1, lag=1)
+            out["rtol_%g" % rtol].update({
+                "mixed_warm_lag": wl, "fp64_mg_pcg_warm_lag": pwl,
+                "speedup_mixed_warm_lag_vs_fp64": wl["value"] / p["value"],
+                "speedup_mixed_warm_lag_vs_fp64_warm_lag": wl["value"] / pwl["value"]})
     # accuracy of one solve on the first design against FP64 at rtol 1e-12
     c = G.Context(nx, ny, nz, device=dev.index)
     c.filter_setup(3.0)
