@@ -317,30 +317,42 @@ __device__ __forceinline__ T st_coef(const T *__restrict__ S, int numnp, long n,
                  : S[(9L * (13 - o) + 3 * d + c) * numnp + m];
 }
 
-template <typename T>
+template <int DZ, typename T>
 __device__ __forceinline__ T stencil_slab(const GridDev &g, const T *__restrict__ S,
-                                          const T *__restrict__ x, int n, int c, int dz)
+                                          const T *__restrict__ x, int n, int c)
 {
   const int X = n % g.NX, Y = (n / g.NX) % g.NY, Z = n / (g.NX * g.NY);
+  const bool zin = Z + DZ >= 0 && Z + DZ < g.NZ;
+  // every load is issued (out-of-mesh neighbours read node n and count 0),
+  // so that the 54 loads of a slab need not wait for one another
   T acc = T(0);
-  const int Z2 = Z + dz;
-  if(Z2 < 0 || Z2 >= g.NZ)
-    return acc;
 #pragma unroll
   for(int dy = -1; dy <= 1; dy++)
 #pragma unroll
     for(int dx = -1; dx <= 1; dx++)
     {
-      const int X2 = X + dx, Y2 = Y + dy;
-      if(X2 < 0 || X2 >= g.NX || Y2 < 0 || Y2 >= g.NY)
-        continue;
-      const int o = 9 * (dz + 1) + 3 * (dy + 1) + (dx + 1);
-      const long m = n + dx + (long)dy * g.NX + (long)dz * g.NX * g.NY;
+      const bool in =
+          zin && X + dx >= 0 && X + dx < g.NX && Y + dy >= 0 && Y + dy < g.NY;
+      constexpr int o0 = 9 * (DZ + 1);
+      const int o = o0 + 3 * (dy + 1) + (dx + 1);
+      const long m = in ? n + dx + (long)dy * g.NX + (long)DZ * g.NX * g.NY : n;
 #pragma unroll
       for(int d = 0; d < 3; d++)
-        acc = fma(st_coef(S, g.numnp, n, m, o, c, d), x[(long)d * g.numnp + m], acc);
+      {
+        const T a = st_coef(S, g.numnp, n, m, o, c, d);
+        acc = fma(in ? a : T(0), x[(long)d * g.numnp + m], acc);
+      }
     }
   return acc;
+}
+
+template <typename T>
+__device__ __forceinline__ T stencil_slab_any(const GridDev &g, const T *__restrict__ S,
+                                              const T *__restrict__ x, int n, int c, int p)
+{
+  // p is uniform over a warp (threadIdx.y)
+  return p == 0 ? stencil_slab<-1>(g, S, x, n, c)
+                : (p == 1 ? stencil_slab<0>(g, S, x, n, c) : stencil_slab<1>(g, S, x, n, c));
 }
 
 // (A x)_{n, c} for the block's node lane; true on the thread that holds the
@@ -352,7 +364,7 @@ __device__ __forceinline__ bool stencil_row(const GridDev &g, const T *__restric
                                             T &row)
 {
   const int c = threadIdx.y / 3, p = threadIdx.y % 3;
-  ps[threadIdx.y][threadIdx.x] = n < g.numnp ? (double)stencil_slab(g, S, x, n, c, p - 1) : 0.0;
+  ps[threadIdx.y][threadIdx.x] = n < g.numnp ? (double)stencil_slab_any(g, S, x, n, c, p) : 0.0;
   __syncthreads();
   row = T((ps[3 * c][threadIdx.x] + ps[3 * c + 1][threadIdx.x]) + ps[3 * c + 2][threadIdx.x]);
   const bool mine = p == 0 && n < g.numnp;
