@@ -102,8 +102,12 @@ __global__ void k_cast(long n, const Tin *__restrict__ in, Tout *__restrict__ ou
 // coarse b = R r  (R = P^T, 27 fine nodes per coarse node, weights 1/2^d;
 // restrict_node / prolong_node in stencil.cuh)
 template <typename T>
+// With xc set, also the coarse level's first Chebyshev step from zero
+// (k_cheb_first fused): dc = xc = inv_theta invd_c bc.
 __global__ void k_restrict(GridDev f, GridDev c, const T *__restrict__ rf,
-                           const uint8_t *__restrict__ fixc, T *__restrict__ bc)
+                           const uint8_t *__restrict__ fixc, T *__restrict__ bc,
+                           const T *__restrict__ invd_c, T inv_theta, T *__restrict__ xc,
+                           T *__restrict__ dc)
 {
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.numnp;
       n += gridDim.x * blockDim.x)
@@ -111,9 +115,19 @@ __global__ void k_restrict(GridDev f, GridDev c, const T *__restrict__ rf,
     T s[3];
     restrict_node<T, false>(f, c, rf, n, s);
     const unsigned fx = fixc[n];
-    bc[n] = (fx & 1u) ? T(0) : s[0];
-    bc[(long)c.numnp + n] = (fx & 2u) ? T(0) : s[1];
-    bc[2L * c.numnp + n] = (fx & 4u) ? T(0) : s[2];
+#pragma unroll
+    for(int q = 0; q < 3; q++)
+    {
+      const long id = (long)q * c.numnp + n;
+      const T bq = ((fx >> q) & 1u) ? T(0) : s[q];
+      bc[id] = bq;
+      if(xc)
+      {
+        const T di = inv_theta * invd_c[id] * bq;
+        dc[id] = di;
+        xc[id] = di;
+      }
+    }
   }
 }
 
@@ -921,7 +935,8 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
 // Chebyshev smoothing of K x = b on level lvl, deg steps.  from_zero: x = 0
 // on entry (the first step needs no product).
 template <typename T>
-static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool from_zero)
+static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool from_zero,
+                   bool first_done = false)
 {
   using B = LevelBuf<T>;
   if(lvl > 0 && c->mg_galerkin)
@@ -967,9 +982,12 @@ static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool
   int k0 = 0;
   if(from_zero)
   {
-    note_launch();
-    k_cheb_first<<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, B::invd(L),
-                                                             T(1.0 / theta), x, d);
+    if(!first_done) // else the restriction that produced b took this step
+    {
+      note_launch();
+      k_cheb_first<<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, B::invd(L),
+                                                               T(1.0 / theta), x, d);
+    }
     k0 = 1;
   }
   else
@@ -990,7 +1008,8 @@ static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool
     ICK(cudaMemcpyAsync(B::x(L), x, sizeof(T) * nv, cudaMemcpyDeviceToDevice, c->stream));
 }
 
-template <typename T> static void vcycle(icarat_ctx *c, int l, const T *b, int deg)
+template <typename T>
+static void vcycle(icarat_ctx *c, int l, const T *b, int deg, bool first_done = false)
 {
   using B = LevelBuf<T>;
   MgLevel &L = c->mg[l];
@@ -1016,13 +1035,18 @@ template <typename T> static void vcycle(icarat_ctx *c, int l, const T *b, int d
     return;
   }
   MgLevel &C = c->mg[l + 1];
-  smooth<T>(c, L, l, b, deg, true);
+  smooth<T>(c, L, l, b, deg, true, first_done);
   // residual into r (smooth() used r as scratch; done with it now)
   mg_residual<T>(c, L, l, b, B::x(L), B::r(L));
+  // the coarse level's first smoothing step rides on the restriction when
+  // that level is smoothed with the shared rediscretised bound
+  const bool fuse = l + 1 < levels - 1 && !c->mg_galerkin;
+  const double lm = c->lam_max_dk, theta = 0.5 * (lm + 0.1 * lm);
   note_launch();
-  k_restrict<<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, B::r(L), C.fix,
-                                                                B::b(C));
-  vcycle<T>(c, l + 1, B::b(C), deg);
+  k_restrict<<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(
+      L.g, C.g, B::r(L), C.fix, B::b(C), B::invd(C), T(1.0 / theta), fuse ? B::x(C) : nullptr,
+      B::r(C));
+  vcycle<T>(c, l + 1, B::b(C), deg, fuse);
   note_launch();
   k_prolong_add<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, B::x(C),
                                                                    L.fix, B::x(L));
