@@ -80,10 +80,34 @@ __global__ void k_filter_fwd(ElemGrid g, int nofs, const int *__restrict__ ofs,
   }
 }
 
+// n / b rounded to nearest from y = RN(1 / b): q0 = RN(n y) is within one ulp
+// of n / b, the remainder n - b q0 is exact in one FMA, and RN(q0 + r y) is
+// the correctly rounded quotient (Markstein's theorem: P. Markstein, "Computation
+// of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34 (1990); Muller et al., Handbook of Floating-Point Arithmetic, on
+// division with a fused multiply-add), for normal operands as here (sums of
+// positive filter weights, finite terms).  Two FMAs and a product instead of
+// a full division per term; the transposed filters stay bit-identical to the
+// per-term division of the reference.
+__device__ __forceinline__ double div_by_recip(double n, double b, double y)
+{
+  const double q0 = __dmul_rn(n, y);
+  const double r = __fma_rn(-q0, b, n);
+  return __fma_rn(r, y, q0);
+}
+
+// ra = RN(1 / aa) (IEEE division, once per filter set-up)
+__global__ void k_filter_recip(int n, const double *__restrict__ aa, double *__restrict__ ra)
+{
+  for(int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    ra[e] = __ddiv_rn(1.0, aa[e]);
+}
+
 // transposed: out_i = sum_j w_ij in_j / a_j   (filter.hpp:145-152)
 __global__ void k_filter_trans(ElemGrid g, int nofs, const int *__restrict__ ofs,
                                const double *__restrict__ w,
                                const double *__restrict__ aa,
+                               const double *__restrict__ ra,
                                const double *__restrict__ in,
                                double *__restrict__ out)
 {
@@ -105,7 +129,7 @@ __global__ void k_filter_trans(ElemGrid g, int nofs, const int *__restrict__ ofs
       const long f = ii + (long)jj * g.nx + (long)kk * g.nx * g.ny;
       if(g.mask && !g.mask[f])
         continue;
-      s = __dadd_rn(s, __ddiv_rn(__dmul_rn(w[q], __ldg(in + f)), __ldg(aa + f)));
+      s = __dadd_rn(s, div_by_recip(__dmul_rn(w[q], __ldg(in + f)), __ldg(aa + f), __ldg(ra + f)));
     }
     out[e] = s;
   }
@@ -116,6 +140,7 @@ __global__ void k_filter_trans(ElemGrid g, int nofs, const int *__restrict__ ofs
 // output summed in the order and with the operations of k_filter_trans
 __global__ void k_filter_trans2(ElemGrid g, int nofs, const int *__restrict__ ofs,
                                 const double *__restrict__ w, const double *__restrict__ aa,
+                                const double *__restrict__ ra,
                                 const double *__restrict__ in1, const double *__restrict__ in2,
                                 double *__restrict__ out1, double *__restrict__ out2)
 {
@@ -138,9 +163,9 @@ __global__ void k_filter_trans2(ElemGrid g, int nofs, const int *__restrict__ of
       const long f = ii + (long)jj * g.nx + (long)kk * g.nx * g.ny;
       if(g.mask && !g.mask[f])
         continue;
-      const double wq = w[q], af = __ldg(aa + f);
-      s1 = __dadd_rn(s1, __ddiv_rn(__dmul_rn(wq, __ldg(in1 + f)), af));
-      s2 = __dadd_rn(s2, __ddiv_rn(__dmul_rn(wq, __ldg(in2 + f)), af));
+      const double wq = w[q], af = __ldg(aa + f), rf = __ldg(ra + f);
+      s1 = __dadd_rn(s1, div_by_recip(__dmul_rn(wq, __ldg(in1 + f)), af, rf));
+      s2 = __dadd_rn(s2, div_by_recip(__dmul_rn(wq, __ldg(in2 + f)), af, rf));
     }
     out1[e] = s1;
     out2[e] = s2;
@@ -211,6 +236,7 @@ void filter_free(icarat_ctx *c)
   dfree(c->filt.d_ofs);
   dfree(c->filt.d_w);
   dfree(c->filt.d_aa);
+  dfree(c->filt.d_ra);
   c->filt = FilterState{};
 }
 
@@ -248,6 +274,9 @@ void filter_setup(icarat_ctx *c, double R)
   note_launch();
   k_filter_aa<<<eblocks(c), 256, 0, c->stream>>>(egrid(c), F.nofs, F.d_ofs, F.d_w,
                                                  F.d_aa);
+  F.d_ra = dalloc(c->nelx);
+  note_launch();
+  k_filter_recip<<<eblocks(c), 256, 0, c->stream>>>(c->nelx, F.d_aa, F.d_ra);
   ICK(cudaGetLastError());
   F.have_forward = false;
 }
@@ -273,7 +302,7 @@ void filter_apply(icarat_ctx *c, const double *in, double *out, bool is_sens)
              "transposed filter needs a forward call first (filter.hpp:140-153)");
     note_launch();
     k_filter_trans<<<eblocks(c), 256, 0, c->stream>>>(egrid(c), F.nofs, F.d_ofs,
-                                                      F.d_w, F.d_aa, in, out);
+                                                      F.d_w, F.d_aa, F.d_ra, in, out);
   }
   ICK(cudaGetLastError());
 }
@@ -288,7 +317,7 @@ void filter_trans2(icarat_ctx *c, const double *in1, const double *in2, double *
            "transposed filter needs a forward call first (filter.hpp:140-153)");
   note_launch();
   k_filter_trans2<<<eblocks(c), 256, 0, c->stream>>>(egrid(c), F.nofs, F.d_ofs, F.d_w, F.d_aa,
-                                                     in1, in2, out1, out2);
+                                                     F.d_ra, in1, in2, out1, out2);
   ICK(cudaGetLastError());
 }
 

@@ -243,6 +243,7 @@ struct FilterState
   int *d_ofs = nullptr;
   double *d_w = nullptr;
   double *d_aa = nullptr;       // nelx sums of weights (dfilters_ds)
+  double *d_ra = nullptr;       // nelx correctly rounded reciprocals 1 / aa
   bool have_forward = false;
 };
 

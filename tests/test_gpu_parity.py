@@ -267,6 +267,23 @@ def test_filter_bit_exact(oracle, gpu, R):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("R", [1.5, 2.5])
+def test_transposed_filter_bit_exact_wide_range(oracle, gpu, R):
+    """The transposed filter divides every term by its weight sum in the
+    reference's order; the GPU divides through a correctly rounded reciprocal
+    with one FMA correction (Markstein) and must still give the reference's
+    quotients exactly: 16 k elements, inputs of both signs spread over 16
+    decades, about a million divisions."""
+    P, G = pair(oracle, gpu, 40, 20, 20)
+    F = oracle.Filter(P, R)
+    G.filter_setup(R)
+    rng = np.random.default_rng(int(R * 100))
+    x = rng.uniform(0.0, 1.0, P.nelx)
+    assert np.array_equal(G.density_filter(x), F.density_filter(x))
+    g = rng.standard_normal(P.nelx) * 10.0 ** rng.uniform(-8.0, 8.0, P.nelx)
+    assert np.array_equal(G.density_filter(g, True), F.density_filter(g, True))
+
+
 def test_threshold_matches(oracle, gpu):
     G = gpu.Context(10, 5, 5)
     x = np.random.default_rng(2).uniform(0, 1, G.nelx)
