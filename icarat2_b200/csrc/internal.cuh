@@ -495,7 +495,7 @@ void mg_level_apply(icarat_ctx *c, const icarat_solve_opts *o, int level, const 
 // solve's work, side stream included, ends with the solve)
 void mg_join(icarat_ctx *c);
 double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse);
-void mg_vcycle(icarat_ctx *c, const double *r, double *z, int smooth);
+void mg_vcycle(icarat_ctx *c, const double *r, double *z, int smooth, bool first_done = false);
 void mg_vcycle_f32(icarat_ctx *c, const float *r, float *z, int smooth);
 void mg_free(icarat_ctx *c);
 

@@ -1053,9 +1053,9 @@ static void vcycle(icarat_ctx *c, int l, const T *b, int deg, bool first_done = 
   smooth<T>(c, L, l, b, deg, false);
 }
 
-void mg_vcycle(icarat_ctx *c, const double *r, double *z, int deg)
+void mg_vcycle(icarat_ctx *c, const double *r, double *z, int deg, bool first_done)
 {
-  vcycle<double>(c, 0, r, deg);
+  vcycle<double>(c, 0, r, deg, first_done);
   ICK(cudaMemcpyAsync(z, c->mg[0].x, sizeof(double) * c->neq, cudaMemcpyDeviceToDevice,
                       c->stream));
   ICK(cudaGetLastError());

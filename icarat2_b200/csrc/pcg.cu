@@ -234,11 +234,15 @@ __global__ void k_cg_update_jacobi(int n, const double *__restrict__ invd,
 }
 
 // MG: x += alpha p, r -= alpha Ap; ||r||, stop test (z comes from a V-cycle).
+// With x0 set, also the V-cycle's first Chebyshev step on the finest level
+// from zero (k_cheb_first fused): d0 = x0 = inv_theta invd0 r.
 __global__ void k_cg_update_r(int n, double *__restrict__ x,
                               double *__restrict__ r,
                               const double *__restrict__ p,
                               const double *__restrict__ Ap,
-                              double *__restrict__ partials, CgScalars *s)
+                              double *__restrict__ partials, CgScalars *s,
+                              const double *__restrict__ invd0, double inv_theta,
+                              double *__restrict__ x0, double *__restrict__ d0)
 {
   __shared__ double sh[32];
   if(s->done)
@@ -252,6 +256,12 @@ __global__ void k_cg_update_r(int n, double *__restrict__ x,
     const double ri = r[i] - alpha * Ap[i];
     r[i] = ri;
     rr += ri * ri;
+    if(x0)
+    {
+      const double di = inv_theta * invd0[i] * ri;
+      d0[i] = di;
+      x0[i] = di;
+    }
   }
   double v[1] = {rr};
   block_sum<1>(v, sh);
@@ -362,9 +372,12 @@ static void enqueue_iteration(icarat_ctx *c, int method, int smooth,
   else
   {
     note_launch();
+    // the update also takes the finest level's first smoothing step
+    MgLevel &L0 = c->mg[0];
+    const double lm = c->lam_max_dk, theta = 0.5 * (lm + 0.1 * lm);
     k_cg_update_r<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
-        n, x, c->d_r, c->d_p, c->d_Ap, c->d_partials, c->d_cg);
-    mg_vcycle(c, c->d_r, c->d_z, smooth);
+        n, x, c->d_r, c->d_p, c->d_Ap, c->d_partials, c->d_cg, L0.invd, 1.0 / theta, L0.x, L0.r);
+    mg_vcycle(c, c->d_r, c->d_z, smooth, true);
     note_launch();
     k_cg_zr<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->d_z, c->d_r,
                                                           c->d_partials, c->d_cg, 0);
