@@ -524,19 +524,43 @@ double galerkin_child_matrices(const double *ke0, double *G)
   return lam;
 }
 
-template __global__ void k_st_first<double>(int, const double *, const double *,
-                                            const double *, double *, double *);
-template __global__ void k_st_first<float>(int, const float *, const float *, const double *,
-                                           float *, float *);
-template __global__ void k_st_cheb<double>(GridDev, const double *, const uint8_t *,
-                                           const double *, const double *, const double *,
-                                           double *, double *, const double *, int);
-template __global__ void k_st_cheb<float>(GridDev, const float *, const uint8_t *,
-                                          const float *, const float *, const float *, float *,
-                                          float *, const double *, int);
-template __global__ void k_st_residual<double>(GridDev, const double *, const uint8_t *,
-                                               const double *, const double *, double *);
-template __global__ void k_st_residual<float>(GridDev, const float *, const uint8_t *,
-                                              const float *, const float *, float *);
+// host launches of the stencil-level kernels (the kernels stay in this
+// translation unit)
+template <typename T>
+void st_first_launch(cudaStream_t st, int n, const T *b, const T *invd, const double *coef,
+                     T *x, T *d)
+{
+  note_launch();
+  k_st_first<T><<<(n + 255) / 256, 256, 0, st>>>(n, b, invd, coef, x, d);
+}
+template <typename T>
+void st_cheb_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
+                    const T *invd, const T *b, const T *x, T *d, T *xo, const double *coef, int k)
+{
+  note_launch();
+  k_st_cheb<T><<<st_blocks(g.numnp), st_block(), 0, st>>>(g, S, fix, invd, b, x, d, xo, coef, k);
+}
+template <typename T>
+void st_residual_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
+                        const T *b, const T *x, T *r)
+{
+  note_launch();
+  k_st_residual<T><<<st_blocks(g.numnp), st_block(), 0, st>>>(g, S, fix, b, x, r);
+}
+template void st_first_launch<double>(cudaStream_t, int, const double *, const double *,
+                                      const double *, double *, double *);
+template void st_first_launch<float>(cudaStream_t, int, const float *, const float *,
+                                     const double *, float *, float *);
+template void st_cheb_launch<double>(cudaStream_t, const GridDev &, const double *,
+                                     const uint8_t *, const double *, const double *,
+                                     const double *, double *, double *, const double *, int);
+template void st_cheb_launch<float>(cudaStream_t, const GridDev &, const float *,
+                                    const uint8_t *, const float *, const float *, const float *,
+                                    float *, float *, const double *, int);
+template void st_residual_launch<double>(cudaStream_t, const GridDev &, const double *,
+                                         const uint8_t *, const double *, const double *,
+                                         double *);
+template void st_residual_launch<float>(cudaStream_t, const GridDev &, const float *,
+                                        const uint8_t *, const float *, const float *, float *);
 
 } // namespace icarat_b200

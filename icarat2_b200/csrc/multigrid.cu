@@ -50,20 +50,14 @@ __global__ void k_gal_coefs(int levels, const double *__restrict__ lmax, double 
                             double *__restrict__ coef);
 double galerkin_child_matrices(const double *ke0, double *G);
 template <typename T>
-__global__ void k_st_first(int n, const T *__restrict__ b, const T *__restrict__ invd,
-                           const double *__restrict__ coef, T *__restrict__ x,
-                           T *__restrict__ d);
+void st_first_launch(cudaStream_t st, int n, const T *b, const T *invd, const double *coef,
+                     T *x, T *d);
 template <typename T>
-__global__ void k_st_cheb(GridDev g, const T *__restrict__ S, const uint8_t *__restrict__ fix,
-                          const T *__restrict__ invd, const T *__restrict__ b,
-                          const T *__restrict__ x, T *__restrict__ d, T *__restrict__ xo,
-                          const double *__restrict__ coef, int k);
+void st_cheb_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
+                    const T *invd, const T *b, const T *x, T *d, T *xo, const double *coef, int k);
 template <typename T>
-__global__ void k_st_residual(GridDev g, const T *__restrict__ S,
-                              const uint8_t *__restrict__ fix, const T *__restrict__ b,
-                              const T *__restrict__ x, T *__restrict__ r);
-dim3 st_block();
-int st_blocks(int numnp);
+void st_residual_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
+                        const T *b, const T *x, T *r);
 __global__ void k_coarse_assemble_st(GridDev g, const double *__restrict__ S,
                                      const int *__restrict__ rowmap,
                                      const int *__restrict__ colmap, int nfree,
@@ -652,9 +646,7 @@ double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
   {
     // A x with the stencil: the residual of b = 0 is -A x
     ICK(cudaMemsetAsync(C.b, 0, sizeof(double) * nv, c->stream));
-    note_launch();
-    k_st_residual<double><<<st_blocks(C.g.numnp), st_block(), 0, c->stream>>>(C.g, C.S, C.fix,
-                                                                             C.b, C.x, C.t);
+    st_residual_launch<double>(c->stream, C.g, C.S, C.fix, C.b, C.x, C.t);
     ICK(cudaStreamSynchronize(c->stream));
     std::vector<double> tmp(nv);
     ICK(cudaMemcpy(tmp.data(), C.t, sizeof(double) * nv, cudaMemcpyDeviceToHost));
@@ -694,9 +686,7 @@ void mg_level_apply(icarat_ctx *c, const icarat_solve_opts *o, int level, const 
   if(level > 0 && c->mg_galerkin)
   {
     ICK(cudaMemsetAsync(L.b, 0, sizeof(double) * nv, c->stream));
-    note_launch();
-    k_st_residual<double><<<st_blocks(L.g.numnp), st_block(), 0, c->stream>>>(L.g, L.S, L.fix,
-                                                                             L.b, L.x, L.t);
+    st_residual_launch<double>(c->stream, L.g, L.S, L.fix, L.b, L.x, L.t);
     ICK(cudaMemcpyAsync(y, L.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
     ICK(cudaStreamSynchronize(c->stream));
     for(size_t i = 0; i < nv; i++)
@@ -894,9 +884,7 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
   using B = LevelBuf<T>;
   if(lvl > 0 && c->mg_galerkin)
   {
-    note_launch();
-    k_st_residual<T><<<st_blocks(L.g.numnp), st_block(), 0, c->stream>>>(L.g, B::S(L), L.fix, b,
-                                                                        x, r);
+    st_residual_launch<T>(c->stream, L.g, B::S(L), L.fix, b, x, r);
     return;
   }
   if(tc_level<T>(c, lvl))
@@ -948,24 +936,16 @@ static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool
     const double *coef = c->gal_coef + (size_t)lvl * kGalCoef;
     const int nv = 3 * L.g.numnp;
     T *x = B::x(L), *xo = B::t(L), *d = B::r(L);
-    const int nb = st_blocks(L.g.numnp);
     if(from_zero)
-    {
-      note_launch();
-      k_st_first<T><<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, B::invd(L), coef, x, d);
-    }
+      st_first_launch<T>(c->stream, nv, b, B::invd(L), coef, x, d);
     else
     {
-      note_launch();
-      k_st_cheb<T><<<nb, st_block(), 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
-                                               coef, 0);
+      st_cheb_launch<T>(c->stream, L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo, coef, 0);
       std::swap(x, xo);
     }
     for(int k = 1; k < deg; k++)
     {
-      note_launch();
-      k_st_cheb<T><<<nb, st_block(), 0, c->stream>>>(L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo,
-                                               coef, k);
+      st_cheb_launch<T>(c->stream, L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo, coef, k);
       std::swap(x, xo);
     }
     if(x != B::x(L))
