@@ -88,6 +88,7 @@ __device__ __forceinline__ void gemm_b_idx(int tb, int t, int &kr, int &jc)
 // the next chunk is fetched into registers while the current one is used.
 __global__ void __launch_bounds__(128) k_gemm_f64(GemmArgs g)
 {
+  chain_wait();
   const int tm = blockIdx.y, tn = blockIdx.x;
   if(g.lower && tn > tm)
     return;
@@ -236,6 +237,7 @@ __device__ __forceinline__ double rsqrt_newton(double x)
 
 __global__ void __launch_bounds__(256) k_potrf64(double *A, double *W, int n, int k0)
 {
+  chain_wait();
   extern __shared__ double potrf_smem[];
   double(*colbuf)[64] = reinterpret_cast<double(*)[64]>(potrf_smem); // [2][64] column j of a
   double(*rowbuf)[64] = colbuf + 2;                                  // [2][64] row j of e
@@ -344,21 +346,53 @@ __global__ void __launch_bounds__(256) k_potrf64(double *A, double *W, int n, in
     }
 }
 
+// The row a warp takes in the triangular products: even warps the short
+// rows from the top, odd warps the long ones from the bottom, so every pair
+// of neighbouring warps reads n + 1 coefficients and the blocks stay balanced.
+__device__ __forceinline__ int trmv_row(int warp, int n)
+{
+  return (warp & 1) ? n - 1 - (warp >> 1) : (warp >> 1);
+}
+
+// sum over q in [q0, q1) of row[q] v[q] by one warp: eight independent
+// partial sums per lane (eight coefficient loads in flight), summed in a
+// fixed order, then across the warp
+__device__ __forceinline__ double warp_row_dot(const double *__restrict__ row,
+                                               const double *__restrict__ v, int q0, int q1,
+                                               int lane)
+{
+  double s[8];
+#pragma unroll
+  for(int u = 0; u < 8; u++)
+    s[u] = 0.0;
+  int q = q0 + lane;
+  for(; q + 224 < q1; q += 256)
+#pragma unroll
+    for(int u = 0; u < 8; u++)
+      s[u] = fma(row[q + 32 * u], v[q + 32 * u], s[u]);
+  for(; q < q1; q += 32)
+    s[0] = fma(row[q], v[q], s[0]);
+  double a = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
+  for(int o = 16; o > 0; o >>= 1)
+    a += __shfl_down_sync(0xffffffffu, a, o);
+  return a;
+}
+
 // t = W v (W lower triangular), one warp per row
 __global__ void k_trmv_lower(int n, const double *__restrict__ W,
-                             const double *__restrict__ v, double *__restrict__ t)
+                             const double *__restrict__ v, double *__restrict__ t,
+                             const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  for(int r = warp; r < n; r += nw)
+  for(int w = warp; w < n; w += nw)
   {
-    const double *row = W + (long)r * n;
-    double s = 0.0;
-    for(int q = lane; q <= r; q += 32)
-      s = fma(row[q], v[q], s);
-    for(int o = 16; o > 0; o >>= 1)
-      s += __shfl_down_sync(0xffffffffu, s, o);
+    const int r = trmv_row(w, n);
+    const double s = warp_row_dot(W + (long)r * n, v, 0, r + 1, lane);
     if(lane == 0)
       t[r] = s;
   }
@@ -368,6 +402,7 @@ __global__ void k_trmv_lower(int n, const double *__restrict__ W,
 __global__ void k_transpose_lower(int n, const double *__restrict__ W,
                                   double *__restrict__ WT)
 {
+  chain_wait();
   __shared__ double tile[32][33];
   const int bi = blockIdx.y * 32, bj = blockIdx.x * 32; // source tile rows / cols
   if(bj > bi + 31)
@@ -389,19 +424,18 @@ __global__ void k_transpose_lower(int n, const double *__restrict__ W,
 // x[rowmap] = WT t (WT upper), one warp per row; rows are contiguous
 __global__ void k_trmv_upper(int n, const double *__restrict__ WT,
                              const double *__restrict__ t, const int *__restrict__ rowmap,
-                             double *__restrict__ x)
+                             double *__restrict__ x, const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  for(int r = warp; r < n; r += nw)
+  for(int w = warp; w < n; w += nw)
   {
-    const double *row = WT + (long)r * n;
-    double s = 0.0;
-    for(int q = r + lane; q < n; q += 32)
-      s = fma(row[q], t[q], s);
-    for(int o = 16; o > 0; o >>= 1)
-      s += __shfl_down_sync(0xffffffffu, s, o);
+    const int r = trmv_row(w, n);
+    const double s = warp_row_dot(WT + (long)r * n, t, r, n, lane);
     if(lane == 0)
       x[rowmap[r]] = s;
   }
@@ -418,7 +452,7 @@ static void gemm(cudaStream_t st, int M, int N, int K, double alpha, const doubl
              B,   ldb, tb, C,    ldc,  lower, a_lower, b_lower, 0, 0, 0, 0, 0, 0};
   dim3 grid((N + 63) / 64, (M + 63) / 64);
   note_launch();
-  k_gemm_f64<<<grid, 128, 0, st>>>(g);
+  launch_chained(k_gemm_f64, grid, 128, 0, st, g);
 }
 
 // W = L^-1 from the diagonal blocks W_kk by doubling: at block size s every
@@ -445,11 +479,11 @@ static void trinv_banded(cudaStream_t st, const double *L, double *W, double *T,
     // T_z = L21 W11 (rows clipped to the short second block of the last pair)
     GemmArgs g1{r, s, k, 1.0, 0.0, L + (long)s * n + s - k, n, 0, W + (long)(s - k) * n, n, 0,
                 T, s, 0, 0, 0, step, step, tslab, n - s, 2 * s, 0};
-    k_gemm_f64<<<dim3((s + 63) / 64, (r + 63) / 64, pairs), 128, 0, st>>>(g1);
+    launch_chained(k_gemm_f64, dim3((s + 63) / 64, (r + 63) / 64, pairs), 128, 0, st, g1);
     // W21_z = -W22 T_z (K clipped like the rows: W22 has s2 columns)
     GemmArgs g2{s, s, r, -1.0, 0.0, W + (long)s * n + s, n, 0, T, s, 0, W + (long)s * n, n,
                 0, 1, 0, step, tslab, step, n - s, 2 * s, 1};
-    k_gemm_f64<<<dim3((s + 63) / 64, (s + 63) / 64, pairs), 128, 0, st>>>(g2);
+    launch_chained(k_gemm_f64, dim3((s + 63) / 64, (s + 63) / 64, pairs), 128, 0, st, g2);
   }
 }
 
@@ -469,7 +503,7 @@ void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, 
   {
     const int k0 = k * 64;
     note_launch();
-    k_potrf64<<<1, 256, kPotrfSmem, st>>>(A, W, n, k0);
+    launch_chained(k_potrf64, 1, 256, kPotrfSmem, st, A, W, n, k0);
     const int rest = std::min(n - k0 - 64, bw);
     if(rest > 0)
     {
@@ -484,17 +518,21 @@ void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, 
   }
   trinv_banded(st, A, W, T, n, bw);
   note_launch();
-  k_transpose_lower<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, st>>>(n, W, T);
+  launch_chained(k_transpose_lower, dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, st, n,
+                 (const double *)W, T);
   ICK(cudaGetLastError());
 }
 
-// x[rowmap] = W^T W b[rowmap]  (WT = W^T from dense_spd_inverse_factor)
+// x[rowmap] = W^T W b[rowmap]  (WT = W^T from dense_spd_inverse_factor); both
+// products return at entry while *halt != 0 (halt null: never)
 void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
-                     const double *v, double *t, const int *rowmap, double *x)
+                     const double *v, double *t, const int *rowmap, double *x,
+                     const int *halt)
 {
   note_launch(2);
-  k_trmv_lower<<<(n * 32 + 255) / 256, 256, 0, st>>>(n, W, v, t);
-  k_trmv_upper<<<(n * 32 + 255) / 256, 256, 0, st>>>(n, WT, t, rowmap, x);
+  const int blocks = (n * 32 + 255) / 256;
+  launch_chained(k_trmv_lower, blocks, 256, 0, st, n, W, v, t, halt);
+  launch_chained(k_trmv_upper, blocks, 256, 0, st, n, WT, t, rowmap, x, halt);
 }
 
 } // namespace icarat_b200

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(dm::kThreads, 2) k_ku_dmma(DmArgs a)
   using namespace dm;
   extern __shared__ __align__(16) uint8_t dm_smem_raw[];
   Smem &sm = *reinterpret_cast<Smem *>(dm_smem_raw);
-  if(OP == TC_DOT && a.s->done)
+  if(halted(a.halt) || (OP == TC_DOT && a.s->done))
     return;
   const int t = threadIdx.x, w = t >> 5, l = t & 31;
   const int q = l & 3, r = l >> 2;

@@ -376,8 +376,11 @@ __device__ __forceinline__ bool stencil_row(const GridDev &g, const T *__restric
 template <typename T>
 __global__ void k_st_first(int n, const T *__restrict__ b, const T *__restrict__ invd,
                            const double *__restrict__ coef, T *__restrict__ x,
-                           T *__restrict__ d)
+                           T *__restrict__ d, const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   const T it = T(coef[0]);
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
   {
@@ -393,8 +396,12 @@ template <typename T>
 __global__ void __launch_bounds__(kStNodes * 9, 3)
     k_st_cheb(GridDev g, const T *__restrict__ S, const uint8_t *__restrict__ fix,
               const T *__restrict__ invd, const T *__restrict__ b, const T *__restrict__ x,
-              T *__restrict__ d, T *__restrict__ xo, const double *__restrict__ coef, int k)
+              T *__restrict__ d, T *__restrict__ xo, const double *__restrict__ coef, int k,
+              const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   __shared__ double ps[9][kStNodes];
   const T c1 = k == 0 ? T(0) : T(coef[2 * k - 1]);
   const T c2 = k == 0 ? T(coef[0]) : T(coef[2 * k]);
@@ -418,8 +425,12 @@ __global__ void __launch_bounds__(kStNodes * 9, 3)
 template <typename T>
 __global__ void __launch_bounds__(kStNodes * 9, 3)
     k_st_residual(GridDev g, const T *__restrict__ S, const uint8_t *__restrict__ fix,
-                  const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ r)
+                  const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ r,
+                  const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   __shared__ double ps[9][kStNodes];
   const int q = threadIdx.y / 3;
   for(int nb = blockIdx.x * kStNodes; nb < g.numnp; nb += gridDim.x * kStNodes)
@@ -525,42 +536,47 @@ double galerkin_child_matrices(const double *ke0, double *G)
 }
 
 // host launches of the stencil-level kernels (the kernels stay in this
-// translation unit)
+// translation unit); halt: the V-cycle stop flag (null: never stop)
 template <typename T>
 void st_first_launch(cudaStream_t st, int n, const T *b, const T *invd, const double *coef,
-                     T *x, T *d)
+                     T *x, T *d, const int *halt)
 {
   note_launch();
-  k_st_first<T><<<(n + 255) / 256, 256, 0, st>>>(n, b, invd, coef, x, d);
+  launch_chained(k_st_first<T>, (n + 255) / 256, 256, 0, st, n, b, invd, coef, x, d, halt);
 }
 template <typename T>
 void st_cheb_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
-                    const T *invd, const T *b, const T *x, T *d, T *xo, const double *coef, int k)
+                    const T *invd, const T *b, const T *x, T *d, T *xo, const double *coef, int k,
+                    const int *halt)
 {
   note_launch();
-  k_st_cheb<T><<<st_blocks(g.numnp), st_block(), 0, st>>>(g, S, fix, invd, b, x, d, xo, coef, k);
+  launch_chained(k_st_cheb<T>, st_blocks(g.numnp), st_block(), 0, st, g, S, fix, invd, b, x, d,
+                 xo, coef, k, halt);
 }
 template <typename T>
 void st_residual_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
-                        const T *b, const T *x, T *r)
+                        const T *b, const T *x, T *r, const int *halt)
 {
   note_launch();
-  k_st_residual<T><<<st_blocks(g.numnp), st_block(), 0, st>>>(g, S, fix, b, x, r);
+  launch_chained(k_st_residual<T>, st_blocks(g.numnp), st_block(), 0, st, g, S, fix, b, x, r,
+                 halt);
 }
 template void st_first_launch<double>(cudaStream_t, int, const double *, const double *,
-                                      const double *, double *, double *);
+                                      const double *, double *, double *, const int *);
 template void st_first_launch<float>(cudaStream_t, int, const float *, const float *,
-                                     const double *, float *, float *);
+                                     const double *, float *, float *, const int *);
 template void st_cheb_launch<double>(cudaStream_t, const GridDev &, const double *,
                                      const uint8_t *, const double *, const double *,
-                                     const double *, double *, double *, const double *, int);
+                                     const double *, double *, double *, const double *, int,
+                                     const int *);
 template void st_cheb_launch<float>(cudaStream_t, const GridDev &, const float *,
                                     const uint8_t *, const float *, const float *, const float *,
-                                    float *, float *, const double *, int);
+                                    float *, float *, const double *, int, const int *);
 template void st_residual_launch<double>(cudaStream_t, const GridDev &, const double *,
                                          const uint8_t *, const double *, const double *,
-                                         double *);
+                                         double *, const int *);
 template void st_residual_launch<float>(cudaStream_t, const GridDev &, const float *,
-                                        const uint8_t *, const float *, const float *, float *);
+                                        const uint8_t *, const float *, const float *, float *,
+                                        const int *);
 
 } // namespace icarat_b200

@@ -75,6 +75,42 @@ void set_capturing(bool on);
       throw ::icarat_b200::Error{status, msg};                                  \
   } while(0)
 
+// Programmatic dependent launch.  A kernel launched by launch_chained() may
+// be scheduled while the kernel before it in the stream is still draining
+// (its launch overlaps the predecessor's tail and completion); every such
+// kernel calls chain_wait() before its first global memory access, which
+// returns once the predecessor has completed and its writes are visible
+// (griddepcontrol.wait, a no-op in a kernel launched without the attribute).
+// Nothing triggers dependents early: a dependent is scheduled only after
+// every block of its predecessor has exited.
+__device__ __forceinline__ void chain_wait()
+{
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// the stop flag of a V-cycle kernel (null: never stop)
+__device__ __forceinline__ bool halted(const int *halt)
+{
+  return halt != nullptr && *halt != 0;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                           cudaStream_t st, Args... args)
+{
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ICK(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+}
+
 // Element stiffness (E = 1), passed by value as a kernel parameter: every
 // coefficient index is a compile-time constant after unrolling, so the
 // 576 entries are read as uniform constant-bank operands.
@@ -152,6 +188,7 @@ struct TcArgs
   double *partials = nullptr;
   MxScalars *s = nullptr;
   int *err = nullptr;
+  const int *halt = nullptr; // return at entry while *halt != 0
 };
 
 // Arguments of the FP64 tensor-core element-by-element operator
@@ -170,6 +207,7 @@ struct DmArgs
   double *partials = nullptr;
   CgScalars *s = nullptr;
   int tiles_x = 0, tiles = 0, kc = 0; // tiles along x, tiles, node layers per CTA
+  const int *halt = nullptr;          // return at entry while *halt != 0
 };
 
 // Kernel attributes (the dynamic shared-memory limit) and occupancies are per
@@ -368,6 +406,11 @@ struct icarat_ctx
   // multigrid
   std::vector<icarat_b200::MgLevel> mg;
   int mg_built_levels = 0;
+  // device stop flag of the Krylov iteration whose V-cycles are being
+  // enqueued (its scalars' done field; null outside one): the V-cycle
+  // kernels return at entry once it is set, so the iterations a graph chunk
+  // holds past convergence cost launches only
+  const int *mg_halt = nullptr;
   // Galerkin coarse operators: requested by the current solve's options,
   // and built into the hierarchy (which is rebuilt when they differ)
   int mg_galerkin_req = 0, mg_galerkin = 0;
@@ -495,8 +538,19 @@ void mg_level_apply(icarat_ctx *c, const icarat_solve_opts *o, int level, const 
 // solve's work, side stream included, ends with the solve)
 void mg_join(icarat_ctx *c);
 double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse);
+// z = M r by one V-cycle (z null: the result stays in the finest level's x)
 void mg_vcycle(icarat_ctx *c, const double *r, double *z, int smooth, bool first_done = false);
 void mg_vcycle_f32(icarat_ctx *c, const float *r, float *z, int smooth);
+// the context's V-cycle stop flag (icarat_ctx::mg_halt) for one scope
+struct HaltScope
+{
+  icarat_ctx *c;
+  const int *prev;
+  HaltScope(icarat_ctx *c_, const int *h) : c(c_), prev(c_->mg_halt) { c->mg_halt = h; }
+  ~HaltScope() { c->mg_halt = prev; }
+  HaltScope(const HaltScope &) = delete;
+  HaltScope &operator=(const HaltScope &) = delete;
+};
 void mg_free(icarat_ctx *c);
 
 // filter.cu

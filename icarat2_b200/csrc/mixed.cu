@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(128)
               const uint8_t *__restrict__ fix, const float *__restrict__ p,
               float *__restrict__ Ap, double *__restrict__ partials, MxScalars *s)
 {
+  chain_wait();
   __shared__ double sh[32];
   if(s->done)
     return;
@@ -198,6 +199,7 @@ __global__ void k_mx_update(int n, float *__restrict__ x32, float *__restrict__ 
                             const float *__restrict__ p, const float *__restrict__ Ap,
                             double *__restrict__ partials, MxScalars *s)
 {
+  chain_wait();
   __shared__ double sh[32];
   if(s->done)
     return;
@@ -245,6 +247,7 @@ __global__ void k_mx_update(int n, float *__restrict__ x32, float *__restrict__ 
 __global__ void k_mx_flush(int n, double *__restrict__ x, float *__restrict__ x32,
                            const MxScalars *s)
 {
+  chain_wait();
   if(s->done || !s->refresh)
     return;
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -261,6 +264,7 @@ __global__ void __launch_bounds__(128)
                   const double *__restrict__ x, float *__restrict__ r32,
                   double *__restrict__ partials, MxScalars *s)
 {
+  chain_wait();
   __shared__ double sh[32];
   if(s->done || !s->refresh)
     return;
@@ -333,6 +337,7 @@ __global__ void k_mx_zr(int n, const float *__restrict__ z, const float *__restr
                         const float *__restrict__ Ap, double *__restrict__ partials,
                         MxScalars *s, int first)
 {
+  chain_wait();
   __shared__ double sh[64];
   if(s->done)
     return;
@@ -368,6 +373,7 @@ __global__ void k_mx_zr(int n, const float *__restrict__ z, const float *__restr
 __global__ void k_mx_pupdate(int n, const float *__restrict__ z, float *__restrict__ p,
                              const MxScalars *s, int first)
 {
+  chain_wait();
   if(s->done)
     return;
   const float beta = (float)s->beta;
@@ -483,12 +489,15 @@ static int spmv_blocks(const icarat_ctx *c)
 static void enqueue_precondition(icarat_ctx *c, int smooth, int first)
 {
   const int n = c->neq;
-  mg_vcycle_f32(c, c->f_r, c->f_z, smooth);
+  // z stays in the finest level's x32 (read by z . r and the p update
+  // before the next V-cycle overwrites it)
+  mg_vcycle_f32(c, c->f_r, nullptr, smooth);
+  const float *z = c->mg[0].x32;
   note_launch(2);
-  k_mx_zr<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_z, c->f_r, c->f_Ap,
-                                                        c->d_partials, c->d_mx, first);
-  k_mx_pupdate<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_z, c->f_p, c->d_mx,
-                                                             first);
+  launch_chained(k_mx_zr, c->red_blocks, kRedThreads, 0, c->stream, n, z, c->f_r, c->f_Ap,
+                 c->d_partials, c->d_mx, first);
+  launch_chained(k_mx_pupdate, c->red_blocks, kRedThreads, 0, c->stream, n, z, c->f_p,
+                 c->d_mx, first);
 }
 
 // K p, the updates of x32 and r, and the FP64 refresh when one is due
@@ -510,8 +519,9 @@ static void enqueue_krylov_step(icarat_ctx *c, int krylov_op, const double *b, d
     int blocks;
     const MarchPlan m = march_launch(L.g, (const void *)k_mx_spmv, 128, c->sm_count, blocks);
     note_launch();
-    k_mx_spmv<<<blocks < kMaxRedBlocks ? blocks : kMaxRedBlocks, 128, 0, c->stream>>>(
-        L.g, m, c->ke0f, L.E32, L.fix, c->f_p, c->f_Ap, c->d_partials, c->d_mx);
+    launch_chained(k_mx_spmv, blocks < kMaxRedBlocks ? blocks : kMaxRedBlocks, 128, 0,
+                   c->stream, L.g, m, c->ke0f, L.E32, L.fix, c->f_p, c->f_Ap, c->d_partials,
+                   c->d_mx);
   }
   else
   {
@@ -526,15 +536,15 @@ static void enqueue_krylov_step(icarat_ctx *c, int krylov_op, const double *b, d
     launch_ku_tc(c, TC_DOT, krylov_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
   }
   note_launch(3);
-  k_mx_update<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->f_x, c->f_r, c->f_p,
-                                                            c->f_Ap, c->d_partials,
-                                                            c->d_mx);
-  k_mx_flush<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, x, c->f_x, c->d_mx);
+  launch_chained(k_mx_update, c->red_blocks, kRedThreads, 0, c->stream, n, c->f_x, c->f_r,
+                 c->f_p, c->f_Ap, c->d_partials, c->d_mx);
+  launch_chained(k_mx_flush, c->red_blocks, kRedThreads, 0, c->stream, n, x, c->f_x, c->d_mx);
   int rblocks;
   const MarchPlan rm =
       march_launch(L.g, (const void *)k_mx_residual, 128, c->sm_count, rblocks);
-  k_mx_residual<<<rblocks < kMaxRedBlocks ? rblocks : kMaxRedBlocks, 128, 0, c->stream>>>(
-      L.g, rm, c->ke0, c->d_E, L.fix, b, x, c->f_r, c->d_partials, c->d_mx);
+  launch_chained(k_mx_residual, rblocks < kMaxRedBlocks ? rblocks : kMaxRedBlocks, 128, 0,
+                 c->stream, L.g, rm, c->ke0, c->d_E, L.fix, b, (const double *)x, c->f_r,
+                 c->d_partials, c->d_mx);
 }
 
 static const MxScalars &read_scalars(icarat_ctx *c)
@@ -574,6 +584,8 @@ void mixed_begin(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b, d
   c->mg_galerkin_req = o->coarse_op == ICARAT_COARSE_GALERKIN ? 1 : 0;
   mg_setup(c, levels, o->coarse_lag != 0);
   mixed_alloc(c);
+  // the V-cycles enqueued and captured here stop with the iteration
+  HaltScope halt(c, &c->d_mx->done);
   const int n = c->neq;
   const double nfree = c->numeq > 0 ? (double)c->numeq : 1.0;
   if(learned)

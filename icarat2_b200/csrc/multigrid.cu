@@ -33,7 +33,8 @@ namespace icarat_b200
 
 void dense_spd_inverse_factor(cudaStream_t st, double *A, double *W, double *T, int n, int bw);
 void dense_spd_solve(cudaStream_t st, const double *W, const double *WT, int n,
-                     const double *v, double *t, const int *rowmap, double *x);
+                     const double *v, double *t, const int *rowmap, double *x,
+                     const int *halt = nullptr);
 
 // Galerkin coarse operators (galerkin.cu)
 __global__ void k_gal_cells_free(GridDev f, GridDev c, const double *__restrict__ E,
@@ -51,13 +52,14 @@ __global__ void k_gal_coefs(int levels, const double *__restrict__ lmax, double 
 double galerkin_child_matrices(const double *ke0, double *G);
 template <typename T>
 void st_first_launch(cudaStream_t st, int n, const T *b, const T *invd, const double *coef,
-                     T *x, T *d);
+                     T *x, T *d, const int *halt);
 template <typename T>
 void st_cheb_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
-                    const T *invd, const T *b, const T *x, T *d, T *xo, const double *coef, int k);
+                    const T *invd, const T *b, const T *x, T *d, T *xo, const double *coef, int k,
+                    const int *halt);
 template <typename T>
 void st_residual_launch(cudaStream_t st, const GridDev &g, const T *S, const uint8_t *fix,
-                        const T *b, const T *x, T *r);
+                        const T *b, const T *x, T *r, const int *halt);
 __global__ void k_coarse_assemble_st(GridDev g, const double *__restrict__ S,
                                      const int *__restrict__ rowmap,
                                      const int *__restrict__ colmap, int nfree,
@@ -87,6 +89,7 @@ __global__ void k_coarsen_E(GridDev f, GridDev c, const double *__restrict__ Ef,
 template <typename Tin, typename Tout>
 __global__ void k_cast(long n, const Tin *__restrict__ in, Tout *__restrict__ out)
 {
+  chain_wait();
   for(long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
       i += (long)gridDim.x * blockDim.x)
     out[i] = (Tout)in[i];
@@ -101,8 +104,11 @@ template <typename T>
 __global__ void k_restrict(GridDev f, GridDev c, const T *__restrict__ rf,
                            const uint8_t *__restrict__ fixc, T *__restrict__ bc,
                            const T *__restrict__ invd_c, T inv_theta, T *__restrict__ xc,
-                           T *__restrict__ dc)
+                           T *__restrict__ dc, const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.numnp;
       n += gridDim.x * blockDim.x)
   {
@@ -128,8 +134,12 @@ __global__ void k_restrict(GridDev f, GridDev c, const T *__restrict__ rf,
 // fine x += P xc (masked)
 template <typename T>
 __global__ void k_prolong_add(GridDev f, GridDev c, const T *__restrict__ xc,
-                              const uint8_t *__restrict__ fixf, T *__restrict__ xf)
+                              const uint8_t *__restrict__ fixf, T *__restrict__ xf,
+                              const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   for(int n = blockIdx.x * blockDim.x + threadIdx.x; n < f.numnp;
       n += gridDim.x * blockDim.x)
   {
@@ -147,8 +157,12 @@ __global__ void k_prolong_add(GridDev f, GridDev c, const T *__restrict__ xc,
 // First Chebyshev step from x = 0: d = invd b / theta, x = d.
 template <typename T>
 __global__ void k_cheb_first(int n, const T *__restrict__ b, const T *__restrict__ invd,
-                             T inv_theta, T *__restrict__ x, T *__restrict__ d)
+                             T inv_theta, T *__restrict__ x, T *__restrict__ d,
+                             const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
       i += gridDim.x * blockDim.x)
   {
@@ -165,8 +179,11 @@ __global__ void __launch_bounds__(128)
     k_cheb_step(GridDev g, MarchPlan m, KP ke, const T *__restrict__ E,
                 const uint8_t *__restrict__ fix, const T *__restrict__ invd,
                 const T *__restrict__ b, const T *__restrict__ x, T *__restrict__ d,
-                T *__restrict__ xo, T c1, T c2)
+                T *__restrict__ xo, T c1, T c2, const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
       t += (long)gridDim.x * blockDim.x)
   {
@@ -197,8 +214,11 @@ template <typename T, typename KP>
 __global__ void __launch_bounds__(128)
     k_mg_residual(GridDev g, MarchPlan m, KP ke, const T *__restrict__ E,
                   const uint8_t *__restrict__ fix, const T *__restrict__ b,
-                  const T *__restrict__ x, T *__restrict__ r)
+                  const T *__restrict__ x, T *__restrict__ r, const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   for(long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < m.items;
       t += (long)gridDim.x * blockDim.x)
   {
@@ -262,8 +282,12 @@ __global__ void k_coarse_assemble(GridDev g, KeParam ke, const double *__restric
 // free coarse components of b (any precision) into the dense solve's vector
 template <typename T>
 __global__ void k_coarse_gather(int nfree, const int *__restrict__ rowmap,
-                                const T *__restrict__ b, double *__restrict__ v)
+                                const T *__restrict__ b, double *__restrict__ v,
+                                const int *__restrict__ halt)
 {
+  chain_wait();
+  if(halted(halt))
+    return;
   for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree;
       r += gridDim.x * blockDim.x)
     v[r] = (double)b[rowmap[r]];
@@ -646,7 +670,7 @@ double mg_coarse_check(icarat_ctx *c, int levels, int *n_coarse)
   {
     // A x with the stencil: the residual of b = 0 is -A x
     ICK(cudaMemsetAsync(C.b, 0, sizeof(double) * nv, c->stream));
-    st_residual_launch<double>(c->stream, C.g, C.S, C.fix, C.b, C.x, C.t);
+    st_residual_launch<double>(c->stream, C.g, C.S, C.fix, C.b, C.x, C.t, nullptr);
     ICK(cudaStreamSynchronize(c->stream));
     std::vector<double> tmp(nv);
     ICK(cudaMemcpy(tmp.data(), C.t, sizeof(double) * nv, cudaMemcpyDeviceToHost));
@@ -686,7 +710,7 @@ void mg_level_apply(icarat_ctx *c, const icarat_solve_opts *o, int level, const 
   if(level > 0 && c->mg_galerkin)
   {
     ICK(cudaMemsetAsync(L.b, 0, sizeof(double) * nv, c->stream));
-    st_residual_launch<double>(c->stream, L.g, L.S, L.fix, L.b, L.x, L.t);
+    st_residual_launch<double>(c->stream, L.g, L.S, L.fix, L.b, L.x, L.t, nullptr);
     ICK(cudaMemcpyAsync(y, L.t, sizeof(double) * nv, cudaMemcpyDeviceToHost, c->stream));
     ICK(cudaStreamSynchronize(c->stream));
     for(size_t i = 0; i < nv; i++)
@@ -848,6 +872,7 @@ static void cheb_step(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x
     a.d = reinterpret_cast<float *>(d);
     a.c1 = (float)c1;
     a.c2 = (float)c2;
+    a.halt = c->mg_halt;
     launch_ku_tc(c, TC_CHEB, c->mx_fine_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
     return;
   }
@@ -865,6 +890,7 @@ static void cheb_step(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x
       a.d = d;
       a.c1 = c1;
       a.c2 = c2;
+      a.halt = c->mg_halt;
       launch_ku_dmma(c, TC_CHEB, a, c->stream);
       return;
     }
@@ -873,8 +899,8 @@ static void cheb_step(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T *x
       march_launch(L.g, (const void *)k_cheb_step<T, typename KeOf<T>::type>, 128,
                    c->sm_count, blocks);
   note_launch();
-  k_cheb_step<<<blocks, 128, 0, c->stream>>>(L.g, m, B::ke(c), B::E(L), L.fix, B::invd(L), b,
-                                             x, d, xo, T(c1), T(c2));
+  launch_chained(k_cheb_step<T, typename KeOf<T>::type>, blocks, 128, 0, c->stream, L.g, m,
+                 B::ke(c), B::E(L), L.fix, B::invd(L), b, x, d, xo, T(c1), T(c2), c->mg_halt);
 }
 
 // r = b - K x on level lvl
@@ -884,7 +910,7 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
   using B = LevelBuf<T>;
   if(lvl > 0 && c->mg_galerkin)
   {
-    st_residual_launch<T>(c->stream, L.g, B::S(L), L.fix, b, x, r);
+    st_residual_launch<T>(c->stream, L.g, B::S(L), L.fix, b, x, r, c->mg_halt);
     return;
   }
   if(tc_level<T>(c, lvl))
@@ -896,6 +922,7 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
     a.u = reinterpret_cast<const float *>(x);
     a.y = reinterpret_cast<float *>(r);
     a.b = reinterpret_cast<const float *>(b);
+    a.halt = c->mg_halt;
     launch_ku_tc(c, TC_RESID, c->mx_fine_op == ICARAT_OP_TC_BF16X3 ? 3 : 1, a, c->stream);
     return;
   }
@@ -909,6 +936,7 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
       a.u = x;
       a.y = r;
       a.b = b;
+      a.halt = c->mg_halt;
       launch_ku_dmma(c, TC_RESID, a, c->stream);
       return;
     }
@@ -917,7 +945,8 @@ static void mg_residual(icarat_ctx *c, MgLevel &L, int lvl, const T *b, const T 
       march_launch(L.g, (const void *)k_mg_residual<T, typename KeOf<T>::type>, 128,
                    c->sm_count, blocks);
   note_launch();
-  k_mg_residual<<<blocks, 128, 0, c->stream>>>(L.g, m, B::ke(c), B::E(L), L.fix, b, x, r);
+  launch_chained(k_mg_residual<T, typename KeOf<T>::type>, blocks, 128, 0, c->stream, L.g, m,
+                 B::ke(c), B::E(L), L.fix, b, x, r, c->mg_halt);
 }
 
 // Chebyshev smoothing of K x = b on level lvl, deg steps.  from_zero: x = 0
@@ -937,15 +966,17 @@ static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool
     const int nv = 3 * L.g.numnp;
     T *x = B::x(L), *xo = B::t(L), *d = B::r(L);
     if(from_zero)
-      st_first_launch<T>(c->stream, nv, b, B::invd(L), coef, x, d);
+      st_first_launch<T>(c->stream, nv, b, B::invd(L), coef, x, d, c->mg_halt);
     else
     {
-      st_cheb_launch<T>(c->stream, L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo, coef, 0);
+      st_cheb_launch<T>(c->stream, L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo, coef, 0,
+                        c->mg_halt);
       std::swap(x, xo);
     }
     for(int k = 1; k < deg; k++)
     {
-      st_cheb_launch<T>(c->stream, L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo, coef, k);
+      st_cheb_launch<T>(c->stream, L.g, B::S(L), L.fix, B::invd(L), b, x, d, xo, coef, k,
+                        c->mg_halt);
       std::swap(x, xo);
     }
     if(x != B::x(L))
@@ -965,8 +996,8 @@ static void smooth(icarat_ctx *c, MgLevel &L, int lvl, const T *b, int deg, bool
     if(!first_done) // else the restriction that produced b took this step
     {
       note_launch();
-      k_cheb_first<<<blocks_for(nv, 256), 256, 0, c->stream>>>(nv, b, B::invd(L),
-                                                               T(1.0 / theta), x, d);
+      launch_chained(k_cheb_first<T>, blocks_for(nv, 256), 256, 0, c->stream, nv, b,
+                     B::invd(L), T(1.0 / theta), x, d, c->mg_halt);
     }
     k0 = 1;
   }
@@ -1001,16 +1032,16 @@ static void vcycle(icarat_ctx *c, int l, const T *b, int deg, bool first_done = 
     if(n > 0)
     {
       note_launch();
-      k_coarse_gather<<<blocks_for(n, 256), 256, 0, c->stream>>>(n, c->coarse.map, b,
-                                                                 c->coarse.vin);
+      launch_chained(k_coarse_gather<T>, blocks_for(n, 256), 256, 0, c->stream, n,
+                     c->coarse.map, b, c->coarse.vin, c->mg_halt);
       dense_spd_solve(c->stream, c->coarse.W[c->coarse.cur], c->coarse.work[c->coarse.cur],
-                      n, c->coarse.vin, c->coarse.vout, c->coarse.map, L.x);
+                      n, c->coarse.vin, c->coarse.vout, c->coarse.map, L.x, c->mg_halt);
     }
     if(!std::is_same<T, double>::value)
     {
       note_launch();
-      k_cast<<<blocks_for(3L * L.g.numnp, 256), 256, 0, c->stream>>>(3L * L.g.numnp, L.x,
-                                                                     B::x(L));
+      launch_chained(k_cast<double, T>, blocks_for(3L * L.g.numnp, 256), 256, 0, c->stream,
+                     3L * L.g.numnp, L.x, B::x(L));
     }
     return;
   }
@@ -1023,29 +1054,31 @@ static void vcycle(icarat_ctx *c, int l, const T *b, int deg, bool first_done = 
   const bool fuse = l + 1 < levels - 1 && !c->mg_galerkin;
   const double lm = c->lam_max_dk, theta = 0.5 * (lm + 0.1 * lm);
   note_launch();
-  k_restrict<<<blocks_for(C.g.numnp, 128), 128, 0, c->stream>>>(
-      L.g, C.g, B::r(L), C.fix, B::b(C), B::invd(C), T(1.0 / theta), fuse ? B::x(C) : nullptr,
-      B::r(C));
+  launch_chained(k_restrict<T>, blocks_for(C.g.numnp, 128), 128, 0, c->stream, L.g, C.g,
+                 B::r(L), C.fix, B::b(C), B::invd(C), T(1.0 / theta),
+                 fuse ? B::x(C) : (T *)nullptr, B::r(C), c->mg_halt);
   vcycle<T>(c, l + 1, B::b(C), deg, fuse);
   note_launch();
-  k_prolong_add<<<blocks_for(L.g.numnp, 128), 128, 0, c->stream>>>(L.g, C.g, B::x(C),
-                                                                   L.fix, B::x(L));
+  launch_chained(k_prolong_add<T>, blocks_for(L.g.numnp, 128), 128, 0, c->stream, L.g, C.g,
+                 B::x(C), L.fix, B::x(L), c->mg_halt);
   smooth<T>(c, L, l, b, deg, false);
 }
 
 void mg_vcycle(icarat_ctx *c, const double *r, double *z, int deg, bool first_done)
 {
   vcycle<double>(c, 0, r, deg, first_done);
-  ICK(cudaMemcpyAsync(z, c->mg[0].x, sizeof(double) * c->neq, cudaMemcpyDeviceToDevice,
-                      c->stream));
+  if(z)
+    ICK(cudaMemcpyAsync(z, c->mg[0].x, sizeof(double) * c->neq, cudaMemcpyDeviceToDevice,
+                        c->stream));
   ICK(cudaGetLastError());
 }
 
 void mg_vcycle_f32(icarat_ctx *c, const float *r, float *z, int deg)
 {
   vcycle<float>(c, 0, r, deg);
-  ICK(cudaMemcpyAsync(z, c->mg[0].x32, sizeof(float) * c->neq, cudaMemcpyDeviceToDevice,
-                      c->stream));
+  if(z)
+    ICK(cudaMemcpyAsync(z, c->mg[0].x32, sizeof(float) * c->neq, cudaMemcpyDeviceToDevice,
+                        c->stream));
   ICK(cudaGetLastError());
 }
 

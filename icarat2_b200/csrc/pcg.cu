@@ -28,6 +28,7 @@ __global__ void k_cg_init(int n, const double *__restrict__ b,
                           double *__restrict__ p, double *__restrict__ partials,
                           CgScalars *s, double tol, int maxit, int jacobi)
 {
+  chain_wait();
   __shared__ double sh[64];
   double zr = 0.0, bb = 0.0;
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -87,6 +88,7 @@ __global__ void k_cg_init_warm(int n, const double *__restrict__ b,
                                double *__restrict__ partials, CgScalars *s, double tol,
                                int maxit, int jacobi)
 {
+  chain_wait();
   __shared__ double sh[96];
   double zr = 0.0, bb = 0.0, rr = 0.0;
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -145,6 +147,7 @@ __global__ void __launch_bounds__(128)
               double *__restrict__ Ap, double *__restrict__ partials,
               CgScalars *s)
 {
+  chain_wait();
   __shared__ double sh[32];
   if(s->done)
     return;
@@ -195,6 +198,7 @@ __global__ void k_cg_update_jacobi(int n, const double *__restrict__ invd,
                                    const double *__restrict__ Ap,
                                    double *__restrict__ partials, CgScalars *s)
 {
+  chain_wait();
   __shared__ double sh[64];
   if(s->done)
     return;
@@ -244,6 +248,7 @@ __global__ void k_cg_update_r(int n, double *__restrict__ x,
                               const double *__restrict__ invd0, double inv_theta,
                               double *__restrict__ x0, double *__restrict__ d0)
 {
+  chain_wait();
   __shared__ double sh[32];
   if(s->done)
     return;
@@ -284,6 +289,7 @@ __global__ void k_cg_zr(int n, const double *__restrict__ z,
                         const double *__restrict__ r, double *__restrict__ partials,
                         CgScalars *s, int first)
 {
+  chain_wait();
   __shared__ double sh[32];
   if(s->done)
     return;
@@ -313,6 +319,7 @@ __global__ void k_cg_zr(int n, const double *__restrict__ z,
 __global__ void k_cg_pupdate(int n, const double *__restrict__ z,
                              double *__restrict__ p, const CgScalars *s)
 {
+  chain_wait();
   if(s->done)
     return;
   const double beta = s->beta;
@@ -343,6 +350,7 @@ static void enqueue_iteration(icarat_ctx *c, int method, int smooth,
   (void)b;
   const GridDev g = fine_grid(c);
   const int n = c->neq;
+  const double *z = c->d_z;
   if(use_dmma(c, g))
   {
     DmArgs a;
@@ -360,14 +368,14 @@ static void enqueue_iteration(icarat_ctx *c, int method, int smooth,
     int blocks;
     const MarchPlan m = spmv_plan(c, g, blocks);
     note_launch();
-    k_cg_spmv<<<blocks, 128, 0, c->stream>>>(g, m, c->ke0, c->d_E, c->d_fix, c->d_p,
-                                             c->d_Ap, c->d_partials, c->d_cg);
+    launch_chained(k_cg_spmv, blocks, 128, 0, c->stream, g, m, c->ke0, c->d_E, c->d_fix,
+                   c->d_p, c->d_Ap, c->d_partials, c->d_cg);
   }
   if(method == ICARAT_SOLVER_JACOBI_PCG)
   {
     note_launch();
-    k_cg_update_jacobi<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
-        n, c->d_invd, x, c->d_r, c->d_z, c->d_p, c->d_Ap, c->d_partials, c->d_cg);
+    launch_chained(k_cg_update_jacobi, c->red_blocks, kRedThreads, 0, c->stream, n,
+                   c->d_invd, x, c->d_r, c->d_z, c->d_p, c->d_Ap, c->d_partials, c->d_cg);
   }
   else
   {
@@ -375,16 +383,19 @@ static void enqueue_iteration(icarat_ctx *c, int method, int smooth,
     // the update also takes the finest level's first smoothing step
     MgLevel &L0 = c->mg[0];
     const double lm = c->lam_max_dk, theta = 0.5 * (lm + 0.1 * lm);
-    k_cg_update_r<<<c->red_blocks, kRedThreads, 0, c->stream>>>(
-        n, x, c->d_r, c->d_p, c->d_Ap, c->d_partials, c->d_cg, L0.invd, 1.0 / theta, L0.x, L0.r);
-    mg_vcycle(c, c->d_r, c->d_z, smooth, true);
+    launch_chained(k_cg_update_r, c->red_blocks, kRedThreads, 0, c->stream, n, x, c->d_r,
+                   c->d_p, c->d_Ap, c->d_partials, c->d_cg, L0.invd, 1.0 / theta, L0.x, L0.r);
+    // z stays in the finest level's x (overwritten only by the next
+    // iteration's update, after z . r and the p update have read it)
+    mg_vcycle(c, c->d_r, nullptr, smooth, true);
+    z = c->mg[0].x;
     note_launch();
-    k_cg_zr<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->d_z, c->d_r,
-                                                          c->d_partials, c->d_cg, 0);
+    launch_chained(k_cg_zr, c->red_blocks, kRedThreads, 0, c->stream, n, z, c->d_r,
+                   c->d_partials, c->d_cg, 0);
   }
   note_launch();
-  k_cg_pupdate<<<c->red_blocks, kRedThreads, 0, c->stream>>>(n, c->d_z, c->d_p,
-                                                             c->d_cg);
+  launch_chained(k_cg_pupdate, c->red_blocks, kRedThreads, 0, c->stream, n, z, c->d_p,
+                 c->d_cg);
 }
 
 void release_graphs(icarat_ctx *c)
@@ -403,6 +414,9 @@ int solve_full(icarat_ctx *c, const icarat_solve_opts *o, const double *d_b,
   const int method = o->method;
   IREQUIRE(method == ICARAT_SOLVER_JACOBI_PCG || method == ICARAT_SOLVER_MG_PCG,
            ICARAT_ERR_ARG, "unknown solver method");
+  // the V-cycles of this solve stop with it (the iterations a graph chunk
+  // holds past convergence launch, find the flag set and return)
+  HaltScope halt(c, method == ICARAT_SOLVER_MG_PCG ? &c->d_cg->done : nullptr);
   const GridDev g = fine_grid(c);
   const int n = c->neq;
   IREQUIRE(o->fp64_tc >= -1 && o->fp64_tc <= 1, ICARAT_ERR_ARG, "fp64_tc must be -1, 0 or 1");

@@ -160,7 +160,8 @@ __global__ void __launch_bounds__(tc::kThreads, TERMS == 1 ? 3 : 2) k_ku_tc(TcAr
   using namespace tc;
   extern __shared__ __align__(128) uint8_t tc_smem_raw[];
   Smem<TERMS> &sm = *reinterpret_cast<Smem<TERMS> *>(tc_smem_raw);
-  if(OP == TC_DOT && a.s->done)
+  chain_wait();
+  if(halted(a.halt) || (OP == TC_DOT && a.s->done))
     return;
   const int t = threadIdx.x, w = t >> 5, l = t & 31;
   const GridDev g = a.g;
@@ -586,7 +587,7 @@ void launch_ku_tc(icarat_ctx *c, int op, int terms, TcArgs a, cudaStream_t st)
                        O == TC_DOT ? (long)kMaxRedBlocks : (1L << 30));         \
     const dim3 grid((unsigned)txy, (unsigned)((g.NZ + a.kc - 1) / a.kc));       \
     note_launch();                                                              \
-    k_ku_tc<O, T><<<grid, tc::kThreads, tc_smem_bytes<T>(), st>>>(a);           \
+    launch_chained(k_ku_tc<O, T>, grid, tc::kThreads, tc_smem_bytes<T>(), st, a); \
     ICK(cudaGetLastError());                                                    \
     return;                                                                     \
   }
