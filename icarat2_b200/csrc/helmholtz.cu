@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(kHelmTx * kHelmWarps)
     k_helm_spmv(HelmGrid g, HelmAxes ax, const double *__restrict__ p,
                 double *__restrict__ Ap, double *__restrict__ partials, CgScalars *s)
 {
+  chain_wait();
   __shared__ double ring[kHelmDepth][kHalo];
   __shared__ double sh[64];
   if(s->done)
@@ -342,6 +343,7 @@ __global__ void k_helm_update(HelmGrid g, HelmInvd iv, double *__restrict__ x,
                               const double *__restrict__ Ap, double *__restrict__ partials,
                               CgScalars *s)
 {
+  chain_wait();
   __shared__ double sh[64];
   if(s->done)
     return;
@@ -383,6 +385,7 @@ __global__ void k_helm_update(HelmGrid g, HelmInvd iv, double *__restrict__ x,
 __global__ void k_helm_pupdate(HelmGrid g, HelmInvd iv, const double *__restrict__ r,
                                double *__restrict__ p, const CgScalars *s)
 {
+  chain_wait();
   if(s->done)
     return;
   const double beta = s->beta;
@@ -593,15 +596,16 @@ static void helm_iteration(icarat_ctx *c)
   const long tiles = (long)((c->NX + kHelmTx - 1) / kHelmTx) *
                     ((c->NY + kHelmTy - 1) / kHelmTy) * ((c->NZ + kHelmTz - 1) / kHelmTz);
   note_launch(3);
-  k_helm_spmv<<<blocks_for(tiles, 1, kMaxRedBlocks), kHelmTx * kHelmWarps, 0, c->stream>>>(
-      hgrid(c), helm_axes(c), H.d_p, H.d_Ap, H.d_partials, H.d_cg);
+  launch_chained(k_helm_spmv, blocks_for(tiles, 1, kMaxRedBlocks), kHelmTx * kHelmWarps, 0,
+                 c->stream, hgrid(c), helm_axes(c), H.d_p, H.d_Ap, H.d_partials, H.d_cg);
   HelmInvd iv;
   for(int q = 0; q < kHelmClasses; q++)
     iv.v[q] = H.invd_cls[q];
   (void)n;
-  k_helm_update<<<rb, kRedThreads, 0, c->stream>>>(hgrid(c), iv, H.d_val, H.d_r, H.d_p, H.d_Ap,
-                                                   H.d_partials, H.d_cg);
-  k_helm_pupdate<<<rb, kRedThreads, 0, c->stream>>>(hgrid(c), iv, H.d_r, H.d_p, H.d_cg);
+  launch_chained(k_helm_update, rb, kRedThreads, 0, c->stream, hgrid(c), iv, H.d_val, H.d_r,
+                 H.d_p, H.d_Ap, H.d_partials, H.d_cg);
+  launch_chained(k_helm_pupdate, rb, kRedThreads, 0, c->stream, hgrid(c), iv, H.d_r, H.d_p,
+                 H.d_cg);
   ICK(cudaGetLastError());
 }
 
