@@ -102,7 +102,9 @@ typedef struct
   int maxit;     /* iteration cap (solvers.hpp:90: 10000) */
   int mg_levels; /* multigrid levels incl. the finest (MG_PCG, MIXED_IR) */
   int mg_smooth; /* smoothing sweeps per level and direction (MG_PCG, MIXED_IR) */
-  int chunk;     /* iterations per host convergence check (0 = default) */
+  int chunk;     /* iterations per host convergence check (0 = default: 4 for
+                    MG_PCG and MIXED_IR, 16 for JACOBI_PCG); the iterations of
+                    a chunk past convergence return at entry and change nothing */
   double refresh; /* MIXED_IR: recompute the residual in FP64 once the FP32
                      recurrence has fallen by this factor (0 = 1e-2) */
   int fine_op;    /* MIXED_IR: ICARAT_OP_* of the finest-level smoothing and
