@@ -283,13 +283,16 @@ struct MarchPlan
 };
 
 // node layers per chunk: the largest count that still gives every resident
-// thread slot (slots) about two items, at least 4
+// thread slot (slots) about two items, down to one layer per item on the
+// small multigrid levels, which are latency-bound (their operands sit in L2,
+// so the layers a short chunk re-reads cost little; results do not depend on
+// the chunking)
 inline MarchPlan march_plan(const GridDev &g, long slots)
 {
   MarchPlan m;
   m.ncol = ((g.NX * g.NY + 31) / 32) * 32;
   int kc = g.NZ;
-  while(kc > 4 && (long)m.ncol * ((g.NZ + kc - 1) / kc) < 2 * slots)
+  while(kc > 1 && (long)m.ncol * ((g.NZ + kc - 1) / kc) < 2 * slots)
     kc = (kc + 1) / 2;
   m.kc = kc < 1 ? 1 : kc;
   m.items = (long)m.ncol * ((g.NZ + m.kc - 1) / m.kc);

@@ -35,9 +35,18 @@ def test_warm_solve_matches_cold(gpu, method):
     assert iw.status == 0 and ic.status == 0
     assert rel(uw, uc) <= 1e-8
     assert iw.iterations < ic.iterations
-    # the held solution of the same system already meets the tolerance
+    # the held solution is the next solve's start: no iteration when it
+    # already meets the tolerance.  CG stops on its recurrence residual, so
+    # the true residual of the solution it returned can sit just above rtol;
+    # then a few iterations bring it below.
+    f = warm.fext()
+    r_true = np.linalg.norm(f - warm.apply_K(uw)) / np.linalg.norm(f)
     u3, i3 = warm.solve(ow)
-    assert i3.status == 0 and i3.iterations == 0 and np.array_equal(u3, uw)
+    assert i3.status == 0 and rel(u3, uw) <= 1e-10
+    if r_true < 0.99e-12:
+        assert i3.iterations == 0 and np.array_equal(u3, uw)
+    elif r_true > 1.01e-12:
+        assert 1 <= i3.iterations < ic.iterations // 10, (r_true, i3.iterations)
 
 
 def test_warm_loop_and_multi_load_track_oracle(oracle, gpu):
